@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit FV residual/update path on the half-cylinder workload.
+
+Workload (the metric's configuration): supersonic flow (M = 3, rho = 1, p = 1/1.4) around a half
+cylinder on a body-fitted O-grid, body radius 1, outer radius 4, 1024 circumferential x 512
+radial cells (524,288 cells), radial stretching 1.005; second-order MUSCL on primitive variables
+with the Van Leer limiter, Roe flux with entropy fix, the reference's TVD-RK3 with local time
+stepping at CFL 0.8, FP64.  One step = one pseudo-time step (3 RK stages) of all cells.
+Synthetic, seeded: the mesh is generated in-repo and the flow starts from freestream.
+
+Metric: cell-updates/s (cells x pseudo-steps / s), higher is better.
+
+  python bench.py [--gpus N --steps K --warmup W]          the CUDA library (one rank per GPU;
+                                                             ranks run independent replicas)
+  python bench.py --impl reference [...]                   the reference's own CPU code
+                                                             (oracle/_ref) on the host cores
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GAMMA = 1.4
+NTHETA, NR, R_BODY, R_OUTER, RATIO = 1024, 512, 1.0, 4.0, 1.005
+MACH = 3.0
+WORKLOAD = "half_cylinder_M3_ogrid_1024x512_roe_muscl_vanleer_prim_rk3_lts_cfl0.8"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def workload_state(cb):
+    m = cb.Mesh.half_cylinder(NTHETA, NR, R_BODY, R_OUTER, RATIO)
+    NP = m.n_physical
+    rho, p = 1.0, 1.0 / GAMMA
+    u = MACH * np.sqrt(GAMMA * p / rho)
+    U = cb.conserved_from_primitive(np.full(NP, rho), np.full(NP, u), np.zeros(NP), np.full(NP, p))
+    full = np.zeros((m.n_total, 4))
+    full[:NP] = U
+    full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
+    kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
+              limiter=2, reconstruct_primitive=1, inlet_rho=rho, inlet_p=p)
+    return m, full, kw
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def flux_bytes_per_cell(NP, nbytes_geom_face=48):
+    """Algorithmic DRAM bytes of one flux-kernel launch per cell (each array touched once):
+    own primitives 40 B, per face the neighbour id 4 B, nx/ny/dl 24 B, second-neighbour id 4 B and
+    limiter distances 16 B (48 B x 4 faces), face count / mask / area 13 B, writes R 32 B + dt 8 B."""
+    return 40 + 4 * nbytes_geom_face + 13 + 40
+
+
+def cpu_baseline(steps=3):
+    """The reference's own CPU code (oracle/_ref, single-threaded as the reference is) timed on a
+    bounded sample: `steps` pseudo-steps of the full workload mesh, mesh load excluded.  The
+    reference's CPU path has no Van Leer / primitive MUSCL, so it runs its own 2-argument MinMod
+    on conserved variables with otherwise identical settings."""
+    import cfd_solver_withcuda_b200 as cb
+    from oracle import refpy
+    if not refpy.ref_available():
+        return None
+    m, U0, kw = workload_state(cb)
+    r = refpy.RefRun(m, {"CFL": kw["cfl"], "Time_Accurate": 1, "Dissipation_Type": 3, "Is_Second_Order": 1,
+                         "Local_Time_Stepping": 1, "Inlet_Rho": kw["inlet_rho"], "Inlet_P": kw["inlet_p"]})
+    r.set_state(U0)
+    r.iterate(1)
+    t = time.perf_counter()
+    r.iterate(steps)
+    el = time.perf_counter() - t
+    cpu = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            cpu = next(l.split(":", 1)[1].strip() for l in f if l.startswith("model name"))
+    except (OSError, StopIteration):
+        pass
+    return {"value": m.n_physical * steps / el, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "sample": "%d pseudo-steps (3 RK stages each) of the full %d-cell mesh, mesh load excluded; "
+                      "reference MinMod limiter (its CPU path has no Van Leer); CPU: %s" % (steps, m.n_physical, cpu),
+            "seconds": el}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU path on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import refpy
+    if not refpy.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdref.so was not built "
+                          "(the reference sources were absent when build() ran)"}))
+        return
+    steps = max(1, min(args.steps, 20))
+    base = cpu_baseline(steps=steps)
+    v = base["value"]
+    out = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": steps,
+           "warmup": 1, "ms_per_step": 1e3 * base["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (in-repo O-grid generator, freestream start)",
+           "impl": "reference",
+           "config": {"workload": WORKLOAD, "cells": NTHETA * NR, "limiter": "reference MinMod (conserved)",
+                      "parallelism": "single-threaded reference CPU code"},
+           "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import cfd_solver_withcuda_b200 as cb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    m, U0, kw = workload_state(cb)
+    NP = m.n_physical
+    s = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **kw))
+    s.set_option("keep_delu", 0)
+    s.upload_state(U0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # Warm-up (graph capture happens on the first multi-step call).
+    s.step_async(max(args.warmup, 3))
+    s.sync()
+    barrier()
+    launches0 = s.kernel_launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        ev0.record(stream)
+        s.step_async(args.steps)
+        ev1.record(stream)
+        info = s.sync()
+        barrier()
+    launches = s.kernel_launches - launches0
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = world * NP * args.steps / (ms_max * 1e-3)
+
+    # Kernel-level timing of the same workload (separate pass, events around every launch).
+    s.set_option("profile", 1)
+    nprof = min(args.steps, 200)
+    s.step_async(nprof)
+    s.sync()
+    flux_ms, flux_n = s.kernel_time("flux")
+    stage_ms, stage_n = s.kernel_time("stage")
+    bc_ms, bc_n = s.kernel_time("bc")
+    s.set_option("profile", 0)
+    peaks, peak_kind = measured_peaks()
+    flux_avg_ms = flux_ms / max(flux_n, 1)
+    bytes_launch = flux_bytes_per_cell(NP) * NP
+    achieved = bytes_launch / (flux_avg_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "flux_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    # End to end through the public C ABI with host buffers: every step uploads U from pinned
+    # host memory, runs one pseudo-step and reads back U and the residual norm.
+    pin = torch.empty((m.n_total, 4), dtype=torch.float64, pin_memory=True)
+    pin.copy_(torch.from_numpy(U0))
+    host_U = pin.numpy()
+    out_pin = torch.empty((m.n_total, 4), dtype=torch.float64, pin_memory=True).numpy()
+    s.set_option("use_graph", 0)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        s.upload_state(host_U)
+        s.step(1)
+        s.download_U(out_pin)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * NP * args.e2e_steps / float(te.item())
+    h2d = host_U.nbytes
+    d2h = out_pin.nbytes + 8 * 16
+
+    if rank == 0:
+        out = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+               "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (in-repo O-grid generator, freestream start)",
+               "config": {"workload": WORKLOAD, "cells": NP, "ghost_cells": m.n_ghost, "global_cells": world * NP,
+                          "parallelism": "replicas (one independent solve per GPU)" if world > 1 else "single GPU",
+                          "l2": "working set %.0f MB > 126 MB L2 (no flush needed)" % (s.device_bytes / 1e6),
+                          "cuda_graph": True},
+               "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
+               "gpu_launches": int(launches),
+               "roofline": {"kernel": "k_flux<ROE,2nd order> (fused residual + dt + min)", "bound": "hbm",
+                            "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                            "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
+                            "avg_launch_ms": flux_avg_ms},
+               "kernel_ms_per_step": {"flux": flux_ms / nprof, "stage": stage_ms / nprof, "bc": bc_ms / nprof},
+               "clocks": clk.summary(),
+               "final_residual_rho": info.error[0]}
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                base = cpu_baseline()
+            except Exception as e:  # the baseline is reported, never required
+                base = {"error": str(e)}
+            if base is not None:
+                out["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample") if k in base}
+        print(json.dumps(out))
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,854 @@
+// Host runtime of the C ABI (include/cfd_b200.h): mesh API, device upload / reorder layer,
+// stage sequencing, CUDA-graph replay of whole pseudo-steps, downloads.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/cfd_b200.h"
+#include "kernels.cuh"
+#include "mesh.hpp"
+#include "physics.cuh"
+
+namespace cfdb {
+std::string config_from_json(const std::string &text, cfd_config *cfg);
+}
+
+using namespace cfdb;
+
+namespace {
+std::string g_err;  // last error message (per process)
+
+cfd_status fail(cfd_status s, const std::string &msg) {
+  g_err = msg;
+  return s;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+  do {                                                                                              \
+    cudaError_t _e = (expr);                                                                        \
+    if (_e != cudaSuccess) return fail(CFD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+std::vector<int> rcm_from_arrays(int NP, const int *nf, const int *nbr) {
+  std::vector<int> deg(NP, 0);
+  for (int c = 0; c < NP; c++)
+    for (int f = 0; f < nf[c]; f++)
+      if (nbr[4 * c + f] >= 0 && nbr[4 * c + f] < NP) deg[c]++;
+  std::vector<int> by_deg(NP);
+  for (int i = 0; i < NP; i++) by_deg[i] = i;
+  std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+  std::vector<int> order;
+  order.reserve(NP);
+  std::vector<char> seen(NP, 0);
+  std::vector<int> q, nb;
+  q.reserve(NP);
+  for (int start : by_deg) {
+    if (seen[start]) continue;
+    size_t head = q.size();
+    q.push_back(start);
+    seen[start] = 1;
+    while (head < q.size()) {
+      int c = q[head++];
+      order.push_back(c);
+      nb.clear();
+      for (int f = 0; f < nf[c]; f++) {
+        int n = nbr[4 * c + f];
+        if (n >= 0 && n < NP && !seen[n]) nb.push_back(n);
+      }
+      std::stable_sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+      for (int n : nb) {
+        seen[n] = 1;
+        q.push_back(n);
+      }
+    }
+  }
+  std::reverse(order.begin(), order.end());
+  return order;
+}
+
+template <typename T>
+cfd_status dev_upload(T **dst, const std::vector<T> &v) {
+  CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), std::max<size_t>(1, v.size()) * sizeof(T)));
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return CFD_OK;
+}
+}  // namespace
+
+struct cfd_mesh {
+  Mesh m;
+};
+
+struct cfd_ctx {
+  cfd_config cfg{};
+  int NP = 0, NG = 0, NT = 0, NB = 0;
+  std::vector<int> perm;  // device index -> reference index (physical)
+  std::vector<int> inv;   // reference index -> device index (physical)
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  DevMesh dm{};
+  DevState ds{};
+  FluxParams fp{};
+  BcParams bp{};
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+  long long launches = 0;
+  bool prim_from_S = false;
+  int keep_delu = 1;
+  int use_graph = 1;
+  cudaGraphExec_t graph = nullptr;
+  int graph_launches = 0;
+  double *h_ctl = nullptr;  // pinned mirror of the control block
+  int *d_perm = nullptr;    // device copy of perm
+  // Per-kernel timing (option "profile"): event pairs recorded around each launch on the
+  // context's stream, resolved lazily by cfd_kernel_time.
+  int profile = 0;
+  struct Timed {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Timed> timed;
+  double kind_ms[3] = {0, 0, 0};
+  long long kind_n[3] = {0, 0, 0};
+  double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
+};
+
+namespace {
+
+cfd_status ctx_alloc(cfd_ctx *ctx, void **p, size_t bytes) {
+  CUDA_TRY(cudaMalloc(p, std::max<size_t>(bytes, 16)));
+  ctx->allocs.push_back(*p);
+  ctx->bytes += bytes;
+  return CFD_OK;
+}
+
+template <typename T>
+cfd_status ctx_upload(cfd_ctx *ctx, T **dst, const std::vector<T> &v) {
+  cfd_status s = ctx_alloc(ctx, reinterpret_cast<void **>(dst), v.size() * sizeof(T));
+  if (s != CFD_OK) return s;
+  if (!v.empty()) CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return CFD_OK;
+}
+
+int dev_of(const cfd_ctx *ctx, int ref) { return ref < ctx->NP ? ctx->inv[ref] : ref; }
+
+enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2 };
+
+struct TimedScope {
+  cfd_ctx *ctx;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  TimedScope(cfd_ctx *c, int k) : ctx(c), kind(k) {
+    if (!ctx->profile) return;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, ctx->stream);
+  }
+  ~TimedScope() {
+    if (!ctx->profile) return;
+    cudaEventRecord(b, ctx->stream);
+    ctx->timed.push_back({kind, a, b});
+  }
+};
+
+// Launch sequence of one pseudo-step (loop body of src/Solver.cpp:94-125).
+int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
+  const cfd_config &c = ctx->cfg;
+  cudaStream_t s = ctx->stream;
+  DevMesh &m = ctx->dm;
+  DevState &st = ctx->ds;
+  int n = 0;
+  const int cons = ctx->fp.consistent;
+  if (c.integrator == CFD_INT_REFERENCE && !c.time_accurate) {
+    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, 0); }
+    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, 0); }
+    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, 0, 0, fuse_final, ctx->keep_delu); }
+    return n;
+  }
+  if (c.integrator == CFD_INT_RK4) {
+    const int lts = c.local_time_stepping ? 2 : 3;
+    for (int k = 0; k < 4; k++) {
+      { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0); }
+      { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
+      { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, 11 + k, lts, k == 3 ? fuse_final : 0, ctx->keep_delu); }
+    }
+    return n;
+  }
+  // Three-stage forms: the reference's Runge_Kutta_Method (LTS in stage 1 only, Min_dt of the
+  // current evaluation in stages 2-3) or the stage-consistent SSP-RK3 (dt frozen per step).
+  const bool ssp = c.integrator == CFD_INT_SSPRK3;
+  for (int k = 0; k < 3; k++) {
+    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0 && cons); }
+    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
+    int lts;
+    if (ssp) lts = c.local_time_stepping ? 2 : 3;
+    else lts = (k == 0 && c.local_time_stepping) ? 1 : 0;
+    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu); }
+  }
+  return n;
+}
+
+cfd_status sync_status(cfd_ctx *ctx, cfd_step_info *info) {
+  CUDA_TRY(cudaMemcpyAsync(ctx->h_ctl, ctx->ds.ctl, sizeof(double) * CTL_SIZE, cudaMemcpyDeviceToHost, ctx->stream));
+  int h_status[2];
+  CUDA_TRY(cudaMemcpyAsync(h_status, ctx->ds.status, sizeof(h_status), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  CUDA_TRY(cudaGetLastError());
+  cfd_status st = static_cast<cfd_status>(h_status[0]);
+  int bad = -1;
+  if (st == CFD_ERR_NONPHYSICAL && h_status[1] != INT_MAX) {
+    bad = h_status[1] < ctx->NP ? ctx->perm[h_status[1]] : h_status[1];
+  }
+  if (info) {
+    info->iterations = static_cast<int>(ctx->h_ctl[CTL_ITER]);
+    info->min_dt = ctx->h_ctl[CTL_DTMIN];
+    info->total_time = ctx->h_ctl[CTL_TOTAL_TIME];
+    for (int k = 0; k < 4; k++) {
+      info->error[k] = ctx->h_ctl[CTL_ERR + k];
+      info->res_l2[k] = ctx->h_ctl[CTL_RES + k];
+    }
+    info->bad_cell = bad;
+    info->status = st;
+  }
+  if (st == CFD_ERR_NONPHYSICAL) return fail(st, "non-physical state (NaN sound speed) at cell " + std::to_string(bad));
+  if (st != CFD_OK) return fail(st, "device status " + std::to_string(st));
+  return CFD_OK;
+}
+
+cfd_status clear_status(cfd_ctx *ctx) {
+  int h[2] = {0, INT_MAX};
+  CUDA_TRY(cudaMemcpyAsync(ctx->ds.status, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CFD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+const char *cfd_last_error(void) { return g_err.c_str(); }
+const char *cfd_version(void) { return "cfd-b200 0.1 (sm_100a, fp64 exact)"; }
+
+// ----------------------------------------- mesh -------------------------------------------
+static cfd_status finish_mesh(cfd_mesh *h, const std::string &gen_err, cfd_mesh **out) {
+  if (!gen_err.empty()) {
+    delete h;
+    return fail(CFD_ERR_MESH, gen_err);
+  }
+  std::string e = h->m.build();
+  if (!e.empty()) {
+    delete h;
+    return fail(CFD_ERR_MESH, e);
+  }
+  *out = h;
+  return CFD_OK;
+}
+
+cfd_status cfd_mesh_box(int nx, int ny, double x0, double x1, double y0, double y1, cfd_mesh **out) {
+  if (!out) return fail(CFD_ERR_BAD_ARG, "null out");
+  cfd_mesh *h = new cfd_mesh;
+  return finish_mesh(h, generate_box(h->m, nx, ny, x0, x1, y0, y1), out);
+}
+cfd_status cfd_mesh_half_cylinder(int ntheta, int nr, double r_body, double r_outer, double ratio, cfd_mesh **out) {
+  if (!out) return fail(CFD_ERR_BAD_ARG, "null out");
+  cfd_mesh *h = new cfd_mesh;
+  return finish_mesh(h, generate_half_cylinder(h->m, ntheta, nr, r_body, r_outer, ratio), out);
+}
+cfd_status cfd_mesh_ramp(int nx, int ny, double length, double height, double x_corner, double angle_deg,
+                         cfd_mesh **out) {
+  if (!out) return fail(CFD_ERR_BAD_ARG, "null out");
+  cfd_mesh *h = new cfd_mesh;
+  return finish_mesh(h, generate_ramp(h->m, nx, ny, length, height, x_corner, angle_deg), out);
+}
+cfd_status cfd_mesh_bump(int nx, int ny, double length, double height, double thickness, int n_quad_layers,
+                         double jitter, uint64_t seed, int triangles, cfd_mesh **out) {
+  if (!out) return fail(CFD_ERR_BAD_ARG, "null out");
+  cfd_mesh *h = new cfd_mesh;
+  return finish_mesh(h, generate_bump(h->m, nx, ny, length, height, thickness, n_quad_layers, jitter, seed, triangles),
+                     out);
+}
+cfd_status cfd_mesh_read_vtk(const char *path, cfd_mesh **out) {
+  if (!out || !path) return fail(CFD_ERR_BAD_ARG, "null argument");
+  cfd_mesh *h = new cfd_mesh;
+  std::string e = read_vtk(h->m, path);
+  if (!e.empty()) {
+    delete h;
+    return fail(CFD_ERR_IO, e);
+  }
+  return finish_mesh(h, "", out);
+}
+cfd_status cfd_mesh_write_vtk(const cfd_mesh *m, const char *path) {
+  if (!m || !path) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::string e = write_vtk(m->m, path);
+  return e.empty() ? CFD_OK : fail(CFD_ERR_IO, e);
+}
+cfd_status cfd_mesh_describe(const cfd_mesh *h, cfd_mesh_desc *d) {
+  if (!h || !d) return fail(CFD_ERR_BAD_ARG, "null argument");
+  const Mesh &m = h->m;
+  d->n_physical = m.n_physical;
+  d->n_ghost = m.n_ghost;
+  d->n_faces = m.n_faces.data();
+  d->neighbours = m.nbr.data();
+  d->face_normals = m.normals.data();
+  d->face_lengths = m.lengths.data();
+  d->center_distances = m.ccd.data();
+  d->area = m.area.data();
+  d->inv_area = m.inv_area.data();
+  d->n_boundary = static_cast<int>(m.boundary.size() / 4);
+  d->boundary = m.boundary.data();
+  return CFD_OK;
+}
+cfd_status cfd_mesh_centers(const cfd_mesh *h, double *out) {
+  if (!h || !out) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::memcpy(out, h->m.centers.data(), h->m.centers.size() * sizeof(double));
+  return CFD_OK;
+}
+cfd_status cfd_mesh_points(const cfd_mesh *h, int *n_points, const double **points) {
+  if (!h || !n_points || !points) return fail(CFD_ERR_BAD_ARG, "null argument");
+  *n_points = static_cast<int>(h->m.points.size() / 3);
+  *points = h->m.points.data();
+  return CFD_OK;
+}
+void cfd_mesh_destroy(cfd_mesh *m) { delete m; }
+
+// ----------------------------------------- config -----------------------------------------
+void cfd_config_default(cfd_config *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->dissipation_type = CFD_DISS_ROE;
+  c->is_second_order = 1;
+  c->time_accurate = 0;
+  c->local_time_stepping = 0;
+  c->integrator = CFD_INT_REFERENCE;
+  c->limiter = CFD_LIM_REF_MINMOD;
+  c->cfl = 0.1;
+  c->limiter_zeta = 0.5;
+  c->limiter_zeta1 = 0.5;
+  c->inlet_rho = 1.0;
+  c->inlet_p = 1.0 / 1.4;
+  c->r_gas = 287.0;
+  c->reorder = 1;
+}
+
+cfd_status cfd_config_read_json(const char *path, cfd_config *cfg) {
+  if (!path || !cfg) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::ifstream in(path);
+  if (!in) return fail(CFD_ERR_IO, std::string("cannot open ") + path);
+  std::stringstream ss;
+  ss << in.rdbuf();
+  std::string e = config_from_json(ss.str(), cfg);
+  return e.empty() ? CFD_OK : fail(CFD_ERR_BAD_ARG, "JSON: " + e);
+}
+
+// ----------------------------------------- context ----------------------------------------
+void cfd_destroy(cfd_ctx *ctx) {
+  if (!ctx) return;
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  for (auto &t : ctx->timed) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **out) {
+  if (!d || !cfg || !out) return fail(CFD_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  const int NP = d->n_physical, NG = d->n_ghost, NB = d->n_boundary;
+  if (NP <= 0 || NG < 0 || NB < 0) return fail(CFD_ERR_BAD_ARG, "bad mesh sizes");
+  if (!d->n_faces || !d->neighbours || !d->face_normals || !d->face_lengths || !d->area || !d->inv_area ||
+      (NB > 0 && !d->boundary))
+    return fail(CFD_ERR_BAD_ARG, "missing mesh arrays");
+  if (cfg->is_second_order && !d->center_distances) return fail(CFD_ERR_BAD_ARG, "second order needs centre distances");
+  const int NT = NP + NG;
+  for (int c = 0; c < NP; c++) {
+    int nf = d->n_faces[c];
+    if (nf != 3 && nf != 4) return fail(CFD_ERR_MESH, "cell " + std::to_string(c) + " must have 3 or 4 faces");
+    for (int f = 0; f < nf; f++) {
+      int n = d->neighbours[4 * c + f];
+      if (n < 0 || n >= NT) return fail(CFD_ERR_MESH, "cell " + std::to_string(c) + " has an invalid neighbour");
+    }
+  }
+  for (int e = 0; e < NB; e++) {
+    const int *b = d->boundary + 4 * e;
+    if (b[0] < 0 || b[0] > 3 || b[1] < 0 || b[1] >= NP || b[2] < 0 || b[2] >= d->n_faces[b[1]] || b[3] < NP || b[3] >= NT)
+      return fail(CFD_ERR_MESH, "invalid boundary entry " + std::to_string(e));
+  }
+  const int diss = cfg->dissipation_type;
+  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF)
+    return fail(CFD_ERR_BAD_ARG, "dissipation type " + std::to_string(diss) + " is not available in this build");
+  if (diss == CFD_DISS_LLF && cfg->is_second_order)
+    return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
+  if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
+  if (cfg->precision != CFD_PREC_FP64) return fail(CFD_ERR_BAD_ARG, "precision form not available in this build");
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CFD_ERR_NO_DEVICE, "no CUDA device");
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(CFD_ERR_BAD_ARG, "bad device ordinal");
+  CUDA_TRY(cudaSetDevice(cfg->device));
+
+  cfd_ctx *ctx = new cfd_ctx;
+  ctx->cfg = *cfg;
+  ctx->NP = NP;
+  ctx->NG = NG;
+  ctx->NT = NT;
+  ctx->NB = NB;
+  auto bail = [&](cfd_status s) {
+    cfd_destroy(ctx);
+    return s;
+  };
+  if (cfg->stream) {
+    ctx->stream = static_cast<cudaStream_t>(cfg->stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return bail(fail(CFD_ERR_CUDA, "stream creation failed"));
+    ctx->own_stream = true;
+  }
+  if (cudaMallocHost(reinterpret_cast<void **>(&ctx->h_ctl), sizeof(double) * CTL_SIZE) != cudaSuccess)
+    return bail(fail(CFD_ERR_CUDA, "pinned allocation failed"));
+
+  // Renumbering (reverse Cuthill-McKee over physical cells; ghosts keep their ids).
+  if (cfg->reorder) ctx->perm = rcm_from_arrays(NP, d->n_faces, d->neighbours);
+  else {
+    ctx->perm.resize(NP);
+    for (int i = 0; i < NP; i++) ctx->perm[i] = i;
+  }
+  ctx->inv.assign(NP, 0);
+  for (int i = 0; i < NP; i++) ctx->inv[ctx->perm[i]] = i;
+
+  // Face-major SoA geometry in device order, plus the limiter stencil of
+  // Second_Order_Limiter (src/Limiters.cpp:136-191) resolved once on the host.
+  std::vector<int> nf(NP), nbr(4 * (size_t)NP, 0), n2(4 * (size_t)NP, 0);
+  std::vector<double> nx(4 * (size_t)NP, 0.0), ny(4 * (size_t)NP, 0.0), dl(4 * (size_t)NP, 0.0);
+  std::vector<double> d1l(4 * (size_t)NP, 1.0), d2l(4 * (size_t)NP, 1.0), area(NP), inva(NP);
+  std::vector<uint8_t> degen(NP, 0);
+  const double *ccd = d->center_distances;
+  for (int i = 0; i < NP; i++) {
+    const int r = ctx->perm[i];
+    const int nfr = d->n_faces[r];
+    nf[i] = nfr;
+    area[i] = d->area[r];
+    inva[i] = d->inv_area[r];
+    for (int f = 0; f < nfr; f++) {
+      const size_t idx = (size_t)f * NP + i;
+      const int N = d->neighbours[4 * r + f];
+      nbr[idx] = dev_of(ctx, N);
+      const double fx = d->face_normals[8 * r + 2 * f], fy = d->face_normals[8 * r + 2 * f + 1];
+      nx[idx] = fx;
+      ny[idx] = fy;
+      dl[idx] = d->face_lengths[4 * r + f];
+      if (std::sqrt(fx * fx + fy * fy) < 1e-12) degen[i] |= static_cast<uint8_t>(1u << f);
+      if (ccd) {
+        int N2;
+        double d1, d2;
+        if (nfr != 4) {
+          d1 = ccd[4 * r + f];
+          if (d1 <= 0.0) d1 = 1.0;
+          N2 = N;
+          d2 = d1;
+        } else if (f == 0 || f == 1) {
+          d1 = ccd[4 * r + f];
+          N2 = (N >= NP) ? N : d->neighbours[4 * N + f];
+          d2 = (N >= NP) ? d1 : ccd[4 * N + f];
+        } else {
+          const int o = f - 2;
+          d1 = ccd[4 * r + f];
+          N2 = d->neighbours[4 * r + o];
+          d2 = ccd[4 * r + o];
+        }
+        n2[idx] = dev_of(ctx, N2);
+        d1l[idx] = d1;
+        d2l[idx] = d2;
+      }
+    }
+  }
+  std::vector<int4> bnd(NB);
+  for (int e = 0; e < NB; e++) {
+    const int *b = d->boundary + 4 * e;
+    bnd[e] = make_int4(b[0], dev_of(ctx, b[1]), b[2], b[3]);
+  }
+
+  DevMesh &m = ctx->dm;
+  m.NP = NP;
+  m.NT = NT;
+  m.NB = NB;
+  cfd_status s;
+  if ((s = ctx_upload(ctx, const_cast<int **>(&m.nf), nf)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<int **>(&m.nbr), nbr)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.nx), nx)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.ny), ny)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.dl), dl)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.area), area)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.inv_area), inva)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<int **>(&m.n2), n2)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.d1l), d1l)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.d2l), d2l)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<uint8_t **>(&m.degen), degen)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.bnd), bnd)) != CFD_OK) return bail(s);
+
+  DevState &st = ctx->ds;
+  const size_t dsz = sizeof(double);
+  const int nblk = flux_block_count(NP);
+  if ((s = ctx_alloc(ctx, (void **)&st.U, 4 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.S, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.prim, 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.R, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.dtc, (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.dtk, (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.dU, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  if (cfg->integrator == CFD_INT_RK4) {
+    if ((s = ctx_alloc(ctx, (void **)&st.Racc, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  }
+  if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)nblk * dsz)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.counter, 64)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.status, 64)) != CFD_OK) return bail(s);
+  if (cudaMemset(st.U, 0, 4 * (size_t)NT * dsz) != cudaSuccess || cudaMemset(st.S, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
+      cudaMemset(st.prim, 0, 5 * (size_t)NT * dsz) != cudaSuccess || cudaMemset(st.R, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
+      cudaMemset(st.dtc, 0, (size_t)NP * dsz) != cudaSuccess || cudaMemset(st.dU, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
+      cudaMemset(st.ctl, 0, CTL_SIZE * dsz) != cudaSuccess || cudaMemset(st.counter, 0, 64) != cudaSuccess)
+    return bail(fail(CFD_ERR_CUDA, "memset failed"));
+  int hs[2] = {0, INT_MAX};
+  if (cudaMemcpy(st.status, hs, sizeof(hs), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(CFD_ERR_CUDA, "status init failed"));
+  if ((s = ctx_upload(ctx, &ctx->d_perm, ctx->perm)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&ctx->d_stage, 4 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
+
+  FluxParams &fp = ctx->fp;
+  fp.dissipation = diss;
+  fp.second_order = cfg->is_second_order;
+  fp.limiter = cfg->limiter;
+  fp.recon_prim = cfg->reconstruct_primitive;
+  fp.consistent = (cfg->integrator != CFD_INT_REFERENCE) ? 1 : 0;
+  fp.precision = cfg->precision;
+  fp.cfl = cfg->cfl;
+  fp.zeta = cfg->limiter_zeta;
+  fp.zeta1 = cfg->limiter_zeta1;
+  BcParams &bp = ctx->bp;
+  bp.inlet_bc = cfg->inlet_bc;
+  bp.exit_bc = cfg->exit_bc;
+  bp.inlet_rho = cfg->inlet_rho;
+  bp.inlet_p = cfg->inlet_p;
+  bp.inlet_u = cfg->inlet_u;
+  bp.inlet_v = cfg->inlet_v;
+  bp.inlet_p0 = cfg->inlet_p0;
+  bp.inlet_t0 = cfg->inlet_t0;
+  bp.exit_p = cfg->exit_p;
+  bp.r_gas = cfg->r_gas > 0.0 ? cfg->r_gas : 287.0;
+  *out = ctx;
+  return CFD_OK;
+}
+
+cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
+  if (!ctx || !name) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::string n(name);
+  if (n == "keep_delu") ctx->keep_delu = value != 0.0;
+  else if (n == "use_graph") ctx->use_graph = value != 0.0;
+  else if (n == "profile") ctx->profile = value != 0.0;
+  else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_upload_state(cfd_ctx *ctx, const double *U, int n) {
+  if (!ctx || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  if (n != ctx->NP && n != ctx->NT) return fail(CFD_ERR_BAD_ARG, "n must be NP or NP+NG");
+  const int NT = ctx->NT, NP = ctx->NP;
+  // Rows go to a device staging buffer in reference order; a kernel gathers them into the
+  // device-order planes.  With n = NP the ghost rows are filled from their owner cell first.
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_stage, U, 4 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (n == NP && ctx->NB > 0) {
+    std::vector<int4> bnd(ctx->NB);
+    CUDA_TRY(cudaMemcpy(bnd.data(), ctx->dm.bnd, ctx->NB * sizeof(int4), cudaMemcpyDeviceToHost));
+    for (const int4 &b : bnd)
+      CUDA_TRY(cudaMemcpyAsync(ctx->d_stage + 4 * (size_t)b.w, U + 4 * (size_t)ctx->perm[b.y], 4 * sizeof(double),
+                               cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->launches += launch_import_aos(ctx->stream, ctx->d_stage, ctx->d_perm, NP, NT, ctx->ds.U);
+  ctx->launches += launch_prim_all(ctx->stream, ctx->dm, ctx->ds);
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = false;
+  return sync_status(ctx, nullptr);
+}
+
+// Conserved rows U_Cells [(NP+NG)*4] in reference order, gathered on the device.
+cfd_status cfd_download_U(cfd_ctx *ctx, double *U) {
+  if (!ctx || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  ctx->launches += launch_export_aos(ctx->stream, ctx->ds.U, ctx->d_perm, ctx->NP, ctx->NT, ctx->NT, ctx->d_stage);
+  CUDA_TRY(cudaMemcpyAsync(U, ctx->d_stage, 4 * (size_t)ctx->NT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CFD_OK;
+}
+
+static cfd_status enqueue_steps(cfd_ctx *ctx, int n_steps) {
+  if (ctx->use_graph && !ctx->profile && n_steps > 1) {
+    if (!ctx->graph) {
+      cudaGraph_t g;
+      CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      ctx->graph_launches = enqueue_step(ctx, true);
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (e != cudaSuccess) return fail(CFD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&ctx->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(CFD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    for (int i = 0; i < n_steps; i++) {
+      CUDA_TRY(cudaGraphLaunch(ctx->graph, ctx->stream));
+      ctx->launches += ctx->graph_launches;
+    }
+  } else {
+    for (int i = 0; i < n_steps; i++) ctx->launches += enqueue_step(ctx, true);
+  }
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = false;
+  return CFD_OK;
+}
+
+cfd_status cfd_step(cfd_ctx *ctx, int n_steps, double t_end, cfd_step_info *info) {
+  if (!ctx || n_steps < 0) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  ctx->launches += launch_set_ctl(ctx->stream, ctx->ds, CTL_TEND, t_end);
+  ctx->launches += launch_set_ctl(ctx->stream, ctx->ds, CTL_DONE, 0.0);
+  CUDA_TRY(cudaGetLastError());
+  if (t_end > 0.0) {
+    // Steps past t_end are no-ops on the device; check the done flag between chunks so that a
+    // large n_steps does not queue work that will be skipped.
+    const int chunk = 64;
+    for (int done = 0; done < n_steps; done += chunk) {
+      cfd_status s = enqueue_steps(ctx, std::min(chunk, n_steps - done));
+      if (s != CFD_OK) return s;
+      s = sync_status(ctx, info);
+      if (s != CFD_OK) return s;
+      if (ctx->h_ctl[CTL_DONE] != 0.0) break;
+    }
+    return sync_status(ctx, info);
+  }
+  cfd_status s = enqueue_steps(ctx, n_steps);
+  if (s != CFD_OK) return s;
+  return sync_status(ctx, info);
+}
+
+// Enqueues n pseudo-steps without waiting (benchmark helper); cfd_sync collects the status.
+cfd_status cfd_step_async(cfd_ctx *ctx, int n_steps) {
+  if (!ctx || n_steps < 0) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  return enqueue_steps(ctx, n_steps);
+}
+
+cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  return sync_status(ctx, info);
+}
+
+cfd_status cfd_apply_boundary_conditions(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, 0);
+  CUDA_TRY(cudaGetLastError());
+  return sync_status(ctx, nullptr);
+}
+
+cfd_status cfd_evaluate_net_flux(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  ctx->launches += launch_flux(ctx->stream, ctx->dm, ctx->ds, ctx->fp, 0);
+  CUDA_TRY(cudaGetLastError());
+  return sync_status(ctx, nullptr);
+}
+
+cfd_status cfd_explicit_method(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  ctx->launches += launch_flux(ctx->stream, ctx->dm, ctx->ds, ctx->fp, 0);
+  cfd_status s = sync_status(ctx, nullptr);
+  if (s != CFD_OK) return s;
+  if (!(ctx->h_ctl[CTL_DTMIN] > 0.0)) return fail(CFD_ERR_DT_NONPOSITIVE, "Min_dt is not positive");
+  ctx->launches += launch_stage(ctx->stream, ctx->dm, ctx->ds, 0, 0, 0, 1);
+  CUDA_TRY(cudaGetLastError());
+  return sync_status(ctx, nullptr);
+}
+
+cfd_status cfd_runge_kutta_method(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  const cfd_config &c = ctx->cfg;
+  const int cons = ctx->fp.consistent;
+  const bool ssp = c.integrator == CFD_INT_SSPRK3;
+  for (int k = 0; k < 3; k++) {
+    if (k > 0) ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, cons);
+    ctx->launches += launch_flux(ctx->stream, ctx->dm, ctx->ds, ctx->fp, k > 0);
+    int lts = ssp ? (c.local_time_stepping ? 2 : 3) : ((k == 0 && c.local_time_stepping) ? 1 : 0);
+    ctx->launches += launch_stage(ctx->stream, ctx->dm, ctx->ds, k + 1, lts, 0, 1);
+  }
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = true;
+  return sync_status(ctx, nullptr);
+}
+
+cfd_status cfd_estimate_error(cfd_ctx *ctx, double error[4]) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  ctx->launches += launch_error(ctx->stream, ctx->dm, ctx->ds);
+  CUDA_TRY(cudaGetLastError());
+  cfd_status s = sync_status(ctx, nullptr);
+  if (s == CFD_OK && error)
+    for (int k = 0; k < 4; k++) error[k] = ctx->h_ctl[CTL_ERR + k];
+  return s;
+}
+
+cfd_status cfd_update(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  ctx->launches += launch_update(ctx->stream, ctx->dm, ctx->ds);
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = false;
+  return sync_status(ctx, nullptr);
+}
+
+cfd_status cfd_get_min_dt(cfd_ctx *ctx, double *min_dt) {
+  if (!ctx || !min_dt) return fail(CFD_ERR_BAD_ARG, "null argument");
+  cfd_status s = sync_status(ctx, nullptr);
+  *min_dt = ctx->h_ctl[CTL_DTMIN];
+  return s;
+}
+
+cfd_status cfd_download(cfd_ctx *ctx, double *U, double *prim, double *dt, double *net, double *delu) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  const int NP = ctx->NP, NT = ctx->NT;
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> hU(4 * (size_t)NT), hS, hP;
+  CUDA_TRY(cudaMemcpy(hU.data(), ctx->ds.U, hU.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  if (U) {
+    cfd_status su = cfd_download_U(ctx, U);
+    if (su != CFD_OK) return su;
+  }
+  if (prim) {
+    hP.resize(5 * (size_t)NT);
+    CUDA_TRY(cudaMemcpy(hP.data(), ctx->ds.prim, hP.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ctx->prim_from_S) {
+      hS.resize(4 * (size_t)NP);
+      CUDA_TRY(cudaMemcpy(hS.data(), ctx->ds.S, hS.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (int i = 0; i < NT; i++) {
+      const int r = i < NP ? ctx->perm[i] : i;
+      const double rho = hP[i], u = hP[(size_t)NT + i], v = hP[2 * (size_t)NT + i], p = hP[3 * (size_t)NT + i],
+                   a = hP[4 * (size_t)NT + i];
+      const double E = (ctx->prim_from_S && i < NP) ? hS[3 * (size_t)NP + i] : hU[3 * (size_t)NT + i];
+      // The remaining slots of src/Basic_Functions.cpp:162-219 from the stored ones.
+      const double inv = 1.0 / rho;
+      const double T = (p * inv / 287.0);
+      const double vmag = (u * u + v * v);
+      const double M = std::sqrt(vmag) / a;
+      double *o = prim + 11 * (size_t)r;
+      o[0] = rho;
+      o[1] = u;
+      o[2] = v;
+      o[3] = T;
+      o[4] = p;
+      o[5] = a;
+      o[6] = E;
+      o[7] = M;
+      o[8] = 0.0;
+      o[9] = 0.0;
+      o[10] = p * std::pow((1.0 + 0.5 * kGM1 * M * M), kGamma1);
+    }
+  }
+  auto fetch_np = [&](const double *src, int ncomp, double *dst) -> cfd_status {
+    std::vector<double> h((size_t)ncomp * NP);
+    CUDA_TRY(cudaMemcpy(h.data(), src, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < NP; i++) {
+      const int r = ctx->perm[i];
+      for (int k = 0; k < ncomp; k++) dst[(size_t)ncomp * r + k] = h[(size_t)k * NP + i];
+    }
+    return CFD_OK;
+  };
+  cfd_status s;
+  if (dt && (s = fetch_np(ctx->ds.dtc, 1, dt)) != CFD_OK) return s;
+  if (net && (s = fetch_np(ctx->ds.R, 4, net)) != CFD_OK) return s;
+  if (delu && (s = fetch_np(ctx->ds.dU, 4, delu)) != CFD_OK) return s;
+  return CFD_OK;
+}
+
+cfd_status cfd_download_stage_state(cfd_ctx *ctx, double *S) {
+  if (!ctx || !S) return fail(CFD_ERR_BAD_ARG, "null argument");
+  const int NP = ctx->NP;
+  std::vector<double> h(4 * (size_t)NP);
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  CUDA_TRY(cudaMemcpy(h.data(), ctx->ds.S, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < NP; i++) {
+    const int r = ctx->perm[i];
+    for (int k = 0; k < 4; k++) S[4 * (size_t)r + k] = h[(size_t)k * NP + i];
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad) {
+  if (!ctx || !grad) return fail(CFD_ERR_BAD_ARG, "null argument");
+  const int map[6] = {0, 1, 2, -1, 3, 4};
+  if (var < 0 || var > 5 || map[var] < 0) return fail(CFD_ERR_BAD_ARG, "gradient slot must be 0,1,2,4 or 5");
+  const int NP = ctx->NP;
+  double *dg = nullptr;
+  CUDA_TRY(cudaMalloc(&dg, 2 * (size_t)NP * sizeof(double)));
+  ctx->launches += launch_gradient(ctx->stream, ctx->dm, ctx->ds, map[var], dg);
+  std::vector<double> h(2 * (size_t)NP);
+  cudaError_t e = cudaMemcpyAsync(h.data(), dg, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dg);
+  if (e != cudaSuccess) return fail(CFD_ERR_CUDA, cudaGetErrorString(e));
+  for (int i = 0; i < NP; i++) {
+    const int r = ctx->perm[i];
+    grad[2 * (size_t)r] = h[2 * (size_t)i];
+    grad[2 * (size_t)r + 1] = h[2 * (size_t)i + 1];
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  (void)threshold;
+  (void)max_fraction;
+  (void)tags;
+  const int NP = ctx->NP;
+  double *dind = nullptr;
+  CUDA_TRY(cudaMalloc(&dind, (size_t)NP * sizeof(double)));
+  ctx->launches += launch_amr_indicator(ctx->stream, ctx->dm, ctx->ds, dind);
+  std::vector<double> h(NP);
+  cudaError_t e = cudaMemcpyAsync(h.data(), dind, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dind);
+  if (e != cudaSuccess) return fail(CFD_ERR_CUDA, cudaGetErrorString(e));
+  if (indicator)
+    for (int i = 0; i < NP; i++) indicator[ctx->perm[i]] = h[i];
+  if (tags) return fail(CFD_ERR_BAD_ARG, "tags not available in this build");
+  return CFD_OK;
+}
+
+cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches) {
+  if (!ctx || !kernel || !total_ms || !launches) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::string k(kernel);
+  int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : -1;
+  if (kind < 0) return fail(CFD_ERR_BAD_ARG, "unknown kernel " + k);
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (auto &t : ctx->timed) {
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, t.a, t.b));
+    ctx->kind_ms[t.kind] += ms;
+    ctx->kind_n[t.kind] += 1;
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  ctx->timed.clear();
+  *total_ms = ctx->kind_ms[kind];
+  *launches = ctx->kind_n[kind];
+  return CFD_OK;
+}
+
+long long cfd_kernel_launches(const cfd_ctx *ctx) { return ctx ? ctx->launches : 0; }
+size_t cfd_device_bytes(const cfd_ctx *ctx) { return ctx ? ctx->bytes : 0; }
+
+}  // extern "C"

@@ -1,0 +1,622 @@
+// CUDA kernels of the explicit FV residual/update path (sm_100a, FP64, --fmad=false).
+//
+// One thread per physical cell gathers its own faces in the reference's face order 0..nF-1,
+// so every per-cell sum is formed in the same order as the reference's serial loop and the
+// result is deterministic and bit-identical; there are no atomics on data.  Reductions (min dt,
+// residual norms) use a fixed-shape warp-shuffle tree per block and a last-block pass over the
+// per-block partials in block order.
+#include <climits>
+
+#include "kernels.cuh"
+#include "physics.cuh"
+
+namespace cfdb {
+
+namespace {
+
+constexpr int kFluxBlock = 128;
+constexpr int kBlock = 256;
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ bool step_done(const double *ctl) { return ctl[CTL_DONE] != 0.0; }
+
+__device__ __forceinline__ void flag_bad(int *status, int cell) {
+  atomicMin(&status[1], cell);
+  atomicCAS(&status[0], 0, 3 /* CFD_ERR_NONPHYSICAL */);
+}
+
+__device__ __forceinline__ void store_prim(double *prim, int NT, int c, const Prim &q) {
+  prim[c] = q.rho;
+  prim[NT + c] = q.u;
+  prim[2 * NT + c] = q.v;
+  prim[3 * NT + c] = q.p;
+  prim[4 * NT + c] = q.a;
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double w = __shfl_xor_sync(kFull, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Block-wide min; result valid in thread 0.
+__device__ __forceinline__ double block_min(double v, double *sh) {
+  v = warp_min(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < nw ? sh[lane] : 1e308 * 10.0;
+    v = warp_min(v);
+  }
+  return v;
+}
+
+// Block-wide sum (fixed tree); result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < nw ? sh[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+// Returns true in every thread of the block that finished last among the grid's blocks.
+__device__ __forceinline__ bool last_block(unsigned int *counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return is_last;
+}
+
+// ---------------------------------------------------------------------------------------------
+__global__ void k_prim_all(DevMesh m, DevState st) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.NT) return;
+  const double *U = st.U;
+  Prim q;
+  bool ok = eos_prim(U[c], U[m.NT + c], U[2 * m.NT + c], U[3 * m.NT + c], q);
+  store_prim(st.prim, m.NT, c, q);
+  if (!ok) flag_bad(st.status, c);
+}
+
+// Apply_Boundary_Conditions (src/Boundary_Conditions.cpp:12-61): one thread per
+// (kind, cell, face, ghost) entry writes U and primitives of the ghost row.
+//   wall / symmetry  src/Wall_Boundary_Conditions.cpp:8-53, :79-124 (reflect V about the face normal)
+//   supersonic inlet src/Inlet_Boundary_Conditions.cpp:41-74 (rho, p prescribed, V extrapolated)
+//   subsonic inlet   src/Inlet_Boundary_Conditions.cpp:7-39 (reference energy form)
+//   supersonic exit  src/Exit_Boundary_Conditions.cpp:68-94 (copy of U_Cells of the interior cell)
+//   subsonic exit    src/Exit_Boundary_Conditions.cpp:83-85 (no-op in the reference)
+// Additive forms: total-(p, T) characteristic inflow and static-pressure outflow.
+__global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.NB || step_done(st.ctl)) return;
+  const int4 b = m.bnd[e];
+  const int kind = b.x, c = b.y, f = b.z, g = b.w;
+  const int NT = m.NT, NP = m.NP;
+  const double *prim = st.prim;
+  const double rho = prim[c], u = prim[NT + c], v = prim[2 * NT + c], p = prim[3 * NT + c];
+  double G0, G1, G2, G3;
+  if (kind == 2 || kind == 3) {
+    const double n1 = m.nx[f * NP + c], n2 = m.ny[f * NP + c];
+    double vdotn = (u * n1 + v * n2);
+    double v1g = u - 2.0 * vdotn * n1;
+    double v2g = v - 2.0 * vdotn * n2;
+    double vmag = 0.5 * (v1g * v1g + v2g * v2g);
+    G0 = rho;
+    G1 = rho * v1g;
+    G2 = rho * v2g;
+    G3 = ((p / kGM1) + rho * vmag);
+  } else if (kind == 0) {
+    if (bp.inlet_bc == 0) {
+      double vmag = (u * u + v * v) * 0.5;
+      G0 = bp.inlet_rho;
+      G1 = bp.inlet_rho * u;
+      G2 = bp.inlet_rho * v;
+      G3 = (bp.inlet_p / kGM1) + bp.inlet_rho * vmag;
+    } else if (bp.inlet_bc == 1) {
+      double Vm = 0.5 * (u * u + v * v);
+      G0 = bp.inlet_rho;
+      G1 = bp.inlet_rho * u;
+      G2 = bp.inlet_rho * v;
+      G3 = (bp.inlet_p / kGM1) + bp.inlet_rho * Vm * Vm;
+    } else {
+      // Subsonic inflow with total pressure p0 and total temperature T0 (no reference
+      // counterpart: the reference's subsonic inlet is the form above).  n is the outward
+      // normal, so inflow has Vn < 0 and the characteristic Vn + a leaves the domain: its
+      // invariant R+ = Vn + 2a/(g-1) comes from the interior.  With V = Vn n and
+      // H0 = a0^2/(g-1) = a^2/(g-1) + Vn^2/2 this gives
+      //   (g+1)/(g-1) a^2 - 2 R+ a + (g-1)/2 R+^2 - a0^2 = 0   (larger root),
+      // then Vn = R+ - 2a/(g-1), T = a^2/(g R), p = p0 (T/T0)^(g/(g-1)), rho = p/(R T).
+      const double n1 = m.nx[f * NP + c], n2 = m.ny[f * NP + c];
+      const double a_i = prim[4 * NT + c];
+      const double vn_i = u * n1 + v * n2;
+      const double Rp = vn_i + 2.0 * a_i / kGM1;
+      const double a0sq = kGamma * bp.r_gas * bp.inlet_t0;
+      const double qa = (kGamma + 1.0) / kGM1, qb = -2.0 * Rp, qc = 0.5 * kGM1 * Rp * Rp - a0sq;
+      const double disc = qb * qb - 4.0 * qa * qc;
+      const double ab = (-qb + sqrt(disc > 0.0 ? disc : 0.0)) / (2.0 * qa);
+      double vn = Rp - 2.0 * ab / kGM1;
+      if (vn > 0.0) vn = 0.0;
+      const double Tb = ab * ab / (kGamma * bp.r_gas);
+      const double pb = bp.inlet_p0 * pow(Tb / bp.inlet_t0, kGamma / kGM1);
+      const double rb = pb / (bp.r_gas * Tb);
+      const double ub = vn * n1, vb = vn * n2;
+      G0 = rb;
+      G1 = rb * ub;
+      G2 = rb * vb;
+      G3 = pb / kGM1 + 0.5 * rb * (ub * ub + vb * vb);
+    }
+  } else {  // exit
+    if (bp.exit_bc == 1) return;
+    const double *Us = src_is_S ? st.S : st.U;
+    const int ld = src_is_S ? NP : NT;
+    if (bp.exit_bc == 0) {
+      G0 = Us[c];
+      G1 = Us[ld + c];
+      G2 = Us[2 * ld + c];
+      G3 = Us[3 * ld + c];
+    } else {
+      // Static-pressure outflow: rho, V extrapolated; p prescribed when the normal Mach
+      // number is subsonic, extrapolated otherwise.
+      const double n1 = m.nx[f * NP + c], n2 = m.ny[f * NP + c];
+      const double a_i = prim[4 * NT + c];
+      const double vn = u * n1 + v * n2;
+      const double pb = (vn < a_i) ? bp.exit_p : p;
+      G0 = rho;
+      G1 = rho * u;
+      G2 = rho * v;
+      G3 = pb / kGM1 + 0.5 * rho * (u * u + v * v);
+    }
+  }
+  double *U = st.U;
+  U[g] = G0;
+  U[NT + g] = G1;
+  U[2 * NT + g] = G2;
+  U[3 * NT + g] = G3;
+  Prim q;
+  bool ok = eos_prim(G0, G1, G2, G3, q);
+  store_prim(st.prim, NT, g, q);
+  if (!ok) flag_bad(st.status, g);
+}
+
+// Conserved state of cell n for the limiter / LLF: U_Cells (U^n on physical rows, boundary
+// values on ghost rows) in the reference's semantics, or the current stage state.
+struct USrc {
+  const double *U, *S;
+  int NT, NP, use_S;
+  __device__ __forceinline__ double get(int k, int n) const {
+    return (use_S && n < NP) ? S[k * NP + n] : U[k * NT + n];
+  }
+};
+
+// Evaluate_Cell_Net_Flux_1O/2O (src/Net_Flux.cpp:46-129) + Evaluate_Time_Step (src/Time_Step.cpp:293-359)
+// fused: per cell, faces in order, Net += avg - diss; then dt = CFL*A / sum(|V.n|+a)dl.  The block
+// min of dt goes to `partial`; the last block writes Min_dt (get_Min_dt, src/Numerical_Method.cpp:322).
+template <int DISS, int ORDER>
+__global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
+  __shared__ double sh[32];
+  const int NP = m.NP, NT = m.NT;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool done = step_done(st.ctl);
+  double dt = 1e308 * 10.0;
+  if (c < NP && !done) {
+    const double *prim = st.prim;
+    const double rc = prim[c], uc = prim[NT + c], vc = prim[2 * NT + c], pc = prim[3 * NT + c], ac = prim[4 * NT + c];
+    const USrc us{st.U, st.S, NT, NP, fp.consistent && src_is_S};
+    double Uc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (DISS == 1 || ORDER == 2) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) Uc[k] = us.get(k, c);
+    }
+    const int nf = m.nf[c];
+    const uint8_t degen = m.degen[c];
+    double N0 = 0.0, N1s = 0.0, N2s = 0.0, N3s = 0.0;
+    double den = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      if (f < nf) {
+        const int idx = f * NP + c;
+        const int N = m.nbr[idx];
+        const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
+        const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
+        double A[4], D[4];
+        average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
+        if (DISS == 3 && ORDER == 1) {
+          if (N >= NP)
+            roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (degen >> f) & 1, D);
+          else
+            roe_1o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, (degen >> f) & 1, D);
+        } else if (DISS == 3 && ORDER == 2) {
+          const int n2 = m.n2[idx];
+          const double d1 = m.d1l[idx], d2 = m.d2l[idx];
+          double dU[4];
+          if (!fp.recon_prim) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const double q1 = us.get(k, N), q2 = us.get(k, n2);
+              const double phi = limited_slope<double>(fp.limiter, Uc[k], q1, q2, d1, d2, fp.zeta, fp.zeta1);
+              const double VR = q1 + 0.5 * phi * d1;
+              const double VL = Uc[k] - 0.5 * phi * d1;
+              dU[k] = VR - VL;
+            }
+          } else {
+            // MUSCL on (rho, u, v, p) of the stage primitives; the conserved jump of the two
+            // reconstructed face states drives the Roe wave strengths.
+            const double qc[4] = {rc, uc, vc, pc};
+            const double q1v[4] = {rn, un, vn, pn};
+            const double q2v[4] = {prim[n2], prim[NT + n2], prim[2 * NT + n2], prim[3 * NT + n2]};
+            double qR[4], qL[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const double phi = limited_slope<double>(fp.limiter, qc[k], q1v[k], q2v[k], d1, d2, fp.zeta, fp.zeta1);
+              qR[k] = q1v[k] + 0.5 * phi * d1;
+              qL[k] = qc[k] - 0.5 * phi * d1;
+            }
+            dU[0] = qR[0] - qL[0];
+            dU[1] = qR[0] * qR[1] - qL[0] * qL[1];
+            dU[2] = qR[0] * qR[2] - qL[0] * qL[2];
+            dU[3] = (qR[3] / kGM1 + 0.5 * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])) -
+                    (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
+          }
+          roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
+        } else {  // LLF 1O
+          double UR[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) UR[k] = us.get(k, N);
+          llf_1o<double>(uc, vc, ac, un, vn, an, Uc, UR, nx, ny, dl, D);
+        }
+        N0 += A[0] - D[0];
+        N1s += A[1] - D[1];
+        N2s += A[2] - D[2];
+        N3s += A[3] - D[3];
+        const double vnf = uc * nx + vc * ny;
+        den += (fabs(vnf) + ac) * dl;
+      }
+    }
+    if (den <= 0.0 || !isfinite(den)) dt = 0.0;
+    else dt = fp.cfl * m.area[c] / den;
+    st.R[c] = N0;
+    st.R[NP + c] = N1s;
+    st.R[2 * NP + c] = N2s;
+    st.R[3 * NP + c] = N3s;
+    st.dtc[c] = dt;
+  }
+  double bm = block_min(dt, sh);
+  if (done) return;
+  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
+  if (last_block(st.counter)) {
+    double v = 1e308 * 10.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      double w = __ldcg(&st.partial[i]);
+      v = w < v ? w : v;
+    }
+    v = block_min(v, sh);
+    if (threadIdx.x == 0) {
+      st.ctl[CTL_DTMIN] = v;
+      *st.counter = 0u;
+    }
+  }
+}
+
+// Estimate_Error (src/Error_Estimate_Update.cpp:10-28) terms of one cell; dU < 1e-9 is the
+// reference's signed test.
+__device__ __forceinline__ double err_term(double du, double u) {
+  double t = (du < 1e-9) ? fabs(du) : (fabs(du) / u);
+  return t * t;
+}
+
+// Per-block partial sums (4 error terms, 4 residual squares), then the last block reduces the
+// partials in block order and applies the step epilogue (Total_Time += Min_dt, iterations++).
+__device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const double e[8], bool advance_time,
+                                                        double dt_for_time) {
+  __shared__ double sh[32];
+  for (int q = 0; q < 8; q++) {
+    double s = block_sum(e[q], sh);
+    if (threadIdx.x == 0) st.partial[q * gridDim.x + blockIdx.x] = s;
+  }
+  if (last_block(st.counter)) {
+    if (threadIdx.x < 8) {
+      const int q = threadIdx.x;
+      double s = 0.0;
+      for (int i = 0; i < (int)gridDim.x; i++) s += __ldcg(&st.partial[q * gridDim.x + i]);
+      st.ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(s);
+    }
+    if (threadIdx.x == 0) {
+      if (advance_time) {
+        double t = st.ctl[CTL_TOTAL_TIME] + dt_for_time;
+        st.ctl[CTL_TOTAL_TIME] = t;
+        st.ctl[CTL_ITER] += 1.0;
+        double te = st.ctl[CTL_TEND];
+        if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
+      }
+      *st.counter = 0u;
+    }
+  }
+}
+
+// Stage updates of Runge_Kutta_Method (src/Numerical_Method.cpp:342-457) and Explicit_Method
+// (:26-103), written with the reference's association order.  kind: 1,2,3 RK3 stages, 0
+// explicit, 11..14 classical RK4.  lts: 0 Min_dt, 1 Cell::del_t (reference stage 1 only), 2 dt
+// frozen per cell at the first stage, 3 Min_dt frozen at the first stage.
+__global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int kind, int lts, int fuse_final,
+                                                  int keep_delu) {
+  const int NP = m.NP, NT = m.NT;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool done = step_done(st.ctl);
+  const bool active = c < NP && !done;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const double dtmin = st.ctl[CTL_DTMIN];
+  if (active) {
+    if (kind == 1 || kind == 11) {
+      if (lts == 2) st.dtk[c] = st.dtc[c];
+    }
+    double dt;
+    if (lts == 0) dt = dtmin;
+    else if (lts == 1) dt = st.dtc[c];
+    else if (lts == 2) dt = (kind == 1 || kind == 11) ? st.dtc[c] : st.dtk[c];
+    else dt = (kind == 1 || kind == 11) ? dtmin : st.ctl[CTL_DTSTEP];
+    const double invA = m.inv_area[c];
+    double Un[4], Rk[4], out[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      Un[k] = st.U[k * NT + c];
+      Rk[k] = st.R[k * NP + c];
+    }
+    bool final_stage = false;
+    if (kind == 1) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
+    } else if (kind == 2) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) out[k] = 0.25 * (st.S[k * NP + c] + 3.0 * Un[k] - dt * invA * Rk[k]);
+    } else if (kind == 3) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) out[k] = (2.0 / 3.0) * (st.S[k * NP + c] - Un[k] - dt * invA * Rk[k]);
+      final_stage = true;
+    } else if (kind == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) out[k] = -dt * invA * Rk[k];
+      final_stage = true;
+    } else if (kind == 11) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        st.Racc[k * NP + c] = Rk[k];
+        out[k] = Un[k] - 0.5 * (dt * invA) * Rk[k];
+      }
+    } else if (kind == 12 || kind == 13) {
+      const double w = (kind == 12) ? 0.5 : 1.0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        st.Racc[k * NP + c] = st.Racc[k * NP + c] + 2.0 * Rk[k];
+        out[k] = Un[k] - w * (dt * invA) * Rk[k];
+      }
+    } else {  // 14
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        double acc = st.Racc[k * NP + c] + Rk[k];
+        out[k] = -((dt * invA) * acc) / 6.0;
+      }
+      final_stage = true;
+    }
+    if (!final_stage) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) st.S[k * NP + c] = out[k];
+      Prim q;
+      bool ok = eos_prim(out[0], out[1], out[2], out[3], q);
+      store_prim(st.prim, NT, c, q);
+      if (!ok) flag_bad(st.status, c);
+    } else {
+      if (keep_delu || !fuse_final) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) st.dU[k * NP + c] = out[k];
+      }
+      if (fuse_final) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          e[k] = err_term(out[k], Un[k]);
+          e[4 + k] = Rk[k] * Rk[k];
+          double nu = Un[k] + out[k];
+          st.U[k * NT + c] = nu;
+          Un[k] = nu;
+        }
+        Prim q;
+        bool ok = eos_prim(Un[0], Un[1], Un[2], Un[3], q);
+        store_prim(st.prim, NT, c, q);
+        if (!ok) flag_bad(st.status, c);
+      }
+    }
+  }
+  if ((kind == 1 || kind == 11) && c == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
+  if (fuse_final && (kind == 3 || kind == 0 || kind == 14)) {
+    if (done) return;
+    const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : dtmin;
+    reduce_err_and_epilogue(st, e, true, dt_time);
+  }
+}
+
+// Estimate_Error alone (src/Error_Estimate_Update.cpp:10-28).
+__global__ void __launch_bounds__(kBlock) k_error(DevMesh m, DevState st) {
+  const int NP = m.NP, NT = m.NT;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (c < NP) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      e[k] = err_term(st.dU[k * NP + c], st.U[k * NT + c]);
+      double r = st.R[k * NP + c];
+      e[4 + k] = r * r;
+    }
+  }
+  reduce_err_and_epilogue(st, e, false, 0.0);
+}
+
+// Update() (src/Error_Estimate_Update.cpp:31-43): U += dU, primitives refreshed.
+__global__ void __launch_bounds__(kBlock) k_update(DevMesh m, DevState st) {
+  const int NP = m.NP, NT = m.NT;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= NP) return;
+  double u[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    u[k] = st.U[k * NT + c] + st.dU[k * NP + c];
+    st.U[k * NT + c] = u[k];
+  }
+  Prim q;
+  bool ok = eos_prim(u[0], u[1], u[2], u[3], q);
+  store_prim(st.prim, NT, c, q);
+  if (!ok) flag_bad(st.status, c);
+}
+
+// Calculate_Gradient_At_Cell_Center (src/Grid_Refine_Functions.cpp:221-246); var indexes the
+// device primitive planes (0 rho, 1 u, 2 v, 3 p, 4 a).
+__device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, int c, double &g0, double &g1) {
+  g0 = 0.0;
+  g1 = 0.0;
+  const int nf = m.nf[c];
+  if (nf <= 0 || m.area[c] <= 0.0) return;
+  const double pc = q[c];
+  for (int f = 0; f < nf; f++) {
+    const int idx = f * m.NP + c;
+    const int N = m.nbr[idx];
+    double pn = pc;
+    if (N >= 0 && N < m.NP) pn = q[N];
+    const double pf = 0.5 * (pc + pn);
+    g0 += pf * m.nx[idx] * m.dl[idx];
+    g1 += pf * m.ny[idx] * m.dl[idx];
+  }
+  g0 *= m.inv_area[c];
+  g1 *= m.inv_area[c];
+}
+
+__global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.NP) return;
+  double g0, g1;
+  gg_gradient(m, st.prim + (size_t)var * m.NT, c, g0, g1);
+  grad[2 * c] = g0;
+  grad[2 * c + 1] = g1;
+}
+
+// Compute_Gradient_Refinement_Indicator (src/Grid_Refine_Functions.cpp:8-31).
+__global__ void k_amr_indicator(DevMesh m, DevState st, double *ind) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.NP) return;
+  double v = 0.0;
+  const double h = sqrt(m.area[c]);
+  double g0, g1;
+  gg_gradient(m, st.prim, c, g0, g1);
+  v += sqrt(g0 * g0 + g1 * g1) * h;
+  gg_gradient(m, st.prim + 3 * (size_t)m.NT, c, g0, g1);
+  const double P = st.prim[3 * m.NT + c];
+  if (P > 1e-14) v += (sqrt(g0 * g0 + g1 * g1) / P) * h;
+  ind[c] = v;
+}
+
+__global__ void k_set_ctl(double *ctl, int idx, double v) { ctl[idx] = v; }
+
+// Reference-order AoS rows [NT][4] <-> device-order SoA planes [4][NT] (perm: device -> reference).
+__global__ void k_import_aos(const double *__restrict__ aos, const int *__restrict__ perm, int NP, int NT, double *U) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NT) return;
+  const int r = i < NP ? perm[i] : i;
+  const double4 v = reinterpret_cast<const double4 *>(aos)[r];
+  U[i] = v.x;
+  U[NT + i] = v.y;
+  U[2 * NT + i] = v.z;
+  U[3 * NT + i] = v.w;
+}
+
+__global__ void k_export_aos(const double *__restrict__ U, const int *__restrict__ perm, int NP, int NT, int ld,
+                             double *aos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NT) return;
+  const int r = i < NP ? perm[i] : i;
+  reinterpret_cast<double4 *>(aos)[r] = make_double4(U[i], U[ld + i], U[2 * ld + i], U[3 * ld + i]);
+}
+
+inline int nblk(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+int flux_block_count(int NP) { return nblk(NP, kFluxBlock) > nblk(NP, kBlock) ? nblk(NP, kFluxBlock) : nblk(NP, kBlock); }
+
+int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st) {
+  k_prim_all<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
+  return 1;
+}
+
+int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int src_is_S) {
+  if (m.NB == 0) return 0;
+  k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S);
+  return 1;
+}
+
+int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
+  const int g = nblk(m.NP, kFluxBlock);
+  if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  return 1;
+}
+
+int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu) {
+  k_stage<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, kind, lts, fuse_final, keep_delu);
+  return 1;
+}
+
+int launch_error(cudaStream_t s, const DevMesh &m, DevState &st) {
+  k_error<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st);
+  return 1;
+}
+
+int launch_update(cudaStream_t s, const DevMesh &m, DevState &st) {
+  k_update<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st);
+  return 1;
+}
+
+int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad) {
+  k_gradient<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, var, grad);
+  return 1;
+}
+
+int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind) {
+  k_amr_indicator<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, ind);
+  return 1;
+}
+
+int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP, int NT, double *U) {
+  k_import_aos<<<nblk(NT, kBlock), kBlock, 0, s>>>(aos, perm, NP, NT, U);
+  return 1;
+}
+
+int launch_export_aos(cudaStream_t s, const double *U, const int *perm, int NP, int NT, int ld, double *aos) {
+  k_export_aos<<<nblk(NT, kBlock), kBlock, 0, s>>>(U, perm, NP, NT, ld, aos);
+  return 1;
+}
+
+int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v) {
+  k_set_ctl<<<1, 1, 0, s>>>(st.ctl, idx, v);
+  return 1;
+}
+
+}  // namespace cfdb

@@ -1,0 +1,90 @@
+// Device data layout and kernel declarations of the residual/update path.
+//
+// HBM layout (all arrays in device cell order; physical cells 0..NP-1 possibly RCM-renumbered,
+// ghost cells NP..NT-1 in the reference's ghost order):
+//   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l
+//   per cell [NP]: nf, area, inv_area, degenerate-face mask
+//   state, component-major SoA: U[4][NT] (U^n on physical rows, boundary values on ghost rows),
+//   S[4][NP] (RK stage state), prim[5][NT] (rho, u, v, p, a), R[4][NP] (net flux),
+//   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cfdb {
+
+struct DevMesh {
+  int NP, NT, NB;
+  const int *nf;
+  const int *nbr;
+  const double *nx, *ny, *dl;
+  const double *area, *inv_area;
+  const int *n2;
+  const double *d1l, *d2l;
+  const uint8_t *degen;
+  const int4 *bnd;  // kind, cell, face, ghost
+};
+
+struct DevState {
+  double *U;     // [4][NT]
+  double *S;     // [4][NP]
+  double *prim;  // [5][NT]
+  double *R;     // [4][NP]
+  double *Racc;  // [4][NP] (RK4 accumulator)
+  double *dtc;   // [NP]
+  double *dtk;   // [NP] dt kept for the whole step (RK4 / SSP with LTS)
+  double *dU;    // [4][NP]
+  // reduction / control block (see CtrlIdx)
+  double *ctl;
+  double *partial;     // [nblk_max * 9]
+  unsigned int *counter;
+  int *status;         // [0] status code, [1] first bad cell (device order)
+};
+
+// Slots of the device control block `ctl`.
+enum CtrlIdx : int {
+  CTL_DTMIN = 0,       // Min_dt of the last flux evaluation
+  CTL_DTSTEP = 1,      // dt frozen for the current step (RK4 / SSP-RK3)
+  CTL_TOTAL_TIME = 2,  // Total_Time
+  CTL_ITER = 3,        // iterations (as double)
+  CTL_DONE = 4,        // 1 when Total_Time >= t_end
+  CTL_TEND = 5,        // t_end (<= 0: none)
+  CTL_ERR = 8,         // Error[0..3]
+  CTL_RES = 12,        // plain ||R||_2 [4]
+  CTL_SIZE = 16
+};
+
+struct FluxParams {
+  int dissipation;      // 1 LLF, 3 ROE, 6 AUSM, 7 HLLC
+  int second_order;
+  int limiter;
+  int recon_prim;
+  int consistent;       // 1: limiter/LLF/exit read the stage state instead of U^n
+  int precision;
+  double cfl, zeta, zeta1;
+};
+
+struct BcParams {
+  int inlet_bc, exit_bc;
+  double inlet_rho, inlet_p, inlet_u, inlet_v, inlet_p0, inlet_t0, exit_p, r_gas;
+};
+
+// Kernel launchers (stream-ordered, no host synchronisation).  Each returns the number of
+// kernels launched.
+int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st);
+int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int stage_src_is_S);
+int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int stage_src_is_S);
+// kind: 1,2,3 = reference RK3 stages; 0 = Explicit; 11..14 = RK4 stages; fuse_final = apply
+// Estimate_Error + Update in the last stage's kernel.
+int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu);
+int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
+int launch_update(cudaStream_t s, const DevMesh &m, DevState &st);
+int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
+int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
+int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
+int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP, int NT, double *U);
+int launch_export_aos(cudaStream_t s, const double *U, const int *perm, int NP, int NT, int ld, double *aos);
+
+int flux_block_count(int NP);
+
+}  // namespace cfdb

@@ -1,0 +1,225 @@
+// Device-side arithmetic of the explicit FV residual path.
+//
+// Every function follows the reference's CPU code operation by operation (same association
+// order, same constants as the reference's macros expand them), so that, compiled with
+// --fmad=false, each result is bit-identical to the reference built with -ffp-contract=off.
+// IEEE double +, -, *, /, sqrt are correctly rounded on both sides.
+//
+// Macro constants of include/definitions.h:63-65 as the preprocessor expands them:
+//   gamma_M_1 -> (1.4 - 1.0)            gamma1 * x -> 1.4 / (1.4 - 1.0) * x
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace cfdb {
+
+constexpr double kGamma = 1.4;
+constexpr double kGM1 = 1.4 - 1.0;               // gamma_M_1 and (gamma - 1.0)
+constexpr double kGamma1 = 1.4 / (1.4 - 1.0);    // gamma1 (left operand of a product)
+
+struct Prim {  // the five primitive slots the fluxes read: Primitive_Cells[c][0,1,2,4,5]
+  double rho, u, v, p, a;
+};
+
+// Calculate_Primitive_Variables, src/Basic_Functions.cpp:100-156 (slots 0,1,2,4,5).
+// Returns false when the sound speed is NaN (the reference exits there, :151-155).
+__host__ __device__ inline bool eos_prim(double U0, double U1, double U2, double U3, Prim &q) {
+  double Rho = U0;
+  double inv = 1.0 / Rho;
+  double v1 = U1 * inv;
+  double v2 = U2 * inv;
+  if (fabs(v1) <= 1e-10) v1 = 0.0;
+  if (fabs(v2) <= 1e-10) v2 = 0.0;
+  double vmag = (v1 * v1 + v2 * v2);
+  double P = kGM1 * (U3 - 0.5 * Rho * vmag);
+  double C = sqrt(kGamma * P * inv);
+  q.rho = Rho;
+  q.u = v1;
+  q.v = v2;
+  q.p = P;
+  q.a = C;
+  return !(C != C);
+}
+
+// Calculate_Face_Average_Flux, src/Average_Interface_Flux.cpp:20-82 (wall flag is never set on
+// the reference path, src/Initialize.cpp:100).
+template <typename T>
+__device__ __forceinline__ void average_flux(const T rL, const T uL, const T vL, const T pL, const T rR, const T uR,
+                                             const T vR, const T pR, const T nx, const T ny, const T dl, T F[4]) {
+  const T g1 = T(kGamma1);
+  T VnL = (uL * nx + vL * ny);
+  T VnR = (uR * nx + vR * ny);
+  T VmL = T(0.5) * (uL * uL + vL * vL);
+  T VmR = T(0.5) * (uR * uR + vR * vR);
+  T VnLdl = VnL * dl;
+  T VnRdl = VnR * dl;
+  T FL0 = rL * VnLdl, FL1 = rL * uL * VnLdl + pL * nx * dl, FL2 = rL * vL * VnLdl + pL * ny * dl,
+    FL3 = (g1 * pL + rL * VmL) * VnLdl;
+  T FR0 = rR * VnRdl, FR1 = rR * uR * VnRdl + pR * nx * dl, FR2 = rR * vR * VnRdl + pR * ny * dl,
+    FR3 = (g1 * pR + rR * VmR) * VnRdl;
+  F[0] = T(0.5) * (FL0 + FR0);
+  F[1] = T(0.5) * (FL1 + FR1);
+  F[2] = T(0.5) * (FL2 + FR2);
+  F[3] = T(0.5) * (FL3 + FR3);
+}
+
+// The wave-decomposition tail shared by ROE and ROE_2O (src/Roe_Scheme.cpp:193-228, :376-423):
+// eigenvalues with Harten's fix delta = 0.1*a_Roe, right eigenvectors, D = 0.5*sum|l|a r*dl.
+template <typename T>
+__device__ __forceinline__ void roe_tail(const T Ru, const T Rv, const T RH, const T RVm, const T Ra, const T RoeRho,
+                                         const T Un, const T Ut, const T dP, const T dRho, const T dUn, const T dUt,
+                                         const T nx, const T ny, const T dl, T D[4]) {
+  T R11 = T(1.0), R12 = Ru - nx * Ra, R13 = Rv - ny * Ra, R14 = RH - Ra * Un;
+  T R21 = T(1.0), R22 = Ru, R23 = Rv, R24 = RVm;
+  T R31 = T(0.0), R32 = -ny, R33 = nx, R34 = Ut;
+  T R41 = T(1.0), R42 = Ru + nx * Ra, R43 = Rv + ny * Ra, R44 = RH + Ra * Un;
+  T Term2 = T(1.0) / (Ra * Ra);
+  T a1 = T(0.5) * Term2 * (dP - RoeRho * Ra * dUn);
+  T a2 = dRho - Term2 * dP;
+  T a3 = RoeRho * dUt;
+  T a4 = T(0.5) * Term2 * (dP + RoeRho * Ra * dUn);
+  T L1 = fabs(Un - Ra), L2 = fabs(Un), L3 = fabs(Un), L4 = fabs(Un + Ra);
+  T ef = T(0.1) * Ra;
+  if (L1 < ef) L1 = T(0.5) * (L1 * L1 / ef + ef);
+  if (L4 < ef) L4 = T(0.5) * (L4 * L4 / ef + ef);
+  D[0] = T(0.5) * (L1 * a1 * R11 + L2 * a2 * R21 + L3 * a3 * R31 + L4 * a4 * R41) * dl;
+  D[1] = T(0.5) * (L1 * a1 * R12 + L2 * a2 * R22 + L3 * a3 * R32 + L4 * a4 * R42) * dl;
+  D[2] = T(0.5) * (L1 * a1 * R13 + L2 * a2 * R23 + L3 * a3 * R33 + L4 * a4 * R43) * dl;
+  D[3] = T(0.5) * (L1 * a1 * R14 + L2 * a2 * R24 + L3 * a3 * R34 + L4 * a4 * R44) * dl;
+}
+
+// ROE, src/Roe_Scheme.cpp:6-256.  `degenerate` is the precomputed |n| < 1e-12 test (:71-76);
+// a ghost neighbour has already been replaced by the cell itself (:79-84) by the caller.
+template <typename T>
+__device__ __forceinline__ void roe_1o(const T rL, const T uL, const T vL, const T pL, const T cL, const T rR,
+                                       const T uR, const T vR, const T pR, const T cR, const T nx, const T ny,
+                                       const T dl, bool degenerate, T D[4]) {
+  D[0] = D[1] = D[2] = D[3] = T(0.0);
+  if (degenerate) return;
+  if (rL <= T(0.0) || pL <= T(0.0) || cL <= T(0.0)) return;
+  T VmL = T(0.5) * (uL * uL + vL * vL);
+  T HL = ((cL * cL) / T(kGM1)) + VmL;
+  if (rR <= T(0.0) || pR <= T(0.0) || cR <= T(0.0)) return;
+  T VmR = T(0.5) * (uR * uR + vR * vR);
+  T HR = ((cR * cR) / T(kGM1)) + VmR;
+  T sL = sqrt(rL), sR = sqrt(rR);
+  T Term1 = T(1.0) / (sL + sR);
+  T RoeRho = sqrt(rL * rR);
+  T Ru = Term1 * (uR * sR + uL * sL);
+  T Rv = Term1 * (vR * sR + vL * sL);
+  T RH = Term1 * (HR * sR + HL * sL);
+  T RVm = T(0.5) * (Ru * Ru + Rv * Rv);
+  T Ra = sqrt(T(kGM1) * (RH - RVm));
+  if (Ra <= T(0.0)) {
+    Ra = T(0.5) * (cL + cR);
+    if (Ra <= T(0.0)) return;
+  }
+  T Un = nx * Ru + ny * Rv;
+  T Ut = -ny * Ru + nx * Rv;
+  T du = (uR - uL), dv = (vR - vL), dP = (pR - pL), dRho = (rR - rL);
+  T dUn = nx * du + ny * dv;
+  T dUt = -ny * du + nx * dv;
+  roe_tail<T>(Ru, Rv, RH, RVm, Ra, RoeRho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
+}
+
+// ROE_2O, src/Roe_Scheme.cpp:257-447: Roe averages of the unreconstructed cell states, wave
+// strengths from the limited conserved jump dU (Second_Order_Limiter).
+template <typename T>
+__device__ __forceinline__ void roe_2o(const T rL, const T uL, const T vL, const T pL, const T cL, const T rR,
+                                       const T uR, const T vR, const T pR, const T cR, const T nx, const T ny,
+                                       const T dl, const T dU[4], T D[4]) {
+  T VmL = T(0.5) * (uL * uL + vL * vL);
+  T HL = ((cL * cL) / T(kGM1)) + VmL;
+  T VmR = T(0.5) * (uR * uR + vR * vR);
+  T HR = ((cR * cR) / T(kGM1)) + VmR;
+  T sR = sqrt(rR), sL = sqrt(rL);
+  T Term1 = T(1.0) / (sL + sR);
+  T RoeRho = sqrt(rL * rR);
+  T Ru = Term1 * (uR * sR + uL * sL);
+  T Rv = Term1 * (vR * sR + vL * sL);
+  T RH = Term1 * (HR * sR + HL * sL);
+  T RVm = T(0.5) * (Ru * Ru + Rv * Rv);
+  T Un = nx * Ru + ny * Rv;
+  T Ut = -ny * Ru + nx * Rv;
+  T Ra = sqrt(T(kGM1) * (RH - RVm));
+  T du = dU[1] / RoeRho - dU[0] * Ru / (RoeRho * RoeRho);
+  T dv = dU[2] / RoeRho - dU[0] * Rv / (RoeRho * RoeRho);
+  T dE = dU[3] - T(0.5) * RoeRho * (T(2.0) * (Ru * du + Rv * dv) + du * du + dv * dv) - T(0.5) * dU[0] * RVm;
+  T dP = T(kGM1) * dE;
+  T dRho = dU[0];
+  T dUn = nx * du + ny * dv;
+  T dUt = -ny * du + nx * dv;
+  roe_tail<T>(Ru, Rv, RH, RVm, Ra, RoeRho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
+}
+
+// Maximum(a,b,c) / Maximum(a,b), src/Utility_Files.cpp:5-31.
+template <typename T>
+__device__ __forceinline__ T max3_ref(T a, T b, T c) {
+  if ((a >= b) && (a >= c)) return a;
+  if ((b >= a) && (b >= c)) return b;
+  return c;
+}
+template <typename T>
+__device__ __forceinline__ T max2_ref(T a, T b) {
+  return (a >= b) ? a : b;
+}
+
+// LLF, src/LLF.cpp:8-83: 0.5 * max|lambda|*dl * (U_R - U_L) with U from U_Cells.
+template <typename T>
+__device__ __forceinline__ void llf_1o(const T uL, const T vL, const T cL, const T uR, const T vR, const T cR,
+                                       const T UL[4], const T UR[4], const T nx, const T ny, const T dl, T D[4]) {
+  T VnL = (uL * nx + vL * ny);
+  T VnR = (uR * nx + vR * ny);
+  T S0 = fabs(VnL - cL) * dl, S1 = fabs(VnL + cL) * dl, S2 = fabs(VnL) * dl;
+  T S3 = fabs(VnR - cR) * dl, S4 = fabs(VnR + cR) * dl, S5 = fabs(VnR) * dl;
+  T M1 = max3_ref<T>(S0, S1, S2);
+  T M2 = max3_ref<T>(S3, S4, S5);
+  T mev = max2_ref<T>(M1, M2);
+  for (int k = 0; k < 4; k++) D[k] = T(0.5) * mev * (UR[k] - UL[k]);
+}
+
+// Sign(a), include/definitions.h:76.
+template <typename T>
+__device__ __forceinline__ int sign_ref(T a) {
+  return (a > T(0.0)) - (a < T(0.0));
+}
+
+// Limiter functions phi(a, b), r = a / b, as the reference's GPU limiter family defines them
+// (CUDA_KERNELS/Limiter_Cuda_Kernels.cu:89-154): phi = 0 when |b| < 1e-12 or r <= 0, else
+//   minmod min(r, 1); Van Leer 2r/(1+r); superbee max(min(2r,1), min(r,2)); Van Albada (r^2+r)/(r^2+1).
+enum LimiterKind : int { LIM_REF_MINMOD = 0, LIM_MINMOD = 1, LIM_VANLEER = 2, LIM_SUPERBEE = 3, LIM_VANALBADA = 4 };
+
+template <typename T>
+__device__ __forceinline__ T phi_ab(int kind, T a, T b) {
+  if (fabs(b) < T(1e-12)) return T(0.0);
+  T r = a / b;
+  if (r <= T(0.0)) return T(0.0);
+  switch (kind) {
+    case LIM_MINMOD: return fmin(r, T(1.0));
+    case LIM_VANLEER: return T(2.0) * r / (T(1.0) + r);
+    case LIM_SUPERBEE: return fmax(fmin(T(2.0) * r, T(1.0)), fmin(r, T(2.0)));
+    case LIM_VANALBADA: {
+      T r_sq = r * r;
+      return (r_sq + r) / (r_sq + T(1.0));
+    }
+    default: return T(0.0);
+  }
+}
+
+// Limited slope of one variable on the reference's directional stencil (src/Limiters.cpp:109-134):
+//   S1 = zeta*(q_c - q_N1)/d1 (across the face), S2 = zeta1*(q_N1 - q_N2)/d2 (beyond N1)
+// Reference minmod (src/Limiters.cpp:58-63): 0.5*(sgn S1 + sgn S2)*min(|S1|,|S2|).
+// phi forms: phi(S2, S1) * S1.
+template <typename T>
+__device__ __forceinline__ T limited_slope(int kind, T qc, T q1, T q2, T d1, T d2, T zeta, T zeta1) {
+  T S1 = zeta * (qc - q1) / d1;
+  T S2 = zeta1 * (q1 - q2) / d2;
+  if (kind == LIM_REF_MINMOD) {
+    T a1 = fabs(S1), b1 = fabs(S2);
+    T m = (b1 < a1) ? b1 : a1;
+    return T(0.5) * T(sign_ref<T>(S1) + sign_ref<T>(S2)) * m;
+  }
+  return phi_ab<T>(kind, S2, S1) * S1;
+}
+
+}  // namespace cfdb

@@ -1,0 +1,205 @@
+/*
+ * cfd_b200.h — C ABI of the B200-native explicit finite-volume residual/update path.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or torch types in any signature.
+ * The library owns all device memory of a context; host pointers are borrowed for the call.
+ * No function calls exit(): every failure is a status code (the reference exits on errors,
+ * e.g. src/Basic_Functions.cpp:151-155, src/Numerical_Method.cpp:66-75).
+ * One context per host thread; contexts are independent; a context is not re-entrant.
+ *
+ * Reference entry points (rameshkolluru43/CFD_Solver_withCUDA) each function replaces are
+ * cited beside it.  Indices, face order and ghost numbering follow the reference's mesh
+ * layout (include/Globals.h:313-328; ghosts numbered from No_Physical_Cells, cell-major,
+ * face-minor, src/Read_Gmsh_File.cpp:360-402).
+ */
+#ifndef CFD_B200_H
+#define CFD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CFD_OK = 0,
+  CFD_ERR_BAD_ARG = 1,
+  CFD_ERR_CUDA = 2,
+  CFD_ERR_NONPHYSICAL = 3,    /* NaN sound speed (negative pressure/density); see cfd_step_info.bad_cell */
+  CFD_ERR_DT_NONPOSITIVE = 4, /* global time step <= 0 (src/Numerical_Method.cpp:66-75) */
+  CFD_ERR_TIMEOUT = 5,        /* a bounded device wait ran out */
+  CFD_ERR_DIVERGED = 6,       /* residual growth beyond the configured limit */
+  CFD_ERR_MESH = 7,
+  CFD_ERR_IO = 8,
+  CFD_ERR_NO_DEVICE = 9
+} cfd_status;
+
+/* Message for the last error on this thread. */
+const char *cfd_last_error(void);
+/* Library version string. */
+const char *cfd_version(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Mesh layer (host only; no device needed).  Replaces the reference's mesh ingest
+ * Read_VTK_Grid (src/Read_Gmsh_File.cpp:11) + Construct_Ghost_Cells
+ * (src/Grid_Computations.cpp:394) + Calculate_Cell_Center_Distances (:802), and adds seeded
+ * generators for the benchmark geometries.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cfd_mesh cfd_mesh;
+
+/* Boundary kinds of a (cell, face, ghost) entry: the reference's Inlet/Exit/Wall/Symmetry
+ * cell lists (include/Globals.h:385). */
+enum { CFD_BC_INLET = 0, CFD_BC_EXIT = 1, CFD_BC_WALL = 2, CFD_BC_SYMMETRY = 3 };
+
+/* Borrowed view of a mesh in the reference's layout.  Arrays are indexed by reference cell id. */
+typedef struct {
+  int n_physical;                 /* No_Physical_Cells */
+  int n_ghost;                    /* No_Ghost_Cells */
+  const int *n_faces;             /* [NP] Cell::numFaces (3 or 4) */
+  const int *neighbours;          /* [NP*4] Cell::Neighbours, -1 padded */
+  const double *face_normals;     /* [NP*8] Cell::Face_Normals (nx, ny per face) */
+  const double *face_lengths;     /* [NP*4] Cell::Face_Areas */
+  const double *center_distances; /* [NP*4] Cell::Cell_Center_Distances */
+  const double *area;             /* [NP] Cell::Area */
+  const double *inv_area;         /* [NP] Cell::Inv_Area */
+  int n_boundary;                 /* number of boundary entries (== n_ghost) */
+  const int *boundary;            /* [n_boundary*4] kind, cell, face, ghost */
+} cfd_mesh_desc;
+
+cfd_status cfd_mesh_box(int nx, int ny, double x0, double x1, double y0, double y1, cfd_mesh **out);
+cfd_status cfd_mesh_half_cylinder(int ntheta, int nr, double r_body, double r_outer, double ratio, cfd_mesh **out);
+cfd_status cfd_mesh_ramp(int nx, int ny, double length, double height, double x_corner, double angle_deg,
+                         cfd_mesh **out);
+cfd_status cfd_mesh_bump(int nx, int ny, double length, double height, double thickness, int n_quad_layers,
+                         double jitter, uint64_t seed, int triangles, cfd_mesh **out);
+cfd_status cfd_mesh_read_vtk(const char *path, cfd_mesh **out);
+cfd_status cfd_mesh_write_vtk(const cfd_mesh *m, const char *path);
+cfd_status cfd_mesh_describe(const cfd_mesh *m, cfd_mesh_desc *out);
+/* Cell centres of physical and ghost cells, [(NP+NG)*3] (Cell::Cell_Center). */
+cfd_status cfd_mesh_centers(const cfd_mesh *m, double *out);
+/* Points and cell node lists as given ([npts*3], [ncells*4] -1 padded). */
+cfd_status cfd_mesh_points(const cfd_mesh *m, int *n_points, const double **points);
+void cfd_mesh_destroy(cfd_mesh *m);
+
+/* ------------------------------------------------------------------------------------------
+ * Solver configuration: the reference's Solver_Config keys (json_Files/Solver_Config.json:1-38,
+ * read at src/Configuration_Read.cpp:23-87) plus additive keys.
+ * ------------------------------------------------------------------------------------------ */
+enum { CFD_DISS_LLF = 1, CFD_DISS_ROE = 3, CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7 };
+enum { CFD_LIM_REF_MINMOD = 0, CFD_LIM_MINMOD = 1, CFD_LIM_VANLEER = 2, CFD_LIM_SUPERBEE = 3, CFD_LIM_VANALBADA = 4 };
+enum { CFD_INT_REFERENCE = 0, CFD_INT_RK4 = 1, CFD_INT_SSPRK3 = 2 };
+enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2 };
+enum { CFD_EXIT_SUPERSONIC = 0, CFD_EXIT_SUBSONIC_REF = 1, CFD_EXIT_STATIC_P = 2 };
+enum { CFD_PREC_FP64 = 0, CFD_PREC_FP32_FLUX = 1 };
+
+typedef struct {
+  int dissipation_type;      /* Dissipation_Type: 1 LLF, 3 ROE; additive 6 AUSM, 7 HLLC */
+  int is_second_order;       /* Is_Second_Order */
+  int time_accurate;         /* Time_Accurate: 1 -> Runge_Kutta_Method, 0 -> Explicit_Method */
+  int local_time_stepping;   /* Local_Time_Stepping */
+  int integrator;            /* CFD_INT_*: reference forms, classical RK4, standard SSP-RK3 */
+  int limiter;               /* CFD_LIM_*: 0 = reference 2-argument MinMod (src/Limiters.cpp:58-63) */
+  int reconstruct_primitive; /* MUSCL on (rho,u,v,p) instead of conserved variables */
+  int inlet_bc;              /* CFD_INLET_* (reference: Is_Inlet_SubSonic) */
+  int exit_bc;               /* CFD_EXIT_*  (reference: Is_Exit_SubSonic) */
+  int precision;             /* CFD_PREC_* */
+  int reorder;               /* 1: reverse Cuthill-McKee renumbering on the device */
+  double cfl;                /* CFL */
+  double limiter_zeta;       /* Limiter_Zeta */
+  double limiter_zeta1;      /* Limiter_Zeta1 */
+  double inlet_rho, inlet_p, inlet_u, inlet_v; /* inletCond (Rho, P, u, v) */
+  double inlet_p0, inlet_t0;                   /* total pressure / temperature (CFD_INLET_TOTAL_PT) */
+  double exit_p;                               /* static exit pressure (CFD_EXIT_STATIC_P) */
+  double r_gas;                                /* gas constant for total-temperature inflow */
+  int device;                /* CUDA device ordinal */
+  void *stream;              /* cudaStream_t to launch on (NULL: the context creates its own) */
+} cfd_config;
+
+/* Defaults of json_Files/Solver_Config.json with Dissipation_Type = ROE. */
+void cfd_config_default(cfd_config *cfg);
+/* Parses a Solver_Config JSON file (the reference schema; // comments allowed) into cfg.
+ * Unknown keys are ignored; additive keys: Limiter_Type, Flux_Scheme, Integrator, Precision,
+ * Inlet_BC, Exit_BC, Reorder. */
+cfd_status cfd_config_read_json(const char *path, cfd_config *cfg);
+
+/* ------------------------------------------------------------------------------------------
+ * Solver context
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cfd_ctx cfd_ctx;
+
+typedef struct {
+  int iterations;      /* iterations (src/Solver.cpp:116) */
+  double min_dt;       /* Min_dt after the last step */
+  double total_time;   /* Total_Time */
+  double error[4];     /* Error[0..3] of Estimate_Error (src/Error_Estimate_Update.cpp:10-28) */
+  double res_l2[4];    /* plain ||R_k||_2 over physical cells of the last stage */
+  int bad_cell;        /* first cell (reference id) with a NaN sound speed, or -1 */
+  int status;          /* cfd_status of the step */
+} cfd_step_info;
+
+cfd_status cfd_create(const cfd_mesh_desc *mesh, const cfd_config *cfg, cfd_ctx **out);
+void cfd_destroy(cfd_ctx *ctx);
+
+/* Uploads conserved variables U [n*4] (rows in reference cell order; n = NP or NP+NG) and
+ * recomputes primitives on the device, as Initialize_TestCase does (src/Initialize_TestCase.cpp:36-58).
+ * With n = NP, ghost rows are initialised from their owner cell. */
+cfd_status cfd_upload_state(cfd_ctx *ctx, const double *U, int n);
+
+/* Whole pseudo-steps: n_steps repetitions of the loop body of Inviscid_Solver
+ * (src/Solver.cpp:94-125): Apply_Boundary_Conditions -> Runge_Kutta_Method | Explicit_Method ->
+ * Total_Time += Min_dt -> Estimate_Error -> Update.  Stops early when t_end > 0 and
+ * Total_Time >= t_end.  info may be NULL. */
+cfd_status cfd_step(cfd_ctx *ctx, int n_steps, double t_end, cfd_step_info *info);
+
+/* Enqueue n pseudo-steps on the context's stream without waiting; cfd_sync waits and
+ * collects the status (used to time the device path without host round trips). */
+cfd_status cfd_step_async(cfd_ctx *ctx, int n_steps);
+cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
+/* Runtime options: "keep_delu" (write Cells_DelU in fused steps, default 1),
+ * "use_graph" (replay pseudo-steps from a captured CUDA graph, default 1),
+ * "profile" (time every launch with CUDA events; disables graph replay, default 0). */
+cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
+
+/* Entry points of the reference path, one call each, same semantics and post-conditions. */
+cfd_status cfd_apply_boundary_conditions(cfd_ctx *ctx); /* Apply_Boundary_Conditions, src/Boundary_Conditions.cpp:12 */
+cfd_status cfd_evaluate_net_flux(cfd_ctx *ctx);         /* Evaluate_Cell_Net_Flux_1O/2O, src/Net_Flux.cpp:46,97 */
+cfd_status cfd_explicit_method(cfd_ctx *ctx);           /* Explicit_Method, src/Numerical_Method.cpp:26 */
+cfd_status cfd_runge_kutta_method(cfd_ctx *ctx);        /* Runge_Kutta_Method, src/Numerical_Method.cpp:342 */
+cfd_status cfd_estimate_error(cfd_ctx *ctx, double error[4]); /* Estimate_Error, src/Error_Estimate_Update.cpp:10 */
+cfd_status cfd_update(cfd_ctx *ctx);                    /* Update(), src/Error_Estimate_Update.cpp:31 */
+cfd_status cfd_get_min_dt(cfd_ctx *ctx, double *min_dt); /* get_Min_dt, src/Numerical_Method.cpp:322 */
+
+/* Downloads (reference cell order).  Any pointer may be NULL.
+ *   U      [(NP+NG)*4] U_Cells
+ *   prim   [(NP+NG)*11] Primitive_Cells (all 11 slots, src/Basic_Functions.cpp:162-219)
+ *   dt     [NP] Cell::del_t of the last flux evaluation
+ *   net    [NP*4] Cells_Net_Flux of the last flux evaluation
+ *   delu   [NP*4] Cells_DelU */
+cfd_status cfd_download(cfd_ctx *ctx, double *U, double *prim, double *dt, double *net, double *delu);
+/* Conserved rows U_Cells [(NP+NG)*4] only (gathered into reference order on the device; a
+ * pinned destination gives full PCIe/C2C bandwidth). */
+cfd_status cfd_download_U(cfd_ctx *ctx, double *U);
+/* Stage state [NP*4]: after Runge_Kutta_Method it holds U_Cells_RK_2 (the stage buffer is
+ * shared by U_Cells_RK_1 and U_Cells_RK_2, src/Numerical_Method.cpp:372-416). */
+cfd_status cfd_download_stage_state(cfd_ctx *ctx, double *S);
+
+/* Green-Gauss gradient of primitive slot var (0 rho, 1 u, 2 v, 4 p) at cell centres, [NP*2]
+ * (Calculate_Gradient_At_Cell_Center, src/Grid_Refine_Functions.cpp:221-246). */
+cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad);
+/* AMR indicator [NP] and tags [NP] (Compute_Gradient_Refinement_Indicator / TagRefinableCells,
+ * src/Grid_Refine_Functions.cpp:8-63).  Either output may be NULL. */
+cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags);
+
+/* Accumulated device time of one kernel family ("flux", "stage", "bc") over the launches made
+ * while option "profile" was set (CUDA events on the context's stream around each launch). */
+cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches);
+/* Number of CUDA kernel launches this context has issued so far. */
+long long cfd_kernel_launches(const cfd_ctx *ctx);
+/* Device bytes held by the context. */
+size_t cfd_device_bytes(const cfd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFD_B200_H */

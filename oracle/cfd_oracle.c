@@ -1,0 +1,621 @@
+/* Test infrastructure only: plain-C restatement of the reference's explicit FV residual/update
+ * path (rameshkolluru43/CFD_Solver_withCUDA).  It is the checker for the CUDA library and is
+ * never linked into it.  Each function names the reference file:line it restates; the
+ * arithmetic keeps the reference's association order, and this file is compiled without FMA
+ * contraction, so results are bit-identical to the reference built the same way. */
+#include "cfd_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define GM1 (1.4 - 1.0)          /* gamma_M_1, include/definitions.h:64 */
+#define G1 (1.4 / (1.4 - 1.0))   /* gamma1 as it expands in a product, include/definitions.h:65 */
+#define RGC 287.0                /* R_GC, include/definitions.h:66 */
+
+struct orc_state {
+  int NP, NG, NT, NB;
+  const int *nf, *nbr, *bnd;
+  const double *nrm, *len, *ccd, *area, *inva;
+  orc_config c;
+  double *U, *P, *R, *dt, *dU, *S1, *S2, *Racc, *dtk, *Urd;
+  double err[4], min_dt, dt_step, total_time;
+  int iterations, bad_cell;
+  int stage;   /* 0: flux of U^n, >0: a later stage of the current step */
+};
+
+/* Calculate_Primitive_Variables, src/Basic_Functions.cpp:162-219 (inviscid: mu = K = 0). */
+static void eos(orc_state *s, int cell, const double *Uv, double *G) {
+  double Rho = Uv[0];
+  double inv = 1.0 / Rho;
+  double v1 = Uv[1] * inv, v2 = Uv[2] * inv;
+  if (fabs(v1) <= 1e-10) v1 = 0.0;
+  if (fabs(v2) <= 1e-10) v2 = 0.0;
+  double vmag = (v1 * v1 + v2 * v2);
+  double Pr = GM1 * (Uv[3] - 0.5 * Rho * vmag);
+  double T = (Pr * inv / RGC);
+  double C = sqrt(1.4 * Pr * inv);
+  double M = sqrt(vmag) / C;
+  G[0] = Rho;
+  G[1] = v1;
+  G[2] = v2;
+  G[3] = T;
+  G[4] = Pr;
+  G[5] = C;
+  G[6] = Uv[3];
+  G[7] = M;
+  G[8] = 0.0;
+  G[9] = 0.0;
+  G[10] = Pr * pow((1.0 + 0.5 * GM1 * M * M), G1);
+  if (isnan(C) && (s->bad_cell < 0 || cell < s->bad_cell)) s->bad_cell = cell;
+}
+
+orc_state *orc_create(int NP, int NG, const int *nf, const int *nbr, const double *normals, const double *lengths,
+                      const double *ccd, const double *area, const double *inv_area, int NB, const int *bnd,
+                      const orc_config *cfg) {
+  orc_state *s = (orc_state *)calloc(1, sizeof(orc_state));
+  s->NP = NP;
+  s->NG = NG;
+  s->NT = NP + NG;
+  s->NB = NB;
+  s->nf = nf;
+  s->nbr = nbr;
+  s->nrm = normals;
+  s->len = lengths;
+  s->ccd = ccd;
+  s->area = area;
+  s->inva = inv_area;
+  s->bnd = bnd;
+  s->c = *cfg;
+  size_t NT = (size_t)s->NT;
+  s->U = (double *)calloc(4 * NT, sizeof(double));
+  s->Urd = (double *)calloc(4 * NT, sizeof(double));
+  s->P = (double *)calloc(11 * NT, sizeof(double));
+  s->R = (double *)calloc(4 * (size_t)NP, sizeof(double));
+  s->dt = (double *)calloc(NT, sizeof(double));
+  s->dU = (double *)calloc(4 * (size_t)NP, sizeof(double));
+  s->S1 = (double *)calloc(4 * (size_t)NP, sizeof(double));
+  s->S2 = (double *)calloc(4 * (size_t)NP, sizeof(double));
+  s->Racc = (double *)calloc(4 * (size_t)NP, sizeof(double));
+  s->dtk = (double *)calloc((size_t)NP, sizeof(double));
+  for (size_t g = (size_t)NP; g < NT; g++) s->dt[g] = 1e300; /* ghost del_t never written (harness fix) */
+  s->bad_cell = -1;
+  return s;
+}
+
+void orc_destroy(orc_state *s) {
+  if (!s) return;
+  free(s->U);
+  free(s->Urd);
+  free(s->P);
+  free(s->R);
+  free(s->dt);
+  free(s->dU);
+  free(s->S1);
+  free(s->S2);
+  free(s->Racc);
+  free(s->dtk);
+  free(s);
+}
+
+/* Initialize_TestCase, src/Initialize_TestCase.cpp:36-58: U given, primitives from the EOS.
+ * With n == NP the ghost rows copy their owner cell. */
+void orc_set_state(orc_state *s, const double *U, int n) {
+  for (int c = 0; c < n; c++) memcpy(s->U + 4 * (size_t)c, U + 4 * (size_t)c, 4 * sizeof(double));
+  if (n == s->NP)
+    for (int e = 0; e < s->NB; e++) memcpy(s->U + 4 * (size_t)s->bnd[4 * e + 3], U + 4 * (size_t)s->bnd[4 * e + 1], 4 * sizeof(double));
+  for (int c = 0; c < s->NT; c++) eos(s, c, s->U + 4 * (size_t)c, s->P + 11 * (size_t)c);
+  s->stage = 0;
+}
+
+/* The conserved state the limiter, LLF and the exit BC read: U_Cells (U^n on physical rows,
+ * boundary values on ghost rows) for the reference integrator; the current stage state for the
+ * stage-consistent integrators. */
+static const double *uread(orc_state *s) {
+  if (s->c.integrator == 0 || s->stage == 0) return s->U;
+  memcpy(s->Urd, s->U, 4 * (size_t)s->NT * sizeof(double));
+  const double *src = (s->c.integrator == 1) ? s->S1 : (s->stage == 1 ? s->S1 : s->S2);
+  memcpy(s->Urd, src, 4 * (size_t)s->NP * sizeof(double));
+  return s->Urd;
+}
+
+/* Apply_Boundary_Conditions, src/Boundary_Conditions.cpp:12-61 and the per-kind functions:
+ * wall/symmetry src/Wall_Boundary_Conditions.cpp:8-53,79-124; supersonic inlet
+ * src/Inlet_Boundary_Conditions.cpp:41-74; subsonic inlet :7-39; supersonic exit
+ * src/Exit_Boundary_Conditions.cpp:68-94; subsonic exit :83-85 (empty).  Additive: total-(p,T)
+ * inflow and static-pressure outflow. */
+void orc_apply_bc(orc_state *s) {
+  const double *Ur = uread(s);
+  for (int e = 0; e < s->NB; e++) {
+    const int kind = s->bnd[4 * e], c = s->bnd[4 * e + 1], f = s->bnd[4 * e + 2], g = s->bnd[4 * e + 3];
+    const double *Pc = s->P + 11 * (size_t)c;
+    double G[4];
+    if (kind == 2 || kind == 3) {
+      double v1 = Pc[1], v2 = Pc[2];
+      double n1 = s->nrm[8 * c + 2 * f], n2 = s->nrm[8 * c + 2 * f + 1];
+      double vdotn = (v1 * n1 + v2 * n2);
+      double v1g = v1 - 2.0 * vdotn * n1;
+      double v2g = v2 - 2.0 * vdotn * n2;
+      double vmag = 0.5 * (v1g * v1g + v2g * v2g);
+      G[0] = Pc[0];
+      G[1] = Pc[0] * v1g;
+      G[2] = Pc[0] * v2g;
+      G[3] = ((Pc[4] / GM1) + Pc[0] * vmag);
+    } else if (kind == 0) {
+      double u = Pc[1], v = Pc[2];
+      if (s->c.inlet_bc == 0) {
+        double vmag = (u * u + v * v) * 0.5;
+        G[0] = s->c.inlet_rho;
+        G[1] = s->c.inlet_rho * u;
+        G[2] = s->c.inlet_rho * v;
+        G[3] = (s->c.inlet_p / GM1) + s->c.inlet_rho * vmag;
+      } else if (s->c.inlet_bc == 1) {
+        double Vm = 0.5 * (u * u + v * v);
+        G[0] = s->c.inlet_rho;
+        G[1] = s->c.inlet_rho * u;
+        G[2] = s->c.inlet_rho * v;
+        G[3] = (s->c.inlet_p / GM1) + s->c.inlet_rho * Vm * Vm;
+      } else {
+        /* Characteristic total-(p, T) inflow (no reference counterpart): R+ = Vn + 2a/(g-1)
+         * from the interior, H0 = a0^2/(g-1) fixed, flow along the inward normal. */
+        double n1 = s->nrm[8 * c + 2 * f], n2 = s->nrm[8 * c + 2 * f + 1];
+        double Rp = (u * n1 + v * n2) + 2.0 * Pc[5] / GM1;
+        double a0sq = 1.4 * s->c.r_gas * s->c.inlet_t0;
+        double qa = (1.4 + 1.0) / GM1, qb = -2.0 * Rp, qc = 0.5 * GM1 * Rp * Rp - a0sq;
+        double disc = qb * qb - 4.0 * qa * qc;
+        double ab = (-qb + sqrt(disc > 0.0 ? disc : 0.0)) / (2.0 * qa);
+        double vn = Rp - 2.0 * ab / GM1;
+        if (vn > 0.0) vn = 0.0;
+        double Tb = ab * ab / (1.4 * s->c.r_gas);
+        double pb = s->c.inlet_p0 * pow(Tb / s->c.inlet_t0, 1.4 / GM1);
+        double rb = pb / (s->c.r_gas * Tb);
+        double ub = vn * n1, vb = vn * n2;
+        G[0] = rb;
+        G[1] = rb * ub;
+        G[2] = rb * vb;
+        G[3] = pb / GM1 + 0.5 * rb * (ub * ub + vb * vb);
+      }
+    } else {
+      if (s->c.exit_bc == 1) continue;
+      if (s->c.exit_bc == 0) {
+        for (int k = 0; k < 4; k++) G[k] = Ur[4 * (size_t)c + k];
+      } else {
+        double n1 = s->nrm[8 * c + 2 * f], n2 = s->nrm[8 * c + 2 * f + 1];
+        double vn = Pc[1] * n1 + Pc[2] * n2;
+        double pb = (vn < Pc[5]) ? s->c.exit_p : Pc[4];
+        G[0] = Pc[0];
+        G[1] = Pc[0] * Pc[1];
+        G[2] = Pc[0] * Pc[2];
+        G[3] = pb / GM1 + 0.5 * Pc[0] * (Pc[1] * Pc[1] + Pc[2] * Pc[2]);
+      }
+    }
+    memcpy(s->U + 4 * (size_t)g, G, sizeof(G));
+    eos(s, g, G, s->P + 11 * (size_t)g);
+  }
+}
+
+/* Calculate_Face_Average_Flux, src/Average_Interface_Flux.cpp:20-82. */
+static void avg_flux(const double *PL, const double *PR, double nx, double ny, double dl, double *F) {
+  double Rho_L = PL[0], u_L = PL[1], v_L = PL[2], P_L = PL[4];
+  double Rho_R = PR[0], u_R = PR[1], v_R = PR[2], P_R = PR[4];
+  double Vdotn_L = (u_L * nx + v_L * ny), Vdotn_R = (u_R * nx + v_R * ny);
+  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L), Vmag_R = 0.5 * (u_R * u_R + v_R * v_R);
+  double a = Vdotn_L * dl, b = Vdotn_R * dl;
+  double FL[4] = {Rho_L * a, Rho_L * u_L * a + P_L * nx * dl, Rho_L * v_L * a + P_L * ny * dl, (G1 * P_L + Rho_L * Vmag_L) * a};
+  double FR[4] = {Rho_R * b, Rho_R * u_R * b + P_R * nx * dl, Rho_R * v_R * b + P_R * ny * dl, (G1 * P_R + Rho_R * Vmag_R) * b};
+  for (int i = 0; i < 4; i++) F[i] = 0.5 * (FL[i] + FR[i]);
+}
+
+/* Eigen-decomposition tail of ROE / ROE_2O, src/Roe_Scheme.cpp:164-228 and :376-423. */
+static void roe_tail(double Roe_u, double Roe_v, double Roe_H, double Roe_Vmag, double Roe_a, double Roe_Rho,
+                     double Un, double Ut, double dP, double dRho, double dUn, double dUt, double nx, double ny,
+                     double dl, double *D) {
+  double R1[4] = {1.0, Roe_u - nx * Roe_a, Roe_v - ny * Roe_a, Roe_H - Roe_a * Un};
+  double R2[4] = {1.0, Roe_u, Roe_v, Roe_Vmag};
+  double R3[4] = {0.0, -ny, nx, Ut};
+  double R4[4] = {1.0, Roe_u + nx * Roe_a, Roe_v + ny * Roe_a, Roe_H + Roe_a * Un};
+  double Term2 = 1.0 / (Roe_a * Roe_a);
+  double a1 = 0.5 * Term2 * (dP - Roe_Rho * Roe_a * dUn);
+  double a2 = dRho - Term2 * dP;
+  double a3 = Roe_Rho * dUt;
+  double a4 = 0.5 * Term2 * (dP + Roe_Rho * Roe_a * dUn);
+  double L1 = fabs(Un - Roe_a), L2 = fabs(Un), L3 = fabs(Un), L4 = fabs(Un + Roe_a);
+  double ef = 0.1 * Roe_a;
+  if (L1 < ef) L1 = 0.5 * (L1 * L1 / ef + ef);
+  if (L4 < ef) L4 = 0.5 * (L4 * L4 / ef + ef);
+  for (int k = 0; k < 4; k++) D[k] = 0.5 * (L1 * a1 * R1[k] + L2 * a2 * R2[k] + L3 * a3 * R3[k] + L4 * a4 * R4[k]) * dl;
+}
+
+/* ROE, src/Roe_Scheme.cpp:6-256. */
+static void roe_1o(orc_state *s, int c, int N, int f, double *D) {
+  D[0] = D[1] = D[2] = D[3] = 0.0;
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  if (sqrt(nx * nx + ny * ny) < 1e-12) return;
+  if (N < 0 || N >= s->NP) N = c;
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double Rho_L = L[0], u_L = L[1], v_L = L[2], P_L = L[4], C_L = L[5];
+  if (Rho_L <= 0.0 || P_L <= 0.0 || C_L <= 0.0) return;
+  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L);
+  double H_L = ((C_L * C_L) / (1.4 - 1.0)) + Vmag_L;
+  double Rho_R = R[0], u_R = R[1], v_R = R[2], P_R = R[4], C_R = R[5];
+  if (Rho_R <= 0.0 || P_R <= 0.0 || C_R <= 0.0) return;
+  double Vmag_R = 0.5 * (u_R * u_R + v_R * v_R);
+  double H_R = ((C_R * C_R) / (1.4 - 1.0)) + Vmag_R;
+  double sL = sqrt(Rho_L), sR = sqrt(Rho_R);
+  double Term1 = 1.0 / (sL + sR);
+  double Roe_Rho = sqrt(Rho_L * Rho_R);
+  double Roe_u = Term1 * (u_R * sR + u_L * sL);
+  double Roe_v = Term1 * (v_R * sR + v_L * sL);
+  double Roe_H = Term1 * (H_R * sR + H_L * sL);
+  double Roe_Vmag = 0.5 * (Roe_u * Roe_u + Roe_v * Roe_v);
+  double Roe_a = sqrt((1.4 - 1.0) * (Roe_H - Roe_Vmag));
+  if (Roe_a <= 0.0) {
+    Roe_a = 0.5 * (C_L + C_R);
+    if (Roe_a <= 0.0) return;
+  }
+  double Un = nx * Roe_u + ny * Roe_v, Ut = -ny * Roe_u + nx * Roe_v;
+  double du = (u_R - u_L), dv = (v_R - v_L), dP = (P_R - P_L), dRho = (Rho_R - Rho_L);
+  double dUn = nx * du + ny * dv, dUt = -ny * du + nx * dv;
+  roe_tail(Roe_u, Roe_v, Roe_H, Roe_Vmag, Roe_a, Roe_Rho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
+}
+
+static int sgn(double a) { return (a > 0.0) - (a < 0.0); }
+
+/* phi(a, b), r = a/b: the reference GPU limiter family, CUDA_KERNELS/Limiter_Cuda_Kernels.cu:89-154. */
+static double phi_ab(int kind, double a, double b) {
+  if (fabs(b) < 1e-12) return 0.0;
+  double r = a / b;
+  if (r <= 0.0) return 0.0;
+  switch (kind) {
+    case 1: return fmin(r, 1.0);
+    case 2: return 2.0 * r / (1.0 + r);
+    case 3: return fmax(fmin(2.0 * r, 1.0), fmin(r, 2.0));
+    case 4: {
+      double r_sq = r * r;
+      return (r_sq + r) / (r_sq + 1.0);
+    }
+    default: return 0.0;
+  }
+}
+
+/* Slope limiting of Second_Order_Limiter, src/Limiters.cpp:58-63,109-134 (kind 0: the
+ * reference 2-argument MinMod; kinds 1-4: phi(S2, S1) * S1). */
+static double slope(int kind, double qc, double q1, double q2, double d1, double d2, double z, double z1) {
+  double S1 = z * (qc - q1) / d1;
+  double S2 = z1 * (q1 - q2) / d2;
+  if (kind == 0) {
+    double a1 = fabs(S1), b1 = fabs(S2);
+    return 0.5 * (sgn(S1) + sgn(S2)) * ((b1 < a1) ? b1 : a1);
+  }
+  return phi_ab(kind, S2, S1) * S1;
+}
+
+/* Directional stencil of Second_Order_Limiter, src/Limiters.cpp:136-191. */
+static void stencil(const orc_state *s, int c, int f, int *N1, int *N2, double *d1, double *d2) {
+  const int NP = s->NP;
+  if (s->nf[c] != 4) {
+    *N1 = s->nbr[4 * c + f];
+    *d1 = s->ccd[4 * c + f];
+    if (*d1 <= 0.0) *d1 = 1.0;
+    *N2 = *N1;
+    *d2 = *d1;
+    return;
+  }
+  *N1 = s->nbr[4 * c + f];
+  *d1 = s->ccd[4 * c + f];
+  if (f < 2) {
+    *N2 = (*N1 >= NP) ? *N1 : s->nbr[4 * *N1 + f];
+    *d2 = (*N1 >= NP) ? *d1 : s->ccd[4 * *N1 + f];
+  } else {
+    *N2 = s->nbr[4 * c + f - 2];
+    *d2 = s->ccd[4 * c + f - 2];
+  }
+}
+
+/* Second_Order_Limiter (src/Limiters.cpp:97-200) on conserved variables, or the same stencil on
+ * (rho, u, v, p) of the stage primitives (additive), giving the conserved jump d_U. */
+static void limited_jump(orc_state *s, const double *Ur, int c, int f, double *dU) {
+  int N1, N2;
+  double d1, d2;
+  stencil(s, c, f, &N1, &N2, &d1, &d2);
+  if (!s->c.reconstruct_primitive) {
+    for (int k = 0; k < 4; k++) {
+      double q1 = Ur[4 * (size_t)N1 + k], q2 = Ur[4 * (size_t)N2 + k], qc = Ur[4 * (size_t)c + k];
+      double phi = slope(s->c.limiter, qc, q1, q2, d1, d2, s->c.zeta, s->c.zeta1);
+      double VR = q1 + 0.5 * phi * d1;
+      double VL = qc - 0.5 * phi * d1;
+      dU[k] = VR - VL;
+    }
+  } else {
+    static const int slot[4] = {0, 1, 2, 4};
+    double qR[4], qL[4];
+    for (int k = 0; k < 4; k++) {
+      double qc = s->P[11 * (size_t)c + slot[k]], q1 = s->P[11 * (size_t)N1 + slot[k]], q2 = s->P[11 * (size_t)N2 + slot[k]];
+      double phi = slope(s->c.limiter, qc, q1, q2, d1, d2, s->c.zeta, s->c.zeta1);
+      qR[k] = q1 + 0.5 * phi * d1;
+      qL[k] = qc - 0.5 * phi * d1;
+    }
+    dU[0] = qR[0] - qL[0];
+    dU[1] = qR[0] * qR[1] - qL[0] * qL[1];
+    dU[2] = qR[0] * qR[2] - qL[0] * qL[2];
+    dU[3] = (qR[3] / GM1 + 0.5 * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])) -
+            (qL[3] / GM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
+  }
+}
+
+/* ROE_2O, src/Roe_Scheme.cpp:257-447. */
+static void roe_2o(orc_state *s, const double *Ur, int c, int N, int f, double *D) {
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double Rho_L = L[0], u_L = L[1], v_L = L[2], C_L = L[5];
+  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L), H_L = ((C_L * C_L) / (1.4 - 1.0)) + Vmag_L;
+  double Rho_R = R[0], u_R = R[1], v_R = R[2], C_R = R[5];
+  double Vmag_R = 0.5 * (u_R * u_R + v_R * v_R), H_R = ((C_R * C_R) / (1.4 - 1.0)) + Vmag_R;
+  double sR = sqrt(Rho_R), sL = sqrt(Rho_L);
+  double Term1 = 1.0 / (sL + sR);
+  double Roe_Rho = sqrt(Rho_L * Rho_R);
+  double Roe_u = Term1 * (u_R * sR + u_L * sL);
+  double Roe_v = Term1 * (v_R * sR + v_L * sL);
+  double Roe_H = Term1 * (H_R * sR + H_L * sL);
+  double Roe_Vmag = 0.5 * (Roe_u * Roe_u + Roe_v * Roe_v);
+  double Un = nx * Roe_u + ny * Roe_v, Ut = -ny * Roe_u + nx * Roe_v;
+  double Roe_a = sqrt((1.4 - 1.0) * (Roe_H - Roe_Vmag));
+  double d_U[4];
+  limited_jump(s, Ur, c, f, d_U);
+  double du = d_U[1] / Roe_Rho - d_U[0] * Roe_u / (Roe_Rho * Roe_Rho);
+  double dv = d_U[2] / Roe_Rho - d_U[0] * Roe_v / (Roe_Rho * Roe_Rho);
+  double dE = d_U[3] - 0.5 * Roe_Rho * (2.0 * (Roe_u * du + Roe_v * dv) + du * du + dv * dv) - 0.5 * d_U[0] * Roe_Vmag;
+  double dP = (1.4 - 1.0) * dE, dRho = d_U[0];
+  double dUn = nx * du + ny * dv, dUt = -ny * du + nx * dv;
+  roe_tail(Roe_u, Roe_v, Roe_H, Roe_Vmag, Roe_a, Roe_Rho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
+}
+
+static double max3(double a, double b, double c) {
+  if ((a >= b) && (a >= c)) return a;
+  if ((b >= a) && (b >= c)) return b;
+  return c;
+}
+
+/* LLF, src/LLF.cpp:8-83. */
+static void llf_1o(orc_state *s, const double *Ur, int c, int N, int f, double *D) {
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  double Vdotn_L = (L[1] * nx + L[2] * ny), Vdotn_R = (R[1] * nx + R[2] * ny);
+  double S[6] = {fabs(Vdotn_L - L[5]) * dl, fabs(Vdotn_L + L[5]) * dl, fabs(Vdotn_L) * dl,
+                 fabs(Vdotn_R - R[5]) * dl, fabs(Vdotn_R + R[5]) * dl, fabs(Vdotn_R) * dl};
+  double M1 = max3(S[0], S[1], S[2]), M2 = max3(S[3], S[4], S[5]);
+  double mev = (M1 >= M2) ? M1 : M2;
+  for (int k = 0; k < 4; k++) D[k] = 0.5 * mev * (Ur[4 * (size_t)N + k] - Ur[4 * (size_t)c + k]);
+}
+
+/* Evaluate_Cell_Net_Flux_1O/2O + Calculate_Flux_For_All_Faces, src/Net_Flux.cpp:7-129;
+ * Inviscid_Time_Step, src/Time_Step.cpp:293-329. */
+void orc_net_flux(orc_state *s) {
+  const double *Ur = uread(s);
+  for (int c = 0; c < s->NP; c++) {
+    double net[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int f = 0; f < s->nf[c]; f++) {
+      int N = s->nbr[4 * c + f];
+      if (N < 0) continue;
+      double A[4], D[4];
+      avg_flux(s->P + 11 * (size_t)c, s->P + 11 * (size_t)N, s->nrm[8 * c + 2 * f], s->nrm[8 * c + 2 * f + 1],
+               s->len[4 * c + f], A);
+      if (s->c.dissipation_type == 3 && !s->c.is_second_order) roe_1o(s, c, N, f, D);
+      else if (s->c.dissipation_type == 3) roe_2o(s, Ur, c, N, f, D);
+      else llf_1o(s, Ur, c, N, f, D);
+      for (int v = 0; v < 4; v++) net[v] += A[v] - D[v];
+    }
+    memcpy(s->R + 4 * (size_t)c, net, sizeof(net));
+    const double u0 = s->P[11 * (size_t)c + 1], v0 = s->P[11 * (size_t)c + 2], a0 = s->P[11 * (size_t)c + 5];
+    double denom = 0.0;
+    for (int f = 0; f < s->nf[c]; f++) {
+      double vn = u0 * s->nrm[8 * c + 2 * f] + v0 * s->nrm[8 * c + 2 * f + 1];
+      denom += (fabs(vn) + a0) * s->len[4 * c + f];
+    }
+    s->dt[c] = (denom <= 0.0 || !isfinite(denom)) ? 0.0 : s->c.cfl * s->area[c] / denom;
+  }
+  /* get_Min_dt, src/Numerical_Method.cpp:322-330 (ghost del_t = 1e300). */
+  double m = s->dt[0];
+  for (int c = 1; c < s->NT; c++)
+    if (s->dt[c] < m) m = s->dt[c];
+  s->min_dt = m;
+}
+
+/* Explicit_Method, src/Numerical_Method.cpp:26-103.  Returns -1 when Min_dt <= 0. */
+int orc_explicit(orc_state *s) {
+  s->stage = 0;
+  orc_net_flux(s);
+  if (!(s->min_dt > 0.0)) return -1;
+  for (int c = 0; c < s->NP; c++)
+    for (int k = 0; k < 4; k++) s->dU[4 * c + k] = -s->min_dt * s->inva[c] * s->R[4 * c + k];
+  return 0;
+}
+
+static void refresh_prims(orc_state *s, const double *src) {
+  for (int c = 0; c < s->NP; c++) eos(s, c, src + 4 * (size_t)c, s->P + 11 * (size_t)c);
+}
+
+/* Runge_Kutta_Method, src/Numerical_Method.cpp:342-457 (integrator 0); stage-consistent SSP-RK3
+ * with dt frozen per step (integrator 2); classical RK4 (integrator 1). */
+void orc_rk(orc_state *s) {
+  const int NP = s->NP, integ = s->c.integrator, lts = s->c.local_time_stepping;
+  if (integ == 1) {
+    const double w[3] = {0.5, 0.5, 1.0};
+    for (int st = 0; st < 4; st++) {
+      s->stage = st;
+      if (st > 0) orc_apply_bc(s);
+      orc_net_flux(s);
+      if (st == 0) {
+        s->dt_step = s->min_dt;
+        memcpy(s->dtk, s->dt, (size_t)NP * sizeof(double));
+      }
+      for (int c = 0; c < NP; c++) {
+        double dt = lts ? s->dtk[c] : s->dt_step, invA = s->inva[c];
+        for (int k = 0; k < 4; k++) {
+          size_t i = 4 * (size_t)c + k;
+          double Rk = s->R[i];
+          if (st == 0) {
+            s->Racc[i] = Rk;
+            s->S1[i] = s->U[i] - w[0] * (dt * invA) * Rk;
+          } else if (st < 3) {
+            s->Racc[i] = s->Racc[i] + 2.0 * Rk;
+            s->S1[i] = s->U[i] - w[st] * (dt * invA) * Rk;
+          } else {
+            double acc = s->Racc[i] + Rk;
+            s->dU[i] = -((dt * invA) * acc) / 6.0;
+          }
+        }
+      }
+      if (st < 3) refresh_prims(s, s->S1);
+    }
+    s->min_dt = s->dt_step;
+    s->stage = 0;
+    return;
+  }
+  const int ssp = integ == 2;
+  for (int st = 0; st < 3; st++) {
+    s->stage = st;
+    if (st > 0) orc_apply_bc(s);
+    orc_net_flux(s);
+    if (st == 0) {
+      s->dt_step = s->min_dt;
+      memcpy(s->dtk, s->dt, (size_t)NP * sizeof(double));
+    }
+    for (int c = 0; c < NP; c++) {
+      double dt;
+      if (ssp) dt = lts ? s->dtk[c] : s->dt_step;
+      else dt = (st == 0 && lts) ? s->dt[c] : s->min_dt;
+      double invA = s->inva[c];
+      for (int k = 0; k < 4; k++) {
+        size_t i = 4 * (size_t)c + k;
+        double RV = s->R[i] - 0.0; /* Cells_Net_Flux - Cells_Viscous_Flux (zero when inviscid) */
+        if (st == 0) s->S1[i] = s->U[i] - dt * invA * RV;
+        else if (st == 1) s->S2[i] = 0.25 * (s->S1[i] + 3.0 * s->U[i] - dt * invA * RV);
+        else s->dU[i] = (2.0 / 3.0) * (s->S2[i] - s->U[i] - dt * invA * RV);
+      }
+    }
+    if (st == 0) refresh_prims(s, s->S1);
+    else if (st == 1) refresh_prims(s, s->S2);
+  }
+  if (ssp) s->min_dt = s->dt_step;
+  s->stage = 0;
+}
+
+/* Estimate_Error, src/Error_Estimate_Update.cpp:10-28. */
+void orc_estimate_error(orc_state *s) {
+  double e[4] = {0, 0, 0, 0};
+  for (int c = 0; c < s->NP; c++)
+    for (int i = 0; i < 4; i++) {
+      double d = s->dU[4 * c + i], t;
+      if (d < 1e-9) t = fabs(d);
+      else t = (fabs(d) / s->U[4 * c + i]);
+      e[i] += t * t;
+    }
+  for (int i = 0; i < 4; i++) s->err[i] = sqrt(e[i]);
+}
+
+/* Update(), src/Error_Estimate_Update.cpp:31-43. */
+void orc_update(orc_state *s) {
+  for (int c = 0; c < s->NP; c++) {
+    for (int k = 0; k < 4; k++) s->U[4 * c + k] += s->dU[4 * c + k];
+    eos(s, c, s->U + 4 * (size_t)c, s->P + 11 * (size_t)c);
+  }
+}
+
+/* Loop body of Inviscid_Solver, src/Solver.cpp:94-125; stops at t_end (> 0) like the harness. */
+int orc_iterate(orc_state *s, int n, double t_end) {
+  int done = 0;
+  for (int it = 0; it < n; it++) {
+    s->stage = 0;
+    orc_apply_bc(s);
+    if (s->c.time_accurate || s->c.integrator != 0) orc_rk(s);
+    else if (orc_explicit(s) != 0) return -1 - done;
+    s->total_time += s->min_dt;
+    s->iterations++;
+    orc_estimate_error(s);
+    orc_update(s);
+    done++;
+    if (t_end > 0.0 && s->total_time >= t_end) break;
+  }
+  return done;
+}
+
+void orc_get(const orc_state *s, double *U, double *prim11, double *dt, double *net, double *delu) {
+  if (U) memcpy(U, s->U, 4 * (size_t)s->NT * sizeof(double));
+  if (prim11) memcpy(prim11, s->P, 11 * (size_t)s->NT * sizeof(double));
+  if (dt) memcpy(dt, s->dt, (size_t)s->NP * sizeof(double));
+  if (net) memcpy(net, s->R, 4 * (size_t)s->NP * sizeof(double));
+  if (delu) memcpy(delu, s->dU, 4 * (size_t)s->NP * sizeof(double));
+}
+
+void orc_get_stage(const orc_state *s, double *S) { memcpy(S, s->S2, 4 * (size_t)s->NP * sizeof(double)); }
+double orc_min_dt(const orc_state *s) { return s->min_dt; }
+double orc_total_time(const orc_state *s) { return s->total_time; }
+void orc_error(const orc_state *s, double *err) { memcpy(err, s->err, sizeof(s->err)); }
+int orc_bad_cell(const orc_state *s) { return s->bad_cell; }
+
+/* Calculate_Gradient_At_Cell_Center, src/Grid_Refine_Functions.cpp:221-246. */
+void orc_gradient(orc_state *s, int slot, double *grad) {
+  for (int c = 0; c < s->NP; c++) {
+    double g0 = 0.0, g1 = 0.0;
+    if (s->nf[c] > 0 && s->area[c] > 0.0) {
+      double pc = s->P[11 * (size_t)c + slot];
+      for (int f = 0; f < s->nf[c]; f++) {
+        int N = s->nbr[4 * c + f];
+        double pn = pc;
+        if (N >= 0 && N < s->NP) pn = s->P[11 * (size_t)N + slot];
+        double pf = 0.5 * (pc + pn);
+        g0 += pf * s->nrm[8 * c + 2 * f] * s->len[4 * c + f];
+        g1 += pf * s->nrm[8 * c + 2 * f + 1] * s->len[4 * c + f];
+      }
+      g0 *= s->inva[c];
+      g1 *= s->inva[c];
+    }
+    grad[2 * c] = g0;
+    grad[2 * c + 1] = g1;
+  }
+}
+
+static const double *g_sort_key;
+static int cmp_desc(const void *a, const void *b) {
+  int i = *(const int *)a, j = *(const int *)b;
+  double x = g_sort_key[i], y = g_sort_key[j];
+  if (x > y) return -1;
+  if (x < y) return 1;
+  return (i > j) - (i < j);
+}
+
+/* Compute_Gradient_Refinement_Indicator + TagRefinableCells, src/Grid_Refine_Functions.cpp:8-63
+ * (ties at the cut are broken by lower cell index; the reference's std::sort leaves them
+ * implementation-defined). */
+void orc_amr(orc_state *s, double threshold, double max_fraction, double *indicator, unsigned char *tags) {
+  const int NP = s->NP;
+  double *gr = (double *)malloc(2 * (size_t)NP * sizeof(double));
+  double *gp = (double *)malloc(2 * (size_t)NP * sizeof(double));
+  orc_gradient(s, 0, gr);
+  orc_gradient(s, 4, gp);
+  for (int i = 0; i < NP; i++) {
+    double ind = 0.0, h = sqrt(s->area[i]);
+    ind += sqrt(gr[2 * i] * gr[2 * i] + gr[2 * i + 1] * gr[2 * i + 1]) * h;
+    double P = s->P[11 * (size_t)i + 4];
+    if (P > 1e-14) ind += (sqrt(gp[2 * i] * gp[2 * i] + gp[2 * i + 1] * gp[2 * i + 1]) / P) * h;
+    indicator[i] = ind;
+    tags[i] = 0;
+  }
+  if (max_fraction > 0.0 && max_fraction < 1.0) {
+    int *order = (int *)malloc((size_t)NP * sizeof(int));
+    for (int i = 0; i < NP; i++) order[i] = i;
+    g_sort_key = indicator;
+    qsort(order, NP, sizeof(int), cmp_desc);
+    int nRefine = (int)(max_fraction * NP);
+    if (nRefine < 1) nRefine = 1;
+    for (int k = 0; k < nRefine && k < NP; k++)
+      if (indicator[order[k]] >= threshold) tags[order[k]] = 1;
+    free(order);
+  } else {
+    for (int i = 0; i < NP; i++)
+      if (indicator[i] > threshold) tags[i] = 1;
+  }
+  free(gr);
+  free(gp);
+}

@@ -1,0 +1,49 @@
+/* Test infrastructure only: plain-C restatement of the reference's explicit FV residual/update
+ * path, used as the checker for the CUDA library (never linked into it).
+ *
+ * Parity pin: every form the reference implements (ROE/ROE_2O with the reference MinMod, LLF,
+ * the ghost-cell BCs, Runge_Kutta_Method, Explicit_Method, Estimate_Error/Update, Green-Gauss
+ * gradients, AMR indicator) is checked bit-for-bit against the reference's own CPU code built
+ * from its sources (oracle/_ref, tests/test_oracle_vs_reference.py).  The additive forms with no
+ * reference counterpart (phi(r) limiters inside the MUSCL stencil, MUSCL on primitives,
+ * stage-consistent SSP-RK3, classical RK4, total-(p,T) inflow, static-pressure outflow) are
+ * "parity unpinned": this restatement is their only oracle. */
+#ifndef CFD_ORACLE_H
+#define CFD_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int dissipation_type, is_second_order, time_accurate, local_time_stepping, integrator, limiter,
+      reconstruct_primitive, inlet_bc, exit_bc;
+  double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas;
+} orc_config;
+
+typedef struct orc_state orc_state;
+
+orc_state *orc_create(int NP, int NG, const int *nf, const int *nbr, const double *normals, const double *lengths,
+                      const double *ccd, const double *area, const double *inv_area, int NB, const int *bnd,
+                      const orc_config *cfg);
+void orc_destroy(orc_state *s);
+void orc_set_state(orc_state *s, const double *U, int n);
+void orc_apply_bc(orc_state *s);
+void orc_net_flux(orc_state *s);
+int orc_explicit(orc_state *s);
+void orc_rk(orc_state *s);
+void orc_estimate_error(orc_state *s);
+void orc_update(orc_state *s);
+int orc_iterate(orc_state *s, int n, double t_end);
+void orc_get(const orc_state *s, double *U, double *prim11, double *dt, double *net, double *delu);
+void orc_get_stage(const orc_state *s, double *S);
+double orc_min_dt(const orc_state *s);
+double orc_total_time(const orc_state *s);
+void orc_error(const orc_state *s, double *err);
+void orc_gradient(orc_state *s, int slot, double *grad);
+void orc_amr(orc_state *s, double threshold, double max_fraction, double *indicator, unsigned char *tags);
+int orc_bad_cell(const orc_state *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,319 @@
+"""Test infrastructure only: ctypes bindings of the two CPU checkers.
+
+  RefRun    oracle/_ref/libcfdref.so — the reference's own CPU code (see ref_harness.cpp)
+  OracleRun oracle/_build/liboracle.so — the plain-C restatement (cfd_oracle.c)
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg only.
+"""
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libcfdref.so")
+ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_SRC = os.environ.get("CFD_REFERENCE_DIR", "/root/reference")
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_IP)
+
+
+def build_oracle():
+    """Compiles the C restatement (needs only gcc)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+    return ORACLE_LIB
+
+
+def build_ref():
+    """Compiles the reference CPU path from its sources when they are present."""
+    if not os.path.isdir(os.path.join(REF_SRC, "src")):
+        return None
+    subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "REF=" + REF_SRC])
+    return REF_LIB
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+_ref = None
+
+
+def reflib():
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(REF_LIB)
+        for n in ["refh_reset", "refh_clear_boundary_lists", "refh_apply_bc", "refh_net_flux", "refh_explicit",
+                  "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux"]:
+            getattr(L, n).restype = None
+        L.refh_load_vtk.argtypes = [ctypes.c_char_p]
+        L.refh_load_vtk.restype = ctypes.c_int
+        L.refh_add_boundary.argtypes = [ctypes.c_int] * 4
+        L.refh_finalize_mesh.restype = ctypes.c_int
+        L.refh_counts.argtypes = [_IP]
+        L.refh_get_boundary_list.argtypes = [ctypes.c_int, _IP]
+        L.refh_get_geometry.argtypes = [_IP, _IP, _DP, _DP, _DP, _DP, _DP, _DP]
+        L.refh_set_param.argtypes = [ctypes.c_char_p, ctypes.c_double]
+        L.refh_set_param.restype = ctypes.c_int
+        L.refh_set_state.argtypes = [_DP, ctypes.c_int]
+        for n in ["refh_get_U", "refh_get_prim", "refh_get_net_flux", "refh_get_delU", "refh_get_dt",
+                  "refh_get_error"]:
+            getattr(L, n).argtypes = [_DP]
+        L.refh_get_rk_states.argtypes = [_DP, _DP]
+        for n in ["refh_min_dt", "refh_total_time", "refh_get_min_dt"]:
+            getattr(L, n).restype = ctypes.c_double
+        L.refh_iterations.restype = ctypes.c_int
+        L.refh_iterate.argtypes = [ctypes.c_int, ctypes.c_double]
+        L.refh_iterate.restype = ctypes.c_int
+        L.refh_gradient.argtypes = [ctypes.c_int, _DP]
+        L.refh_amr.argtypes = [ctypes.c_double, ctypes.c_double, _DP, ctypes.POINTER(ctypes.c_uint8)]
+        _ref = L
+    return _ref
+
+
+class RefRun:
+    """The reference CPU path on one mesh (process-global state: one instance at a time)."""
+
+    def __init__(self, mesh, params):
+        L = reflib()
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "mesh.vtk")
+            mesh.write_vtk(path)
+            np_ = L.refh_load_vtk(path.encode())
+        if np_ != mesh.n_physical:
+            raise RuntimeError("reference reader returned %d cells, expected %d" % (np_, mesh.n_physical))
+        # Boundary lists from the mesh layer (identical to the bounding-box lists on box domains).
+        L.refh_clear_boundary_lists()
+        for kind, c, f, g in mesh.boundary:
+            L.refh_add_boundary(int(kind), int(c), int(f), int(g))
+        for k, v in params.items():
+            if L.refh_set_param(k.encode(), float(v)) != 0:
+                raise KeyError(k)
+        self.NT = L.refh_finalize_mesh()
+        self.NP = mesh.n_physical
+        self.L = L
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, np.float64)
+        self.L.refh_set_state(_dp(U), U.shape[0])
+
+    def geometry(self):
+        NP, NT = self.NP, self.NT
+        nf = np.zeros(NP, np.int32)
+        nbr = np.zeros((NP, 4), np.int32)
+        nrm = np.zeros((NP, 8))
+        ln = np.zeros((NP, 4))
+        ccd = np.zeros((NP, 4))
+        ar = np.zeros(NP)
+        ia = np.zeros(NP)
+        cen = np.zeros((NT, 3))
+        self.L.refh_get_geometry(_ip(nf), _ip(nbr), _dp(nrm), _dp(ln), _dp(ccd), _dp(ar), _dp(ia), _dp(cen))
+        return dict(n_faces=nf, neighbours=nbr, face_normals=nrm, face_lengths=ln, center_distances=ccd, area=ar,
+                    inv_area=ia, centers=cen)
+
+    def boundary_lists(self):
+        cnt = np.zeros(6, np.int32)
+        self.L.refh_counts(_ip(cnt))
+        out = []
+        for kind in range(4):
+            a = np.zeros(max(1, 3 * cnt[2 + kind]), np.int32)
+            self.L.refh_get_boundary_list(kind, _ip(a))
+            out.append(a[:3 * cnt[2 + kind]].reshape(-1, 3))
+        return out
+
+    def state(self):
+        NP, NT = self.NP, self.NT
+        U = np.zeros((NT, 4))
+        P = np.zeros((NT, 11))
+        dt = np.zeros(NP)
+        net = np.zeros((NP, 4))
+        dU = np.zeros((NP, 4))
+        self.L.refh_get_U(_dp(U))
+        self.L.refh_get_prim(_dp(P))
+        self.L.refh_get_dt(_dp(dt))
+        self.L.refh_get_net_flux(_dp(net))
+        self.L.refh_get_delU(_dp(dU))
+        return {"U": U, "prim": P, "dt": dt, "net_flux": net, "delU": dU}
+
+    def rk_states(self):
+        u1 = np.zeros((self.NP, 4))
+        u2 = np.zeros((self.NP, 4))
+        self.L.refh_get_rk_states(_dp(u1), _dp(u2))
+        return u1, u2
+
+    def error(self):
+        e = np.zeros(4)
+        self.L.refh_get_error(_dp(e))
+        return e
+
+    def iterate(self, n, t_end=0.0):
+        return self.L.refh_iterate(n, t_end)
+
+    def min_dt(self):
+        return self.L.refh_min_dt()
+
+    def total_time(self):
+        return self.L.refh_total_time()
+
+    def gradient(self, var):
+        g = np.zeros((self.NP, 2))
+        self.L.refh_gradient(var, _dp(g))
+        return g
+
+    def amr(self, threshold, max_fraction):
+        ind = np.zeros(self.NP)
+        tags = np.zeros(self.NP, np.uint8)
+        self.L.refh_amr(threshold, max_fraction, _dp(ind), tags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        return ind, tags
+
+
+class _OrcConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ["dissipation_type", "is_second_order", "time_accurate",
+                                            "local_time_stepping", "integrator", "limiter", "reconstruct_primitive",
+                                            "inlet_bc", "exit_bc"]] + \
+               [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
+                                               "exit_p", "r_gas"]]
+
+
+_orc = None
+
+
+def oraclelib():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_LIB):
+            build_oracle()
+        L = ctypes.CDLL(ORACLE_LIB)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _IP, _IP, _DP, _DP, _DP, _DP, _DP, ctypes.c_int, _IP,
+                                 ctypes.POINTER(_OrcConfig)]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_state.argtypes = [ctypes.c_void_p, _DP, ctypes.c_int]
+        for n in ["orc_apply_bc", "orc_net_flux", "orc_rk", "orc_estimate_error", "orc_update"]:
+            getattr(L, n).argtypes = [ctypes.c_void_p]
+            getattr(L, n).restype = None
+        L.orc_explicit.argtypes = [ctypes.c_void_p]
+        L.orc_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.orc_get.argtypes = [ctypes.c_void_p, _DP, _DP, _DP, _DP, _DP]
+        L.orc_get_stage.argtypes = [ctypes.c_void_p, _DP]
+        for n in ["orc_min_dt", "orc_total_time"]:
+            getattr(L, n).argtypes = [ctypes.c_void_p]
+            getattr(L, n).restype = ctypes.c_double
+        L.orc_error.argtypes = [ctypes.c_void_p, _DP]
+        L.orc_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
+        L.orc_amr.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, _DP, ctypes.POINTER(ctypes.c_uint8)]
+        L.orc_bad_cell.argtypes = [ctypes.c_void_p]
+        _orc = L
+    return _orc
+
+
+class OracleRun:
+    """The C restatement on one mesh; params use the solver-config field names."""
+
+    def __init__(self, mesh, **params):
+        L = oraclelib()
+        c = _OrcConfig()
+        c.dissipation_type = params.get("dissipation_type", 3)
+        c.is_second_order = params.get("is_second_order", 0)
+        c.time_accurate = params.get("time_accurate", 1)
+        c.local_time_stepping = params.get("local_time_stepping", 0)
+        c.integrator = params.get("integrator", 0)
+        c.limiter = params.get("limiter", 0)
+        c.reconstruct_primitive = params.get("reconstruct_primitive", 0)
+        c.inlet_bc = params.get("inlet_bc", 0)
+        c.exit_bc = params.get("exit_bc", 0)
+        c.cfl = params.get("cfl", 0.5)
+        c.zeta = params.get("limiter_zeta", 0.5)
+        c.zeta1 = params.get("limiter_zeta1", 0.5)
+        c.inlet_rho = params.get("inlet_rho", 1.0)
+        c.inlet_p = params.get("inlet_p", 1.0)
+        c.inlet_p0 = params.get("inlet_p0", 0.0)
+        c.inlet_t0 = params.get("inlet_t0", 0.0)
+        c.exit_p = params.get("exit_p", 0.0)
+        c.r_gas = params.get("r_gas", 287.0)
+        self.m = mesh
+        self._keep = [np.ascontiguousarray(a) for a in (
+            mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,
+            mesh.center_distances, mesh.area, mesh.inv_area, mesh.boundary.astype(np.int32).reshape(-1))]
+        k = self._keep
+        self.h = L.orc_create(mesh.n_physical, mesh.n_ghost, _ip(k[0]), _ip(k[1]), _dp(k[2]), _dp(k[3]), _dp(k[4]),
+                              _dp(k[5]), _dp(k[6]), mesh.boundary.shape[0], _ip(k[7]), ctypes.byref(c))
+        self.L = L
+        self.NP, self.NT = mesh.n_physical, mesh.n_total
+
+    def __del__(self):
+        try:
+            self.L.orc_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, np.float64)
+        self.L.orc_set_state(self.h, _dp(U), U.shape[0])
+
+    def state(self):
+        NP, NT = self.NP, self.NT
+        out = {"U": np.zeros((NT, 4)), "prim": np.zeros((NT, 11)), "dt": np.zeros(NP), "net_flux": np.zeros((NP, 4)),
+               "delU": np.zeros((NP, 4))}
+        self.L.orc_get(self.h, _dp(out["U"]), _dp(out["prim"]), _dp(out["dt"]), _dp(out["net_flux"]), _dp(out["delU"]))
+        return out
+
+    def stage_state(self):
+        S = np.zeros((self.NP, 4))
+        self.L.orc_get_stage(self.h, _dp(S))
+        return S
+
+    def iterate(self, n, t_end=0.0):
+        return self.L.orc_iterate(self.h, n, t_end)
+
+    def apply_bc(self):
+        self.L.orc_apply_bc(self.h)
+
+    def net_flux(self):
+        self.L.orc_net_flux(self.h)
+
+    def explicit(self):
+        return self.L.orc_explicit(self.h)
+
+    def rk(self):
+        self.L.orc_rk(self.h)
+
+    def estimate_error(self):
+        self.L.orc_estimate_error(self.h)
+        return self.error()
+
+    def update(self):
+        self.L.orc_update(self.h)
+
+    def error(self):
+        e = np.zeros(4)
+        self.L.orc_error(self.h, _dp(e))
+        return e
+
+    def min_dt(self):
+        return self.L.orc_min_dt(self.h)
+
+    def total_time(self):
+        return self.L.orc_total_time(self.h)
+
+    def gradient(self, slot):
+        g = np.zeros((self.NP, 2))
+        self.L.orc_gradient(self.h, slot, _dp(g))
+        return g
+
+    def amr(self, threshold, max_fraction):
+        ind = np.zeros(self.NP)
+        tags = np.zeros(self.NP, np.uint8)
+        self.L.orc_amr(self.h, threshold, max_fraction, _dp(ind), tags.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        return ind, tags

@@ -1,0 +1,77 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own CPU code.
+
+Run in a container where the reference sources are present:
+    python tests/golden/make_golden.py
+It builds oracle/_ref/libcfdref.so from the reference's src/*.cpp (oracle/Makefile), builds the
+meshes with the mesh layer, runs the reference loop (src/Solver.cpp:94-125) through the harness,
+and stores inputs and outputs as compressed .npz.  The fixtures travel with the repository, so
+tests that use them never need the reference itself.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import cfd_solver_withcuda_b200 as cb  # noqa: E402
+from oracle import refpy  # noqa: E402
+
+from cases import CASES, make_mesh, initial_state  # noqa: E402
+
+
+def ref_params(case):
+    p = {"CFL": case["cfl"], "Time_Accurate": case["time_accurate"], "Dissipation_Type": case["dissipation_type"],
+         "Is_Second_Order": case["is_second_order"], "Local_Time_Stepping": case.get("local_time_stepping", 0),
+         "Limiter_Zeta": case.get("limiter_zeta", 0.5), "Limiter_Zeta1": case.get("limiter_zeta1", 0.5),
+         "Inlet_Rho": case["inlet_rho"], "Inlet_P": case["inlet_p"],
+         "Is_Inlet_SubSonic": 1 if case.get("inlet_bc", 0) == 1 else 0,
+         "Is_Exit_SubSonic": 1 if case.get("exit_bc", 0) == 1 else 0}
+    return p
+
+
+def main():
+    refpy.build_ref()
+    manifest = {}
+    for name, case in CASES.items():
+        mesh = make_mesh(case)
+        U0 = initial_state(case, mesh)
+        r = refpy.RefRun(mesh, ref_params(case))
+        r.set_state(U0)
+        # Single entry-point results after the first BC + flux evaluation.
+        r.L.refh_apply_bc()
+        r.L.refh_net_flux()
+        first = r.state()
+        r = refpy.RefRun(mesh, ref_params(case))
+        r.set_state(U0)
+        n = r.iterate(case["steps"], case.get("t_end", 0.0))
+        st = r.state()
+        out = {
+            "U0": U0,
+            "first_net_flux": first["net_flux"], "first_dt": first["dt"],
+            "first_ghost_U": first["U"][mesh.n_physical:],
+            "U": st["U"], "prim": st["prim"], "dt": st["dt"], "net_flux": st["net_flux"], "delU": st["delU"],
+            "error": r.error(), "total_time": np.array([r.total_time()]), "iterations": np.array([n]),
+            "min_dt": np.array([r.min_dt()]),
+        }
+        if case.get("amr"):
+            out["grad_rho"] = r.gradient(0)
+            out["grad_p"] = r.gradient(4)
+            ind, tags = r.amr(case["amr"][0], case["amr"][1])
+            out["amr_indicator"] = ind
+            out["amr_tags"] = tags
+        geo = r.geometry()
+        for k in ("neighbours", "face_normals", "face_lengths", "center_distances", "area", "inv_area", "centers"):
+            out["geo_" + k] = geo[k]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        manifest[name] = {"iterations": int(n), "np": mesh.n_physical, "ng": mesh.n_ghost}
+        print(name, manifest[name])
+    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()

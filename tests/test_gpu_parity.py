@@ -1,0 +1,156 @@
+"""CUDA path vs the reference (golden fixtures from its own CPU code) and vs the C restatement.
+
+Conserved fields, primitives, del_t, net flux and Cells_DelU are compared bit for bit; the
+residual norm Error[] is a tree reduction on the device (the reference sums serially), so it is
+compared within 1e-12 relative."""
+import numpy as np
+import pytest
+
+import cfd_solver_withcuda_b200 as cb
+from cases import CASES, initial_state, make_mesh, oracle_params, solver_config
+from conftest import assert_bits_equal, load_golden
+
+pytestmark = pytest.mark.gpu
+ERR_RTOL = 1e-12
+
+
+def check_state(st, ref, what, keys=("U", "prim", "dt", "net_flux", "delU")):
+    for k in keys:
+        assert_bits_equal(st[k], ref[k], what + ":" + k)
+
+
+@pytest.mark.parametrize("reorder", [0, 1])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_cuda_matches_reference_fixture(name, reorder):
+    case = CASES[name]
+    g = load_golden(name)
+    m = make_mesh(case)
+    s = cb.Solver(m, solver_config(case, reorder=reorder))
+    s.upload_state(g["U0"])
+    info = s.step(case["steps"], case.get("t_end", 0.0))
+    assert info.iterations == int(g["iterations"][0])
+    check_state(s.download(), g, name)
+    assert_bits_equal(np.array([info.total_time]), g["total_time"], "Total_Time")
+    assert_bits_equal(np.array([info.min_dt]), g["min_dt"], "Min_dt")
+    np.testing.assert_allclose(np.array(info.error[:]), g["error"], rtol=ERR_RTOL, atol=0)
+    if "amr_indicator" in g:
+        assert_bits_equal(s.gradient(0), g["grad_rho"], "grad rho")
+        assert_bits_equal(s.gradient(4), g["grad_p"], "grad p")
+        assert_bits_equal(s.amr_indicator(), g["amr_indicator"], "AMR indicator")
+
+
+@pytest.mark.parametrize("name", ["sod_roe2_rk3", "cyl_roe2_lts", "bump_roe2_rk3", "sod_llf1_rk3"])
+def test_entry_points_one_by_one(name, oracle_lib):
+    """Apply_Boundary_Conditions / Evaluate_Cell_Net_Flux / Runge_Kutta_Method | Explicit_Method /
+    Estimate_Error / Update called separately, as the reference's driver does."""
+    case = CASES[name]
+    g = load_golden(name)
+    m = make_mesh(case)
+    s = cb.Solver(m, solver_config(case))
+    s.upload_state(g["U0"])
+    s.Apply_Boundary_Conditions()
+    s.Evaluate_Cell_Net_Flux()
+    st = s.download()
+    assert_bits_equal(st["net_flux"], g["first_net_flux"], "first net flux")
+    assert_bits_equal(st["dt"], g["first_dt"], "first dt")
+    assert_bits_equal(st["U"][m.n_physical:], g["first_ghost_U"], "first ghost U")
+    o = oracle_lib.OracleRun(m, **oracle_params(case))
+    o.set_state(g["U0"])
+    s.upload_state(g["U0"])
+    for it in range(5):
+        s.Apply_Boundary_Conditions()
+        o.apply_bc()
+        if case["time_accurate"]:
+            s.Runge_Kutta_Method()
+            o.rk()
+            # Primitive_Cells hold the second-stage primitives here; U_Cells is still U^n.
+            check_state(s.download(), o.state(), "after RK %d" % it, keys=("U", "prim", "dt", "net_flux", "delU"))
+            assert_bits_equal(s.stage_state(), o.stage_state(), "U_Cells_RK_2")
+        else:
+            s.Explicit_Method()
+            assert o.explicit() == 0
+        assert s.get_Min_dt() == o.min_dt()
+        e = s.Estimate_Error()
+        np.testing.assert_allclose(e, o.estimate_error(), rtol=ERR_RTOL, atol=0)
+        s.Update()
+        o.update()
+        check_state(s.download(), o.state(), "after Update %d" % it)
+
+
+ADDITIVE = {
+    "vanleer_cons": dict(limiter=cb.LIM_VANLEER),
+    "superbee_cons": dict(limiter=cb.LIM_SUPERBEE),
+    "minmod_phi_cons": dict(limiter=cb.LIM_MINMOD),
+    "vanalbada_cons": dict(limiter=cb.LIM_VANALBADA),
+    "vanleer_prim": dict(limiter=cb.LIM_VANLEER, reconstruct_primitive=1),
+    "ssprk3": dict(integrator=cb.INT_SSPRK3, limiter=cb.LIM_VANLEER),
+    "ssprk3_lts": dict(integrator=cb.INT_SSPRK3, local_time_stepping=1, limiter=cb.LIM_SUPERBEE),
+    "rk4": dict(integrator=cb.INT_RK4, limiter=cb.LIM_VANLEER, reconstruct_primitive=1),
+    "rk4_lts": dict(integrator=cb.INT_RK4, local_time_stepping=1),
+}
+
+
+@pytest.mark.parametrize("base", ["cyl_roe2_lts", "bump_roe2_rk3"])
+@pytest.mark.parametrize("form", sorted(ADDITIVE))
+def test_additive_forms_match_oracle(form, base, oracle_lib):
+    """Forms with no reference counterpart (parity unpinned) vs the C restatement, bit for bit."""
+    case = CASES[base]
+    over = ADDITIVE[form]
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.step(20)
+    o = oracle_lib.OracleRun(m, **oracle_params(case, **over))
+    o.set_state(U0)
+    o.iterate(20)
+    check_state(s.download(), o.state(), form)
+    assert s.info.total_time == o.total_time()
+
+
+def test_characteristic_bcs_match_oracle(oracle_lib):
+    """Total-(p,T) inflow and static-pressure outflow on the bump channel; pow() on the device is
+    not correctly rounded, so these compare within 1e-12 relative."""
+    case = dict(CASES["bump_llf1_subsonic"])
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    p_static = 1.0 / 1.4
+    over = dict(inlet_bc=cb.INLET_TOTAL_PT, exit_bc=cb.EXIT_STATIC_P, inlet_p0=p_static * (1 + 0.2 * 0.25) ** 3.5,
+                inlet_t0=p_static / 287.0 * (1 + 0.2 * 0.25), exit_p=p_static, dissipation_type=3, is_second_order=1)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.step(25)
+    o = oracle_lib.OracleRun(m, **oracle_params(case, **over))
+    o.set_state(U0)
+    o.iterate(25)
+    a, b = s.download(), o.state()
+    for k in ("U", "net_flux", "delU"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-12, atol=1e-13, err_msg=k)
+
+
+def test_deterministic_and_graph_equivalent():
+    case = CASES["cyl_roe2_lts"]
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    outs = []
+    for use_graph in (1, 0, 1):
+        s = cb.Solver(m, solver_config(case))
+        s.set_option("use_graph", use_graph)
+        s.upload_state(U0)
+        s.step(15)
+        outs.append(s.download())
+    for o in outs[1:]:
+        check_state(o, outs[0], "rerun")
+
+
+def test_nonphysical_state_is_reported():
+    """A planted negative pressure (host-side input) comes back as a status with the cell id."""
+    case = CASES["sod_roe1_rk3"]
+    m = make_mesh(case)
+    U0 = initial_state(case, m).copy()
+    U0[37, 3] = -1.0
+    s = cb.Solver(m, solver_config(case))
+    with pytest.raises(cb.CfdError) as e:
+        s.upload_state(U0)
+    assert e.value.status == 3
+    assert "37" in str(e.value)
