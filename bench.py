@@ -4,8 +4,9 @@
 Workload (the metric's configuration): supersonic flow (M = 3, rho = 1, p = 1/1.4) around a half
 cylinder on a body-fitted O-grid, body radius 1, outer radius 4, 1024 circumferential x 512
 radial cells (524,288 cells), radial stretching 1.005; second-order MUSCL on primitive variables
-with the Van Leer limiter, Roe flux with entropy fix, the reference's TVD-RK3 with local time
-stepping at CFL 0.8, FP64.  One step = one pseudo-time step (3 RK stages) of all cells.
+(Green-Gauss gradients, Van Leer limiter), Roe flux with entropy fix, TVD-RK3 (Shu-Osher form of
+the reference's Runge_Kutta_Method, stage-consistent) with local time stepping at CFL 0.8, FP64.
+One step = one pseudo-time step (3 RK stages) of all cells.
 Synthetic, seeded: the mesh is generated in-repo and the flow starts from freestream.
 
 Metric: cell-updates/s (cells x pseudo-steps / s), higher is better.
@@ -31,7 +32,7 @@ sys.path.insert(0, ROOT)
 GAMMA = 1.4
 NTHETA, NR, R_BODY, R_OUTER, RATIO = 1024, 512, 1.0, 4.0, 1.005
 MACH = 3.0
-WORKLOAD = "half_cylinder_M3_ogrid_1024x512_roe_muscl_vanleer_prim_rk3_lts_cfl0.8"
+WORKLOAD = "half_cylinder_M3_ogrid_1024x512_roe_gg_muscl_vanleer_prim_tvdrk3_lts_cfl0.8"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 
@@ -45,7 +46,7 @@ def workload_state(cb):
     full[:NP] = U
     full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
     kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
-              limiter=2, reconstruct_primitive=1, inlet_rho=rho, inlet_p=p)
+              limiter=2, muscl=1, integrator=2, inlet_rho=rho, inlet_p=p)
     return m, full, kw
 
 
@@ -105,18 +106,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def flux_bytes_per_cell(NP, nbytes_geom_face=48):
-    """Algorithmic DRAM bytes of one flux-kernel launch per cell (each array touched once):
-    own primitives 40 B, per face the neighbour id 4 B, nx/ny/dl 24 B, second-neighbour id 4 B and
-    limiter distances 16 B (48 B x 4 faces), face count / mask / area 13 B, writes R 32 B + dt 8 B."""
-    return 40 + 4 * nbytes_geom_face + 13 + 40
+def flux_bytes_per_cell(NP):
+    """Algorithmic DRAM bytes of one gradient-MUSCL flux-kernel launch per cell (each array
+    touched once): own primitives 40 B and gradients 64 B; per face the neighbour id 4 B,
+    nx/ny/dl 24 B and the centre vector 16 B (44 B x 4 faces); face count / mask / area 13 B;
+    writes R 32 B + del_t 8 B."""
+    return 40 + 64 + 4 * 44 + 13 + 40
 
 
 def cpu_baseline(steps=3):
     """The reference's own CPU code (oracle/_ref, single-threaded as the reference is) timed on a
     bounded sample: `steps` pseudo-steps of the full workload mesh, mesh load excluded.  The
-    reference's CPU path has no Van Leer / primitive MUSCL, so it runs its own 2-argument MinMod
-    on conserved variables with otherwise identical settings."""
+    reference's CPU path has no Van Leer / gradient MUSCL, so it runs its own ROE_2O with the
+    2-argument MinMod stencil (src/Limiters.cpp:97-200) and its Runge_Kutta_Method with local dt,
+    otherwise the same mesh, state and CFL."""
     import cfd_solver_withcuda_b200 as cb
     from oracle import refpy
     if not refpy.ref_available():

@@ -25,6 +25,7 @@ INT_REFERENCE, INT_RK4, INT_SSPRK3 = 0, 1, 2
 INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT = 0, 1, 2
 EXIT_SUPERSONIC, EXIT_SUBSONIC_REF, EXIT_STATIC_P = 0, 1, 2
 PREC_FP64, PREC_FP32_FLUX = 0, 1
+MUSCL_REFERENCE, MUSCL_GRADIENT = 0, 1
 
 
 class CfdError(RuntimeError):
@@ -37,7 +38,8 @@ class MeshDesc(ctypes.Structure):
     _fields_ = [("n_physical", ctypes.c_int), ("n_ghost", ctypes.c_int),
                 ("n_faces", ctypes.POINTER(ctypes.c_int)), ("neighbours", ctypes.POINTER(ctypes.c_int)),
                 ("face_normals", ctypes.POINTER(ctypes.c_double)), ("face_lengths", ctypes.POINTER(ctypes.c_double)),
-                ("center_distances", ctypes.POINTER(ctypes.c_double)), ("area", ctypes.POINTER(ctypes.c_double)),
+                ("center_distances", ctypes.POINTER(ctypes.c_double)),
+                ("center_vectors", ctypes.POINTER(ctypes.c_double)), ("area", ctypes.POINTER(ctypes.c_double)),
                 ("inv_area", ctypes.POINTER(ctypes.c_double)), ("n_boundary", ctypes.c_int),
                 ("boundary", ctypes.POINTER(ctypes.c_int))]
 
@@ -46,6 +48,7 @@ class Config(ctypes.Structure):
     _fields_ = [("dissipation_type", ctypes.c_int), ("is_second_order", ctypes.c_int),
                 ("time_accurate", ctypes.c_int), ("local_time_stepping", ctypes.c_int),
                 ("integrator", ctypes.c_int), ("limiter", ctypes.c_int), ("reconstruct_primitive", ctypes.c_int),
+                ("muscl", ctypes.c_int),
                 ("inlet_bc", ctypes.c_int), ("exit_bc", ctypes.c_int), ("precision", ctypes.c_int),
                 ("reorder", ctypes.c_int), ("cfl", ctypes.c_double), ("limiter_zeta", ctypes.c_double),
                 ("limiter_zeta1", ctypes.c_double), ("inlet_rho", ctypes.c_double), ("inlet_p", ctypes.c_double),
@@ -150,6 +153,7 @@ class Mesh:
         self.face_normals = np.ctypeslib.as_array(d.face_normals, (NP, 8)).copy()
         self.face_lengths = np.ctypeslib.as_array(d.face_lengths, (NP, 4)).copy()
         self.center_distances = np.ctypeslib.as_array(d.center_distances, (NP, 4)).copy()
+        self.center_vectors = np.ctypeslib.as_array(d.center_vectors, (NP, 8)).copy()
         self.area = np.ctypeslib.as_array(d.area, (NP,)).copy()
         self.inv_area = np.ctypeslib.as_array(d.inv_area, (NP,)).copy()
         self.boundary = np.ctypeslib.as_array(d.boundary, (d.n_boundary, 4)).copy() if d.n_boundary else \

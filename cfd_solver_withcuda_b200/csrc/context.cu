@@ -300,6 +300,7 @@ cfd_status cfd_mesh_describe(const cfd_mesh *h, cfd_mesh_desc *d) {
   d->face_normals = m.normals.data();
   d->face_lengths = m.lengths.data();
   d->center_distances = m.ccd.data();
+  d->center_vectors = m.cvec.data();
   d->area = m.area.data();
   d->inv_area = m.inv_area.data();
   d->n_boundary = static_cast<int>(m.boundary.size() / 4);
@@ -431,6 +432,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   std::vector<int> nf(NP), nbr(4 * (size_t)NP, 0), n2(4 * (size_t)NP, 0);
   std::vector<double> nx(4 * (size_t)NP, 0.0), ny(4 * (size_t)NP, 0.0), dl(4 * (size_t)NP, 0.0);
   std::vector<double> d1l(4 * (size_t)NP, 1.0), d2l(4 * (size_t)NP, 1.0), area(NP), inva(NP);
+  std::vector<double> cvx(4 * (size_t)NP, 0.0), cvy(4 * (size_t)NP, 0.0);
+  if (cfg->muscl && cfg->is_second_order && !d->center_vectors)
+    return bail(fail(CFD_ERR_BAD_ARG, "gradient MUSCL needs centre vectors"));
   std::vector<uint8_t> degen(NP, 0);
   const double *ccd = d->center_distances;
   for (int i = 0; i < NP; i++) {
@@ -448,6 +452,10 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       ny[idx] = fy;
       dl[idx] = d->face_lengths[4 * r + f];
       if (std::sqrt(fx * fx + fy * fy) < 1e-12) degen[i] |= static_cast<uint8_t>(1u << f);
+      if (d->center_vectors) {
+        cvx[idx] = d->center_vectors[8 * r + 2 * f];
+        cvy[idx] = d->center_vectors[8 * r + 2 * f + 1];
+      }
       if (ccd) {
         int N2;
         double d1, d2;
@@ -494,6 +502,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.d1l), d1l)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.d2l), d2l)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<uint8_t **>(&m.degen), degen)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvx), cvx)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvy), cvy)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.bnd), bnd)) != CFD_OK) return bail(s);
 
   DevState &st = ctx->ds;
@@ -508,6 +518,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if ((s = ctx_alloc(ctx, (void **)&st.dU, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   if (cfg->integrator == CFD_INT_RK4) {
     if ((s = ctx_alloc(ctx, (void **)&st.Racc, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  }
+  if (cfg->muscl) {
+    if ((s = ctx_alloc(ctx, (void **)&st.grad, 8 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)nblk * dsz)) != CFD_OK) return bail(s);
@@ -529,6 +542,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.second_order = cfg->is_second_order;
   fp.limiter = cfg->limiter;
   fp.recon_prim = cfg->reconstruct_primitive;
+  fp.muscl = cfg->muscl && cfg->is_second_order;
   fp.consistent = (cfg->integrator != CFD_INT_REFERENCE) ? 1 : 0;
   fp.precision = cfg->precision;
   fp.cfl = cfg->cfl;

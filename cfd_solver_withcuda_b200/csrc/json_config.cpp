@@ -232,6 +232,7 @@ std::string config_from_json(const std::string &text, cfd_config *cfg) {
     cfg->precision = enum_from(sol->get("Precision"), {"fp64", "fp32_flux"}, cfg->precision);
     cfg->reconstruct_primitive = enum_from(sol->get("Reconstruction"), {"conserved", "primitive"}, cfg->reconstruct_primitive);
     as_bool(sol->get("Reorder"), cfg->reorder);
+    cfg->muscl = enum_from(sol->get("MUSCL"), {"reference", "gradient"}, cfg->muscl);
   }
   if (lim) {
     as_double(lim->get("Limiter_Zeta"), cfg->limiter_zeta);

@@ -230,6 +230,12 @@ __global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, Flu
     }
     const int nf = m.nf[c];
     const uint8_t degen = m.degen[c];
+    double gc[8];
+    const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+    if (ORDER == 3) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) gc[k] = st.grad[k * NP + c];
+    }
     double N0 = 0.0, N1s = 0.0, N2s = 0.0, N3s = 0.0;
     double den = 0.0;
 #pragma unroll
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, Flu
         const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
         const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
         double A[4], D[4];
-        average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
+        if (ORDER != 3) average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
         if (DISS == 3 && ORDER == 1) {
           if (N >= NP)
             roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (degen >> f) & 1, D);
@@ -279,6 +285,41 @@ __global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, Flu
                     (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
           }
           roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
+        } else if (DISS == 3 && ORDER == 3) {
+          // Green-Gauss-gradient MUSCL on (rho, u, v, p) (no reference counterpart; the
+          // reference's second-order form is the ORDER == 2 branch).  With d = x_N - x_c and
+          // D+ = q_N - q_c, the upwind differences are D-_c = 2 grad q_c . d - D+ and
+          // D-_N = 2 grad q_N . d - D+; q_L = q_c + 0.5 phi(D-_c, D+) D+,
+          // q_R = q_N - 0.5 phi(D-_N, D+) D+ (phi(a, b) with r = a/b).  A ghost neighbour uses
+          // the cell's own gradient.  A non-positive reconstructed density or pressure falls
+          // back to the cell-centre state.  Flux: average of the two face states plus Roe
+          // dissipation between them.
+          const double dx = m.cvx[idx], dy = m.cvy[idx];
+          const double *gN = (N < NP) ? st.grad : nullptr;
+          const double qc[4] = {rc, uc, vc, pc};
+          const double qn[4] = {rn, un, vn, pn};
+          double qL[4], qR[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const double gx = gc[2 * k], gy = gc[2 * k + 1];
+            const double nxg = gN ? gN[(2 * k) * NP + N] : gx, nyg = gN ? gN[(2 * k + 1) * NP + N] : gy;
+            const double dp = qn[k] - qc[k];
+            const double dmc = 2.0 * (gx * dx + gy * dy) - dp;
+            const double dmn = 2.0 * (nxg * dx + nyg * dy) - dp;
+            qL[k] = qc[k] + 0.5 * phi_ab<double>(glim, dmc, dp) * dp;
+            qR[k] = qn[k] - 0.5 * phi_ab<double>(glim, dmn, dp) * dp;
+          }
+          if (!(qL[0] > 0.0) || !(qL[3] > 0.0)) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) qL[k] = qc[k];
+          }
+          if (!(qR[0] > 0.0) || !(qR[3] > 0.0)) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) qR[k] = qn[k];
+          }
+          const double aL = sqrt(kGamma * qL[3] / qL[0]), aR = sqrt(kGamma * qR[3] / qR[0]);
+          average_flux<double>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
+          roe_1o<double>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
         } else {  // LLF 1O
           double UR[4];
 #pragma unroll
@@ -508,6 +549,37 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
   g1 *= m.inv_area[c];
 }
 
+// Green-Gauss gradients of (rho, u, v, p) for the gradient MUSCL form: the face value is the
+// mean of the two cell values, ghost cells included (their values carry the boundary state).
+__global__ void k_muscl_gradients(DevMesh m, DevState st) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int NP = m.NP, NT = m.NT;
+  if (c >= NP || step_done(st.ctl)) return;
+  const int nf = m.nf[c];
+  const double ia = m.inv_area[c];
+  const int slot[4] = {0, 1, 2, 3};
+  double qc[4], g[8];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    qc[k] = st.prim[slot[k] * NT + c];
+    g[2 * k] = 0.0;
+    g[2 * k + 1] = 0.0;
+  }
+  for (int f = 0; f < nf; f++) {
+    const int idx = f * NP + c;
+    const int N = m.nbr[idx];
+    const double wx = m.nx[idx] * m.dl[idx], wy = m.ny[idx] * m.dl[idx];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double qf = 0.5 * (qc[k] + st.prim[slot[k] * NT + N]);
+      g[2 * k] += qf * wx;
+      g[2 * k + 1] += qf * wy;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) st.grad[k * NP + c] = g[k] * ia;
+}
+
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.NP) return;
@@ -574,7 +646,11 @@ int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   const int g = nblk(m.NP, kFluxBlock);
   if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-  else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  else if (fp.dissipation == 3 && fp.muscl) {
+    launch_muscl_gradients(s, m, st);
+    k_flux<3, 3><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    return 2;
+  } else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   return 1;
 }
@@ -596,6 +672,11 @@ int launch_update(cudaStream_t s, const DevMesh &m, DevState &st) {
 
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad) {
   k_gradient<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, var, grad);
+  return 1;
+}
+
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st) {
+  k_muscl_gradients<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st);
   return 1;
 }
 

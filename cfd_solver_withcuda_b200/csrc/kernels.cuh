@@ -21,6 +21,7 @@ struct DevMesh {
   const double *area, *inv_area;
   const int *n2;
   const double *d1l, *d2l;
+  const double *cvx, *cvy;  // [4][NP] centre-to-centre vectors (gradient MUSCL)
   const uint8_t *degen;
   const int4 *bnd;  // kind, cell, face, ghost
 };
@@ -34,6 +35,7 @@ struct DevState {
   double *dtc;   // [NP]
   double *dtk;   // [NP] dt kept for the whole step (RK4 / SSP with LTS)
   double *dU;    // [4][NP]
+  double *grad;  // [8][NP] Green-Gauss gradients of (rho, u, v, p) (gradient MUSCL)
   // reduction / control block (see CtrlIdx)
   double *ctl;
   double *partial;     // [nblk_max * 9]
@@ -59,6 +61,7 @@ struct FluxParams {
   int second_order;
   int limiter;
   int recon_prim;
+  int muscl;            // 0 reference stencil, 1 Green-Gauss-gradient MUSCL
   int consistent;       // 1: limiter/LLF/exit read the stage state instead of U^n
   int precision;
   double cfl, zeta, zeta1;
@@ -80,6 +83,7 @@ int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int l
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_update(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
 int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP, int NT, double *U);

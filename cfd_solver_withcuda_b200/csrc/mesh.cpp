@@ -231,9 +231,12 @@ std::string Mesh::build() {
       }
     }
   }
+  cvec.assign(static_cast<size_t>(NP) * 8, 0.0);
   for (int i = 0; i < NP; i++) {
     for (int f = 0; f < n_faces[i]; f++) {
       int N = nbr[4 * i + f];
+      cvec[8 * i + 2 * f] = centers[3 * N] - centers[3 * i];
+      cvec[8 * i + 2 * f + 1] = centers[3 * N + 1] - centers[3 * i + 1];
       double D = 0.0;
       for (int k = 0; k < 3; k++) {
         double t = centers[3 * N + k] - centers[3 * i + k];

@@ -31,6 +31,7 @@ struct Mesh {
   std::vector<double> normals;       // [NP*8]
   std::vector<double> lengths;       // [NP*4]
   std::vector<double> ccd;           // [NP*4] centre-to-centre distances
+  std::vector<double> cvec;          // [NP*8] centre-to-centre vectors (x, y) per face
   std::vector<double> area;          // [NP]
   std::vector<double> inv_area;      // [NP]
   std::vector<double> centers;       // [(NP+NG)*3]

@@ -61,6 +61,8 @@ typedef struct {
   const double *face_normals;     /* [NP*8] Cell::Face_Normals (nx, ny per face) */
   const double *face_lengths;     /* [NP*4] Cell::Face_Areas */
   const double *center_distances; /* [NP*4] Cell::Cell_Center_Distances */
+  const double *center_vectors;   /* [NP*8] Cell::Cell_Center_Vector (x, y of N - c per face);
+                                     needed by the gradient MUSCL form only, may be NULL */
   const double *area;             /* [NP] Cell::Area */
   const double *inv_area;         /* [NP] Cell::Inv_Area */
   int n_boundary;                 /* number of boundary entries (== n_ghost) */
@@ -92,6 +94,7 @@ enum { CFD_INT_REFERENCE = 0, CFD_INT_RK4 = 1, CFD_INT_SSPRK3 = 2 };
 enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2 };
 enum { CFD_EXIT_SUPERSONIC = 0, CFD_EXIT_SUBSONIC_REF = 1, CFD_EXIT_STATIC_P = 2 };
 enum { CFD_PREC_FP64 = 0, CFD_PREC_FP32_FLUX = 1 };
+enum { CFD_MUSCL_REFERENCE = 0, CFD_MUSCL_GRADIENT = 1 };
 
 typedef struct {
   int dissipation_type;      /* Dissipation_Type: 1 LLF, 3 ROE; additive 6 AUSM, 7 HLLC */
@@ -101,6 +104,10 @@ typedef struct {
   int integrator;            /* CFD_INT_*: reference forms, classical RK4, standard SSP-RK3 */
   int limiter;               /* CFD_LIM_*: 0 = reference 2-argument MinMod (src/Limiters.cpp:58-63) */
   int reconstruct_primitive; /* MUSCL on (rho,u,v,p) instead of conserved variables */
+  int muscl;                 /* CFD_MUSCL_REFERENCE: the reference's directional stencil
+                                (src/Limiters.cpp:97-200) in ROE_2O; CFD_MUSCL_GRADIENT:
+                                Green-Gauss-gradient MUSCL on (rho,u,v,p), Roe flux of the two
+                                reconstructed face states */
   int inlet_bc;              /* CFD_INLET_* (reference: Is_Inlet_SubSonic) */
   int exit_bc;               /* CFD_EXIT_*  (reference: Is_Exit_SubSonic) */
   int precision;             /* CFD_PREC_* */

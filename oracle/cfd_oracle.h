@@ -16,15 +16,15 @@ extern "C" {
 
 typedef struct {
   int dissipation_type, is_second_order, time_accurate, local_time_stepping, integrator, limiter,
-      reconstruct_primitive, inlet_bc, exit_bc;
+      reconstruct_primitive, muscl, inlet_bc, exit_bc;
   double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas;
 } orc_config;
 
 typedef struct orc_state orc_state;
 
 orc_state *orc_create(int NP, int NG, const int *nf, const int *nbr, const double *normals, const double *lengths,
-                      const double *ccd, const double *area, const double *inv_area, int NB, const int *bnd,
-                      const orc_config *cfg);
+                      const double *ccd, const double *cvec, const double *area, const double *inv_area, int NB,
+                      const int *bnd, const orc_config *cfg);
 void orc_destroy(orc_state *s);
 void orc_set_state(orc_state *s, const double *U, int n);
 void orc_apply_bc(orc_state *s);

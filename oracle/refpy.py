@@ -181,7 +181,7 @@ class RefRun:
 class _OrcConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ["dissipation_type", "is_second_order", "time_accurate",
                                             "local_time_stepping", "integrator", "limiter", "reconstruct_primitive",
-                                            "inlet_bc", "exit_bc"]] + \
+                                            "muscl", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
                                                "exit_p", "r_gas"]]
 
@@ -196,8 +196,8 @@ def oraclelib():
             build_oracle()
         L = ctypes.CDLL(ORACLE_LIB)
         L.orc_create.restype = ctypes.c_void_p
-        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _IP, _IP, _DP, _DP, _DP, _DP, _DP, ctypes.c_int, _IP,
-                                 ctypes.POINTER(_OrcConfig)]
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _IP, _IP, _DP, _DP, _DP, _DP, _DP, _DP, ctypes.c_int,
+                                 _IP, ctypes.POINTER(_OrcConfig)]
         L.orc_destroy.argtypes = [ctypes.c_void_p]
         L.orc_set_state.argtypes = [ctypes.c_void_p, _DP, ctypes.c_int]
         for n in ["orc_apply_bc", "orc_net_flux", "orc_rk", "orc_estimate_error", "orc_update"]:
@@ -231,6 +231,7 @@ class OracleRun:
         c.integrator = params.get("integrator", 0)
         c.limiter = params.get("limiter", 0)
         c.reconstruct_primitive = params.get("reconstruct_primitive", 0)
+        c.muscl = params.get("muscl", 0)
         c.inlet_bc = params.get("inlet_bc", 0)
         c.exit_bc = params.get("exit_bc", 0)
         c.cfl = params.get("cfl", 0.5)
@@ -245,10 +246,11 @@ class OracleRun:
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,
-            mesh.center_distances, mesh.area, mesh.inv_area, mesh.boundary.astype(np.int32).reshape(-1))]
+            mesh.center_distances, mesh.center_vectors, mesh.area, mesh.inv_area,
+            mesh.boundary.astype(np.int32).reshape(-1))]
         k = self._keep
         self.h = L.orc_create(mesh.n_physical, mesh.n_ghost, _ip(k[0]), _ip(k[1]), _dp(k[2]), _dp(k[3]), _dp(k[4]),
-                              _dp(k[5]), _dp(k[6]), mesh.boundary.shape[0], _ip(k[7]), ctypes.byref(c))
+                              _dp(k[5]), _dp(k[6]), _dp(k[7]), mesh.boundary.shape[0], _ip(k[8]), ctypes.byref(c))
         self.L = L
         self.NP, self.NT = mesh.n_physical, mesh.n_total
 

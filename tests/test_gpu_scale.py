@@ -21,7 +21,7 @@ def c2_setup(**over):
     full[:NP] = U
     full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
     kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
-              limiter=cb.LIM_VANLEER, reconstruct_primitive=1, inlet_rho=rho, inlet_p=p)
+              limiter=cb.LIM_VANLEER, muscl=cb.MUSCL_GRADIENT, integrator=cb.INT_SSPRK3, inlet_rho=rho, inlet_p=p)
     kw.update(over)
     return m, full, kw
 
