@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "cfd_b200.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(cfd_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(cfd_[A-Za-z0-9_]+)\s*\(", text)))
 
 
 def test_every_declared_symbol_is_exported():
