@@ -57,6 +57,14 @@ class Config(ctypes.Structure):
                 ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
 
 
+class FluxArrays(ctypes.Structure):
+    """cfd_flux_arrays: device pointers (integers) of one net-flux evaluation."""
+    _fields_ = [("n_physical", ctypes.c_int), ("n_total", ctypes.c_int)] + \
+               [(n, ctypes.c_void_p) for n in ("n_faces", "neighbours", "nx", "ny", "dl", "area", "inv_area",
+                                                "second_neighbours", "d1", "d2", "degenerate", "prim", "U",
+                                                "net_flux", "dt", "min_dt")]
+
+
 class StepInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("min_dt", ctypes.c_double), ("total_time", ctypes.c_double),
                 ("error", ctypes.c_double * 4), ("res_l2", ctypes.c_double * 4), ("bad_cell", ctypes.c_int),
@@ -103,6 +111,7 @@ SIGNATURES = {
     "cfd_gradient": (_I, [_P, _I, _DP]),
     "cfd_amr_tags": (_I, [_P, _D, _D, _DP, ctypes.POINTER(ctypes.c_uint8)]),
     "cfd_kernel_time": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_longlong)]),
+    "cfd_evaluate_net_flux_noalloc": (_I, [ctypes.POINTER(FluxArrays), ctypes.POINTER(Config), _P]),
     "cfd_kernel_launches": (ctypes.c_longlong, [_P]),
     "cfd_device_bytes": (ctypes.c_size_t, [_P]),
 }

@@ -19,12 +19,18 @@
 
 namespace cfdb {
 std::string config_from_json(const std::string &text, cfd_config *cfg);
+void set_last_error(const std::string &msg);
 }
 
 using namespace cfdb;
 
 namespace {
 std::string g_err;  // last error message (per process)
+}  // namespace
+
+void cfdb::set_last_error(const std::string &msg) { g_err = msg; }
+
+namespace {
 
 cfd_status fail(cfd_status s, const std::string &msg) {
   g_err = msg;

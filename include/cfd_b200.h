@@ -198,6 +198,37 @@ cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad);
  * src/Grid_Refine_Functions.cpp:8-63).  Either output may be NULL. */
 cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags);
 
+/* Device arrays of one net-flux evaluation, in the device layout this library uses internally
+ * (no renumbering): face-major [4][NP] per-face arrays, component-major state planes. */
+typedef struct {
+  int n_physical;                 /* NP */
+  int n_total;                    /* NP + NG */
+  const int *n_faces;             /* [NP] */
+  const int *neighbours;          /* [4][NP] neighbour or ghost id of face f of cell c at f*NP+c */
+  const double *nx, *ny, *dl;     /* [4][NP] face normal and length */
+  const double *area, *inv_area;  /* [NP] */
+  const int *second_neighbours;   /* [4][NP] limiter stencil N2 of src/Limiters.cpp:136-191 (2nd order) */
+  const double *d1, *d2;          /* [4][NP] limiter distances d1, d2 (2nd order) */
+  const uint8_t *degenerate;      /* [NP] bit f set when |n_f| < 1e-12 */
+  const double *prim;             /* [5][NT] rho, u, v, p, a */
+  const double *U;                /* [4][NT] U_Cells */
+  double *net_flux;               /* out [4][NP] Cells_Net_Flux */
+  double *dt;                     /* out [NP] Cell::del_t */
+  double *min_dt;                 /* out [1] Min_dt */
+} cfd_flux_arrays;
+
+/* Evaluate_Cell_Net_Flux + del_t + Min_dt on caller-owned device arrays WITHOUT allocating
+ * device memory.  No counterpart in the reference: it exists for callers that cannot let this
+ * library call cudaMalloc (their own pool allocator owns the device memory, or their loop may not
+ * take cudaMalloc's device synchronisation).  The kernel's scratch (control block, completion
+ * counter, one partial minimum per thread block) is a fixed static device array of 65,560 doubles
+ * (512 KiB) per GPU, held until the process exits; at most 8,388,608 physical cells per call (larger sizes
+ * are rejected with CFD_ERR_BAD_ARG).  The first call on a device resolves the array's device
+ * address, so make that first call before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU (different streams, other threads) race.  Reference MUSCL stencil, FP64,
+ * ROE or first-order LLF only.  stream: cudaStream_t (NULL = default stream). */
+cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_config *cfg, void *stream);
+
 /* Accumulated device time of one kernel family ("flux", "stage", "bc") over the launches made
  * while option "profile" was set (CUDA events on the context's stream around each launch). */
 cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches);
