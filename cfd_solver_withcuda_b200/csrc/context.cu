@@ -397,7 +397,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
-  if (cfg->precision != CFD_PREC_FP64) return fail(CFD_ERR_BAD_ARG, "precision form not available in this build");
+  if (cfg->precision != CFD_PREC_FP64 && !(cfg->precision == CFD_PREC_FP32_FLUX && cfg->muscl && cfg->is_second_order))
+    return fail(CFD_ERR_BAD_ARG, "the FP32-flux form is available for the gradient-MUSCL scheme only");
 
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CFD_ERR_NO_DEVICE, "no CUDA device");
@@ -486,6 +487,63 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       }
     }
   }
+  // Unique faces of the face-based (gradient MUSCL) form, numbered in reference order: a face
+  // belongs to the lower-numbered of its two cells, a boundary face to its physical cell; its
+  // geometry is the owner's.  Faces are stored sorted by owner in device order.
+  std::vector<int> fo, fn, cface;
+  std::vector<double> fnx, fny, fdl, fdx, fdy;
+  if (cfg->muscl && cfg->is_second_order) {
+    std::vector<int> ref_owner, ref_face;
+    std::vector<int> slot_face(4 * (size_t)NP, 0);  // reference cell-major: face id or -(id+1)
+    for (int r = 0; r < NP; r++)
+      for (int f = 0; f < d->n_faces[r]; f++) {
+        const int N = d->neighbours[4 * r + f];
+        if (N < NP && N < r) continue;
+        const int id = static_cast<int>(ref_owner.size());
+        ref_owner.push_back(r);
+        ref_face.push_back(f);
+        slot_face[4 * r + f] = id;
+        if (N < NP) {
+          int g = -1;
+          for (int k = 0; k < d->n_faces[N]; k++)
+            if (d->neighbours[4 * N + k] == r) g = k;
+          if (g < 0) return bail(fail(CFD_ERR_MESH, "non-conforming face between cells " + std::to_string(r) + " and " +
+                                                        std::to_string(N)));
+          slot_face[4 * N + g] = -(id + 1);
+        }
+      }
+    const int NF = static_cast<int>(ref_owner.size());
+    std::vector<int> order(NF);
+    for (int i = 0; i < NF; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ctx->inv[ref_owner[a]] < ctx->inv[ref_owner[b]]; });
+    std::vector<int> pos(NF);
+    for (int i = 0; i < NF; i++) pos[order[i]] = i;
+    fo.resize(NF);
+    fn.resize(NF);
+    fnx.resize(NF);
+    fny.resize(NF);
+    fdl.resize(NF);
+    fdx.resize(NF);
+    fdy.resize(NF);
+    for (int i = 0; i < NF; i++) {
+      const int id = order[i], r = ref_owner[id], f = ref_face[id];
+      fo[i] = ctx->inv[r];
+      fn[i] = dev_of(ctx, d->neighbours[4 * r + f]);
+      fnx[i] = d->face_normals[8 * r + 2 * f];
+      fny[i] = d->face_normals[8 * r + 2 * f + 1];
+      fdl[i] = d->face_lengths[4 * r + f];
+      fdx[i] = d->center_vectors[8 * r + 2 * f];
+      fdy[i] = d->center_vectors[8 * r + 2 * f + 1];
+    }
+    cface.assign(4 * (size_t)NP, 0);
+    for (int i = 0; i < NP; i++) {
+      const int r = ctx->perm[i];
+      for (int f = 0; f < d->n_faces[r]; f++) {
+        const int e = slot_face[4 * r + f];
+        cface[(size_t)f * NP + i] = e >= 0 ? pos[e] : -(pos[-e - 1] + 1);
+      }
+    }
+  }
   std::vector<int4> bnd(NB);
   for (int e = 0; e < NB; e++) {
     const int *b = d->boundary + 4 * e;
@@ -511,6 +569,17 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvx), cvx)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvy), cvy)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.bnd), bnd)) != CFD_OK) return bail(s);
+  m.NF = static_cast<int>(fo.size());
+  if (m.NF > 0) {
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.fo), fo)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.fn), fn)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&m.fnx), fnx)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&m.fny), fny)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdl), fdl)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdx), fdx)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdy), fdy)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.cface), cface)) != CFD_OK) return bail(s);
+  }
 
   DevState &st = ctx->ds;
   const size_t dsz = sizeof(double);
@@ -527,6 +596,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   }
   if (cfg->muscl) {
     if ((s = ctx_alloc(ctx, (void **)&st.grad, 8 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+  }
+  if (m.NF > 0) {
+    if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)nblk * dsz)) != CFD_OK) return bail(s);
@@ -549,6 +621,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.limiter = cfg->limiter;
   fp.recon_prim = cfg->reconstruct_primitive;
   fp.muscl = cfg->muscl && cfg->is_second_order;
+  fp.lanes = 1;
   fp.consistent = (cfg->integrator != CFD_INT_REFERENCE) ? 1 : 0;
   fp.precision = cfg->precision;
   fp.cfl = cfg->cfl;
@@ -574,6 +647,10 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   std::string n(name);
   if (n == "keep_delu") ctx->keep_delu = value != 0.0;
   else if (n == "use_graph") ctx->use_graph = value != 0.0;
+  else if (n == "flux_lanes") {
+    if (value != 1.0 && value != 4.0) return fail(CFD_ERR_BAD_ARG, "flux_lanes must be 1 or 4");
+    ctx->fp.lanes = static_cast<int>(value);
+  }
   else if (n == "profile") ctx->profile = value != 0.0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   if (ctx->graph) {

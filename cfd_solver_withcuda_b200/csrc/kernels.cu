@@ -15,6 +15,7 @@ namespace cfdb {
 namespace {
 
 constexpr int kFluxBlock = 128;
+constexpr int kFlux4Block = 128;  // 32 cells x 4 face lanes
 constexpr int kBlock = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -209,141 +210,145 @@ struct USrc {
   }
 };
 
-// Evaluate_Cell_Net_Flux_1O/2O (src/Net_Flux.cpp:46-129) + Evaluate_Time_Step (src/Time_Step.cpp:293-359)
-// fused: per cell, faces in order, Net += avg - diss; then dt = CFL*A / sum(|V.n|+a)dl.  The block
-// min of dt goes to `partial`; the last block writes Min_dt (get_Min_dt, src/Numerical_Method.cpp:322).
+// The state of the cell whose faces are being evaluated.
+struct CellState {
+  double rc, uc, vc, pc, ac;
+  double Uc[4];
+  double gc[8];
+  uint8_t degen;
+};
+
 template <int DISS, int ORDER>
-__global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
-  __shared__ double sh[32];
-  const int NP = m.NP, NT = m.NT;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool done = step_done(st.ctl);
-  double dt = 1e308 * 10.0;
-  if (c < NP && !done) {
-    const double *prim = st.prim;
-    const double rc = prim[c], uc = prim[NT + c], vc = prim[2 * NT + c], pc = prim[3 * NT + c], ac = prim[4 * NT + c];
-    const USrc us{st.U, st.S, NT, NP, fp.consistent && src_is_S};
-    double Uc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (DISS == 1 || ORDER == 2) {
+__device__ __forceinline__ void load_cell(const DevMesh &m, const DevState &st, const USrc &us, int c, CellState &q) {
+  const int NT = m.NT, NP = m.NP;
+  const double *prim = st.prim;
+  q.rc = prim[c];
+  q.uc = prim[NT + c];
+  q.vc = prim[2 * NT + c];
+  q.pc = prim[3 * NT + c];
+  q.ac = prim[4 * NT + c];
+  if (DISS == 1 || ORDER == 2) {
 #pragma unroll
-      for (int k = 0; k < 4; k++) Uc[k] = us.get(k, c);
-    }
-    const int nf = m.nf[c];
-    const uint8_t degen = m.degen[c];
-    double gc[8];
-    const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
-    if (ORDER == 3) {
-#pragma unroll
-      for (int k = 0; k < 8; k++) gc[k] = st.grad[k * NP + c];
-    }
-    double N0 = 0.0, N1s = 0.0, N2s = 0.0, N3s = 0.0;
-    double den = 0.0;
-#pragma unroll
-    for (int f = 0; f < 4; f++) {
-      if (f < nf) {
-        const int idx = f * NP + c;
-        const int N = m.nbr[idx];
-        const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
-        const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
-        double A[4], D[4];
-        if (ORDER != 3) average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
-        if (DISS == 3 && ORDER == 1) {
-          if (N >= NP)
-            roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (degen >> f) & 1, D);
-          else
-            roe_1o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, (degen >> f) & 1, D);
-        } else if (DISS == 3 && ORDER == 2) {
-          const int n2 = m.n2[idx];
-          const double d1 = m.d1l[idx], d2 = m.d2l[idx];
-          double dU[4];
-          if (!fp.recon_prim) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              const double q1 = us.get(k, N), q2 = us.get(k, n2);
-              const double phi = limited_slope<double>(fp.limiter, Uc[k], q1, q2, d1, d2, fp.zeta, fp.zeta1);
-              const double VR = q1 + 0.5 * phi * d1;
-              const double VL = Uc[k] - 0.5 * phi * d1;
-              dU[k] = VR - VL;
-            }
-          } else {
-            // MUSCL on (rho, u, v, p) of the stage primitives; the conserved jump of the two
-            // reconstructed face states drives the Roe wave strengths.
-            const double qc[4] = {rc, uc, vc, pc};
-            const double q1v[4] = {rn, un, vn, pn};
-            const double q2v[4] = {prim[n2], prim[NT + n2], prim[2 * NT + n2], prim[3 * NT + n2]};
-            double qR[4], qL[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              const double phi = limited_slope<double>(fp.limiter, qc[k], q1v[k], q2v[k], d1, d2, fp.zeta, fp.zeta1);
-              qR[k] = q1v[k] + 0.5 * phi * d1;
-              qL[k] = qc[k] - 0.5 * phi * d1;
-            }
-            dU[0] = qR[0] - qL[0];
-            dU[1] = qR[0] * qR[1] - qL[0] * qL[1];
-            dU[2] = qR[0] * qR[2] - qL[0] * qL[2];
-            dU[3] = (qR[3] / kGM1 + 0.5 * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])) -
-                    (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
-          }
-          roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
-        } else if (DISS == 3 && ORDER == 3) {
-          // Green-Gauss-gradient MUSCL on (rho, u, v, p) (no reference counterpart; the
-          // reference's second-order form is the ORDER == 2 branch).  With d = x_N - x_c and
-          // D+ = q_N - q_c, the upwind differences are D-_c = 2 grad q_c . d - D+ and
-          // D-_N = 2 grad q_N . d - D+; q_L = q_c + 0.5 phi(D-_c, D+) D+,
-          // q_R = q_N - 0.5 phi(D-_N, D+) D+ (phi(a, b) with r = a/b).  A ghost neighbour uses
-          // the cell's own gradient.  A non-positive reconstructed density or pressure falls
-          // back to the cell-centre state.  Flux: average of the two face states plus Roe
-          // dissipation between them.
-          const double dx = m.cvx[idx], dy = m.cvy[idx];
-          const double *gN = (N < NP) ? st.grad : nullptr;
-          const double qc[4] = {rc, uc, vc, pc};
-          const double qn[4] = {rn, un, vn, pn};
-          double qL[4], qR[4];
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const double gx = gc[2 * k], gy = gc[2 * k + 1];
-            const double nxg = gN ? gN[(2 * k) * NP + N] : gx, nyg = gN ? gN[(2 * k + 1) * NP + N] : gy;
-            const double dp = qn[k] - qc[k];
-            const double dmc = 2.0 * (gx * dx + gy * dy) - dp;
-            const double dmn = 2.0 * (nxg * dx + nyg * dy) - dp;
-            qL[k] = qc[k] + 0.5 * phi_ab<double>(glim, dmc, dp) * dp;
-            qR[k] = qn[k] - 0.5 * phi_ab<double>(glim, dmn, dp) * dp;
-          }
-          if (!(qL[0] > 0.0) || !(qL[3] > 0.0)) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) qL[k] = qc[k];
-          }
-          if (!(qR[0] > 0.0) || !(qR[3] > 0.0)) {
-#pragma unroll
-            for (int k = 0; k < 4; k++) qR[k] = qn[k];
-          }
-          const double aL = sqrt(kGamma * qL[3] / qL[0]), aR = sqrt(kGamma * qR[3] / qR[0]);
-          average_flux<double>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
-          roe_1o<double>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
-        } else {  // LLF 1O
-          double UR[4];
-#pragma unroll
-          for (int k = 0; k < 4; k++) UR[k] = us.get(k, N);
-          llf_1o<double>(uc, vc, ac, un, vn, an, Uc, UR, nx, ny, dl, D);
-        }
-        N0 += A[0] - D[0];
-        N1s += A[1] - D[1];
-        N2s += A[2] - D[2];
-        N3s += A[3] - D[3];
-        const double vnf = uc * nx + vc * ny;
-        den += (fabs(vnf) + ac) * dl;
-      }
-    }
-    if (den <= 0.0 || !isfinite(den)) dt = 0.0;
-    else dt = fp.cfl * m.area[c] / den;
-    st.R[c] = N0;
-    st.R[NP + c] = N1s;
-    st.R[2 * NP + c] = N2s;
-    st.R[3 * NP + c] = N3s;
-    st.dtc[c] = dt;
+    for (int k = 0; k < 4; k++) q.Uc[k] = us.get(k, c);
   }
+  if (ORDER == 3) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) q.gc[k] = st.grad[k * NP + c];
+  }
+  q.degen = m.degen[c];
+}
+
+// Contribution of face f of cell c: X = avg - diss (Calculate_Flux_For_All_Faces,
+// src/Net_Flux.cpp:18-43) and the del_t term (|V.n| + a) dl (src/Time_Step.cpp:326-336).
+template <int DISS, int ORDER>
+__device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &st, const FluxParams &fp,
+                                             const USrc &us, const CellState &q, int c, int f, double X[4],
+                                             double &t) {
+  const int NP = m.NP, NT = m.NT;
+  const double *prim = st.prim;
+  const double rc = q.rc, uc = q.uc, vc = q.vc, pc = q.pc, ac = q.ac;
+  const int idx = f * NP + c;
+  const int N = m.nbr[idx];
+  const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
+  const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
+  double A[4], D[4];
+  if (ORDER != 3) average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
+  if (DISS == 3 && ORDER == 1) {
+    if (N >= NP)
+      roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (q.degen >> f) & 1, D);
+    else
+      roe_1o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, (q.degen >> f) & 1, D);
+  } else if (DISS == 3 && ORDER == 2) {
+    const int n2 = m.n2[idx];
+    const double d1 = m.d1l[idx], d2 = m.d2l[idx];
+    double dU[4];
+    if (!fp.recon_prim) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const double q1 = us.get(k, N), q2 = us.get(k, n2);
+        const double phi = limited_slope<double>(fp.limiter, q.Uc[k], q1, q2, d1, d2, fp.zeta, fp.zeta1);
+        const double VR = q1 + 0.5 * phi * d1;
+        const double VL = q.Uc[k] - 0.5 * phi * d1;
+        dU[k] = VR - VL;
+      }
+    } else {
+      // MUSCL on (rho, u, v, p) of the stage primitives on the reference stencil; the
+      // conserved jump of the two reconstructed face states drives the Roe wave strengths.
+      const double qc[4] = {rc, uc, vc, pc};
+      const double q1v[4] = {rn, un, vn, pn};
+      const double q2v[4] = {prim[n2], prim[NT + n2], prim[2 * NT + n2], prim[3 * NT + n2]};
+      double qR[4], qL[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const double phi = limited_slope<double>(fp.limiter, qc[k], q1v[k], q2v[k], d1, d2, fp.zeta, fp.zeta1);
+        qR[k] = q1v[k] + 0.5 * phi * d1;
+        qL[k] = qc[k] - 0.5 * phi * d1;
+      }
+      dU[0] = qR[0] - qL[0];
+      dU[1] = qR[0] * qR[1] - qL[0] * qL[1];
+      dU[2] = qR[0] * qR[2] - qL[0] * qL[2];
+      dU[3] = (qR[3] / kGM1 + 0.5 * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])) -
+              (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
+    }
+    roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
+  } else if (DISS == 3 && ORDER == 3) {
+    // Green-Gauss-gradient MUSCL on (rho, u, v, p) (no reference counterpart; the reference's
+    // second-order form is the ORDER == 2 branch).  With d = x_N - x_c and D+ = q_N - q_c, the
+    // upwind differences are D-_c = 2 grad q_c . d - D+ and D-_N = 2 grad q_N . d - D+;
+    // q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+ (phi(a, b), r = a/b).
+    // A ghost neighbour uses the cell's own gradient.  A non-positive reconstructed density or
+    // pressure falls back to the cell-centre state.  Flux: average of the two face states plus
+    // Roe dissipation between them.
+    const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+    const double dx = m.cvx[idx], dy = m.cvy[idx];
+    const double *gN = (N < NP) ? st.grad : nullptr;
+    const double qc[4] = {rc, uc, vc, pc};
+    const double qn[4] = {rn, un, vn, pn};
+    double qL[4], qR[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double gx = q.gc[2 * k], gy = q.gc[2 * k + 1];
+      const double nxg = gN ? gN[(2 * k) * NP + N] : gx, nyg = gN ? gN[(2 * k + 1) * NP + N] : gy;
+      const double dp = qn[k] - qc[k];
+      const double dmc = 2.0 * (gx * dx + gy * dy) - dp;
+      const double dmn = 2.0 * (nxg * dx + nyg * dy) - dp;
+      qL[k] = qc[k] + 0.5 * phi_ab<double>(glim, dmc, dp) * dp;
+      qR[k] = qn[k] - 0.5 * phi_ab<double>(glim, dmn, dp) * dp;
+    }
+    if (!(qL[0] > 0.0) || !(qL[3] > 0.0)) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) qL[k] = qc[k];
+    }
+    if (!(qR[0] > 0.0) || !(qR[3] > 0.0)) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) qR[k] = qn[k];
+    }
+    const double aL = sqrt(kGamma * qL[3] / qL[0]), aR = sqrt(kGamma * qR[3] / qR[0]);
+    average_flux<double>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
+    roe_1o<double>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
+  } else {  // LLF 1O
+    double UR[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) UR[k] = us.get(k, N);
+    llf_1o<double>(uc, vc, ac, un, vn, an, q.Uc, UR, nx, ny, dl, D);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) X[k] = A[k] - D[k];
+  const double vnf = uc * nx + vc * ny;
+  t = (fabs(vnf) + ac) * dl;
+}
+
+// del_t = CFL * Area / sum (|V.n| + a) dl, 0 when the sum is not a positive finite number
+// (Inviscid_Time_Step, src/Time_Step.cpp:337-358).
+__device__ __forceinline__ double cell_dt(const DevMesh &m, const FluxParams &fp, int c, double den) {
+  if (den <= 0.0 || !isfinite(den)) return 0.0;
+  return fp.cfl * m.area[c] / den;
+}
+
+// Block min of del_t to `partial`; the last block writes Min_dt (get_Min_dt,
+// src/Numerical_Method.cpp:322-330).
+__device__ __forceinline__ void min_dt_epilogue(DevState &st, double dt, double *sh) {
   double bm = block_min(dt, sh);
-  if (done) return;
   if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
   if (last_block(st.counter)) {
     double v = 1e308 * 10.0;
@@ -357,6 +362,186 @@ __global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, Flu
       *st.counter = 0u;
     }
   }
+}
+
+// Evaluate_Cell_Net_Flux_1O/2O (src/Net_Flux.cpp:46-129) + Evaluate_Time_Step (src/Time_Step.cpp:293-359)
+// fused, one thread per cell: faces in order, Net += avg - diss; then del_t; block min + Min_dt.
+template <int DISS, int ORDER>
+__global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
+  __shared__ double sh[32];
+  const int NP = m.NP, NT = m.NT;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool done = step_done(st.ctl);
+  double dt = 1e308 * 10.0;
+  if (c < NP && !done) {
+    const USrc us{st.U, st.S, NT, NP, fp.consistent && src_is_S};
+    CellState q;
+    load_cell<DISS, ORDER>(m, st, us, c, q);
+    const int nf = m.nf[c];
+    double N0 = 0.0, N1s = 0.0, N2s = 0.0, N3s = 0.0;
+    double den = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      if (f < nf) {
+        double X[4], t;
+        face_contrib<DISS, ORDER>(m, st, fp, us, q, c, f, X, t);
+        N0 += X[0];
+        N1s += X[1];
+        N2s += X[2];
+        N3s += X[3];
+        den += t;
+      }
+    }
+    dt = cell_dt(m, fp, c, den);
+    st.R[c] = N0;
+    st.R[NP + c] = N1s;
+    st.R[2 * NP + c] = N2s;
+    st.R[3 * NP + c] = N3s;
+    st.dtc[c] = dt;
+  }
+  if (done) return;
+  min_dt_epilogue(st, dt, sh);
+}
+
+// The same evaluation with four lanes per cell (one face each): lane 0 of each quad adds the
+// quad's face contributions in face order 0..nF-1 (warp shuffles), so every sum keeps the
+// reference's order and value; fewer live registers per thread give the SM more warps to hide
+// the gather and FP64 latencies.
+template <int DISS, int ORDER>
+__global__ void __launch_bounds__(kFlux4Block) k_flux4(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
+  __shared__ double sh[32];
+  const int NP = m.NP, NT = m.NT;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = gid >> 2, f = gid & 3;
+  const bool done = step_done(st.ctl);
+  if (done) return;
+  const bool cell_ok = c < NP;
+  const int nf = cell_ok ? m.nf[c] : 0;
+  double X[4] = {0.0, 0.0, 0.0, 0.0}, t = 0.0;
+  if (f < nf) {
+    const USrc us{st.U, st.S, NT, NP, fp.consistent && src_is_S};
+    CellState q;
+    load_cell<DISS, ORDER>(m, st, us, c, q);
+    face_contrib<DISS, ORDER>(m, st, fp, us, q, c, f, X, t);
+  }
+  double Y[3][4], T[3];
+#pragma unroll
+  for (int d = 1; d < 4; d++) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) Y[d - 1][k] = __shfl_down_sync(kFull, X[k], d, 4);
+    T[d - 1] = __shfl_down_sync(kFull, t, d, 4);
+  }
+  double dt = 1e308 * 10.0;
+  if (cell_ok && f == 0) {
+    double R[4] = {0.0, 0.0, 0.0, 0.0};
+    double den = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) R[k] += X[k];
+    den += t;
+#pragma unroll
+    for (int d = 1; d < 4; d++) {
+      if (d < nf) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) R[k] += Y[d - 1][k];
+        den += T[d - 1];
+      }
+    }
+    dt = cell_dt(m, fp, c, den);
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
+    st.dtc[c] = dt;
+  }
+  min_dt_epilogue(st, dt, sh);
+}
+
+// Face-based evaluation (the Green-Gauss-gradient MUSCL form; no reference counterpart): one
+// thread per unique face computes the flux once from its owner's side, in precision T (double,
+// or float for the FP32-flux form); the neighbour receives exactly the negated flux, so the
+// scheme is conservative to the last bit.  Reconstruction as in face_contrib's ORDER == 3 branch.
+template <typename T>
+__global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParams fp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.NF || step_done(st.ctl)) return;
+  const int NP = m.NP, NT = m.NT;
+  const int c = m.fo[i], N = m.fn[i];
+  const double *prim = st.prim;
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+  const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
+  T qc[4], qn[4], qL[4], qR[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    qc[k] = T(prim[k * NT + c]);
+    qn[k] = T(prim[k * NT + N]);
+  }
+  const bool nphys = N < NP;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const T gx = T(st.grad[(2 * k) * NP + c]), gy = T(st.grad[(2 * k + 1) * NP + c]);
+    const T hx = nphys ? T(st.grad[(2 * k) * NP + N]) : gx, hy = nphys ? T(st.grad[(2 * k + 1) * NP + N]) : gy;
+    const T dp = qn[k] - qc[k];
+    const T dmc = T(2.0) * (gx * dx + gy * dy) - dp;
+    const T dmn = T(2.0) * (hx * dx + hy * dy) - dp;
+    qL[k] = qc[k] + T(0.5) * phi_ab<T>(glim, dmc, dp) * dp;
+    qR[k] = qn[k] - T(0.5) * phi_ab<T>(glim, dmn, dp) * dp;
+  }
+  if (!(qL[0] > T(0.0)) || !(qL[3] > T(0.0))) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) qL[k] = qc[k];
+  }
+  if (!(qR[0] > T(0.0)) || !(qR[3] > T(0.0))) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) qR[k] = qn[k];
+  }
+  const T aL = sqrt(T(kGamma) * qL[3] / qL[0]), aR = sqrt(T(kGamma) * qR[3] / qR[0]);
+  T A[4], D[4];
+  average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
+  roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
+  const int NF = m.NF;
+#pragma unroll
+  for (int k = 0; k < 4; k++) st.F[k * NF + i] = double(A[k] - D[k]);
+}
+
+// Per cell: Net = sum of its face fluxes in face order (+F on the owner side, -F on the
+// neighbour side), del_t from the cell's own state (src/Time_Step.cpp:293-329), block min.
+__global__ void __launch_bounds__(kFluxBlock) k_gather(DevMesh m, DevState st, FluxParams fp) {
+  __shared__ double sh[32];
+  const int NP = m.NP, NT = m.NT, NF = m.NF;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool done = step_done(st.ctl);
+  double dt = 1e308 * 10.0;
+  if (c < NP && !done) {
+    const double uc = st.prim[NT + c], vc = st.prim[2 * NT + c], ac = st.prim[4 * NT + c];
+    const int nf = m.nf[c];
+    double R0 = 0.0, R1 = 0.0, R2 = 0.0, R3 = 0.0, den = 0.0;
+    for (int f = 0; f < nf; f++) {
+      const int idx = f * NP + c;
+      const int e = m.cface[idx];
+      const bool neg = e < 0;
+      const int id = neg ? -e - 1 : e;
+      const double F0 = st.F[id], F1 = st.F[NF + id], F2 = st.F[2 * NF + id], F3 = st.F[3 * NF + id];
+      if (neg) {
+        R0 += -F0;
+        R1 += -F1;
+        R2 += -F2;
+        R3 += -F3;
+      } else {
+        R0 += F0;
+        R1 += F1;
+        R2 += F2;
+        R3 += F3;
+      }
+      const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
+      den += (fabs(vnf) + ac) * m.dl[idx];
+    }
+    dt = cell_dt(m, fp, c, den);
+    st.R[c] = R0;
+    st.R[NP + c] = R1;
+    st.R[2 * NP + c] = R2;
+    st.R[3 * NP + c] = R3;
+    st.dtc[c] = dt;
+  }
+  if (done) return;
+  min_dt_epilogue(st, dt, sh);
 }
 
 // Estimate_Error (src/Error_Estimate_Update.cpp:10-28) terms of one cell; dU < 1e-9 is the
@@ -630,7 +815,11 @@ inline int nblk(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
 
-int flux_block_count(int NP) { return nblk(NP, kFluxBlock) > nblk(NP, kBlock) ? nblk(NP, kFluxBlock) : nblk(NP, kBlock); }
+// Upper bound on the thread blocks of any flux-kernel variant (sizes the partial-min buffer).
+int flux_block_count(int NP) {
+  int a = nblk(NP, kFluxBlock), b = nblk(4 * NP, kFlux4Block), c = nblk(NP, kBlock);
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
 
 int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st) {
   k_prim_all<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
@@ -644,15 +833,28 @@ int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp
 }
 
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
-  const int g = nblk(m.NP, kFluxBlock);
-  if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-  else if (fp.dissipation == 3 && fp.muscl) {
-    launch_muscl_gradients(s, m, st);
-    k_flux<3, 3><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    return 2;
-  } else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-  else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-  return 1;
+  int n = 0;
+  if (fp.dissipation == 3 && fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st);
+  if (fp.dissipation == 3 && fp.second_order && fp.muscl && m.NF > 0) {
+    if (fp.precision == 1) k_faces<float><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+    else k_faces<double><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+    k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
+    return n + 2;
+  }
+  if (fp.lanes == 1) {
+    const int g = nblk(m.NP, kFluxBlock);
+    if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3 && fp.muscl) k_flux<3, 3><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  } else {
+    const int g = nblk(4 * m.NP, kFlux4Block);
+    if (fp.dissipation == 3 && !fp.second_order) k_flux4<3, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3 && fp.muscl) k_flux4<3, 3><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3) k_flux4<3, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else k_flux4<1, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+  }
+  return n + 1;
 }
 
 int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu) {

@@ -24,6 +24,12 @@ struct DevMesh {
   const double *cvx, *cvy;  // [4][NP] centre-to-centre vectors (gradient MUSCL)
   const uint8_t *degen;
   const int4 *bnd;  // kind, cell, face, ghost
+  // Unique faces (face-based forms): owner and neighbour cell, owner-side geometry, and for each
+  // cell slot the face id (owner side) or -(id + 1) (neighbour side).
+  int NF;
+  const int *fo, *fn;
+  const double *fnx, *fny, *fdl, *fdx, *fdy;
+  const int *cface;  // [4][NP]
 };
 
 struct DevState {
@@ -36,6 +42,7 @@ struct DevState {
   double *dtk;   // [NP] dt kept for the whole step (RK4 / SSP with LTS)
   double *dU;    // [4][NP]
   double *grad;  // [8][NP] Green-Gauss gradients of (rho, u, v, p) (gradient MUSCL)
+  double *F;     // [4][NF] face fluxes (face-based forms)
   // reduction / control block (see CtrlIdx)
   double *ctl;
   double *partial;     // [nblk_max * 9]
@@ -62,6 +69,7 @@ struct FluxParams {
   int limiter;
   int recon_prim;
   int muscl;            // 0 reference stencil, 1 Green-Gauss-gradient MUSCL
+  int lanes;            // threads per cell in the flux kernel: 1 or 4
   int consistent;       // 1: limiter/LLF/exit read the stage state instead of U^n
   int precision;
   double cfl, zeta, zeta1;

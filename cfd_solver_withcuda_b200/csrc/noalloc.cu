@@ -17,7 +17,8 @@
 
 namespace {
 
-constexpr int kMaxBlocks = 65536;  // partial-minimum slots: one per flux-kernel thread block
+constexpr int kMaxCells = 8388608;   // largest mesh (physical cells) one call accepts
+constexpr int kMaxBlocks = 262144;   // partial-minimum slots: one per flux-kernel thread block
 constexpr int kCtlDoubles = cfdb::CTL_SIZE;
 constexpr int kCounterDoubles = 8;  // completion counter (unsigned) + status words (2 x int)
 constexpr int kScratchDoubles = kCtlDoubles + kCounterDoubles + kMaxBlocks;
@@ -46,10 +47,9 @@ extern "C" cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, co
   if (!a || !cfg) return noalloc_fail(CFD_ERR_BAD_ARG, "null argument");
   const int NP = a->n_physical, NT = a->n_total;
   if (NP <= 0 || NT < NP) return noalloc_fail(CFD_ERR_BAD_ARG, "bad sizes");
-  if (cfdb::flux_block_count(NP) > kMaxBlocks)
-    return noalloc_fail(CFD_ERR_BAD_ARG, "cfd_evaluate_net_flux_noalloc handles at most " +
-                                             std::to_string(kMaxBlocks) + " thread blocks (" +
-                                             std::to_string(kMaxBlocks * 128) + " cells); got " + std::to_string(NP));
+  if (NP > kMaxCells || cfdb::flux_block_count(NP) > kMaxBlocks)
+    return noalloc_fail(CFD_ERR_BAD_ARG, "cfd_evaluate_net_flux_noalloc handles at most " + std::to_string(kMaxCells) +
+                                             " physical cells; got " + std::to_string(NP));
   if (cfg->dissipation_type != CFD_DISS_ROE && cfg->dissipation_type != CFD_DISS_LLF)
     return noalloc_fail(CFD_ERR_BAD_ARG, "dissipation type must be ROE or LLF");
   if (cfg->dissipation_type == CFD_DISS_LLF && cfg->is_second_order)
@@ -108,6 +108,7 @@ extern "C" cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, co
   fp.recon_prim = cfg->reconstruct_primitive;
   fp.consistent = 0;
   fp.muscl = 0;
+  fp.lanes = 1;
   fp.precision = CFD_PREC_FP64;
   fp.cfl = cfg->cfl;
   fp.zeta = cfg->limiter_zeta;

@@ -221,8 +221,8 @@ typedef struct {
  * device memory.  No counterpart in the reference: it exists for callers that cannot let this
  * library call cudaMalloc (their own pool allocator owns the device memory, or their loop may not
  * take cudaMalloc's device synchronisation).  The kernel's scratch (control block, completion
- * counter, one partial minimum per thread block) is a fixed static device array of 65,560 doubles
- * (512 KiB) per GPU, held until the process exits; at most 8,388,608 physical cells per call (larger sizes
+ * counter, one partial minimum per thread block) is a fixed static device array of 262,168 doubles
+ * (2 MiB) per GPU, held until the process exits; at most 8,388,608 physical cells per call (larger sizes
  * are rejected with CFD_ERR_BAD_ARG).  The first call on a device resolves the array's device
  * address, so make that first call before any stream capture.  Calls share the array: calls that
  * overlap on the GPU (different streams, other threads) race.  Reference MUSCL stencil, FP64,

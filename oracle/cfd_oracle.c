@@ -18,7 +18,8 @@ struct orc_state {
   const int *nf, *nbr, *bnd;
   const double *nrm, *len, *ccd, *cvec, *area, *inva;
   orc_config c;
-  double *U, *P, *R, *dt, *dU, *S1, *S2, *Racc, *dtk, *Urd, *G;
+  double *U, *P, *R, *dt, *dU, *S1, *S2, *Racc, *dtk, *Urd, *G, *Ff;
+  int *slot;
   double err[4], min_dt, dt_step, total_time;
   int iterations, bad_cell;
   int stage;   /* 0: flux of U^n, >0: a later stage of the current step */
@@ -80,6 +81,8 @@ orc_state *orc_create(int NP, int NG, const int *nf, const int *nbr, const doubl
   s->Racc = (double *)calloc(4 * (size_t)NP, sizeof(double));
   s->dtk = (double *)calloc((size_t)NP, sizeof(double));
   s->G = (double *)calloc(8 * (size_t)NP, sizeof(double));
+  s->Ff = (double *)calloc(16 * (size_t)NP, sizeof(double));
+  s->slot = (int *)calloc(4 * (size_t)NP, sizeof(int));
   for (size_t g = (size_t)NP; g < NT; g++) s->dt[g] = 1e300; /* ghost del_t never written (harness fix) */
   s->bad_cell = -1;
   return s;
@@ -98,6 +101,8 @@ void orc_destroy(orc_state *s) {
   free(s->Racc);
   free(s->dtk);
   free(s->G);
+  free(s->Ff);
+  free(s->slot);
   free(s);
 }
 
@@ -410,62 +415,65 @@ static void muscl_gradients(orc_state *s) {
   }
 }
 
-/* Roe dissipation between two face states given as (rho, u, v, p, a) (the ROE arithmetic of
- * src/Roe_Scheme.cpp:86-228 on arbitrary left/right states). */
-static void roe_states(const double *L, const double *R, double nx, double ny, double dl, double *D) {
-  D[0] = D[1] = D[2] = D[3] = 0.0;
-  double Rho_L = L[0], u_L = L[1], v_L = L[2], P_L = L[3], C_L = L[4];
-  if (Rho_L <= 0.0 || P_L <= 0.0 || C_L <= 0.0) return;
-  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L);
-  double H_L = ((C_L * C_L) / (1.4 - 1.0)) + Vmag_L;
-  double Rho_R = R[0], u_R = R[1], v_R = R[2], P_R = R[3], C_R = R[4];
-  if (Rho_R <= 0.0 || P_R <= 0.0 || C_R <= 0.0) return;
-  double Vmag_R = 0.5 * (u_R * u_R + v_R * v_R);
-  double H_R = ((C_R * C_R) / (1.4 - 1.0)) + Vmag_R;
-  double sL = sqrt(Rho_L), sR = sqrt(Rho_R);
-  double Term1 = 1.0 / (sL + sR);
-  double Roe_Rho = sqrt(Rho_L * Rho_R);
-  double Roe_u = Term1 * (u_R * sR + u_L * sL);
-  double Roe_v = Term1 * (v_R * sR + v_L * sL);
-  double Roe_H = Term1 * (H_R * sR + H_L * sL);
-  double Roe_Vmag = 0.5 * (Roe_u * Roe_u + Roe_v * Roe_v);
-  double Roe_a = sqrt((1.4 - 1.0) * (Roe_H - Roe_Vmag));
-  if (Roe_a <= 0.0) {
-    Roe_a = 0.5 * (C_L + C_R);
-    if (Roe_a <= 0.0) return;
-  }
-  double Un = nx * Roe_u + ny * Roe_v, Ut = -ny * Roe_u + nx * Roe_v;
-  double du = (u_R - u_L), dv = (v_R - v_L), dP = (P_R - P_L), dRho = (Rho_R - Rho_L);
-  double dUn = nx * du + ny * dv, dUt = -ny * du + nx * dv;
-  roe_tail(Roe_u, Roe_v, Roe_H, Roe_Vmag, Roe_a, Roe_Rho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
-}
+#define REAL double
+#define FN(x) x##_d
+#define K(x) ((double)(x))
+#define FABS fabs
+#define SQRT sqrt
+#define FMIN fmin
+#define FMAX fmax
+#include "face_flux.inc"
+#undef REAL
+#undef FN
+#undef K
+#undef FABS
+#undef SQRT
+#undef FMIN
+#undef FMAX
+#define REAL float
+#define FN(x) x##_f
+#define K(x) ((float)(x))
+#define FABS fabsf
+#define SQRT sqrtf
+#define FMIN fminf
+#define FMAX fmaxf
+#include "face_flux.inc"
+#undef REAL
+#undef FN
+#undef K
+#undef FABS
+#undef SQRT
+#undef FMIN
+#undef FMAX
 
-/* Gradient-MUSCL face flux: q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+
- * with D+ = q_N - q_c, D-_x = 2 grad q_x . d - D+, d = x_N - x_c; average flux of the two face
- * states plus Roe dissipation between them. */
-static void muscl_face(orc_state *s, int c, int N, int f, double *A, double *D) {
-  static const int slot[4] = {0, 1, 2, 4};
-  int lim = s->c.limiter == 0 ? 1 : s->c.limiter;
-  double dx = s->cvec[8 * c + 2 * f], dy = s->cvec[8 * c + 2 * f + 1];
-  const double *gc = s->G + 8 * (size_t)c, *gn = (N < s->NP) ? s->G + 8 * (size_t)N : gc;
-  double qL[4], qR[4], qc[4], qn[4];
-  for (int k = 0; k < 4; k++) {
-    qc[k] = s->P[11 * (size_t)c + slot[k]];
-    qn[k] = s->P[11 * (size_t)N + slot[k]];
-    double dp = qn[k] - qc[k];
-    double dmc = 2.0 * (gc[2 * k] * dx + gc[2 * k + 1] * dy) - dp;
-    double dmn = 2.0 * (gn[2 * k] * dx + gn[2 * k + 1] * dy) - dp;
-    qL[k] = qc[k] + 0.5 * phi_ab(lim, dmc, dp) * dp;
-    qR[k] = qn[k] - 0.5 * phi_ab(lim, dmn, dp) * dp;
+/* Face-based gradient-MUSCL net flux: faces numbered in reference order (a face belongs to the
+ * lower-numbered cell, a boundary face to its cell), each flux computed once from the owner's
+ * side; every cell sums its faces in face order, +F as owner, -F as neighbour. */
+static void muscl_net_flux(orc_state *s) {
+  const int NP = s->NP;
+  int nfaces = 0;
+  for (int c = 0; c < NP; c++)
+    for (int f = 0; f < s->nf[c]; f++) {
+      int N = s->nbr[4 * c + f];
+      if (N < NP && N < c) continue;
+      double *F = s->Ff + 4 * (size_t)nfaces;
+      if (s->c.precision == 1) face_flux_f(s, c, N, f, F);
+      else face_flux_d(s, c, N, f, F);
+      s->slot[4 * c + f] = nfaces;
+      if (N < NP)
+        for (int k = 0; k < s->nf[N]; k++)
+          if (s->nbr[4 * N + k] == c) s->slot[4 * N + k] = -(nfaces + 1);
+      nfaces++;
+    }
+  for (int c = 0; c < NP; c++) {
+    double net[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int f = 0; f < s->nf[c]; f++) {
+      int e = s->slot[4 * c + f];
+      const double *F = s->Ff + 4 * (size_t)(e < 0 ? -e - 1 : e);
+      for (int v = 0; v < 4; v++) net[v] += (e < 0) ? -F[v] : F[v];
+    }
+    memcpy(s->R + 4 * (size_t)c, net, sizeof(net));
   }
-  if (!(qL[0] > 0.0) || !(qL[3] > 0.0)) memcpy(qL, qc, sizeof(qL));
-  if (!(qR[0] > 0.0) || !(qR[3] > 0.0)) memcpy(qR, qn, sizeof(qR));
-  double Lq[5] = {qL[0], qL[1], qL[2], qL[3], sqrt(1.4 * qL[3] / qL[0])};
-  double Rq[5] = {qR[0], qR[1], qR[2], qR[3], sqrt(1.4 * qR[3] / qR[0])};
-  double PL[11] = {qL[0], qL[1], qL[2], 0.0, qL[3]}, PR[11] = {qR[0], qR[1], qR[2], 0.0, qR[3]};
-  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
-  avg_flux(PL, PR, nx, ny, dl, A);
-  roe_states(Lq, Rq, nx, ny, dl, D);
 }
 
 /* Evaluate_Cell_Net_Flux_1O/2O + Calculate_Flux_For_All_Faces, src/Net_Flux.cpp:7-129;
@@ -473,18 +481,16 @@ static void muscl_face(orc_state *s, int c, int N, int f, double *A, double *D) 
 void orc_net_flux(orc_state *s) {
   const double *Ur = uread(s);
   const int gmuscl = s->c.muscl && s->c.is_second_order && s->c.dissipation_type == 3;
-  if (gmuscl) muscl_gradients(s);
+  if (gmuscl) {
+    muscl_gradients(s);
+    muscl_net_flux(s);
+  }
   for (int c = 0; c < s->NP; c++) {
     double net[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int f = 0; f < s->nf[c]; f++) {
+    for (int f = 0; f < s->nf[c] && !gmuscl; f++) {
       int N = s->nbr[4 * c + f];
       if (N < 0) continue;
       double A[4], D[4];
-      if (gmuscl) {
-        muscl_face(s, c, N, f, A, D);
-        for (int v = 0; v < 4; v++) net[v] += A[v] - D[v];
-        continue;
-      }
       avg_flux(s->P + 11 * (size_t)c, s->P + 11 * (size_t)N, s->nrm[8 * c + 2 * f], s->nrm[8 * c + 2 * f + 1],
                s->len[4 * c + f], A);
       if (s->c.dissipation_type == 3 && !s->c.is_second_order) roe_1o(s, c, N, f, D);
@@ -492,7 +498,7 @@ void orc_net_flux(orc_state *s) {
       else llf_1o(s, Ur, c, N, f, D);
       for (int v = 0; v < 4; v++) net[v] += A[v] - D[v];
     }
-    memcpy(s->R + 4 * (size_t)c, net, sizeof(net));
+    if (!gmuscl) memcpy(s->R + 4 * (size_t)c, net, sizeof(net));
     const double u0 = s->P[11 * (size_t)c + 1], v0 = s->P[11 * (size_t)c + 2], a0 = s->P[11 * (size_t)c + 5];
     double denom = 0.0;
     for (int f = 0; f < s->nf[c]; f++) {

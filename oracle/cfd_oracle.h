@@ -16,7 +16,7 @@ extern "C" {
 
 typedef struct {
   int dissipation_type, is_second_order, time_accurate, local_time_stepping, integrator, limiter,
-      reconstruct_primitive, muscl, inlet_bc, exit_bc;
+      reconstruct_primitive, muscl, precision, inlet_bc, exit_bc;
   double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas;
 } orc_config;
 

@@ -181,7 +181,7 @@ class RefRun:
 class _OrcConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ["dissipation_type", "is_second_order", "time_accurate",
                                             "local_time_stepping", "integrator", "limiter", "reconstruct_primitive",
-                                            "muscl", "inlet_bc", "exit_bc"]] + \
+                                            "muscl", "precision", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
                                                "exit_p", "r_gas"]]
 
@@ -232,6 +232,7 @@ class OracleRun:
         c.limiter = params.get("limiter", 0)
         c.reconstruct_primitive = params.get("reconstruct_primitive", 0)
         c.muscl = params.get("muscl", 0)
+        c.precision = params.get("precision", 0)
         c.inlet_bc = params.get("inlet_bc", 0)
         c.exit_bc = params.get("exit_bc", 0)
         c.cfl = params.get("cfl", 0.5)
