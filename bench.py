@@ -106,12 +106,30 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def flux_bytes_per_cell(NP):
-    """Algorithmic DRAM bytes of one gradient-MUSCL flux-kernel launch per cell (each array
-    touched once): own primitives 40 B and gradients 64 B; per face the neighbour id 4 B,
-    nx/ny/dl 24 B and the centre vector 16 B (44 B x 4 faces); face count / mask / area 13 B;
-    writes R 32 B + del_t 8 B."""
-    return 40 + 64 + 4 * 44 + 13 + 40
+def face_bytes_per_face():
+    """Algorithmic DRAM bytes of the face-flux kernel per face (each array touched once; cell
+    data counted in face_bytes_per_cell): owner and neighbour ids 8 B, owner-side nx, ny, dl and
+    centre vector 40 B, flux write 32 B."""
+    return 8 + 40 + 32
+
+
+def face_bytes_per_cell():
+    """Cell data the face-flux kernel reads once per cell: primitives rho,u,v,p 32 B and the
+    Green-Gauss gradients 64 B."""
+    return 32 + 64
+
+
+def timed_steps(s, stream, steps, torch):
+    """Device-resident throughput of `steps` graph-replayed pseudo-steps (CUDA events)."""
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    s.step_async(steps)
+    ev1.record(stream)
+    info = s.sync()
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), info
 
 
 def cpu_baseline(steps=3):
@@ -225,24 +243,63 @@ def main():
     ms_per_step = ms_max / args.steps
     value = world * NP * args.steps / (ms_max * 1e-3)
 
-    # Kernel-level timing of the same workload (separate pass, events around every launch).
+    # Kernel-level timing of the dominant kernel, the face-flux kernel k_faces, with CUDA events
+    # around its launches on the library's stream (a separate pass with the same workload).
     s.set_option("profile", 1)
     nprof = min(args.steps, 200)
     s.step_async(nprof)
     s.sync()
-    flux_ms, flux_n = s.kernel_time("flux")
-    stage_ms, stage_n = s.kernel_time("stage")
-    bc_ms, bc_n = s.kernel_time("bc")
     s.set_option("profile", 0)
+    face_ms, face_n = s.kernel_time("faces")
+    grad_ms, grad_n = s.kernel_time("gradients")
+    ga_ms, ga_n = s.kernel_time("flux")
+    st_ms, st_n = s.kernel_time("stage")
+    bc_ms, bc_n = s.kernel_time("bc")
     peaks, peak_kind = measured_peaks()
-    flux_avg_ms = flux_ms / max(flux_n, 1)
-    bytes_launch = flux_bytes_per_cell(NP) * NP
-    achieved = bytes_launch / (flux_avg_ms * 1e-3) / 1e9
+    face_avg_ms = face_ms / max(face_n, 1)
+    NF = s.n_faces
+    bytes_launch = face_bytes_per_face() * NF + face_bytes_per_cell() * NP
+    achieved = bytes_launch / (face_avg_ms * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "flux_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "k_faces_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("bytes_per_launch")
+
+    # The other forms on the same mesh: FP32 fluxes with FP64 state (north-star precision form,
+    # its error against the all-FP64 run stated), and the reference-parity second-order Roe path
+    # (ROE_2O with the reference's MinMod stencil, bit-identical to the reference) timed over a
+    # short window from freestream (the reference scheme diverges on this case after ~200 steps).
+    forms = {}
+    nform = min(args.steps, 200)
+    for name, over in [("fp32_flux", dict(precision=1)),
+                       ("reference_roe2_minmod_rk3", dict(muscl=0, limiter=0, integrator=0)),
+                       ("reference_roe1_rk3", dict(muscl=0, is_second_order=0, integrator=0))]:
+        k = dict(kw)
+        k.update(over)
+        f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
+        f.set_option("keep_delu", 0)
+        f.upload_state(U0)
+        f.step_async(3)
+        f.sync()
+        n_timed = min(nform, 50) if name.startswith("reference_roe2") else nform
+        fms, _ = timed_steps(f, stream, n_timed, torch)
+        forms[name] = {"value": NP * n_timed / (fms * 1e-3), "ms_per_step": fms / n_timed, "steps": n_timed}
+        f.close()
+    # FP32-flux error: both precisions from the same freestream start, same number of steps.
+    finals = {}
+    for prec in (0, 1):
+        k = dict(kw)
+        k["precision"] = prec
+        f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
+        f.set_option("keep_delu", 0)
+        f.upload_state(U0)
+        f.step(nform)
+        finals[prec] = f.download_U()[:NP]
+        f.close()
+    forms["fp32_flux"]["rel_l2_error_vs_fp64"] = float(np.linalg.norm(finals[1] - finals[0]) /
+                                                       np.linalg.norm(finals[0]))
+    forms["fp32_flux"]["error_steps"] = nform
 
     # End to end through the public C ABI with host buffers: every step uploads U from pinned
     # host memory, runs one pseudo-step and reads back U and the residual norm.
@@ -278,12 +335,14 @@ def main():
                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
                "gpu_launches": int(launches),
-               "roofline": {"kernel": "k_flux<ROE,2nd order> (fused residual + dt + min)", "bound": "hbm",
+               "roofline": {"kernel": "k_faces<double> (face fluxes, gradient MUSCL + Roe)", "bound": "hbm",
                             "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                            "peak_source": peak_kind, "bytes_per_launch": bytes_launch,
-                            "avg_launch_ms": flux_avg_ms},
-               "kernel_ms_per_step": {"flux": flux_ms / nprof, "stage": stage_ms / nprof, "bc": bc_ms / nprof},
+                            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                            "bytes_per_launch": bytes_launch, "avg_launch_ms": face_avg_ms, "faces": NF},
+               "kernel_ms_per_step": {"faces": face_ms / nprof, "gradients": grad_ms / nprof,
+                                      "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof},
+               "forms": forms,
                "clocks": clk.summary(),
                "final_residual_rho": info.error[0]}
         if not args.no_cpu_baseline and world == 1:

@@ -112,6 +112,7 @@ SIGNATURES = {
     "cfd_amr_tags": (_I, [_P, _D, _D, _DP, ctypes.POINTER(ctypes.c_uint8)]),
     "cfd_kernel_time": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_longlong)]),
     "cfd_evaluate_net_flux_noalloc": (_I, [ctypes.POINTER(FluxArrays), ctypes.POINTER(Config), _P]),
+    "cfd_face_count": (_I, [_P]),
     "cfd_kernel_launches": (ctypes.c_longlong, [_P]),
     "cfd_device_bytes": (ctypes.c_size_t, [_P]),
 }
@@ -347,6 +348,10 @@ class Solver:
         n = ctypes.c_longlong()
         _check(lib().cfd_kernel_time(self._h, kernel.encode(), ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    @property
+    def n_faces(self):
+        return lib().cfd_face_count(self._h)
 
     @property
     def kernel_launches(self):

@@ -109,6 +109,7 @@ struct cfd_ctx {
   bool prim_from_S = false;
   int keep_delu = 1;
   int use_graph = 1;
+  int fuse_gather = 0;  // face-based forms with per-cell dt: fused gather + stage update
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
@@ -121,8 +122,8 @@ struct cfd_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Timed> timed;
-  double kind_ms[3] = {0, 0, 0};
-  long long kind_n[3] = {0, 0, 0};
+  double kind_ms[6] = {0, 0, 0, 0, 0, 0};
+  long long kind_n[6] = {0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
 };
 
@@ -145,7 +146,7 @@ cfd_status ctx_upload(cfd_ctx *ctx, T **dst, const std::vector<T> &v) {
 
 int dev_of(const cfd_ctx *ctx, int ref) { return ref < ctx->NP ? ctx->inv[ref] : ref; }
 
-enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2 };
+enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_N = 6 };
 
 struct TimedScope {
   cfd_ctx *ctx;
@@ -190,12 +191,25 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
   // Three-stage forms: the reference's Runge_Kutta_Method (LTS in stage 1 only, Min_dt of the
   // current evaluation in stages 2-3) or the stage-consistent SSP-RK3 (dt frozen per step).
   const bool ssp = c.integrator == CFD_INT_SSPRK3;
+  const bool faces = ctx->dm.NF > 0;
   for (int k = 0; k < 3; k++) {
     { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0 && cons); }
-    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
     int lts;
     if (ssp) lts = c.local_time_stepping ? 2 : 3;
     else lts = (k == 0 && c.local_time_stepping) ? 1 : 0;
+    if (faces) {
+      { TimedScope ts(ctx, TK_GRAD); n += launch_muscl_gradients(s, m, st); }
+      { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
+      if (ctx->fuse_gather && (lts == 1 || lts == 2)) {
+        TimedScope ts(ctx, TK_GATHER_STAGE);
+        n += launch_gather_stage(s, m, st, ctx->fp, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu);
+      } else {
+        { TimedScope ts(ctx, TK_FLUX); n += launch_gather(s, m, st, ctx->fp); }
+        { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu); }
+      }
+      continue;
+    }
+    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
     { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu); }
   }
   return n;
@@ -595,7 +609,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.Racc, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   }
   if (cfg->muscl) {
-    if ((s = ctx_alloc(ctx, (void **)&st.grad, 8 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+    if ((s = ctx_alloc(ctx, (void **)&st.rec, 12 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
   }
   if (m.NF > 0) {
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
@@ -652,6 +666,7 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
     ctx->fp.lanes = static_cast<int>(value);
   }
   else if (n == "profile") ctx->profile = value != 0.0;
+  else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);
@@ -928,7 +943,8 @@ cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, dou
 cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches) {
   if (!ctx || !kernel || !total_ms || !launches) return fail(CFD_ERR_BAD_ARG, "null argument");
   std::string k(kernel);
-  int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : -1;
+  int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : k == "gradients" ? TK_GRAD
+           : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : -1;
   if (kind < 0) return fail(CFD_ERR_BAD_ARG, "unknown kernel " + k);
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   for (auto &t : ctx->timed) {
@@ -946,6 +962,7 @@ cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, l
 }
 
 long long cfd_kernel_launches(const cfd_ctx *ctx) { return ctx ? ctx->launches : 0; }
+int cfd_face_count(const cfd_ctx *ctx) { return ctx ? ctx->dm.NF : 0; }
 size_t cfd_device_bytes(const cfd_ctx *ctx) { return ctx ? ctx->bytes : 0; }
 
 }  // extern "C"

@@ -214,7 +214,6 @@ struct USrc {
 struct CellState {
   double rc, uc, vc, pc, ac;
   double Uc[4];
-  double gc[8];
   uint8_t degen;
 };
 
@@ -230,10 +229,6 @@ __device__ __forceinline__ void load_cell(const DevMesh &m, const DevState &st, 
   if (DISS == 1 || ORDER == 2) {
 #pragma unroll
     for (int k = 0; k < 4; k++) q.Uc[k] = us.get(k, c);
-  }
-  if (ORDER == 3) {
-#pragma unroll
-    for (int k = 0; k < 8; k++) q.gc[k] = st.grad[k * NP + c];
   }
   q.degen = m.degen[c];
 }
@@ -252,7 +247,7 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
   const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
   const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
   double A[4], D[4];
-  if (ORDER != 3) average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
+  average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
   if (DISS == 3 && ORDER == 1) {
     if (N >= NP)
       roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (q.degen >> f) & 1, D);
@@ -291,41 +286,6 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
               (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
     }
     roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
-  } else if (DISS == 3 && ORDER == 3) {
-    // Green-Gauss-gradient MUSCL on (rho, u, v, p) (no reference counterpart; the reference's
-    // second-order form is the ORDER == 2 branch).  With d = x_N - x_c and D+ = q_N - q_c, the
-    // upwind differences are D-_c = 2 grad q_c . d - D+ and D-_N = 2 grad q_N . d - D+;
-    // q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+ (phi(a, b), r = a/b).
-    // A ghost neighbour uses the cell's own gradient.  A non-positive reconstructed density or
-    // pressure falls back to the cell-centre state.  Flux: average of the two face states plus
-    // Roe dissipation between them.
-    const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
-    const double dx = m.cvx[idx], dy = m.cvy[idx];
-    const double *gN = (N < NP) ? st.grad : nullptr;
-    const double qc[4] = {rc, uc, vc, pc};
-    const double qn[4] = {rn, un, vn, pn};
-    double qL[4], qR[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const double gx = q.gc[2 * k], gy = q.gc[2 * k + 1];
-      const double nxg = gN ? gN[(2 * k) * NP + N] : gx, nyg = gN ? gN[(2 * k + 1) * NP + N] : gy;
-      const double dp = qn[k] - qc[k];
-      const double dmc = 2.0 * (gx * dx + gy * dy) - dp;
-      const double dmn = 2.0 * (nxg * dx + nyg * dy) - dp;
-      qL[k] = qc[k] + 0.5 * phi_ab<double>(glim, dmc, dp) * dp;
-      qR[k] = qn[k] - 0.5 * phi_ab<double>(glim, dmn, dp) * dp;
-    }
-    if (!(qL[0] > 0.0) || !(qL[3] > 0.0)) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) qL[k] = qc[k];
-    }
-    if (!(qR[0] > 0.0) || !(qR[3] > 0.0)) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) qR[k] = qn[k];
-    }
-    const double aL = sqrt(kGamma * qL[3] / qL[0]), aR = sqrt(kGamma * qR[3] / qR[0]);
-    average_flux<double>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
-    roe_1o<double>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
   } else {  // LLF 1O
     double UR[4];
 #pragma unroll
@@ -457,30 +417,36 @@ __global__ void __launch_bounds__(kFlux4Block) k_flux4(DevMesh m, DevState st, F
 // Face-based evaluation (the Green-Gauss-gradient MUSCL form; no reference counterpart): one
 // thread per unique face computes the flux once from its owner's side, in precision T (double,
 // or float for the FP32-flux form); the neighbour receives exactly the negated flux, so the
-// scheme is conservative to the last bit.  Reconstruction as in face_contrib's ORDER == 3 branch.
+// scheme is conservative to the last bit.  MUSCL on (rho, u, v, p): with d = x_N - x_c and
+// D+ = q_N - q_c, the upwind differences are D-_c = 2 grad q_c . d - D+ and
+// D-_N = 2 grad q_N . d - D+; q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+
+// (phi(a, b), r = a/b).  A ghost neighbour uses the owner's gradient.  A non-positive
+// reconstructed density or pressure falls back to the cell-centre state.  Flux: average of the two
+// face states plus Roe dissipation between them.
 template <typename T>
 __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParams fp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.NF || step_done(st.ctl)) return;
-  const int NP = m.NP, NT = m.NT;
+  const int NP = m.NP;
   const int c = m.fo[i], N = m.fn[i];
-  const double *prim = st.prim;
   const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
   const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
-  T qc[4], qn[4], qL[4], qR[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    qc[k] = T(prim[k * NT + c]);
-    qn[k] = T(prim[k * NT + N]);
-  }
+  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)c);
+  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)N);
+  const double4 c0 = rc[0], c1 = rc[1], c2 = rc[2];
+  const double4 n0 = rn[0];
   const bool nphys = N < NP;
+  const double4 n1 = nphys ? rn[1] : c1, n2 = nphys ? rn[2] : c2;
+  const T qc[4] = {T(c0.x), T(c0.y), T(c0.z), T(c0.w)};
+  const T qn[4] = {T(n0.x), T(n0.y), T(n0.z), T(n0.w)};
+  const T gc[8] = {T(c1.x), T(c1.y), T(c1.z), T(c1.w), T(c2.x), T(c2.y), T(c2.z), T(c2.w)};
+  const T gn[8] = {T(n1.x), T(n1.y), T(n1.z), T(n1.w), T(n2.x), T(n2.y), T(n2.z), T(n2.w)};
+  T qL[4], qR[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    const T gx = T(st.grad[(2 * k) * NP + c]), gy = T(st.grad[(2 * k + 1) * NP + c]);
-    const T hx = nphys ? T(st.grad[(2 * k) * NP + N]) : gx, hy = nphys ? T(st.grad[(2 * k + 1) * NP + N]) : gy;
     const T dp = qn[k] - qc[k];
-    const T dmc = T(2.0) * (gx * dx + gy * dy) - dp;
-    const T dmn = T(2.0) * (hx * dx + hy * dy) - dp;
+    const T dmc = T(2.0) * (gc[2 * k] * dx + gc[2 * k + 1] * dy) - dp;
+    const T dmn = T(2.0) * (gn[2 * k] * dx + gn[2 * k + 1] * dy) - dp;
     qL[k] = qc[k] + T(0.5) * phi_ab<T>(glim, dmc, dp) * dp;
     qR[k] = qn[k] - T(0.5) * phi_ab<T>(glim, dmn, dp) * dp;
   }
@@ -496,48 +462,62 @@ __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParam
   T A[4], D[4];
   average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
   roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
-  const int NF = m.NF;
-#pragma unroll
-  for (int k = 0; k < 4; k++) st.F[k * NF + i] = double(A[k] - D[k]);
+  st.F[i] = make_double4(double(A[0] - D[0]), double(A[1] - D[1]), double(A[2] - D[2]), double(A[3] - D[3]));
 }
 
-// Per cell: Net = sum of its face fluxes in face order (+F on the owner side, -F on the
-// neighbour side), del_t from the cell's own state (src/Time_Step.cpp:293-329), block min.
+// Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
+// side) and the del_t denominator.  The four slots are unrolled and predicated, so every face's
+// id and flux loads are in flight together.
+__device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &st, int c, double R[4], double &den) {
+  const int NP = m.NP, NT = m.NT;
+  const double uc = st.prim[NT + c], vc = st.prim[2 * NT + c], ac = st.prim[4 * NT + c];
+  const int nf = m.nf[c];
+  int e[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) e[f] = (f < nf) ? m.cface[f * NP + c] : 0;
+  double4 F[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int id = e[f] < 0 ? -e[f] - 1 : e[f];
+    F[f] = (f < nf) ? st.F[id] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  R[0] = R[1] = R[2] = R[3] = 0.0;
+  den = 0.0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    if (f < nf) {
+      if (e[f] < 0) {
+        R[0] += -F[f].x;
+        R[1] += -F[f].y;
+        R[2] += -F[f].z;
+        R[3] += -F[f].w;
+      } else {
+        R[0] += F[f].x;
+        R[1] += F[f].y;
+        R[2] += F[f].z;
+        R[3] += F[f].w;
+      }
+      const int idx = f * NP + c;
+      const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
+      den += (fabs(vnf) + ac) * m.dl[idx];
+    }
+  }
+}
+
+// Per cell: Net = sum of its face fluxes in face order, del_t from the cell's own state
+// (src/Time_Step.cpp:293-329), block min.
 __global__ void __launch_bounds__(kFluxBlock) k_gather(DevMesh m, DevState st, FluxParams fp) {
   __shared__ double sh[32];
-  const int NP = m.NP, NT = m.NT, NF = m.NF;
+  const int NP = m.NP;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool done = step_done(st.ctl);
   double dt = 1e308 * 10.0;
   if (c < NP && !done) {
-    const double uc = st.prim[NT + c], vc = st.prim[2 * NT + c], ac = st.prim[4 * NT + c];
-    const int nf = m.nf[c];
-    double R0 = 0.0, R1 = 0.0, R2 = 0.0, R3 = 0.0, den = 0.0;
-    for (int f = 0; f < nf; f++) {
-      const int idx = f * NP + c;
-      const int e = m.cface[idx];
-      const bool neg = e < 0;
-      const int id = neg ? -e - 1 : e;
-      const double F0 = st.F[id], F1 = st.F[NF + id], F2 = st.F[2 * NF + id], F3 = st.F[3 * NF + id];
-      if (neg) {
-        R0 += -F0;
-        R1 += -F1;
-        R2 += -F2;
-        R3 += -F3;
-      } else {
-        R0 += F0;
-        R1 += F1;
-        R2 += F2;
-        R3 += F3;
-      }
-      const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
-      den += (fabs(vnf) + ac) * m.dl[idx];
-    }
+    double R[4], den;
+    gather_faces(m, st, c, R, den);
     dt = cell_dt(m, fp, c, den);
-    st.R[c] = R0;
-    st.R[NP + c] = R1;
-    st.R[2 * NP + c] = R2;
-    st.R[3 * NP + c] = R3;
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
     st.dtc[c] = dt;
   }
   if (done) return;
@@ -581,12 +561,86 @@ __device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const doub
 }
 
 // Stage updates of Runge_Kutta_Method (src/Numerical_Method.cpp:342-457) and Explicit_Method
-// (:26-103), written with the reference's association order.  kind: 1,2,3 RK3 stages, 0
-// explicit, 11..14 classical RK4.  lts: 0 Min_dt, 1 Cell::del_t (reference stage 1 only), 2 dt
-// frozen per cell at the first stage, 3 Min_dt frozen at the first stage.
+// (:26-103) for one cell, written with the reference's association order.  kind: 1,2,3 RK3
+// stages, 0 explicit, 11..14 classical RK4.  The final kind writes dU and, with fuse_final,
+// applies Estimate_Error's terms (e[0..3]), the residual squares (e[4..7]) and Update().
+__device__ __forceinline__ void cell_update(const DevMesh &m, DevState &st, int c, int kind, double dt,
+                                            const double Rk[4], int fuse_final, int keep_delu, double e[8]) {
+  const int NP = m.NP, NT = m.NT;
+  const double invA = m.inv_area[c];
+  double Un[4], out[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) Un[k] = st.U[k * NT + c];
+  bool final_stage = false;
+  if (kind == 1) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
+  } else if (kind == 2) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = 0.25 * (st.S[k * NP + c] + 3.0 * Un[k] - dt * invA * Rk[k]);
+  } else if (kind == 3) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = (2.0 / 3.0) * (st.S[k * NP + c] - Un[k] - dt * invA * Rk[k]);
+    final_stage = true;
+  } else if (kind == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = -dt * invA * Rk[k];
+    final_stage = true;
+  } else if (kind == 11) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      st.Racc[k * NP + c] = Rk[k];
+      out[k] = Un[k] - 0.5 * (dt * invA) * Rk[k];
+    }
+  } else if (kind == 12 || kind == 13) {
+    const double w = (kind == 12) ? 0.5 : 1.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      st.Racc[k * NP + c] = st.Racc[k * NP + c] + 2.0 * Rk[k];
+      out[k] = Un[k] - w * (dt * invA) * Rk[k];
+    }
+  } else {  // 14
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      double acc = st.Racc[k * NP + c] + Rk[k];
+      out[k] = -((dt * invA) * acc) / 6.0;
+    }
+    final_stage = true;
+  }
+  if (!final_stage) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.S[k * NP + c] = out[k];
+    Prim q;
+    bool ok = eos_prim(out[0], out[1], out[2], out[3], q);
+    store_prim(st.prim, NT, c, q);
+    if (!ok) flag_bad(st.status, c);
+  } else {
+    if (keep_delu || !fuse_final) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) st.dU[k * NP + c] = out[k];
+    }
+    if (fuse_final) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        e[k] = err_term(out[k], Un[k]);
+        e[4 + k] = Rk[k] * Rk[k];
+        double nu = Un[k] + out[k];
+        st.U[k * NT + c] = nu;
+        Un[k] = nu;
+      }
+      Prim q;
+      bool ok = eos_prim(Un[0], Un[1], Un[2], Un[3], q);
+      store_prim(st.prim, NT, c, q);
+      if (!ok) flag_bad(st.status, c);
+    }
+  }
+}
+
+// lts: 0 Min_dt, 1 Cell::del_t (reference stage 1 only), 2 dt frozen per cell at the first stage,
+// 3 Min_dt frozen at the first stage.
 __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int kind, int lts, int fuse_final,
                                                   int keep_delu) {
-  const int NP = m.NP, NT = m.NT;
+  const int NP = m.NP;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool done = step_done(st.ctl);
   const bool active = c < NP && !done;
@@ -601,82 +655,83 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
     else if (lts == 1) dt = st.dtc[c];
     else if (lts == 2) dt = (kind == 1 || kind == 11) ? st.dtc[c] : st.dtk[c];
     else dt = (kind == 1 || kind == 11) ? dtmin : st.ctl[CTL_DTSTEP];
-    const double invA = m.inv_area[c];
-    double Un[4], Rk[4], out[4];
+    double Rk[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      Un[k] = st.U[k * NT + c];
-      Rk[k] = st.R[k * NP + c];
-    }
-    bool final_stage = false;
-    if (kind == 1) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
-    } else if (kind == 2) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) out[k] = 0.25 * (st.S[k * NP + c] + 3.0 * Un[k] - dt * invA * Rk[k]);
-    } else if (kind == 3) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) out[k] = (2.0 / 3.0) * (st.S[k * NP + c] - Un[k] - dt * invA * Rk[k]);
-      final_stage = true;
-    } else if (kind == 0) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) out[k] = -dt * invA * Rk[k];
-      final_stage = true;
-    } else if (kind == 11) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        st.Racc[k * NP + c] = Rk[k];
-        out[k] = Un[k] - 0.5 * (dt * invA) * Rk[k];
-      }
-    } else if (kind == 12 || kind == 13) {
-      const double w = (kind == 12) ? 0.5 : 1.0;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        st.Racc[k * NP + c] = st.Racc[k * NP + c] + 2.0 * Rk[k];
-        out[k] = Un[k] - w * (dt * invA) * Rk[k];
-      }
-    } else {  // 14
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        double acc = st.Racc[k * NP + c] + Rk[k];
-        out[k] = -((dt * invA) * acc) / 6.0;
-      }
-      final_stage = true;
-    }
-    if (!final_stage) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) st.S[k * NP + c] = out[k];
-      Prim q;
-      bool ok = eos_prim(out[0], out[1], out[2], out[3], q);
-      store_prim(st.prim, NT, c, q);
-      if (!ok) flag_bad(st.status, c);
-    } else {
-      if (keep_delu || !fuse_final) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) st.dU[k * NP + c] = out[k];
-      }
-      if (fuse_final) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          e[k] = err_term(out[k], Un[k]);
-          e[4 + k] = Rk[k] * Rk[k];
-          double nu = Un[k] + out[k];
-          st.U[k * NT + c] = nu;
-          Un[k] = nu;
-        }
-        Prim q;
-        bool ok = eos_prim(Un[0], Un[1], Un[2], Un[3], q);
-        store_prim(st.prim, NT, c, q);
-        if (!ok) flag_bad(st.status, c);
-      }
-    }
+    for (int k = 0; k < 4; k++) Rk[k] = st.R[k * NP + c];
+    cell_update(m, st, c, kind, dt, Rk, fuse_final, keep_delu, e);
   }
   if ((kind == 1 || kind == 11) && c == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
   if (fuse_final && (kind == 3 || kind == 0 || kind == 14)) {
     if (done) return;
     const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : dtmin;
     reduce_err_and_epilogue(st, e, true, dt_time);
+  }
+}
+
+// Face-based forms with a per-cell time step (lts 1 or 2): the gather of k_gather and the stage
+// update of k_stage in one pass, so the residual never leaves registers on its way to the update
+// (it is still stored for downloads).  The last block finishes Min_dt (and the step's frozen dt at
+// the first stage), and at the final stage the error norms and the Total_Time epilogue.
+__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, int kind, int lts,
+                                                             int fuse_final, int keep_delu) {
+  __shared__ double sh[32];
+  const int NP = m.NP;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (step_done(st.ctl)) return;
+  const bool first = (kind == 1 || kind == 11);
+  const bool final_kind = (kind == 3 || kind == 0 || kind == 14);
+  double dtc = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (c < NP) {
+    double R[4], den;
+    gather_faces(m, st, c, R, den);
+    dtc = cell_dt(m, fp, c, den);
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
+    st.dtc[c] = dtc;
+    double dt;
+    if (lts == 1) dt = dtc;
+    else {
+      if (first) st.dtk[c] = dtc;
+      dt = first ? dtc : st.dtk[c];
+    }
+    cell_update(m, st, c, kind, dt, R, fuse_final, keep_delu, e);
+  }
+  const double bm = block_min(dtc, sh);
+  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
+  const bool do_err = fuse_final && final_kind;
+  if (do_err) {
+    for (int q = 0; q < 8; q++) {
+      double sq = block_sum(e[q], sh);
+      if (threadIdx.x == 0) st.partial[(1 + q) * gridDim.x + blockIdx.x] = sq;
+    }
+  }
+  if (last_block(st.counter)) {
+    double v = 1e308 * 10.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      double w = __ldcg(&st.partial[i]);
+      v = w < v ? w : v;
+    }
+    v = block_min(v, sh);
+    if (do_err && threadIdx.x < 8) {
+      const int q = threadIdx.x;
+      double sq = 0.0;
+      for (int i = 0; i < (int)gridDim.x; i++) sq += __ldcg(&st.partial[(1 + q) * gridDim.x + i]);
+      st.ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(sq);
+    }
+    if (threadIdx.x == 0) {
+      st.ctl[CTL_DTMIN] = v;
+      if (first) st.ctl[CTL_DTSTEP] = v;
+      if (do_err) {
+        const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : v;
+        double t = st.ctl[CTL_TOTAL_TIME] + dt_time;
+        st.ctl[CTL_TOTAL_TIME] = t;
+        st.ctl[CTL_ITER] += 1.0;
+        double te = st.ctl[CTL_TEND];
+        if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
+      }
+      *st.counter = 0u;
+    }
   }
 }
 
@@ -734,35 +789,35 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
   g1 *= m.inv_area[c];
 }
 
-// Green-Gauss gradients of (rho, u, v, p) for the gradient MUSCL form: the face value is the
-// mean of the two cell values, ghost cells included (their values carry the boundary state).
+// Records of the face-based forms: (rho, u, v, p) and their Green-Gauss gradients, the face
+// value being the mean of the two cell values, ghost cells included (their values carry the
+// boundary state).  Ghost rows get (rho, u, v, p) only.
 __global__ void k_muscl_gradients(DevMesh m, DevState st) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int NP = m.NP, NT = m.NT;
-  if (c >= NP || step_done(st.ctl)) return;
+  if (c >= NT || step_done(st.ctl)) return;
+  double qc[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) qc[k] = st.prim[k * NT + c];
+  double4 *r = reinterpret_cast<double4 *>(st.rec + 12 * (size_t)c);
+  r[0] = make_double4(qc[0], qc[1], qc[2], qc[3]);
+  if (c >= NP) return;
   const int nf = m.nf[c];
   const double ia = m.inv_area[c];
-  const int slot[4] = {0, 1, 2, 3};
-  double qc[4], g[8];
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    qc[k] = st.prim[slot[k] * NT + c];
-    g[2 * k] = 0.0;
-    g[2 * k + 1] = 0.0;
-  }
+  double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int f = 0; f < nf; f++) {
     const int idx = f * NP + c;
     const int N = m.nbr[idx];
     const double wx = m.nx[idx] * m.dl[idx], wy = m.ny[idx] * m.dl[idx];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const double qf = 0.5 * (qc[k] + st.prim[slot[k] * NT + N]);
+      const double qf = 0.5 * (qc[k] + st.prim[k * NT + N]);
       g[2 * k] += qf * wx;
       g[2 * k + 1] += qf * wy;
     }
   }
-#pragma unroll
-  for (int k = 0; k < 8; k++) st.grad[k * NP + c] = g[k] * ia;
+  r[1] = make_double4(g[0] * ia, g[1] * ia, g[2] * ia, g[3] * ia);
+  r[2] = make_double4(g[4] * ia, g[5] * ia, g[6] * ia, g[7] * ia);
 }
 
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
@@ -844,13 +899,11 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
   if (fp.lanes == 1) {
     const int g = nblk(m.NP, kFluxBlock);
     if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 3 && fp.muscl) k_flux<3, 3><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   } else {
     const int g = nblk(4 * m.NP, kFlux4Block);
     if (fp.dissipation == 3 && !fp.second_order) k_flux4<3, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 3 && fp.muscl) k_flux4<3, 3><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux4<3, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else k_flux4<1, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
   }
@@ -859,6 +912,23 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
 
 int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu) {
   k_stage<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, kind, lts, fuse_final, keep_delu);
+  return 1;
+}
+
+int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
+  k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
+  return 1;
+}
+
+int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
+  if (fp.precision == 1) k_faces<float><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+  else k_faces<double><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+  return 1;
+}
+
+int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
+                        int fuse_final, int keep_delu) {
+  k_gather_stage<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp, kind, lts, fuse_final, keep_delu);
   return 1;
 }
 
@@ -878,7 +948,7 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
 }
 
 int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st) {
-  k_muscl_gradients<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st);
+  k_muscl_gradients<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
   return 1;
 }
 

@@ -41,8 +41,9 @@ struct DevState {
   double *dtc;   // [NP]
   double *dtk;   // [NP] dt kept for the whole step (RK4 / SSP with LTS)
   double *dU;    // [4][NP]
-  double *grad;  // [8][NP] Green-Gauss gradients of (rho, u, v, p) (gradient MUSCL)
-  double *F;     // [4][NF] face fluxes (face-based forms)
+  double *rec;   // [NT][12] per-cell records of the face-based forms: rho, u, v, p and the
+                 // Green-Gauss gradients (x, y) of each (physical cells), 96 B = 3 x 32 B
+  double4 *F;    // [NF] face fluxes (face-based forms)
   // reduction / control block (see CtrlIdx)
   double *ctl;
   double *partial;     // [nblk_max * 9]
@@ -88,6 +89,12 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
 // kind: 1,2,3 = reference RK3 stages; 0 = Explicit; 11..14 = RK4 stages; fuse_final = apply
 // Estimate_Error + Update in the last stage's kernel.
 int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu);
+// Face-based forms with a per-cell stage dt (lts 1 or 2): gradients, face fluxes and the fused
+// gather + stage update.
+int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
+int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
+int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
+                        int fuse_final, int keep_delu);
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_update(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);

@@ -229,9 +229,12 @@ typedef struct {
  * ROE or first-order LLF only.  stream: cudaStream_t (NULL = default stream). */
 cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_config *cfg, void *stream);
 
-/* Accumulated device time of one kernel family ("flux", "stage", "bc") over the launches made
- * while option "profile" was set (CUDA events on the context's stream around each launch). */
+/* Accumulated device time of one kernel family ("flux", "stage", "bc", and for the face-based
+ * forms "gradients", "faces", "gather_stage") over the launches made while option "profile" was
+ * set (CUDA events on the context's stream around each launch). */
 cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches);
+/* Number of unique faces of the face-based forms (0 for the per-cell reference forms). */
+int cfd_face_count(const cfd_ctx *ctx);
 /* Number of CUDA kernel launches this context has issued so far. */
 long long cfd_kernel_launches(const cfd_ctx *ctx);
 /* Device bytes held by the context. */
