@@ -406,8 +406,10 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       return fail(CFD_ERR_MESH, "invalid boundary entry " + std::to_string(e));
   }
   const int diss = cfg->dissipation_type;
-  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF)
+  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && diss != CFD_DISS_AUSM && diss != CFD_DISS_HLLC)
     return fail(CFD_ERR_BAD_ARG, "dissipation type " + std::to_string(diss) + " is not available in this build");
+  if ((diss == CFD_DISS_AUSM || diss == CFD_DISS_HLLC) && cfg->is_second_order && !cfg->muscl)
+    return fail(CFD_ERR_BAD_ARG, "second-order AUSM / HLLC use the gradient-MUSCL form (muscl = 1)");
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");

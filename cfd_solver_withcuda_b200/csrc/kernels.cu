@@ -226,7 +226,7 @@ __device__ __forceinline__ void load_cell(const DevMesh &m, const DevState &st, 
   q.vc = prim[2 * NT + c];
   q.pc = prim[3 * NT + c];
   q.ac = prim[4 * NT + c];
-  if (DISS == 1 || ORDER == 2) {
+  if (DISS == 1 || DISS == 6 || DISS == 7 || ORDER == 2) {
 #pragma unroll
     for (int k = 0; k < 4; k++) q.Uc[k] = us.get(k, c);
   }
@@ -247,7 +247,7 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
   const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
   const double rn = prim[N], un = prim[NT + N], vn = prim[2 * NT + N], pn = prim[3 * NT + N], an = prim[4 * NT + N];
   double A[4], D[4];
-  average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
+  if (DISS != 6 && DISS != 7) average_flux<double>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, A);
   if (DISS == 3 && ORDER == 1) {
     if (N >= NP)
       roe_1o<double>(rc, uc, vc, pc, ac, rc, uc, vc, pc, ac, nx, ny, dl, (q.degen >> f) & 1, D);
@@ -286,6 +286,23 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
               (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
     }
     roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
+  } else if (DISS == 6 || DISS == 7) {
+    // Reference forms of AUSM (src/Ausm_Flux.cpp:26-34, from U_Cells) and HLLC
+    // (CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu:98-100): faces whose neighbour is a ghost are
+    // skipped; the net flux is the sum of the face fluxes.
+#pragma unroll
+    for (int k = 0; k < 4; k++) A[k] = D[k] = 0.0;
+    if (N < NP) {
+      double UR[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) UR[k] = us.get(k, N);
+      if (DISS == 6) {
+        ausm_face<double>(q.Uc, UR, nx, ny, dl, A);
+      } else {
+        const double qL[5] = {rc, uc, vc, pc, ac}, qR[5] = {rn, un, vn, pn, an};
+        hllc_face<double>(qL, q.Uc, qR, UR, nx, ny, dl, A);
+      }
+    }
   } else {  // LLF 1O
     double UR[4];
 #pragma unroll
@@ -459,9 +476,23 @@ __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParam
     for (int k = 0; k < 4; k++) qR[k] = qn[k];
   }
   const T aL = sqrt(T(kGamma) * qL[3] / qL[0]), aR = sqrt(T(kGamma) * qR[3] / qR[0]);
-  T A[4], D[4];
-  average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
-  roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
+  T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
+  if (fp.dissipation == 3) {
+    average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
+    roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
+  } else {
+    // Conserved face states for AUSM / HLLC: E = p/(g-1) + rho |V|^2 / 2.
+    const T UL[4] = {qL[0], qL[0] * qL[1], qL[0] * qL[2],
+                     qL[3] / T(kGM1) + T(0.5) * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2])};
+    const T UR[4] = {qR[0], qR[0] * qR[1], qR[0] * qR[2],
+                     qR[3] / T(kGM1) + T(0.5) * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])};
+    if (fp.dissipation == 6) {
+      ausm_face<T>(UL, UR, nx, ny, dl, A);
+    } else {
+      const T q5L[5] = {qL[0], qL[1], qL[2], qL[3], aL}, q5R[5] = {qR[0], qR[1], qR[2], qR[3], aR};
+      hllc_face<T>(q5L, UL, q5R, UR, nx, ny, dl, A);
+    }
+  }
   st.F[i] = make_double4(double(A[0] - D[0]), double(A[1] - D[1]), double(A[2] - D[2]), double(A[3] - D[3]));
 }
 
@@ -889,8 +920,8 @@ int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp
 
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
-  if (fp.dissipation == 3 && fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st);
-  if (fp.dissipation == 3 && fp.second_order && fp.muscl && m.NF > 0) {
+  if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st);
+  if (fp.second_order && fp.muscl && m.NF > 0) {
     if (fp.precision == 1) k_faces<float><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
     else k_faces<double><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
     k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
@@ -899,11 +930,15 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
   if (fp.lanes == 1) {
     const int g = nblk(m.NP, kFluxBlock);
     if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 6) k_flux<6, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 7) k_flux<7, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   } else {
     const int g = nblk(4 * m.NP, kFlux4Block);
     if (fp.dissipation == 3 && !fp.second_order) k_flux4<3, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 6) k_flux4<6, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 7) k_flux4<7, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux4<3, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else k_flux4<1, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
   }

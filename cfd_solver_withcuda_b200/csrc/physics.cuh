@@ -223,3 +223,111 @@ __device__ __forceinline__ T limited_slope(int kind, T qc, T q1, T q2, T d1, T d
 }
 
 }  // namespace cfdb
+
+namespace cfdb {
+
+// AUSM face flux of Ausm_Flux (src/Ausm_Flux.cpp:36-160) from the two conserved states:
+// velocities and pressure from U, Roe-averaged interface sound speed, M+/- and P+/- splittings,
+// upwinded mass flux; F already multiplied by the face length.
+template <typename T>
+__device__ __forceinline__ void ausm_face(const T UL[4], const T UR[4], const T nx, const T ny, const T area, T F[4]) {
+  const T rho_L = UL[0], rhou_L = UL[1], rhov_L = UL[2], rhoE_L = UL[3];
+  const T u_L = rhou_L / rho_L, v_L = rhov_L / rho_L;
+  const T p_L = T(kGM1) * (rhoE_L - T(0.5) * rho_L * (u_L * u_L + v_L * v_L));
+  const T H_L = (rhoE_L + p_L) / rho_L;
+  const T rho_R = UR[0], rhou_R = UR[1], rhov_R = UR[2], rhoE_R = UR[3];
+  const T u_R = rhou_R / rho_R, v_R = rhov_R / rho_R;
+  const T p_R = T(kGM1) * (rhoE_R - T(0.5) * rho_R * (u_R * u_R + v_R * v_R));
+  const T H_R = (rhoE_R + p_R) / rho_R;
+  const T Vn_L = u_L * nx + v_L * ny, Vn_R = u_R * nx + v_R * ny;
+  const T sqrt_rho_L = sqrt(rho_L), sqrt_rho_R = sqrt(rho_R);
+  const T inv_sqrt_sum = T(1.0) / (sqrt_rho_L + sqrt_rho_R);
+  const T u_roe = (sqrt_rho_L * u_L + sqrt_rho_R * u_R) * inv_sqrt_sum;
+  const T v_roe = (sqrt_rho_L * v_L + sqrt_rho_R * v_R) * inv_sqrt_sum;
+  const T H_roe = (sqrt_rho_L * H_L + sqrt_rho_R * H_R) * inv_sqrt_sum;
+  const T a_roe = sqrt(T(kGM1) * (H_roe - T(0.5) * (u_roe * u_roe + v_roe * v_roe)));
+  const T M_L = Vn_L / a_roe, M_R = Vn_R / a_roe;
+  T M_plus, M_minus, P_plus, P_minus;
+  if (fabs(M_L) >= T(1.0)) M_plus = (M_L > T(0.0)) ? M_L : T(0.0);
+  else M_plus = T(0.25) * (M_L + T(1.0)) * (M_L + T(1.0));
+  if (fabs(M_R) >= T(1.0)) M_minus = (M_R < T(0.0)) ? M_R : T(0.0);
+  else M_minus = T(-0.25) * (M_R - T(1.0)) * (M_R - T(1.0));
+  const T M_interface = M_plus + M_minus;
+  if (fabs(M_L) >= T(1.0)) P_plus = (M_L > T(0.0)) ? T(1.0) : T(0.0);
+  else P_plus = T(0.25) * (M_L + T(1.0)) * (M_L + T(1.0)) * (T(2.0) - M_L);
+  if (fabs(M_R) >= T(1.0)) P_minus = (M_R < T(0.0)) ? T(1.0) : T(0.0);
+  else P_minus = T(0.25) * (M_R - T(1.0)) * (M_R - T(1.0)) * (T(2.0) + M_R);
+  const T p_interface = P_plus * p_L + P_minus * p_R;
+  if (M_interface >= T(0.0)) {
+    const T mass_flux = M_interface * a_roe * rho_L;
+    F[0] = mass_flux * area;
+    F[1] = (mass_flux * u_L + p_interface * nx) * area;
+    F[2] = (mass_flux * v_L + p_interface * ny) * area;
+    F[3] = mass_flux * H_L * area;
+  } else {
+    const T mass_flux = M_interface * a_roe * rho_R;
+    F[0] = mass_flux * area;
+    F[1] = (mass_flux * u_R + p_interface * nx) * area;
+    F[2] = (mass_flux * v_R + p_interface * ny) * area;
+    F[3] = mass_flux * H_R * area;
+  }
+}
+
+// HLLC face flux of the reference's GPU kernel (CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu:25-204):
+// normal renormalised, Davis/Roe wave-speed bounds, contact speed S*, star states; zero flux for
+// a degenerate normal or a non-physical state; F multiplied by the face length.  q = (rho, u, v,
+// p, a) with the conserved U of the same cell.
+template <typename T>
+__device__ __forceinline__ void hllc_face(const T qL[5], const T UL[4], const T qR[5], const T UR[4], T nx, T ny,
+                                          const T area, T F[4]) {
+  F[0] = F[1] = F[2] = F[3] = T(0.0);
+  const T normal_mag = sqrt(nx * nx + ny * ny);
+  if (normal_mag < T(1e-14)) return;
+  nx /= normal_mag;
+  ny /= normal_mag;
+  const T rho_L = qL[0], u_L = qL[1], v_L = qL[2], P_L = qL[3], a_L = qL[4];
+  if (rho_L <= T(0.0) || P_L <= T(0.0) || a_L <= T(0.0)) return;
+  const T rho_R = qR[0], u_R = qR[1], v_R = qR[2], P_R = qR[3], a_R = qR[4];
+  if (rho_R <= T(0.0) || P_R <= T(0.0) || a_R <= T(0.0)) return;
+  const T un_L = nx * u_L + ny * v_L, un_R = nx * u_R + ny * v_R;
+  const T sqrt_rho_L = sqrt(rho_L), sqrt_rho_R = sqrt(rho_R);
+  const T a_roe = (a_L * sqrt_rho_L + a_R * sqrt_rho_R) / (sqrt_rho_L + sqrt_rho_R);
+  const T u_roe = (u_L * sqrt_rho_L + u_R * sqrt_rho_R) / (sqrt_rho_L + sqrt_rho_R);
+  const T v_roe = (v_L * sqrt_rho_L + v_R * sqrt_rho_R) / (sqrt_rho_L + sqrt_rho_R);
+  const T un_roe = nx * u_roe + ny * v_roe;
+  const T S_L = fmin(un_L - a_L, un_roe - a_roe);
+  const T S_R = fmax(un_R + a_R, un_roe + a_roe);
+  const T numer = P_R - P_L + rho_L * un_L * (S_L - un_L) - rho_R * un_R * (S_R - un_R);
+  const T denom = rho_L * (S_L - un_L) - rho_R * (S_R - un_R);
+  T S_star;
+  if (fabs(denom) > T(1e-14)) S_star = numer / denom;
+  else S_star = T(0.5) * (un_L + un_R);
+  T flux[4];
+  if (S_L >= T(0.0)) {
+    flux[0] = rho_L * un_L;
+    flux[1] = rho_L * u_L * un_L + P_L * nx;
+    flux[2] = rho_L * v_L * un_L + P_L * ny;
+    flux[3] = (UL[3] + P_L) * un_L;
+  } else if (S_R <= T(0.0)) {
+    flux[0] = rho_R * un_R;
+    flux[1] = rho_R * u_R * un_R + P_R * nx;
+    flux[2] = rho_R * v_R * un_R + P_R * ny;
+    flux[3] = (UR[3] + P_R) * un_R;
+  } else {
+    const bool left = S_star >= T(0.0);
+    const T rho = left ? rho_L : rho_R, u = left ? u_L : u_R, v = left ? v_L : v_R, P = left ? P_L : P_R;
+    const T *U = left ? UL : UR;
+    const T S_K = left ? S_L : S_R;
+    const T un = nx * u + ny * v;
+    const T FK[4] = {rho * un, rho * u * un + P * nx, rho * v * un + P * ny, (U[3] + P) * un};
+    const T factor = rho * (S_K - un) / (S_K - S_star);
+    const T Us[4] = {factor, factor * (u + (S_star - un) * nx), factor * (v + (S_star - un) * ny),
+                     factor * (U[3] / rho + (S_star - un) * (S_star + P / (rho * (S_K - un))))};
+#pragma unroll
+    for (int i = 0; i < 4; i++) flux[i] = FK[i] + S_K * (Us[i] - U[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) F[i] = flux[i] * area;
+}
+
+}  // namespace cfdb

@@ -480,7 +480,7 @@ static void muscl_net_flux(orc_state *s) {
  * Inviscid_Time_Step, src/Time_Step.cpp:293-329. */
 void orc_net_flux(orc_state *s) {
   const double *Ur = uread(s);
-  const int gmuscl = s->c.muscl && s->c.is_second_order && s->c.dissipation_type == 3;
+  const int gmuscl = s->c.muscl && s->c.is_second_order;
   if (gmuscl) {
     muscl_gradients(s);
     muscl_net_flux(s);
@@ -491,6 +491,22 @@ void orc_net_flux(orc_state *s) {
       int N = s->nbr[4 * c + f];
       if (N < 0) continue;
       double A[4], D[4];
+      if (s->c.dissipation_type == 6 || s->c.dissipation_type == 7) {
+        /* Reference forms: Ausm_Flux (src/Ausm_Flux.cpp:26-169) from U_Cells, and the GPU HLLC
+         * (CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu:93-205); faces to ghost cells skipped. */
+        if (N >= s->NP) continue;
+        double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f], F[4];
+        const double *UL = Ur + 4 * (size_t)c, *UR = Ur + 4 * (size_t)N;
+        if (s->c.dissipation_type == 6) {
+          ausm_face_d(UL, UR, nx, ny, dl, F);
+        } else {
+          const double *PL = s->P + 11 * (size_t)c, *PR = s->P + 11 * (size_t)N;
+          double qL[5] = {PL[0], PL[1], PL[2], PL[4], PL[5]}, qR[5] = {PR[0], PR[1], PR[2], PR[4], PR[5]};
+          hllc_face_d(qL, UL, qR, UR, nx, ny, dl, F);
+        }
+        for (int v = 0; v < 4; v++) net[v] += F[v];
+        continue;
+      }
       avg_flux(s->P + 11 * (size_t)c, s->P + 11 * (size_t)N, s->nrm[8 * c + 2 * f], s->nrm[8 * c + 2 * f + 1],
                s->len[4 * c + f], A);
       if (s->c.dissipation_type == 3 && !s->c.is_second_order) roe_1o(s, c, N, f, D);

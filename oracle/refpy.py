@@ -47,6 +47,30 @@ def ref_available():
     return os.path.exists(REF_LIB)
 
 
+REFCUDA_LIB = os.path.join(HERE, "_ref", "librefcuda.so")
+
+
+def build_refcuda():
+    """Compiles the reference's GPU flux kernels from their sources when they are present."""
+    if not os.path.isdir(os.path.join(REF_SRC, "CUDA_KERNELS")):
+        return None
+    subprocess.check_call(["make", "-s", "-C", HERE, "refcuda", "REF=" + REF_SRC])
+    return REFCUDA_LIB
+
+
+def refcuda_available():
+    return os.path.exists(REFCUDA_LIB)
+
+
+def refcuda_hllc(U, P6, nbr, normals, areas, flux, num_cells):
+    """Runs the reference's hllc_flux_kernel (its launch_hllc_flux) on device arrays given as
+    integer data pointers; returns the CUDA status (0 = success)."""
+    L = ctypes.CDLL(REFCUDA_LIB)
+    L.refcu_hllc_flux.restype = ctypes.c_int
+    L.refcu_hllc_flux.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int]
+    return L.refcu_hllc_flux(U, P6, nbr, normals, areas, flux, num_cells)
+
+
 _ref = None
 
 

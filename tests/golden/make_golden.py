@@ -69,6 +69,16 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         manifest[name] = {"iterations": int(n), "np": mesh.n_physical, "ng": mesh.n_ghost}
         print(name, manifest[name])
+    # Ausm_Flux (src/Ausm_Flux.cpp:5-205) on a non-uniform state of the mixed bump mesh: the final
+    # state of the bump_roe2_rk3 case.
+    case = CASES["bump_roe2_rk3"]
+    mesh = make_mesh(case)
+    U = np.load(os.path.join(HERE, "bump_roe2_rk3.npz"))["U"]
+    r = refpy.RefRun(mesh, ref_params(case))
+    r.set_state(U)
+    r.L.refh_ausm_net_flux()
+    np.savez_compressed(os.path.join(HERE, "ausm_reference.npz"), U=U, net_flux=r.state()["net_flux"])
+    manifest["ausm_reference"] = {"np": mesh.n_physical}
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)
 

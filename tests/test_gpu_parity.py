@@ -86,6 +86,15 @@ ADDITIVE = {
                                       local_time_stepping=1),
     "grad_muscl_superbee_rk4": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_SUPERBEE, integrator=cb.INT_RK4),
     "grad_muscl_vanleer_fp32": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANLEER, precision=cb.PREC_FP32_FLUX),
+    "grad_muscl_hllc_minmod": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, dissipation_type=cb.DISS_HLLC),
+    "grad_muscl_ausm_minmod": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, dissipation_type=cb.DISS_AUSM),
+    "grad_muscl_hllc_fp32": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, dissipation_type=cb.DISS_HLLC,
+                                 precision=cb.PREC_FP32_FLUX),
+    "grad_muscl_ausm_fp32_ssp_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, dissipation_type=cb.DISS_AUSM,
+                                         precision=cb.PREC_FP32_FLUX, integrator=cb.INT_SSPRK3,
+                                         local_time_stepping=1),
+    "hllc_reference_1o": dict(dissipation_type=cb.DISS_HLLC, is_second_order=0),
+    "ausm_reference_1o": dict(dissipation_type=cb.DISS_AUSM, is_second_order=0),
     "grad_muscl_vanalbada_fp32_ssp_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANALBADA,
                                               precision=cb.PREC_FP32_FLUX, integrator=cb.INT_SSPRK3,
                                               local_time_stepping=1),
@@ -118,6 +127,59 @@ def test_additive_forms_match_oracle(form, base, oracle_lib):
     o.iterate(steps)
     check_state(s.download(), o.state(), form)
     assert s.info.total_time == o.total_time()
+
+
+def test_ausm_reference_form_matches_reference():
+    """Per-cell AUSM in the reference form (src/Ausm_Flux.cpp, ghost faces skipped, from U_Cells)
+    against the reference's own Ausm_Flux output, bit for bit."""
+    g = load_golden("ausm_reference")
+    case = CASES["bump_roe2_rk3"]
+    m = make_mesh(case)
+    for reorder in (0, 1):
+        s = cb.Solver(m, solver_config(case, dissipation_type=cb.DISS_AUSM, is_second_order=0, reorder=reorder))
+        s.upload_state(g["U"])
+        s.Evaluate_Cell_Net_Flux()
+        assert_bits_equal(s.download()["net_flux"], g["net_flux"], "AUSM net flux")
+
+
+def test_hllc_matches_reference_gpu_kernel():
+    """The reference's own hllc_flux_kernel (CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu, built from
+    source with --fmad=false into oracle/_ref) and the HLLC reference form of this library, on the
+    same non-uniform state: each cell's sum of its interior-face fluxes in face order, bit for
+    bit."""
+    import torch
+    from oracle import refpy
+    if not refpy.refcuda_available():
+        pytest.skip("oracle/_ref/librefcuda.so not built (reference sources absent at build time)")
+    case = CASES["bump_roe2_rk3"]
+    m = make_mesh(case)
+    U = load_golden("bump_roe2_rk3")["U"]
+    s = cb.Solver(m, solver_config(case, dissipation_type=cb.DISS_HLLC, is_second_order=0, reorder=0))
+    s.upload_state(U)
+    st = s.download()
+    s.Evaluate_Cell_Net_Flux()
+    mine = s.download()["net_flux"]
+    NP = m.n_physical
+    P6 = np.zeros((NP, 6))
+    P6[:, [0, 1, 2, 3, 5]] = st["prim"][:NP][:, [0, 1, 2, 4, 5]]
+    dev = torch.device("cuda", 0)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in dict(
+        U=st["U"][:NP], P=P6, nbr=m.neighbours.astype(np.int32), nrm=m.face_normals, area=m.face_lengths).items()}
+    flux = torch.zeros((NP, 4, 4), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    rc = refpy.refcuda_hllc(t["U"].data_ptr(), t["P"].data_ptr(), t["nbr"].data_ptr(), t["nrm"].data_ptr(),
+                            t["area"].data_ptr(), flux.data_ptr(), NP)
+    assert rc == 0
+    fl = flux.cpu().numpy()
+    want = np.zeros((NP, 4))
+    for c in range(NP):
+        r = np.zeros(4)
+        for f in range(4):
+            n = m.neighbours[c, f]
+            if 0 <= n < NP:
+                r = r + fl[c, f]
+        want[c] = r
+    assert_bits_equal(mine, want, "HLLC net flux vs reference kernel")
 
 
 def test_face_based_form_is_conservative():

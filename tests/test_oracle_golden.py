@@ -41,6 +41,18 @@ def test_oracle_matches_reference(name, oracle_lib):
         assert_bits_equal(tags, g["amr_tags"], "AMR tags")
 
 
+def test_oracle_ausm_matches_reference(oracle_lib):
+    """Ausm_Flux (src/Ausm_Flux.cpp:5-205) on a non-uniform mixed-mesh state: the restatement's
+    per-cell AUSM net flux (ghost faces skipped, from U_Cells) vs the reference's, bit for bit."""
+    g = load_golden("ausm_reference")
+    case = CASES["bump_roe2_rk3"]
+    m = make_mesh(case)
+    o = oracle_lib.OracleRun(m, **oracle_params(case, dissipation_type=6, is_second_order=0))
+    o.set_state(g["U"])
+    o.net_flux()
+    assert_bits_equal(o.state()["net_flux"], g["net_flux"], "AUSM net flux")
+
+
 def test_sod_physics(oracle_lib):
     """Exact Riemann star state of Sod's problem: p* = 0.30313, u* = 0.92745 (first order smears
     the plateau; the mid-plateau values are within 1 %)."""
