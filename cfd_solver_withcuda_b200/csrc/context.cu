@@ -125,6 +125,7 @@ struct cfd_ctx {
   double kind_ms[6] = {0, 0, 0, 0, 0, 0};
   long long kind_n[6] = {0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
+  void *d_amr = nullptr;      // AMR indicator, tags and selection scratch (allocated on first use)
 };
 
 namespace {
@@ -924,21 +925,28 @@ cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad) {
 
 cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
-  (void)threshold;
-  (void)max_fraction;
-  (void)tags;
   const int NP = ctx->NP;
-  double *dind = nullptr;
-  CUDA_TRY(cudaMalloc(&dind, (size_t)NP * sizeof(double)));
+  if (!ctx->d_amr) {
+    // indicator [NP] doubles + tags [NP] bytes + select scratch (2 states + 256 counters)
+    const size_t bytes = (size_t)NP * sizeof(double) + (((size_t)NP + 255) & ~size_t(255)) + 2048;
+    cfd_status s = ctx_alloc(ctx, &ctx->d_amr, bytes);
+    if (s != CFD_OK) return s;
+  }
+  double *dind = static_cast<double *>(ctx->d_amr);
+  uint8_t *dtag = reinterpret_cast<uint8_t *>(dind + NP);
+  void *scratch = dtag + (((size_t)NP + 255) & ~size_t(255));
   ctx->launches += launch_amr_indicator(ctx->stream, ctx->dm, ctx->ds, dind);
+  if (tags) ctx->launches += launch_amr_tags(ctx->stream, dind, ctx->d_perm, NP, threshold, max_fraction, scratch, dtag);
+  CUDA_TRY(cudaGetLastError());
   std::vector<double> h(NP);
-  cudaError_t e = cudaMemcpyAsync(h.data(), dind, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(dind);
-  if (e != cudaSuccess) return fail(CFD_ERR_CUDA, cudaGetErrorString(e));
-  if (indicator)
-    for (int i = 0; i < NP; i++) indicator[ctx->perm[i]] = h[i];
-  if (tags) return fail(CFD_ERR_BAD_ARG, "tags not available in this build");
+  std::vector<uint8_t> ht(tags ? NP : 0);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), dind, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (tags) CUDA_TRY(cudaMemcpyAsync(ht.data(), dtag, ht.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < NP; i++) {
+    if (indicator) indicator[ctx->perm[i]] = h[i];
+    if (tags) tags[ctx->perm[i]] = ht[i];
+  }
   return CFD_OK;
 }
 

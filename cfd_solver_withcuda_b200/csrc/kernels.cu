@@ -877,6 +877,85 @@ __global__ void k_amr_indicator(DevMesh m, DevState st, double *ind) {
 
 __global__ void k_set_ctl(double *ctl, int idx, double v) { ctl[idx] = v; }
 
+// ---- AMR tagging (TagRefinableCells, src/Grid_Refine_Functions.cpp:33-63) on the device ----
+// Top-fraction rule: the nRefine largest indicators are found by a radix select over the bit
+// patterns of the (non-negative) indicators, 8 bits per pass; ties at the cut are resolved by a
+// second radix select over the reference cell ids (lowest ids first).  Counts are integer
+// atomics, so the result is deterministic.
+struct SelectState {
+  unsigned long long prefix;  // key digits fixed so far
+  unsigned long long mask;    // bits of prefix that are fixed
+  long long remaining;        // rank still to find inside the current prefix
+  long long above;            // number of keys strictly beyond the prefix
+};
+
+__device__ __forceinline__ unsigned long long amr_key(double v) {
+  return v > 0.0 ? static_cast<unsigned long long>(__double_as_longlong(v)) : 0ull;
+}
+
+// Histogram of the next 8-bit digit of keys inside the current prefix.  mode 0: keys are the
+// indicator bits (descending select); mode 1: keys are reference ids among cells whose indicator
+// key equals `match` (ascending select).
+__global__ void k_amr_hist(const double *ind, const int *ref, int NP, const SelectState *sel, int shift, int mode,
+                           unsigned long long match, unsigned int *hist) {
+  __shared__ unsigned int h[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0u;
+  __syncthreads();
+  const unsigned long long prefix = sel->prefix, mask = sel->mask;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < NP; c += gridDim.x * blockDim.x) {
+    unsigned long long key;
+    if (mode == 0) key = amr_key(ind[c]);
+    else {
+      if (amr_key(ind[c]) != match) continue;
+      key = static_cast<unsigned long long>(ref[c]);
+    }
+    if ((key & mask) == prefix) atomicAdd(&h[(key >> shift) & 255ull], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// Picks the digit holding the wanted rank (from the top for mode 0, from the bottom for mode 1)
+// and clears the histogram for the next pass.
+__global__ void k_amr_pick(SelectState *sel, int shift, int mode, unsigned int *hist) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  long long rem = sel->remaining;
+  long long skipped = 0;
+  int digit = 0;
+  for (int i = 0; i < 256; i++) {
+    const int d = mode == 0 ? 255 - i : i;
+    const long long cnt = hist[d];
+    if (rem <= cnt) {
+      digit = d;
+      break;
+    }
+    rem -= cnt;
+    skipped += cnt;
+  }
+  sel->prefix |= static_cast<unsigned long long>(digit) << shift;
+  sel->mask |= 255ull << shift;
+  sel->remaining = rem;
+  sel->above += skipped;
+  for (int i = 0; i < 256; i++) hist[i] = 0u;
+}
+
+__global__ void k_amr_tag(const double *ind, const int *ref, int NP, double threshold, int top, const SelectState *sel,
+                          const SelectState *sel_ref, uint8_t *tags) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= NP) return;
+  const double v = ind[c];
+  bool t;
+  if (!top) {
+    t = v > threshold;
+  } else {
+    const unsigned long long k = amr_key(v), K = sel->prefix;
+    const bool in = k > K || (k == K && static_cast<unsigned long long>(ref[c]) <= sel_ref->prefix);
+    t = in && v >= threshold;
+  }
+  tags[c] = t ? 1 : 0;
+}
+
 // Reference-order AoS rows [NT][4] <-> device-order SoA planes [4][NT] (perm: device -> reference).
 __global__ void k_import_aos(const double *__restrict__ aos, const int *__restrict__ perm, int NP, int NT, double *U) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1000,6 +1079,43 @@ int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP
 int launch_export_aos(cudaStream_t s, const double *U, const int *perm, int NP, int NT, int ld, double *aos) {
   k_export_aos<<<nblk(NT, kBlock), kBlock, 0, s>>>(U, perm, NP, NT, ld, aos);
   return 1;
+}
+
+int launch_amr_tags(cudaStream_t s, const double *ind, const int *ref, int NP, double threshold, double max_fraction,
+                    void *scratch, uint8_t *tags) {
+  // scratch: two SelectState + 256 histogram counters
+  SelectState *sel = reinterpret_cast<SelectState *>(scratch);
+  SelectState *sel_ref = sel + 1;
+  unsigned int *hist = reinterpret_cast<unsigned int *>(sel + 2);
+  const bool top = max_fraction > 0.0 && max_fraction < 1.0;
+  int n = 0;
+  if (top) {
+    long long nRefine = static_cast<long long>(max_fraction * NP);
+    if (nRefine < 1) nRefine = 1;
+    SelectState init[2] = {{0ull, 0ull, nRefine, 0}, {0ull, 0ull, 0, 0}};
+    cudaMemcpyAsync(sel, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned int), s);
+    const int g = nblk(NP, kBlock) < 1184 ? nblk(NP, kBlock) : 1184;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+      k_amr_hist<<<g, kBlock, 0, s>>>(ind, ref, NP, sel, shift, 0, 0ull, hist);
+      k_amr_pick<<<1, 32, 0, s>>>(sel, shift, 0, hist);
+      n += 2;
+    }
+    // Among the cells whose key equals the cut value, the `remaining` lowest reference ids.
+    // The key to match is read on the device inside k_amr_hist via sel_ref->... so copy it.
+    SelectState host_sel;
+    cudaMemcpyAsync(&host_sel, sel, sizeof(host_sel), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    SelectState init_ref = {0ull, 0xffffffff00000000ull, host_sel.remaining, 0};
+    cudaMemcpyAsync(sel_ref, &init_ref, sizeof(init_ref), cudaMemcpyHostToDevice, s);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      k_amr_hist<<<g, kBlock, 0, s>>>(ind, ref, NP, sel_ref, shift, 1, host_sel.prefix, hist);
+      k_amr_pick<<<1, 32, 0, s>>>(sel_ref, shift, 1, hist);
+      n += 2;
+    }
+  }
+  k_amr_tag<<<nblk(NP, kBlock), kBlock, 0, s>>>(ind, ref, NP, threshold, top ? 1 : 0, sel, sel_ref, tags);
+  return n + 1;
 }
 
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v) {

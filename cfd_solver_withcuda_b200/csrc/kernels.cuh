@@ -101,6 +101,9 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
 int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
+// TagRefinableCells on the device; scratch holds >= 2 x 32 + 1024 bytes.
+int launch_amr_tags(cudaStream_t s, const double *ind, const int *ref, int NP, double threshold, double max_fraction,
+                    void *scratch, uint8_t *tags);
 int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP, int NT, double *U);
 int launch_export_aos(cudaStream_t s, const double *U, const int *perm, int NP, int NT, int ld, double *aos);
 

@@ -37,6 +37,10 @@ def test_cuda_matches_reference_fixture(name, reorder):
         assert_bits_equal(s.gradient(0), g["grad_rho"], "grad rho")
         assert_bits_equal(s.gradient(4), g["grad_p"], "grad p")
         assert_bits_equal(s.amr_indicator(), g["amr_indicator"], "AMR indicator")
+        lo, frac = case["amr"]
+        ind, tags = s.amr_tags(lo, frac)
+        assert_bits_equal(ind, g["amr_indicator"], "AMR indicator")
+        assert_bits_equal(tags, g["amr_tags"], "AMR tags")
 
 
 @pytest.mark.parametrize("name", ["sod_roe2_rk3", "cyl_roe2_lts", "bump_roe2_rk3", "sod_llf1_rk3"])
@@ -239,6 +243,28 @@ def test_characteristic_bcs_match_oracle(oracle_lib):
     a, b = s.download(), o.state()
     for k in ("U", "net_flux", "delU"):
         np.testing.assert_allclose(a[k], b[k], rtol=1e-12, atol=1e-13, err_msg=k)
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.05, 0.3, 0.5])
+def test_amr_tags_with_ties_match_oracle(frac, oracle_lib):
+    """Sod 400x4: every column of 4 cells has identical indicators, so cuts fall inside tie groups;
+    ties go to the lowest reference cell ids (the reference's std::sort leaves them unspecified),
+    identical to the C restatement, and invariant under renumbering."""
+    case = CASES["sod_roe1_full_t02"]
+    g = load_golden("sod_roe1_full_t02")
+    m = make_mesh(case)
+    thr = 0.01 if frac == 0.0 else 0.0
+    o = oracle_lib.OracleRun(m, **oracle_params(case))
+    o.set_state(g["U"])
+    want_ind, want = o.amr(thr, frac)
+    for reorder in (0, 1):
+        s = cb.Solver(m, solver_config(case, reorder=reorder))
+        s.upload_state(g["U"])
+        ind, tags = s.amr_tags(thr, frac)
+        assert_bits_equal(ind, want_ind, "indicator")
+        assert_bits_equal(tags, want, "tags")
+        if 0.0 < frac < 1.0:
+            assert tags.sum() == max(1, int(frac * m.n_physical))
 
 
 def test_deterministic_and_graph_equivalent():
