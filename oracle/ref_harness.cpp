@@ -40,6 +40,9 @@ extern V_D Cells_DelT;                  // src/Initialize.cpp:48
 extern vector<V_D> Cells_Viscous_Flux;  // src/Initialize.cpp
 void Ausm_Flux(const int &Cell_No);     // src/Ausm_Flux.cpp:5 (no header declaration)
 
+// Present only when the B200 drop-in shim is linked in (oracle/_ref/libcfdref_dropin.so).
+extern "C" void b200_shim_reset() __attribute__((weak));
+
 namespace {
 int g_saved_stdout = -1;
 void quiet_begin() {
@@ -66,6 +69,7 @@ extern "C" {
 
 // Clears every container the reference grows with push_back so a fresh mesh can be loaded.
 void refh_reset() {
+  if (b200_shim_reset) b200_shim_reset();
   Cells.clear();
   Boundary_Cells.clear();
   Inlet_Cells_List.clear();

@@ -71,13 +71,22 @@ def refcuda_hllc(U, P6, nbr, normals, areas, flux, num_cells):
     return L.refcu_hllc_flux(U, P6, nbr, normals, areas, flux, num_cells)
 
 
-_ref = None
+_ref = {}
+DROPIN_LIB = os.path.join(HERE, "_ref", "libcfdref_dropin.so")
 
 
-def reflib():
-    global _ref
-    if _ref is None:
-        L = ctypes.CDLL(REF_LIB)
+def build_dropin():
+    """The reference solver linked with the B200 drop-in shim (needs the reference sources and
+    libcfd_b200.so)."""
+    if not os.path.isdir(os.path.join(REF_SRC, "src")):
+        return None
+    subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "dropin", "REF=" + REF_SRC])
+    return DROPIN_LIB
+
+
+def reflib(path=REF_LIB):
+    if path not in _ref:
+        L = ctypes.CDLL(path)
         for n in ["refh_reset", "refh_clear_boundary_lists", "refh_apply_bc", "refh_net_flux", "refh_explicit",
                   "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux"]:
             getattr(L, n).restype = None
@@ -102,15 +111,15 @@ def reflib():
         L.refh_iterate.restype = ctypes.c_int
         L.refh_gradient.argtypes = [ctypes.c_int, _DP]
         L.refh_amr.argtypes = [ctypes.c_double, ctypes.c_double, _DP, ctypes.POINTER(ctypes.c_uint8)]
-        _ref = L
-    return _ref
+        _ref[path] = L
+    return _ref[path]
 
 
 class RefRun:
     """The reference CPU path on one mesh (process-global state: one instance at a time)."""
 
-    def __init__(self, mesh, params):
-        L = reflib()
+    def __init__(self, mesh, params, lib_path=REF_LIB):
+        L = reflib(lib_path)
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "mesh.vtk")
             mesh.write_vtk(path)

@@ -20,17 +20,7 @@ sys.path.insert(0, ROOT)
 import cfd_solver_withcuda_b200 as cb  # noqa: E402
 from oracle import refpy  # noqa: E402
 
-from cases import CASES, make_mesh, initial_state  # noqa: E402
-
-
-def ref_params(case):
-    p = {"CFL": case["cfl"], "Time_Accurate": case["time_accurate"], "Dissipation_Type": case["dissipation_type"],
-         "Is_Second_Order": case["is_second_order"], "Local_Time_Stepping": case.get("local_time_stepping", 0),
-         "Limiter_Zeta": case.get("limiter_zeta", 0.5), "Limiter_Zeta1": case.get("limiter_zeta1", 0.5),
-         "Inlet_Rho": case["inlet_rho"], "Inlet_P": case["inlet_p"],
-         "Is_Inlet_SubSonic": 1 if case.get("inlet_bc", 0) == 1 else 0,
-         "Is_Exit_SubSonic": 1 if case.get("exit_bc", 0) == 1 else 0}
-    return p
+from cases import CASES, make_mesh, initial_state, ref_params  # noqa: E402
 
 
 def main():
