@@ -203,6 +203,7 @@ def main():
     import torch
     import torch.distributed as dist
     import cfd_solver_withcuda_b200 as cb
+    from cfd_solver_withcuda_b200.shard import max_over_ranks
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -236,10 +237,7 @@ def main():
         barrier()
     launches = s.kernel_launches - launches0
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist if world > 1 else None, device="cuda")
     ms_per_step = ms_max / args.steps
     value = world * NP * args.steps / (ms_max * 1e-3)
 
@@ -316,10 +314,7 @@ def main():
         s.download_U(out_pin)
     barrier()
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * NP * args.e2e_steps / float(te.item())
+    e2e_value = world * NP * args.e2e_steps / max_over_ranks(e2e_s, dist if world > 1 else None, device="cuda")
     h2d = host_U.nbytes
     d2h = out_pin.nbytes + 8 * 16
 
