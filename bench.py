@@ -162,6 +162,87 @@ def cpu_baseline(steps=3):
             "seconds": el}
 
 
+def ramp_instances(n, seed):
+    """Configuration C4: n 15-degree compression ramps, sizes uniform in [64x32, 512x256] cells,
+    M_inf uniform in [1.5, 3.0], drawn from a seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = int(rng.integers(64, 513))
+        ny = max(32, min(256, int(round(nx / 2 + rng.integers(-8, 9)))))
+        mach = float(rng.uniform(1.5, 3.0))
+        out.append((nx, ny, mach))
+    return out
+
+
+def run_ramps(args, rank, world):
+    """--workload ramps: the batched form.  Instances are split across ranks by cell count (no
+    communication); each rank runs its share as one batch; FP64 and the FP32-flux form."""
+    import torch
+    import torch.distributed as dist
+    import cfd_solver_withcuda_b200 as cb
+    from cfd_solver_withcuda_b200.shard import max_over_ranks, shard_instances, sum_over_ranks
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    specs = ramp_instances(args.instances, args.seed)
+    mine = shard_instances([nx * ny for nx, ny, _ in specs], rank, world)
+    meshes, states, inflow = [], [], []
+    for i in mine:
+        nx, ny, mach = specs[i]
+        m = cb.Mesh.ramp(nx, ny, 3.0, 1.0, 1.0, 15.0)
+        rho, p = 1.0, 1.0 / GAMMA
+        u = mach * np.sqrt(GAMMA * p / rho)
+        NP = m.n_physical
+        U = cb.conserved_from_primitive(np.full(NP, rho), np.full(NP, u), np.zeros(NP), np.full(NP, p))
+        full = np.zeros((m.n_total, 4))
+        full[:NP] = U
+        full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
+        meshes.append(m)
+        states.append(full)
+        inflow.append((rho, u, 0.0, p))
+    results = {}
+    for name, prec in (("fp64", 0), ("fp32_flux", 1)):
+        cfg = cb.default_config(device=local, dissipation_type=3, is_second_order=1, time_accurate=1,
+                                local_time_stepping=1, cfl=0.8, limiter=2, muscl=1, integrator=2, inlet_bc=3,
+                                reorder=0, precision=prec)
+        b = cb.Batch(meshes, cfg, inflow=inflow)
+        b.upload_state(states)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = b.run(max_steps=args.max_steps, tol=args.tol, check_every=args.check_every)
+        torch.cuda.synchronize()
+        el = max_over_ranks(time.perf_counter() - t0, dist if world > 1 else None, device="cuda")
+        cu = sum_over_ranks(r["cell_updates"], dist if world > 1 else None, device="cuda")
+        tt = r["time_to_tol"]
+        conv = tt[tt >= 0]
+        results[name] = {"value": cu / el, "seconds": el, "cell_updates": cu, "steps": r["steps"],
+                         "converged": int(conv.size), "instances": len(mine),
+                         "time_to_tol_p50": float(np.percentile(conv, 50)) if conv.size else None,
+                         "time_to_tol_p99": float(np.percentile(conv, 99)) if conv.size else None,
+                         "steps_to_tol_p50": float(np.percentile(r["steps_to_tol"][r["steps_to_tol"] > 0], 50))
+                         if conv.size else None}
+        b.close()
+    if rank == 0:
+        out = {"metric": "cell-updates/s", "value": results["fp64"]["value"], "unit": "cell-updates/s",
+               "n_gpus": world, "steps": results["fp64"]["steps"], "warmup": 0,
+               "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64", "data": "synthetic (seeded ramp generator, freestream start)",
+               "config": {"workload": "batched_ramps_15deg", "instances": args.instances, "seed": args.seed,
+                          "tol": args.tol, "max_steps": args.max_steps, "check_every": args.check_every,
+                          "total_cells": int(sum(nx * ny for nx, ny, _ in specs)),
+                          "parallelism": "instances split across %d GPU(s)" % world},
+               "forms": results}
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -193,12 +274,20 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--max-steps", type=int, default=20000)
+    ap.add_argument("--check-every", type=int, default=100)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "ramps":
+        return run_ramps(args, rank, world)
 
     import torch
     import torch.distributed as dist

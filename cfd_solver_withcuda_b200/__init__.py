@@ -22,7 +22,7 @@ BC_INLET, BC_EXIT, BC_WALL, BC_SYMMETRY = 0, 1, 2, 3
 DISS_LLF, DISS_ROE, DISS_AUSM, DISS_HLLC = 1, 3, 6, 7
 LIM_REF_MINMOD, LIM_MINMOD, LIM_VANLEER, LIM_SUPERBEE, LIM_VANALBADA = 0, 1, 2, 3, 4
 INT_REFERENCE, INT_RK4, INT_SSPRK3 = 0, 1, 2
-INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT = 0, 1, 2
+INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT, INLET_FIXED = 0, 1, 2, 3
 EXIT_SUPERSONIC, EXIT_SUBSONIC_REF, EXIT_STATIC_P = 0, 1, 2
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 MUSCL_REFERENCE, MUSCL_GRADIENT = 0, 1
@@ -113,6 +113,12 @@ SIGNATURES = {
     "cfd_kernel_time": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_longlong)]),
     "cfd_evaluate_net_flux_noalloc": (_I, [ctypes.POINTER(FluxArrays), ctypes.POINTER(Config), _P]),
     "cfd_face_count": (_I, [_P]),
+    "cfd_batch_create": (_I, [_I, ctypes.POINTER(MeshDesc), _DP, ctypes.POINTER(Config), ctypes.POINTER(_P)]),
+    "cfd_batch_upload_state": (_I, [_P, _DP]),
+    "cfd_batch_download_state": (_I, [_P, _DP]),
+    "cfd_batch_run": (_I, [_P, _I, _D, _I, ctypes.POINTER(_I), _DP, _DP, ctypes.POINTER(ctypes.c_longlong),
+                           ctypes.POINTER(_I)]),
+    "cfd_batch_destroy": (None, [_P]),
     "cfd_kernel_launches": (ctypes.c_longlong, [_P]),
     "cfd_device_bytes": (ctypes.c_size_t, [_P]),
 }
@@ -360,6 +366,60 @@ class Solver:
     @property
     def device_bytes(self):
         return lib().cfd_device_bytes(self._h)
+
+
+class Batch:
+    """Many independent meshes solved together (cfd_batch_*)."""
+
+    def __init__(self, meshes, config, inflow=None):
+        self.meshes = list(meshes)
+        n = len(self.meshes)
+        descs = (MeshDesc * n)(*[m.desc for m in self.meshes])
+        self._keep = descs
+        infl = None
+        if inflow is not None:
+            self._inflow = np.ascontiguousarray(inflow, dtype=np.float64).reshape(n, 4)
+            infl = _dp(self._inflow)
+        h = ctypes.c_void_p()
+        _check(lib().cfd_batch_create(n, descs, infl, ctypes.byref(config), ctypes.byref(h)))
+        self._h = h
+        self.rows = [m.n_total for m in self.meshes]
+
+    def upload_state(self, states):
+        U = np.ascontiguousarray(np.concatenate(states, axis=0), dtype=np.float64)
+        _check(lib().cfd_batch_upload_state(self._h, _dp(U)))
+
+    def download_state(self):
+        U = np.zeros((sum(self.rows), 4))
+        _check(lib().cfd_batch_download_state(self._h, _dp(U)))
+        out, r = [], 0
+        for n in self.rows:
+            out.append(U[r:r + n])
+            r += n
+        return out
+
+    def run(self, max_steps, tol, check_every=50):
+        n = len(self.meshes)
+        sto = (ctypes.c_int * n)()
+        tto = np.zeros(n)
+        rr = np.zeros(n)
+        cu = ctypes.c_longlong()
+        sd = ctypes.c_int()
+        _check(lib().cfd_batch_run(self._h, max_steps, tol, check_every, sto, _dp(tto), _dp(rr), ctypes.byref(cu),
+                                   ctypes.byref(sd)))
+        return {"steps_to_tol": np.array(sto[:]), "time_to_tol": tto, "res_ratio": rr, "cell_updates": cu.value,
+                "steps": sd.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def conserved_from_primitive(rho, u, v, p):

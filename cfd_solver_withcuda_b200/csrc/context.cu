@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -126,6 +127,7 @@ struct cfd_ctx {
   long long kind_n[6] = {0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
   void *d_amr = nullptr;      // AMR indicator, tags and selection scratch (allocated on first use)
+  int2 *d_tables = nullptr;   // work lists of batched solves (cells, faces, entries, records)
 };
 
 namespace {
@@ -414,6 +416,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
+  if (cfg->inlet_bc < 0 || cfg->inlet_bc > 3 || cfg->exit_bc < 0 || cfg->exit_bc > 2)
+    return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
   if (cfg->precision != CFD_PREC_FP64 && !(cfg->precision == CFD_PREC_FP32_FLUX && cfg->muscl && cfg->is_second_order))
     return fail(CFD_ERR_BAD_ARG, "the FP32-flux form is available for the gradient-MUSCL scheme only");
 
@@ -968,6 +972,276 @@ cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, l
   ctx->timed.clear();
   *total_ms = ctx->kind_ms[kind];
   *launches = ctx->kind_n[kind];
+  return CFD_OK;
+}
+
+// ------------------------------------ batched solves --------------------------------------
+// Many independent meshes run as one union mesh (instance after instance, no renumbering) through
+// the same kernels; work lists restrict every launch to the cells, faces, boundary entries and
+// record rows of the instances that have not converged yet.
+struct cfd_batch {
+  int n = 0;
+  cfd_ctx *ctx = nullptr;
+  std::vector<int> cs, ce, fs, fe, bs, be, gs, ge;  // per-instance ranges in the union
+  std::vector<uint8_t> active;
+  int *d_start = nullptr, *d_end = nullptr;
+  double *d_res = nullptr;
+  int table_cap[4] = {0, 0, 0, 0};
+  double4 *d_bstate = nullptr;
+};
+
+static cfd_status batch_tables(cfd_batch *b) {
+  std::vector<int2> t[4];
+  auto chunks = [](std::vector<int2> &v, int a, int e, int w) {
+    for (int x = a; x < e; x += w) v.push_back(make_int2(x, std::min(x + w, e)));
+  };
+  for (int i = 0; i < b->n; i++) {
+    if (!b->active[i]) continue;
+    chunks(t[0], b->cs[i], b->ce[i], kWorkCellBlock);
+    chunks(t[1], b->fs[i], b->fe[i], kWorkItemBlock);
+    chunks(t[2], b->bs[i], b->be[i], kWorkItemBlock);
+    chunks(t[3], b->cs[i], b->ce[i], kWorkItemBlock);
+    chunks(t[3], b->gs[i], b->ge[i], kWorkItemBlock);
+  }
+  cfd_ctx *ctx = b->ctx;
+  int2 *base = ctx->d_tables;
+  int2 *p[4];
+  size_t off = 0;
+  for (int k = 0; k < 4; k++) {
+    p[k] = base + off;
+    off += b->table_cap[k];
+    if (!t[k].empty())
+      CUDA_TRY(cudaMemcpyAsync(p[k], t[k].data(), t[k].size() * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->dm.cblk = p[0];
+  ctx->dm.n_cblk = static_cast<int>(t[0].size());
+  ctx->dm.fblk = p[1];
+  ctx->dm.n_fblk = static_cast<int>(t[1].size());
+  ctx->dm.bblk = p[2];
+  ctx->dm.n_bblk = static_cast<int>(t[2].size());
+  ctx->dm.rblk = p[3];
+  ctx->dm.n_rblk = static_cast<int>(t[3].size());
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CFD_OK;
+}
+
+void cfd_batch_destroy(cfd_batch *b) {
+  if (!b) return;
+  cfd_destroy(b->ctx);
+  delete b;
+}
+
+cfd_status cfd_batch_create(int n, const cfd_mesh_desc *meshes, const double *inflow, const cfd_config *cfg,
+                            cfd_batch **out) {
+  if (n <= 0 || !meshes || !cfg || !out) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  if (!(cfg->muscl && cfg->is_second_order)) return fail(CFD_ERR_BAD_ARG, "batched solves use the gradient-MUSCL form");
+  if (cfg->reorder) return fail(CFD_ERR_BAD_ARG, "batched solves keep each instance's own numbering (reorder = 0)");
+  *out = nullptr;
+  long long NPt = 0, NGt = 0, NBt = 0;
+  for (int i = 0; i < n; i++) {
+    NPt += meshes[i].n_physical;
+    NGt += meshes[i].n_ghost;
+    NBt += meshes[i].n_boundary;
+  }
+  if (NPt + NGt > 2000000000LL) return fail(CFD_ERR_BAD_ARG, "batch too large");
+  cfd_batch *b = new cfd_batch;
+  b->n = n;
+  std::vector<int> nf, nbr, bnd;
+  std::vector<double> nrm, len, ccd, cvec, area, inva, bstate;
+  nf.reserve(NPt);
+  int offP = 0, offG = 0, offF = 0;
+  for (int i = 0; i < n; i++) {
+    const cfd_mesh_desc &d = meshes[i];
+    const int NP = d.n_physical;
+    if (!d.center_vectors || !d.center_distances) {
+      delete b;
+      return fail(CFD_ERR_BAD_ARG, "instance " + std::to_string(i) + " lacks centre vectors");
+    }
+    auto map = [&](int id) { return id < NP ? offP + id : static_cast<int>(NPt) + offG + (id - NP); };
+    int nfi = 0;
+    for (int c = 0; c < NP; c++) {
+      nf.push_back(d.n_faces[c]);
+      area.push_back(d.area[c]);
+      inva.push_back(d.inv_area[c]);
+      for (int f = 0; f < 4; f++) {
+        const bool has = f < d.n_faces[c];
+        const int N = d.neighbours[4 * c + f];
+        nbr.push_back(has ? map(N) : -1);
+        if (has && (N >= NP || N > c)) nfi++;
+      }
+      for (int k = 0; k < 8; k++) {
+        nrm.push_back(d.face_normals[8 * c + k]);
+        cvec.push_back(d.center_vectors[8 * c + k]);
+      }
+      for (int k = 0; k < 4; k++) {
+        len.push_back(d.face_lengths[4 * c + k]);
+        ccd.push_back(d.center_distances[4 * c + k]);
+      }
+    }
+    b->bs.push_back(static_cast<int>(bnd.size() / 4));
+    for (int e = 0; e < d.n_boundary; e++) {
+      const int *x = d.boundary + 4 * e;
+      bnd.insert(bnd.end(), {x[0], offP + x[1], x[2], map(x[3])});
+      for (int k = 0; k < 4; k++) bstate.push_back(inflow ? inflow[4 * i + k] : 0.0);
+    }
+    b->be.push_back(static_cast<int>(bnd.size() / 4));
+    b->cs.push_back(offP);
+    b->ce.push_back(offP + NP);
+    b->gs.push_back(static_cast<int>(NPt) + offG);
+    b->ge.push_back(static_cast<int>(NPt) + offG + d.n_ghost);
+    b->fs.push_back(offF);
+    b->fe.push_back(offF + nfi);
+    offP += NP;
+    offG += d.n_ghost;
+    offF += nfi;
+  }
+  cfd_mesh_desc u = {static_cast<int>(NPt), static_cast<int>(NGt), nf.data(), nbr.data(), nrm.data(), len.data(),
+                     ccd.data(), cvec.data(), area.data(), inva.data(), static_cast<int>(bnd.size() / 4), bnd.data()};
+  cfd_status s = cfd_create(&u, cfg, &b->ctx);
+  if (s != CFD_OK) {
+    delete b;
+    return s;
+  }
+  cfd_ctx *ctx = b->ctx;
+  if (ctx->dm.NF != offF) {
+    cfd_batch_destroy(b);
+    return fail(CFD_ERR_MESH, "face count mismatch in the batch union");
+  }
+  std::vector<double4> bs4(bnd.size() / 4);
+  for (size_t e = 0; e < bs4.size(); e++) bs4[e] = make_double4(bstate[4 * e], bstate[4 * e + 1], bstate[4 * e + 2], bstate[4 * e + 3]);
+  if ((s = ctx_upload(ctx, &b->d_bstate, bs4)) != CFD_OK) {
+    cfd_batch_destroy(b);
+    return s;
+  }
+  ctx->dm.bstate = inflow ? b->d_bstate : nullptr;
+  if ((s = ctx_upload(ctx, &b->d_start, b->cs)) != CFD_OK || (s = ctx_upload(ctx, &b->d_end, b->ce)) != CFD_OK ||
+      (s = ctx_alloc(ctx, (void **)&b->d_res, sizeof(double) * n)) != CFD_OK) {
+    cfd_batch_destroy(b);
+    return s;
+  }
+  // Work-list capacity: every instance active.
+  long long cap[4] = {0, 0, 0, 0};
+  for (int i = 0; i < n; i++) {
+    cap[0] += (b->ce[i] - b->cs[i] + kWorkCellBlock - 1) / kWorkCellBlock;
+    cap[1] += (b->fe[i] - b->fs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
+    cap[2] += (b->be[i] - b->bs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
+    cap[3] += (b->ce[i] - b->cs[i] + kWorkItemBlock - 1) / kWorkItemBlock + (b->ge[i] - b->gs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
+  }
+  for (int k = 0; k < 4; k++) b->table_cap[k] = static_cast<int>(cap[k]);
+  if ((s = ctx_alloc(ctx, (void **)&ctx->d_tables, sizeof(int2) * (cap[0] + cap[1] + cap[2] + cap[3]))) != CFD_OK) {
+    cfd_batch_destroy(b);
+    return s;
+  }
+  b->active.assign(n, 1);
+  if ((s = batch_tables(b)) != CFD_OK) {
+    cfd_batch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_upload_state(cfd_batch *b, const double *U) {
+  if (!b || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  // Instance-ordered rows (each instance: NP_i physical rows then NG_i ghost rows) -> union order.
+  const cfd_ctx *ctx = b->ctx;
+  std::vector<double> u(4 * (size_t)ctx->NT);
+  size_t row = 0;
+  for (int i = 0; i < b->n; i++) {
+    for (int c = b->cs[i]; c < b->ce[i]; c++, row++)
+      for (int k = 0; k < 4; k++) u[4 * (size_t)c + k] = U[4 * row + k];
+    for (int g = b->gs[i]; g < b->ge[i]; g++, row++)
+      for (int k = 0; k < 4; k++) u[4 * (size_t)g + k] = U[4 * row + k];
+  }
+  return cfd_upload_state(b->ctx, u.data(), ctx->NT);
+}
+
+cfd_status cfd_batch_download_state(cfd_batch *b, double *U) {
+  if (!b || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  const cfd_ctx *ctx = b->ctx;
+  std::vector<double> u(4 * (size_t)ctx->NT);
+  cfd_status s = cfd_download_U(b->ctx, u.data());
+  if (s != CFD_OK) return s;
+  size_t row = 0;
+  for (int i = 0; i < b->n; i++) {
+    for (int c = b->cs[i]; c < b->ce[i]; c++, row++)
+      for (int k = 0; k < 4; k++) U[4 * row + k] = u[4 * (size_t)c + k];
+    for (int g = b->gs[i]; g < b->ge[i]; g++, row++)
+      for (int k = 0; k < 4; k++) U[4 * row + k] = u[4 * (size_t)g + k];
+  }
+  return CFD_OK;
+}
+
+static cfd_status batch_residuals(cfd_batch *b, std::vector<double> &res) {
+  cfd_ctx *ctx = b->ctx;
+  ctx->launches += launch_instance_residual(ctx->stream, ctx->ds, ctx->NP, b->d_start, b->d_end, b->n, b->d_res);
+  res.resize(b->n);
+  CUDA_TRY(cudaMemcpyAsync(res.data(), b->d_res, sizeof(double) * b->n, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (double &r : res) r = std::sqrt(r);
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,
+                         double *time_to_tol, double *res_ratio, long long *cell_updates, int *steps_done) {
+  if (!b || max_steps < 1 || check_every < 1) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  cfd_ctx *ctx = b->ctx;
+  const int n = b->n;
+  std::vector<double> r0, r;
+  std::vector<int> sto(n, -1);
+  std::vector<double> tto(n, -1.0), ratio(n, 1.0);
+  auto now = [] {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+  };
+  cfd_status s;
+  long long cu = 0;
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  const double t0 = now();
+  if ((s = enqueue_steps(ctx, 1)) != CFD_OK) return s;
+  for (int i = 0; i < n; i++)
+    if (b->active[i]) cu += b->ce[i] - b->cs[i];
+  if ((s = batch_residuals(b, r0)) != CFD_OK) return s;
+  int steps = 1;
+  while (steps < max_steps) {
+    bool any = false;
+    for (int i = 0; i < n; i++) any = any || b->active[i];
+    if (!any) break;
+    const int k = std::min(check_every, max_steps - steps);
+    if ((s = enqueue_steps(ctx, k)) != CFD_OK) return s;
+    steps += k;
+    long long act = 0;
+    for (int i = 0; i < n; i++)
+      if (b->active[i]) act += b->ce[i] - b->cs[i];
+    cu += act * k;
+    if ((s = batch_residuals(b, r)) != CFD_OK) return s;
+    const double t = now() - t0;
+    bool changed = false;
+    for (int i = 0; i < n; i++) {
+      if (!b->active[i]) continue;
+      ratio[i] = r0[i] > 0.0 ? r[i] / r0[i] : 0.0;
+      if (!(ratio[i] > tol)) {
+        b->active[i] = 0;
+        sto[i] = steps;
+        tto[i] = t;
+        changed = true;
+      }
+    }
+    if (changed && (s = batch_tables(b)) != CFD_OK) return s;
+  }
+  if ((s = sync_status(ctx, nullptr)) != CFD_OK) return s;
+  for (int i = 0; i < n; i++) {
+    if (steps_to_tol) steps_to_tol[i] = sto[i];
+    if (time_to_tol) time_to_tol[i] = tto[i];
+    if (res_ratio) res_ratio[i] = ratio[i];
+  }
+  if (cell_updates) *cell_updates = cu;
+  if (steps_done) *steps_done = steps;
   return CFD_OK;
 }
 

@@ -21,6 +21,17 @@ constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ bool step_done(const double *ctl) { return ctl[CTL_DONE] != 0.0; }
 
+// Item handled by this thread: from the block's work-list range when a list is given (n when the
+// thread is past the range's end), else the plain global index.
+__device__ __forceinline__ int item_index(const int2 *blk, int n) {
+  if (blk) {
+    const int2 b = blk[blockIdx.x];
+    const int i = b.x + static_cast<int>(threadIdx.x);
+    return i < b.y ? i : n;
+  }
+  return blockIdx.x * blockDim.x + threadIdx.x;
+}
+
 __device__ __forceinline__ void flag_bad(int *status, int cell) {
   atomicMin(&status[1], cell);
   atomicCAS(&status[0], 0, 3 /* CFD_ERR_NONPHYSICAL */);
@@ -109,7 +120,7 @@ __global__ void k_prim_all(DevMesh m, DevState st) {
 //   subsonic exit    src/Exit_Boundary_Conditions.cpp:83-85 (no-op in the reference)
 // Additive forms: total-(p, T) characteristic inflow and static-pressure outflow.
 __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = item_index(m.bblk, m.NB);
   if (e >= m.NB || step_done(st.ctl)) return;
   const int4 b = m.bnd[e];
   const int kind = b.x, c = b.y, f = b.z, g = b.w;
@@ -128,7 +139,14 @@ __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
     G2 = rho * v2g;
     G3 = ((p / kGM1) + rho * vmag);
   } else if (kind == 0) {
-    if (bp.inlet_bc == 0) {
+    if (bp.inlet_bc == 3) {
+      // Fully prescribed inflow (rho, u, v, p), per boundary entry when given (batched solves).
+      const double4 q = m.bstate ? m.bstate[e] : make_double4(bp.inlet_rho, bp.inlet_u, bp.inlet_v, bp.inlet_p);
+      G0 = q.x;
+      G1 = q.x * q.y;
+      G2 = q.x * q.z;
+      G3 = q.w / kGM1 + 0.5 * q.x * (q.y * q.y + q.z * q.z);
+    } else if (bp.inlet_bc == 0) {
       double vmag = (u * u + v * v) * 0.5;
       G0 = bp.inlet_rho;
       G1 = bp.inlet_rho * u;
@@ -442,7 +460,7 @@ __global__ void __launch_bounds__(kFlux4Block) k_flux4(DevMesh m, DevState st, F
 // face states plus Roe dissipation between them.
 template <typename T>
 __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParams fp) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = item_index(m.fblk, m.NF);
   if (i >= m.NF || step_done(st.ctl)) return;
   const int NP = m.NP;
   const int c = m.fo[i], N = m.fn[i];
@@ -540,7 +558,7 @@ __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &s
 __global__ void __launch_bounds__(kFluxBlock) k_gather(DevMesh m, DevState st, FluxParams fp) {
   __shared__ double sh[32];
   const int NP = m.NP;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = item_index(m.cblk, NP);
   const bool done = step_done(st.ctl);
   double dt = 1e308 * 10.0;
   if (c < NP && !done) {
@@ -672,7 +690,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, DevState &st, int 
 __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int kind, int lts, int fuse_final,
                                                   int keep_delu) {
   const int NP = m.NP;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = item_index(m.cblk, NP);
   const bool done = step_done(st.ctl);
   const bool active = c < NP && !done;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -691,7 +709,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
     for (int k = 0; k < 4; k++) Rk[k] = st.R[k * NP + c];
     cell_update(m, st, c, kind, dt, Rk, fuse_final, keep_delu, e);
   }
-  if ((kind == 1 || kind == 11) && c == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
+  if ((kind == 1 || kind == 11) && blockIdx.x == 0 && threadIdx.x == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
   if (fuse_final && (kind == 3 || kind == 0 || kind == 14)) {
     if (done) return;
     const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : dtmin;
@@ -707,7 +725,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
                                                              int fuse_final, int keep_delu) {
   __shared__ double sh[32];
   const int NP = m.NP;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = item_index(m.cblk, NP);
   if (step_done(st.ctl)) return;
   const bool first = (kind == 1 || kind == 11);
   const bool final_kind = (kind == 3 || kind == 0 || kind == 14);
@@ -824,7 +842,7 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // value being the mean of the two cell values, ghost cells included (their values carry the
 // boundary state).  Ghost rows get (rho, u, v, p) only.
 __global__ void k_muscl_gradients(DevMesh m, DevState st) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
   if (c >= NT || step_done(st.ctl)) return;
   double qc[4];
@@ -876,6 +894,17 @@ __global__ void k_amr_indicator(DevMesh m, DevState st, double *ind) {
 }
 
 __global__ void k_set_ctl(double *ctl, int idx, double v) { ctl[idx] = v; }
+
+// sum(R_rho^2) over one instance's cell range per block: fixed per-thread strides and a fixed
+// block tree, so the value is deterministic.
+__global__ void k_instance_residual(const double *R, const int *start, const int *end, double *out) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x;
+  double acc = 0.0;
+  for (int c = start[i] + threadIdx.x; c < end[i]; c += blockDim.x) acc += R[c] * R[c];
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) out[i] = acc;
+}
 
 // ---- AMR tagging (TagRefinableCells, src/Grid_Refine_Functions.cpp:33-63) on the device ----
 // Top-fraction rule: the nRefine largest indicators are found by a radix select over the bit
@@ -993,7 +1022,20 @@ int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st) {
 
 int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int src_is_S) {
   if (m.NB == 0) return 0;
-  k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S);
+  if (m.bblk) {
+    if (m.n_bblk == 0) return 0;
+    k_bc<<<m.n_bblk, kWorkItemBlock, 0, s>>>(m, st, bp, src_is_S);
+  } else {
+    k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S);
+  }
+  return 1;
+}
+
+int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const int *start, const int *end, int n,
+                             double *out) {
+  (void)NP;
+  if (n <= 0) return 0;
+  k_instance_residual<<<n, 256, 0, s>>>(st.R, start, end, out);
   return 1;
 }
 
@@ -1025,24 +1067,28 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
 }
 
 int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu) {
-  k_stage<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, kind, lts, fuse_final, keep_delu);
+  if (m.cblk) k_stage<<<m.n_cblk, kWorkCellBlock, 0, s>>>(m, st, kind, lts, fuse_final, keep_delu);
+  else k_stage<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, kind, lts, fuse_final, keep_delu);
   return 1;
 }
 
 int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
+  const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
+  k_gather<<<g, kFluxBlock, 0, s>>>(m, st, fp);
   return 1;
 }
 
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  if (fp.precision == 1) k_faces<float><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
-  else k_faces<double><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+  const int g = m.fblk ? m.n_fblk : nblk(m.NF, 256);
+  if (fp.precision == 1) k_faces<float><<<g, 256, 0, s>>>(m, st, fp);
+  else k_faces<double><<<g, 256, 0, s>>>(m, st, fp);
   return 1;
 }
 
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
                         int fuse_final, int keep_delu) {
-  k_gather_stage<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp, kind, lts, fuse_final, keep_delu);
+  const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
+  k_gather_stage<<<g, kFluxBlock, 0, s>>>(m, st, fp, kind, lts, fuse_final, keep_delu);
   return 1;
 }
 
@@ -1062,7 +1108,8 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
 }
 
 int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st) {
-  k_muscl_gradients<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
+  if (m.rblk) k_muscl_gradients<<<m.n_rblk, kWorkItemBlock, 0, s>>>(m, st);
+  else k_muscl_gradients<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
   return 1;
 }
 

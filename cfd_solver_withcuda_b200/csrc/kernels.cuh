@@ -30,7 +30,17 @@ struct DevMesh {
   const int *fo, *fn;
   const double *fnx, *fny, *fdl, *fdx, *fdy;
   const int *cface;  // [4][NP]
+  // Optional work lists (batched solves): each entry is one thread block's [start, end) range of
+  // cells (128 per block), faces (256), boundary entries (256) or record rows (256, physical and
+  // ghost rows); null = all items.
+  const int2 *cblk, *fblk, *bblk, *rblk;
+  int n_cblk, n_fblk, n_bblk, n_rblk;
+  // Prescribed inflow state (rho, u, v, p) per boundary entry (CFD_INLET_FIXED), or null.
+  const double4 *bstate;
 };
+
+constexpr int kWorkCellBlock = 128;
+constexpr int kWorkItemBlock = 256;
 
 struct DevState {
   double *U;     // [4][NT]
@@ -108,5 +118,8 @@ int launch_import_aos(cudaStream_t s, const double *aos, const int *perm, int NP
 int launch_export_aos(cudaStream_t s, const double *U, const int *perm, int NP, int NT, int ld, double *aos);
 
 int flux_block_count(int NP);
+// Per-instance plain residual sum(R_rho^2) over [start[i], end[i]) cell ranges, one block each.
+int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const int *start, const int *end, int n,
+                             double *out);
 
 }  // namespace cfdb

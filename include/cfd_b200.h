@@ -91,7 +91,7 @@ void cfd_mesh_destroy(cfd_mesh *m);
 enum { CFD_DISS_LLF = 1, CFD_DISS_ROE = 3, CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7 };
 enum { CFD_LIM_REF_MINMOD = 0, CFD_LIM_MINMOD = 1, CFD_LIM_VANLEER = 2, CFD_LIM_SUPERBEE = 3, CFD_LIM_VANALBADA = 4 };
 enum { CFD_INT_REFERENCE = 0, CFD_INT_RK4 = 1, CFD_INT_SSPRK3 = 2 };
-enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2 };
+enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2, CFD_INLET_FIXED = 3 };
 enum { CFD_EXIT_SUPERSONIC = 0, CFD_EXIT_SUBSONIC_REF = 1, CFD_EXIT_STATIC_P = 2 };
 enum { CFD_PREC_FP64 = 0, CFD_PREC_FP32_FLUX = 1 };
 enum { CFD_MUSCL_REFERENCE = 0, CFD_MUSCL_GRADIENT = 1 };
@@ -228,6 +228,29 @@ typedef struct {
  * overlap on the GPU (different streams, other threads) race.  Reference MUSCL stencil, FP64,
  * ROE or first-order LLF only.  stream: cudaStream_t (NULL = default stream). */
 cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_config *cfg, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched solves: many independent meshes (uneven sizes) run together as one union mesh through
+ * the same kernels; work lists restrict every launch to instances that have not converged; the
+ * whole pseudo-step is replayed from a CUDA graph that is re-captured when the active set
+ * changes.  No reference counterpart (the reference solves one mesh per process).
+ * Gradient-MUSCL form only, no renumbering (cfg->muscl = 1, cfg->reorder = 0).
+ * inflow: [n*4] (rho, u, v, p) per instance for CFD_INLET_FIXED inlet entries (may be NULL).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cfd_batch cfd_batch;
+cfd_status cfd_batch_create(int n, const cfd_mesh_desc *meshes, const double *inflow, const cfd_config *cfg,
+                            cfd_batch **out);
+/* U: for each instance in order, its NP_i + NG_i rows in reference order. */
+cfd_status cfd_batch_upload_state(cfd_batch *b, const double *U);
+cfd_status cfd_batch_download_state(cfd_batch *b, double *U);
+/* Runs until every instance's plain residual ||R_rho||_2 has dropped by the factor tol from its
+ * first-step value, or max_steps; the residuals are checked every check_every steps (each check
+ * synchronises).  Per instance: steps_to_tol (-1 if not reached), time_to_tol (seconds since the
+ * call, -1 if not reached), res_ratio (last ||R_rho|| / first).  cell_updates counts the cells
+ * actually advanced.  Any output pointer may be NULL. */
+cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,
+                         double *time_to_tol, double *res_ratio, long long *cell_updates, int *steps_done);
+void cfd_batch_destroy(cfd_batch *b);
 
 /* Accumulated device time of one kernel family ("flux", "stage", "bc", and for the face-based
  * forms "gradients", "faces", "gather_stage") over the launches made while option "profile" was
