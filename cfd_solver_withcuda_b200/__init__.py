@@ -81,7 +81,7 @@ SIGNATURES = {
     "cfd_version": (ctypes.c_char_p, []),
     "cfd_mesh_box": (_I, [_I, _I, _D, _D, _D, _D, ctypes.POINTER(_P)]),
     "cfd_mesh_half_cylinder": (_I, [_I, _I, _D, _D, _D, ctypes.POINTER(_P)]),
-    "cfd_mesh_ramp": (_I, [_I, _I, _D, _D, _D, _D, ctypes.POINTER(_P)]),
+    "cfd_mesh_ramp": (_I, [_I, _I, _D, _D, _D, _D, _I, ctypes.POINTER(_P)]),
     "cfd_mesh_bump": (_I, [_I, _I, _D, _D, _D, _I, _D, ctypes.c_uint64, _I, ctypes.POINTER(_P)]),
     "cfd_mesh_read_vtk": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "cfd_mesh_write_vtk": (_I, [_P, ctypes.c_char_p]),
@@ -193,8 +193,8 @@ class Mesh:
         return cls._make(lib().cfd_mesh_half_cylinder, ntheta, nr, r_body, r_outer, ratio)
 
     @classmethod
-    def ramp(cls, nx, ny, length=3.0, height=1.0, x_corner=1.0, angle_deg=15.0):
-        return cls._make(lib().cfd_mesh_ramp, nx, ny, length, height, x_corner, angle_deg)
+    def ramp(cls, nx, ny, length=3.0, height=1.0, x_corner=1.0, angle_deg=15.0, open_top=False):
+        return cls._make(lib().cfd_mesh_ramp, nx, ny, length, height, x_corner, angle_deg, 1 if open_top else 0)
 
     @classmethod
     def bump(cls, nx, ny, length=3.0, height=1.0, thickness=0.1, n_quad_layers=8, jitter=0.3, seed=1234,

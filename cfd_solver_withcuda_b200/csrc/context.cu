@@ -286,10 +286,10 @@ cfd_status cfd_mesh_half_cylinder(int ntheta, int nr, double r_body, double r_ou
   return finish_mesh(h, generate_half_cylinder(h->m, ntheta, nr, r_body, r_outer, ratio), out);
 }
 cfd_status cfd_mesh_ramp(int nx, int ny, double length, double height, double x_corner, double angle_deg,
-                         cfd_mesh **out) {
+                         int open_top, cfd_mesh **out) {
   if (!out) return fail(CFD_ERR_BAD_ARG, "null out");
   cfd_mesh *h = new cfd_mesh;
-  return finish_mesh(h, generate_ramp(h->m, nx, ny, length, height, x_corner, angle_deg), out);
+  return finish_mesh(h, generate_ramp(h->m, nx, ny, length, height, x_corner, angle_deg, open_top), out);
 }
 cfd_status cfd_mesh_bump(int nx, int ny, double length, double height, double thickness, int n_quad_layers,
                          double jitter, uint64_t seed, int triangles, cfd_mesh **out) {

@@ -307,9 +307,11 @@ std::string generate_half_cylinder(Mesh &m, int ntheta, int nr, double r_body, d
 }
 
 // Compression ramp: flat lower wall up to x_corner, then a ramp at angle_deg; the lower wall
-// rises, the upper boundary stays at y = height.  Bounding-box classification applies
-// (left inlet, right exit, everything else wall).
-std::string generate_ramp(Mesh &m, int nx, int ny, double length, double height, double x_corner, double angle_deg) {
+// rises, the upper boundary stays at y = height.  open_top = 0: bounding-box classification
+// (left inlet, right exit, everything else wall, as the reference reader does); open_top = 1:
+// left inlet, right and top outflow, lower boundary wall.
+std::string generate_ramp(Mesh &m, int nx, int ny, double length, double height, double x_corner, double angle_deg,
+                          int open_top) {
   if (nx < 1 || ny < 1) return "bad ramp parameters";
   m = Mesh();
   const double t = std::tan(angle_deg * 3.14159265358979323846 / 180.0);
@@ -325,6 +327,16 @@ std::string generate_ramp(Mesh &m, int nx, int ny, double length, double height,
   auto P = [nx](int i, int j) { return j * (nx + 1) + i; };
   for (int j = 0; j < ny; j++)
     for (int i = 0; i < nx; i++) m.cell_nodes.push_back({P(i, j), P(i + 1, j), P(i + 1, j + 1), P(i, j + 1)});
+  if (open_top) {
+    for (int i = 0; i < nx; i++) {
+      m.edge_kind[edge_key(P(i, 0), P(i + 1, 0))] = BK_WALL;
+      m.edge_kind[edge_key(P(i, ny), P(i + 1, ny))] = BK_EXIT;
+    }
+    for (int j = 0; j < ny; j++) {
+      m.edge_kind[edge_key(P(0, j), P(0, j + 1))] = BK_INLET;
+      m.edge_kind[edge_key(P(nx, j), P(nx, j + 1))] = BK_EXIT;
+    }
+  }
   return "";
 }
 

@@ -44,7 +44,8 @@ struct Mesh {
 // Generators.  All return "" on success.
 std::string generate_box(Mesh &m, int nx, int ny, double x0, double x1, double y0, double y1);
 std::string generate_half_cylinder(Mesh &m, int ntheta, int nr, double r_body, double r_outer, double ratio);
-std::string generate_ramp(Mesh &m, int nx, int ny, double length, double height, double x_corner, double angle_deg);
+std::string generate_ramp(Mesh &m, int nx, int ny, double length, double height, double x_corner, double angle_deg,
+                          int open_top);
 std::string generate_bump(Mesh &m, int nx, int ny, double length, double height, double thickness, int n_quad_layers,
                           double jitter, uint64_t seed, int triangles);
 

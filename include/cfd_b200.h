@@ -71,8 +71,10 @@ typedef struct {
 
 cfd_status cfd_mesh_box(int nx, int ny, double x0, double x1, double y0, double y1, cfd_mesh **out);
 cfd_status cfd_mesh_half_cylinder(int ntheta, int nr, double r_body, double r_outer, double ratio, cfd_mesh **out);
+/* open_top = 0: boundary kinds by the reference reader's bounding-box rule (top = wall);
+ * open_top = 1: top and right outflow, left inflow, lower boundary wall. */
 cfd_status cfd_mesh_ramp(int nx, int ny, double length, double height, double x_corner, double angle_deg,
-                         cfd_mesh **out);
+                         int open_top, cfd_mesh **out);
 cfd_status cfd_mesh_bump(int nx, int ny, double length, double height, double thickness, int n_quad_layers,
                          double jitter, uint64_t seed, int triangles, cfd_mesh **out);
 cfd_status cfd_mesh_read_vtk(const char *path, cfd_mesh **out);

@@ -12,7 +12,7 @@ GAMMA = 1.4
 
 
 def ramp_case(nx, ny, mach):
-    m = cb.Mesh.ramp(nx, ny, 3.0, 1.0, 1.0, 15.0)
+    m = cb.Mesh.ramp(nx, ny, 3.0, 1.0, 1.0, 15.0, open_top=True)
     rho, p = 1.0, 1.0 / GAMMA
     u = mach * np.sqrt(GAMMA * p / rho)
     NP = m.n_physical
@@ -52,7 +52,8 @@ def test_batch_instances_equal_single_solves(precision):
 def test_batch_converged_instances_freeze():
     specs = [(16, 8, 2.0), (48, 16, 2.0)]
     cases = [ramp_case(*sp) for sp in specs]
-    b = cb.Batch([c[0] for c in cases], config(), inflow=[c[2] for c in cases])
+    # MinMod: its residual falls to round-off on these ramps (Van Leer's stalls near 1e-3).
+    b = cb.Batch([c[0] for c in cases], config(limiter=cb.LIM_MINMOD), inflow=[c[2] for c in cases])
     b.upload_state([c[1] for c in cases])
     res = b.run(max_steps=3000, tol=1e-6, check_every=25)
     sto = res["steps_to_tol"]
@@ -61,7 +62,7 @@ def test_batch_converged_instances_freeze():
     got = b.download_state()
     for (m, U0, q), Ub, k in zip(cases, got, sto):
         rho, u, v, p = q
-        s = cb.Solver(m, config(inlet_rho=rho, inlet_u=u, inlet_v=v, inlet_p=p))
+        s = cb.Solver(m, config(limiter=cb.LIM_MINMOD, inlet_rho=rho, inlet_u=u, inlet_v=v, inlet_p=p))
         s.upload_state(U0)
         s.step(int(k))
         assert_bits_equal(Ub, s.download_U(), "frozen instance")

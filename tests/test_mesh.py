@@ -100,3 +100,13 @@ def test_shipped_ramp_grid_known_answers():
         g = r.geometry()
         for k in ("neighbours", "face_normals", "face_lengths", "center_distances", "area", "inv_area"):
             assert_bits_equal(getattr(m, k), g[k], k)
+
+
+def test_ramp_boundary_kinds():
+    """Generated ramps: the bounding-box rule (top = wall) by default, an open top on request."""
+    nx, ny = 8, 4
+    for open_top, want in ((False, [ny, ny, 2 * nx]), (True, [ny, ny + nx, nx])):
+        m = cb.Mesh.ramp(nx, ny, 3.0, 1.0, 1.0, 15.0, open_top=open_top)
+        kinds = np.bincount(m.boundary[:, 0], minlength=3)
+        assert kinds.tolist() == want, (open_top, kinds)
+        assert m.n_physical == nx * ny and m.n_ghost == 2 * (nx + ny)
