@@ -106,6 +106,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def profile_figure(name, key="bytes_per_launch"):
+    """A figure of a committed ncu summary (profiles/*.json), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get(key)
+
+
 def face_bytes_per_face():
     """Algorithmic DRAM bytes of the face-flux kernel per face (each array touched once; cell
     data counted in face_bytes_per_cell): owner and neighbour ids 8 B, owner-side nx, ny, dl and
@@ -117,6 +126,22 @@ def face_bytes_per_cell():
     """Cell data the face-flux kernel reads once per cell: primitives rho,u,v,p 32 B and the
     Green-Gauss gradients 64 B."""
     return 32 + 64
+
+
+def gather_stage_bytes_per_cell():
+    """Algorithmic DRAM bytes per cell of the fused gather + stage kernel k_gather_stage, averaged
+    over the three TVD-RK3 stages with frozen local dt (face fluxes counted per face in
+    gather_stage_bytes_per_face).  Every stage reads nf 4, face ids 16, u, v, a 24, nx, ny, dl of
+    four faces 96, area and 1/area 16, U^n 32 and writes R 32, del_t 8 and the primitives 40;
+    stage 1 also writes the frozen dt 8 and the stage state 32; stage 2 reads the stage state 32
+    and the frozen dt 8 and writes the stage state 32; stage 3 reads the stage state 32 and the
+    frozen dt 8 and writes U 32.  Per stage 308, 340 and 340 B."""
+    return (308 + 340 + 340) / 3.0
+
+
+def gather_stage_bytes_per_face():
+    """Each face flux (double4, 32 B) is read by both of its cells; algorithmically once."""
+    return 32
 
 
 def timed_steps(s, stream, steps, torch):
@@ -348,16 +373,17 @@ def main():
     ga_ms, ga_n = s.kernel_time("flux")
     st_ms, st_n = s.kernel_time("stage")
     bc_ms, bc_n = s.kernel_time("bc")
+    gs_ms, gs_n = s.kernel_time("gather_stage")
     peaks, peak_kind = measured_peaks()
     face_avg_ms = face_ms / max(face_n, 1)
     NF = s.n_faces
     bytes_launch = face_bytes_per_face() * NF + face_bytes_per_cell() * NP
     achieved = bytes_launch / (face_avg_ms * 1e-3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "k_faces_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+    traffic = profile_figure("k_faces_traffic.json")
+    gs_avg_ms = gs_ms / max(gs_n, 1)
+    gs_bytes = gather_stage_bytes_per_cell() * NP + gather_stage_bytes_per_face() * NF
+    gs_achieved = gs_bytes / (gs_avg_ms * 1e-3) / 1e9 if gs_n else None
+    gs_traffic = profile_figure("k_gather_stage_traffic.json")
 
     # The other forms on the same mesh: FP32 fluxes with FP64 state (north-star precision form,
     # its error against the all-FP64 run stated), and the reference-parity second-order Roe path
@@ -425,13 +451,23 @@ def main():
                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
                "gpu_launches": int(launches),
-               "roofline": {"kernel": "k_faces<double> (face fluxes, gradient MUSCL + Roe)", "bound": "hbm",
-                            "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+               "roofline": {"kernel": "k_gather_stage (face-flux gather + RK stage update, the largest "
+                                      "time share)", "bound": "hbm",
+                            "achieved": gs_achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                            "frac": gs_achieved / peaks["hbm_gbs"] if gs_achieved else None,
+                            "traffic": gs_traffic,
                             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-                            "bytes_per_launch": bytes_launch, "avg_launch_ms": face_avg_ms, "faces": NF},
+                            "bytes_per_launch": gs_bytes, "avg_launch_ms": gs_avg_ms, "cells": NP, "faces": NF},
+               "roofline_faces": {"kernel": "k_faces<double> (face fluxes, gradient MUSCL + Roe)", "bound": "hbm",
+                                  "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                                  "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                                  "bytes_per_launch": bytes_launch, "avg_launch_ms": face_avg_ms, "faces": NF,
+                                  "fp64_pipe_active_pct": profile_figure("k_faces_traffic.json",
+                                                                         "fp64_pipe_active_pct"),
+                                  "note": "FP64 issue rather than HBM limits this kernel (ncu)"},
                "kernel_ms_per_step": {"faces": face_ms / nprof, "gradients": grad_ms / nprof,
-                                      "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof},
+                                      "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof,
+                                      "gather_stage": gs_ms / nprof},
                "forms": forms,
                "clocks": clk.summary(),
                "final_residual_rho": info.error[0]}

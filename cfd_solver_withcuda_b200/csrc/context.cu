@@ -110,7 +110,7 @@ struct cfd_ctx {
   bool prim_from_S = false;
   int keep_delu = 1;
   int use_graph = 1;
-  int fuse_gather = 0;  // face-based forms with per-cell dt: fused gather + stage update
+  int fuse_gather = 1;  // face-based forms with per-cell dt: fused gather + stage update
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
@@ -242,13 +242,6 @@ cfd_status sync_status(cfd_ctx *ctx, cfd_step_info *info) {
   }
   if (st == CFD_ERR_NONPHYSICAL) return fail(st, "non-physical state (NaN sound speed) at cell " + std::to_string(bad));
   if (st != CFD_OK) return fail(st, "device status " + std::to_string(st));
-  return CFD_OK;
-}
-
-cfd_status clear_status(cfd_ctx *ctx) {
-  int h[2] = {0, INT_MAX};
-  CUDA_TRY(cudaMemcpyAsync(ctx->ds.status, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
-  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return CFD_OK;
 }
 
@@ -643,6 +636,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.recon_prim = cfg->reconstruct_primitive;
   fp.muscl = cfg->muscl && cfg->is_second_order;
   fp.lanes = 1;
+  fp.faces_shape = 2;
   fp.consistent = (cfg->integrator != CFD_INT_REFERENCE) ? 1 : 0;
   fp.precision = cfg->precision;
   fp.cfl = cfg->cfl;
@@ -671,6 +665,10 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "flux_lanes") {
     if (value != 1.0 && value != 4.0) return fail(CFD_ERR_BAD_ARG, "flux_lanes must be 1 or 4");
     ctx->fp.lanes = static_cast<int>(value);
+  }
+  else if (n == "faces_shape") {
+    if (value != 0.0 && value != 1.0 && value != 2.0) return fail(CFD_ERR_BAD_ARG, "faces_shape must be 0, 1 or 2");
+    ctx->fp.faces_shape = static_cast<int>(value);
   }
   else if (n == "profile") ctx->profile = value != 0.0;
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;

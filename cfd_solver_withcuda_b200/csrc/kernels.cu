@@ -87,6 +87,47 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return v;
 }
 
+// Block sums of NQ per-thread values with one pair of barriers: a shuffle tree per warp, then the
+// warps in order.  The sum of quantity q is returned in thread q (q < NQ).
+template <int NQ>
+__device__ __forceinline__ double block_sums(double v[NQ], double *sh /* NQ * 32 */) {
+#pragma unroll
+  for (int q = 0; q < NQ; q++) v[q] = warp_sum(v[q]);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) sh[q * 32 + w] = v[q];
+  }
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < NQ)
+    for (int i = 0; i < nw; i++) s += sh[threadIdx.x * 32 + i];
+  return s;
+}
+
+// Final sums over the per-block partials partial[q * nb + i] (q < NQ), run by the last block: one
+// warp per quantity, each lane over a fixed stride of blocks, then a shuffle tree.  The sum of q
+// is returned in lane 0 of warp q % (warps per block) for the iteration that handled q.
+template <int NQ, typename Store>
+__device__ __forceinline__ void sum_partials(const double *partial, int nb, Store store) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int q = threadIdx.x >> 5; q < NQ; q += nw) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const double *p = partial + (size_t)q * nb;
+    int i = lane;
+    for (; i + 96 < nb; i += 128) {
+      a0 += __ldcg(p + i);
+      a1 += __ldcg(p + i + 32);
+      a2 += __ldcg(p + i + 64);
+      a3 += __ldcg(p + i + 96);
+    }
+    for (; i < nb; i += 32) a0 += __ldcg(p + i);
+    double a = warp_sum((a0 + a1) + (a2 + a3));
+    if (lane == 0) store(q, a);
+  }
+}
+
 // Returns true in every thread of the block that finished last among the grid's blocks.
 __device__ __forceinline__ bool last_block(unsigned int *counter) {
   __shared__ bool is_last;
@@ -237,7 +278,7 @@ struct CellState {
 
 template <int DISS, int ORDER>
 __device__ __forceinline__ void load_cell(const DevMesh &m, const DevState &st, const USrc &us, int c, CellState &q) {
-  const int NT = m.NT, NP = m.NP;
+  const int NT = m.NT;
   const double *prim = st.prim;
   q.rc = prim[c];
   q.uc = prim[NT + c];
@@ -458,8 +499,8 @@ __global__ void __launch_bounds__(kFlux4Block) k_flux4(DevMesh m, DevState st, F
 // (phi(a, b), r = a/b).  A ghost neighbour uses the owner's gradient.  A non-positive
 // reconstructed density or pressure falls back to the cell-centre state.  Flux: average of the two
 // face states plus Roe dissipation between them.
-template <typename T>
-__global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParams fp) {
+template <typename T, int DISS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
   const int i = item_index(m.fblk, m.NF);
   if (i >= m.NF || step_done(st.ctl)) return;
   const int NP = m.NP;
@@ -495,7 +536,7 @@ __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParam
   }
   const T aL = sqrt(T(kGamma) * qL[3] / qL[0]), aR = sqrt(T(kGamma) * qR[3] / qR[0]);
   T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
-  if (fp.dissipation == 3) {
+  if (DISS == 3) {
     average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
     roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
   } else {
@@ -504,7 +545,7 @@ __global__ void __launch_bounds__(256) k_faces(DevMesh m, DevState st, FluxParam
                      qL[3] / T(kGM1) + T(0.5) * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2])};
     const T UR[4] = {qR[0], qR[0] * qR[1], qR[0] * qR[2],
                      qR[3] / T(kGM1) + T(0.5) * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])};
-    if (fp.dissipation == 6) {
+    if (DISS == 6) {
       ausm_face<T>(UL, UR, nx, ny, dl, A);
     } else {
       const T q5L[5] = {qL[0], qL[1], qL[2], qL[3], aL}, q5R[5] = {qR[0], qR[1], qR[2], qR[3], aR};
@@ -584,18 +625,17 @@ __device__ __forceinline__ double err_term(double du, double u) {
 // partials in block order and applies the step epilogue (Total_Time += Min_dt, iterations++).
 __device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const double e[8], bool advance_time,
                                                         double dt_for_time) {
-  __shared__ double sh[32];
-  for (int q = 0; q < 8; q++) {
-    double s = block_sum(e[q], sh);
-    if (threadIdx.x == 0) st.partial[q * gridDim.x + blockIdx.x] = s;
-  }
+  __shared__ double sh[8 * 32];
+  double v[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = e[q];
+  const double s = block_sums<8>(v, sh);
+  if (threadIdx.x < 8) st.partial[threadIdx.x * gridDim.x + blockIdx.x] = s;
   if (last_block(st.counter)) {
-    if (threadIdx.x < 8) {
-      const int q = threadIdx.x;
-      double s = 0.0;
-      for (int i = 0; i < (int)gridDim.x; i++) s += __ldcg(&st.partial[q * gridDim.x + i]);
-      st.ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(s);
-    }
+    double *ctl = st.ctl;
+    sum_partials<8>(st.partial, (int)gridDim.x,
+                    [ctl](int q, double a) { ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(a); });
+    __syncthreads();
     if (threadIdx.x == 0) {
       if (advance_time) {
         double t = st.ctl[CTL_TOTAL_TIME] + dt_for_time;
@@ -613,23 +653,42 @@ __device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const doub
 // (:26-103) for one cell, written with the reference's association order.  kind: 1,2,3 RK3
 // stages, 0 explicit, 11..14 classical RK4.  The final kind writes dU and, with fuse_final,
 // applies Estimate_Error's terms (e[0..3]), the residual squares (e[4..7]) and Update().
-__device__ __forceinline__ void cell_update(const DevMesh &m, DevState &st, int c, int kind, double dt,
-                                            const double Rk[4], int fuse_final, int keep_delu, double e[8]) {
+// Inputs of one cell's stage update that do not depend on the residual: U^n, the stage state
+// (RK3 stages 2 and 3) and 1/A.  Loaded ahead of the residual gather so that both sets of loads
+// are in flight together.
+struct StageIn {
+  double Un[4], Sk[4], invA;
+};
+
+__device__ __forceinline__ void load_stage_in(const DevMesh &m, const DevState &st, int c, int kind, StageIn &in) {
   const int NP = m.NP, NT = m.NT;
-  const double invA = m.inv_area[c];
+  in.invA = m.inv_area[c];
+#pragma unroll
+  for (int k = 0; k < 4; k++) in.Un[k] = st.U[k * NT + c];
+  if (kind == 2 || kind == 3) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) in.Sk[k] = st.S[k * NP + c];
+  }
+}
+
+__device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, int c, int kind, double dt,
+                                               const double Rk[4], const StageIn &in, int fuse_final, int keep_delu,
+                                               double e[8]) {
+  const int NP = m.NP, NT = m.NT;
+  const double invA = in.invA;
   double Un[4], out[4];
 #pragma unroll
-  for (int k = 0; k < 4; k++) Un[k] = st.U[k * NT + c];
+  for (int k = 0; k < 4; k++) Un[k] = in.Un[k];
   bool final_stage = false;
   if (kind == 1) {
 #pragma unroll
     for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
   } else if (kind == 2) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) out[k] = 0.25 * (st.S[k * NP + c] + 3.0 * Un[k] - dt * invA * Rk[k]);
+    for (int k = 0; k < 4; k++) out[k] = 0.25 * (in.Sk[k] + 3.0 * Un[k] - dt * invA * Rk[k]);
   } else if (kind == 3) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) out[k] = (2.0 / 3.0) * (st.S[k * NP + c] - Un[k] - dt * invA * Rk[k]);
+    for (int k = 0; k < 4; k++) out[k] = (2.0 / 3.0) * (in.Sk[k] - Un[k] - dt * invA * Rk[k]);
     final_stage = true;
   } else if (kind == 0) {
 #pragma unroll
@@ -685,6 +744,13 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, DevState &st, int 
   }
 }
 
+__device__ __forceinline__ void cell_update(const DevMesh &m, DevState &st, int c, int kind, double dt,
+                                            const double Rk[4], int fuse_final, int keep_delu, double e[8]) {
+  StageIn in;
+  load_stage_in(m, st, c, kind, in);
+  cell_update_in(m, st, c, kind, dt, Rk, in, fuse_final, keep_delu, e);
+}
+
 // lts: 0 Min_dt, 1 Cell::del_t (reference stage 1 only), 2 dt frozen per cell at the first stage,
 // 3 Min_dt frozen at the first stage.
 __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int kind, int lts, int fuse_final,
@@ -732,8 +798,13 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
   double dtc = 1e308 * 10.0;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (c < NP) {
+    // The residual gather is issued first; loading the state rows ahead of it (more registers,
+    // fewer resident warps) measured slower on B200.
     double R[4], den;
     gather_faces(m, st, c, R, den);
+    StageIn in;
+    load_stage_in(m, st, c, kind, in);
+    const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
     dtc = cell_dt(m, fp, c, den);
 #pragma unroll
     for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
@@ -742,18 +813,17 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
     if (lts == 1) dt = dtc;
     else {
       if (first) st.dtk[c] = dtc;
-      dt = first ? dtc : st.dtk[c];
+      dt = first ? dtc : dt_frozen;
     }
-    cell_update(m, st, c, kind, dt, R, fuse_final, keep_delu, e);
+    cell_update_in(m, st, c, kind, dt, R, in, fuse_final, keep_delu, e);
   }
   const double bm = block_min(dtc, sh);
   if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
   const bool do_err = fuse_final && final_kind;
   if (do_err) {
-    for (int q = 0; q < 8; q++) {
-      double sq = block_sum(e[q], sh);
-      if (threadIdx.x == 0) st.partial[(1 + q) * gridDim.x + blockIdx.x] = sq;
-    }
+    __shared__ double sh8[8 * 32];
+    const double sq = block_sums<8>(e, sh8);
+    if (threadIdx.x < 8) st.partial[(1 + threadIdx.x) * gridDim.x + blockIdx.x] = sq;
   }
   if (last_block(st.counter)) {
     double v = 1e308 * 10.0;
@@ -762,11 +832,10 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
       v = w < v ? w : v;
     }
     v = block_min(v, sh);
-    if (do_err && threadIdx.x < 8) {
-      const int q = threadIdx.x;
-      double sq = 0.0;
-      for (int i = 0; i < (int)gridDim.x; i++) sq += __ldcg(&st.partial[(1 + q) * gridDim.x + i]);
-      st.ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(sq);
+    if (do_err) {
+      double *ctl = st.ctl;
+      sum_partials<8>(st.partial + gridDim.x, (int)gridDim.x,
+                      [ctl](int q, double a) { ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(a); });
     }
     if (threadIdx.x == 0) {
       st.ctl[CTL_DTMIN] = v;
@@ -1039,12 +1108,15 @@ int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const i
   return 1;
 }
 
+template <typename T>
+void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const FluxParams &fp);
+
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
   if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st);
   if (fp.second_order && fp.muscl && m.NF > 0) {
-    if (fp.precision == 1) k_faces<float><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
-    else k_faces<double><<<nblk(m.NF, 256), 256, 0, s>>>(m, st, fp);
+    if (fp.precision == 1) launch_faces_t<float>(s, nblk(m.NF, 256), m, st, fp);
+    else launch_faces_t<double>(s, nblk(m.NF, 256), m, st, fp);
     k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
     return n + 2;
   }
@@ -1078,10 +1150,28 @@ int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxPara
   return 1;
 }
 
+template <typename T, int MINB>
+void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st, const FluxParams &fp) {
+  if (fp.dissipation == 6) k_faces<T, 6, MINB><<<g, b, 0, s>>>(m, st, fp);
+  else if (fp.dissipation == 7) k_faces<T, 7, MINB><<<g, b, 0, s>>>(m, st, fp);
+  else k_faces<T, 3, MINB><<<g, b, 0, s>>>(m, st, fp);
+}
+
+// Launch shapes of the face kernel (identical results).  The double Roe kernel needs 86
+// registers: 256-thread blocks then fit 2 per SM (16 warps), 256-thread blocks capped at 80
+// registers fit 3 (24 warps, a few bytes of spill), 128-thread blocks fit 5 (20 warps).  Work
+// lists fix 256 faces per block, so shape 2 falls back to shape 1 there.
+template <typename T>
+void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const FluxParams &fp) {
+  if (fp.faces_shape == 2 && !m.fblk) launch_faces_b<T, 1>(s, nblk(m.NF, 128), 128, m, st, fp);
+  else if (fp.faces_shape >= 1) launch_faces_b<T, 3>(s, g, 256, m, st, fp);
+  else launch_faces_b<T, 1>(s, g, 256, m, st, fp);
+}
+
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
   const int g = m.fblk ? m.n_fblk : nblk(m.NF, 256);
-  if (fp.precision == 1) k_faces<float><<<g, 256, 0, s>>>(m, st, fp);
-  else k_faces<double><<<g, 256, 0, s>>>(m, st, fp);
+  if (fp.precision == 1) launch_faces_t<float>(s, g, m, st, fp);
+  else launch_faces_t<double>(s, g, m, st, fp);
   return 1;
 }
 

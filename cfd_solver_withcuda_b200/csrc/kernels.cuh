@@ -81,6 +81,7 @@ struct FluxParams {
   int recon_prim;
   int muscl;            // 0 reference stencil, 1 Green-Gauss-gradient MUSCL
   int lanes;            // threads per cell in the flux kernel: 1 or 4
+  int faces_shape;      // face kernel launch: 0 256 threads, 1 256 threads at <= 80 registers, 2 128 threads
   int consistent;       // 1: limiter/LLF/exit read the stage state instead of U^n
   int precision;
   double cfl, zeta, zeta1;

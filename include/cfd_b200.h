@@ -167,7 +167,11 @@ cfd_status cfd_step_async(cfd_ctx *ctx, int n_steps);
 cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
 /* Runtime options: "keep_delu" (write Cells_DelU in fused steps, default 1),
  * "use_graph" (replay pseudo-steps from a captured CUDA graph, default 1),
- * "profile" (time every launch with CUDA events; disables graph replay, default 0). */
+ * "profile" (time every launch with CUDA events; disables graph replay, default 0),
+ * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
+ * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0/1/2, default 2),
+ * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1).
+ * None of the options changes a result bit. */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
 
 /* Entry points of the reference path, one call each, same semantics and post-conditions. */

@@ -282,6 +282,29 @@ def test_deterministic_and_graph_equivalent():
         check_state(o, outs[0], "rerun")
 
 
+OPTION_SETS = [dict(fuse_gather=0, faces_shape=0), dict(fuse_gather=1, faces_shape=1),
+               dict(fuse_gather=1, faces_shape=2, use_graph=0), dict(fuse_gather=0, faces_shape=2)]
+
+
+@pytest.mark.parametrize("form", ["grad_muscl_minmod_ssp_lts", "grad_muscl_ausm_fp32_ssp_lts", "grad_muscl_hllc_minmod"])
+def test_launch_options_do_not_change_bits(form):
+    """The tuning options (fused gather + stage, face-kernel launch shapes, graph replay) give the
+    same bits as the default configuration."""
+    case = CASES["cyl_roe2_lts"]
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    outs = []
+    for opts in [{}] + OPTION_SETS:
+        s = cb.Solver(m, solver_config(case, **ADDITIVE[form]))
+        for k, v in opts.items():
+            s.set_option(k, v)
+        s.upload_state(U0)
+        s.step(12)
+        outs.append(s.download())
+    for o in outs[1:]:
+        check_state(o, outs[0], form)
+
+
 def test_nonphysical_state_is_reported():
     """A planted negative pressure (host-side input) comes back as a status with the cell id."""
     case = CASES["sod_roe1_rk3"]
