@@ -274,6 +274,106 @@ def run_ramps(args, rank, world):
         dist.destroy_process_group()
 
 
+BUMP_MACH, BUMP_R_GAS = 0.675, 287.0
+
+
+def bump_case(cb, nx, ny, seed):
+    """Configuration C3: 3x1 channel with a 10 %-thick circular-arc bump of chord 1, 8 quad layers
+    along both walls, seeded jittered (+-0.3 h) triangles elsewhere; M 0.675 freestream start with
+    total-(p, T) inflow and static-pressure outflow."""
+    m = cb.Mesh.bump(nx, ny, 3.0, 1.0, 0.1, 8, 0.3, seed, True)
+    NP = m.n_physical
+    rho, p = 1.0, 1.0 / GAMMA
+    u = BUMP_MACH * np.sqrt(GAMMA * p / rho)
+    U = cb.conserved_from_primitive(np.full(NP, rho), np.full(NP, u), np.zeros(NP), np.full(NP, p))
+    full = np.zeros((m.n_total, 4))
+    full[:NP] = U
+    full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
+    T = p / (rho * BUMP_R_GAS)
+    f = 1.0 + 0.5 * (GAMMA - 1.0) * BUMP_MACH ** 2
+    kw = dict(is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8, limiter=1, muscl=1, integrator=2,
+              inlet_rho=rho, inlet_p=p, inlet_bc=2, exit_bc=2, inlet_p0=p * f ** (GAMMA / (GAMMA - 1.0)),
+              inlet_t0=T * f, exit_p=p, r_gas=BUMP_R_GAS)
+    return m, full, kw
+
+
+def run_bump(args, rank, world):
+    """--workload bump: the mixed tri/quad bump channel with HLLC and AUSM fluxes, each in the
+    all-FP64 form and the FP32-flux / FP64-state form.  (1) At full size (about 4.2 M cells) each
+    form is timed over a fixed window of pseudo-steps from the freestream start, and the FP32
+    form's state is compared with the FP64 form's after the same steps.  (2) A mid-size channel is
+    run to a residual drop of --tol (or --max-steps) in both forms and the L2 difference of the
+    converged fields is stated.  The FP64 form is bit-identical to the FP64 C restatement (the
+    parity tests), so it stands for the FP64 oracle at sizes the oracle cannot run."""
+    import torch
+    import cfd_solver_withcuda_b200 as cb
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    out = {"metric": "cell-updates/s", "unit": "cell-updates/s", "n_gpus": world, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bump generator, "
+           "freestream start)", "forms": {}, "steady": {}}
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    m, U0, kw = bump_case(cb, args.bump_nx, args.bump_ny, args.seed)
+    NP = m.n_physical
+    out["config"] = {"workload": "bump_channel_mixed_%dx%d_gg_muscl_minmod_tvdrk3_lts_totalpT_staticp" %
+                     (args.bump_nx, args.bump_ny), "cells": NP, "faces": None, "seed": args.seed,
+                     "steps": args.steps, "mesh_build_s": None}
+    out["config"]["mesh_build_s"] = time.perf_counter() - t0
+    finals = {}
+    for flux, diss in (("hllc", 7), ("ausm", 6)):
+        for prec_name, prec in (("fp64", 0), ("fp32_flux", 1)):
+            s = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, dissipation_type=diss,
+                                               precision=prec, **kw))
+            s.set_option("keep_delu", 0)
+            s.upload_state(U0)
+            out["config"]["faces"] = s.n_faces
+            s.step_async(max(args.warmup, 3))
+            s.sync()
+            ms, info = timed_steps(s, stream, args.steps, torch)
+            steps_done = args.steps + max(args.warmup, 3)
+            finals[(flux, prec_name)] = s.download_U()[:NP]
+            out["forms"]["%s_%s" % (flux, prec_name)] = {
+                "value": NP * args.steps / (ms * 1e-3), "ms_per_step": ms / args.steps, "steps": args.steps,
+                "pseudo_steps_from_start": steps_done, "res_l2_rho": info.res_l2[0]}
+            s.close()
+        a, b = finals[(flux, "fp32_flux")], finals[(flux, "fp64")]
+        out["forms"]["%s_fp32_flux" % flux]["rel_l2_error_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["value"] = out["forms"]["hllc_fp64"]["value"]
+    out["ms_per_step"] = out["forms"]["hllc_fp64"]["ms_per_step"]
+    out["steps"] = args.steps
+    out["warmup"] = max(args.warmup, 3)
+    # Converged fields on a mid-size channel.
+    ms_, U0s, kws = bump_case(cb, args.steady_nx, args.steady_ny, args.seed)
+    NPs = ms_.n_physical
+    for flux, diss in (("hllc", 7), ("ausm", 6)):
+        res = {}
+        for prec_name, prec in (("fp64", 0), ("fp32_flux", 1)):
+            s = cb.Solver(ms_, cb.default_config(device=local, stream=stream.cuda_stream, dissipation_type=diss,
+                                                precision=prec, **kws))
+            s.set_option("keep_delu", 0)
+            s.upload_state(U0s)
+            info = s.step(1)
+            r0 = info.res_l2[0]
+            done, ratio = 1, 1.0
+            while done < args.max_steps:
+                info = s.step(args.check_every)
+                done += args.check_every
+                ratio = info.res_l2[0] / r0
+                if ratio <= args.tol:
+                    break
+            res[prec_name] = (s.download_U()[:NPs], done, ratio)
+            s.close()
+        a, b = res["fp32_flux"][0], res["fp64"][0]
+        out["steady"][flux] = {"cells": NPs, "mesh": "%dx%d" % (args.steady_nx, args.steady_ny),
+                               "steps_fp64": res["fp64"][1], "res_ratio_fp64": res["fp64"][2],
+                               "steps_fp32_flux": res["fp32_flux"][1], "res_ratio_fp32_flux": res["fp32_flux"][2],
+                               "rel_l2_error_fp32_flux_vs_fp64": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    print(json.dumps(out))
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -305,7 +405,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps"])
+    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump"])
+    ap.add_argument("--bump-nx", type=int, default=2520)
+    ap.add_argument("--bump-ny", type=int, default=840)
+    ap.add_argument("--steady-nx", type=int, default=120)
+    ap.add_argument("--steady-ny", type=int, default=40)
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--tol", type=float, default=1e-8)
@@ -319,6 +423,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "ramps":
         return run_ramps(args, rank, world)
+    if args.workload == "bump":
+        return run_bump(args, rank, world)
 
     import torch
     import torch.distributed as dist

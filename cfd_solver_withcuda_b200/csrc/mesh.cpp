@@ -357,8 +357,11 @@ struct SplitMix {
 // Channel [0, length] x [0, height] with a circular-arc bump of chord 1 centred at length/2 on
 // the lower wall (thickness = max height / chord).  n_quad_layers quad rows hug each wall; the
 // core rows are split into triangles (alternating diagonals) when `triangles` is set, and the
-// interior core nodes are jittered by +-jitter*h (seeded).  Left = subsonic inflow, right =
-// outflow, walls elsewhere.
+// interior core nodes are moved by a seeded displacement uniform in the disc of radius
+// jitter * min(hx, hy) (rejection sampling, no transcendental functions, so the mesh is the same
+// on every host).  With jitter < 0.35 no triangle of a split square can invert: its smallest
+// height, h/sqrt(2), loses at most 2 * jitter * h.  Left = subsonic inflow, right = outflow,
+// walls elsewhere.
 std::string generate_bump(Mesh &m, int nx, int ny, double length, double height, double thickness, int n_quad_layers,
                           double jitter, uint64_t seed, int triangles) {
   if (nx < 2 || ny < 2 || thickness < 0.0) return "bad bump parameters";
@@ -382,9 +385,14 @@ std::string generate_bump(Mesh &m, int nx, int ny, double length, double height,
       double s = static_cast<double>(j) / ny;
       double y = yb + (height - yb) * s;
       if (jitter > 0.0 && i > 0 && i < nx && j > nql && j < ny - nql) {
-        double hx = length / nx, hy = (height - yb) / ny;
-        x += jitter * hx * (2.0 * rng.uniform() - 1.0);
-        y += jitter * hy * (2.0 * rng.uniform() - 1.0);
+        const double hx = length / nx, hy = (height - yb) / ny, h = hx < hy ? hx : hy;
+        double a, b;
+        do {
+          a = 2.0 * rng.uniform() - 1.0;
+          b = 2.0 * rng.uniform() - 1.0;
+        } while (a * a + b * b > 1.0);
+        x += jitter * h * a;
+        y += jitter * h * b;
       }
       m.points.push_back(x);
       m.points.push_back(y);
