@@ -19,11 +19,11 @@ STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NONPHYSICAL", 4: "DT_NONPO
                 6: "DIVERGED", 7: "MESH", 8: "IO", 9: "NO_DEVICE"}
 
 BC_INLET, BC_EXIT, BC_WALL, BC_SYMMETRY = 0, 1, 2, 3
-DISS_LLF, DISS_ROE, DISS_AUSM, DISS_HLLC = 1, 3, 6, 7
+DISS_LLF, DISS_ROE, DISS_AUSM, DISS_HLLC, DISS_AUSM_GPU = 1, 3, 6, 7, 8
 LIM_REF_MINMOD, LIM_MINMOD, LIM_VANLEER, LIM_SUPERBEE, LIM_VANALBADA = 0, 1, 2, 3, 4
-INT_REFERENCE, INT_RK4, INT_SSPRK3 = 0, 1, 2
-INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT, INLET_FIXED = 0, 1, 2, 3
-EXIT_SUPERSONIC, EXIT_SUBSONIC_REF, EXIT_STATIC_P = 0, 1, 2
+INT_REFERENCE, INT_RK4, INT_SSPRK3, INT_RK3_GPU_REF, INT_RK4_GPU_REF = 0, 1, 2, 3, 4
+INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT, INLET_FIXED, INLET_FARFIELD = 0, 1, 2, 3, 4
+EXIT_SUPERSONIC, EXIT_SUBSONIC_REF, EXIT_STATIC_P, EXIT_FIXED_P_REF = 0, 1, 2, 3
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 MUSCL_REFERENCE, MUSCL_GRADIENT = 0, 1
 
@@ -109,6 +109,8 @@ SIGNATURES = {
     "cfd_download_stage_state": (_I, [_P, _DP]),
     "cfd_download_U": (_I, [_P, _DP]),
     "cfd_gradient": (_I, [_P, _I, _DP]),
+    "cfd_eval_limiter": (_I, [_I, _DP, _DP, _I, _DP, _I]),
+    "cfd_eval_face_flux": (_I, [_I, _I, _DP, _DP, _DP, _DP, _I, _DP, _I]),
     "cfd_amr_tags": (_I, [_P, _D, _D, _DP, ctypes.POINTER(ctypes.c_uint8)]),
     "cfd_kernel_time": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_longlong)]),
     "cfd_evaluate_net_flux_noalloc": (_I, [ctypes.POINTER(FluxArrays), ctypes.POINTER(Config), _P]),
@@ -420,6 +422,28 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def eval_limiter(limiter, a, b, device=0):
+    """phi(a, b) of the limiter family on the GPU (cfd_eval_limiter)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros_like(a)
+    _check(lib().cfd_eval_limiter(limiter, _dp(a), _dp(b), a.size, _dp(out), device))
+    return out
+
+
+def eval_face_flux(scheme, UL, UR, normals, lengths, precision=PREC_FP64, device=0):
+    """Face fluxes [n, 4] of conserved left/right states [n, 4] on the GPU (cfd_eval_face_flux)."""
+    UL = np.ascontiguousarray(UL, dtype=np.float64)
+    UR = np.ascontiguousarray(UR, dtype=np.float64)
+    normals = np.ascontiguousarray(normals, dtype=np.float64)
+    lengths = np.ascontiguousarray(lengths, dtype=np.float64)
+    n = UL.shape[0]
+    F = np.zeros((n, 4))
+    _check(lib().cfd_eval_face_flux(scheme, precision, _dp(UL), _dp(UR), _dp(normals), _dp(lengths), n, _dp(F),
+                                    device))
+    return F
 
 
 def conserved_from_primitive(rho, u, v, p):

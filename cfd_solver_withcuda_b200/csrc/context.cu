@@ -168,52 +168,59 @@ struct TimedScope {
   }
 };
 
-// Launch sequence of one pseudo-step (loop body of src/Solver.cpp:94-125).
+// Stage sequence of one pseudo-step for the configured integrator.
+struct StagePlan {
+  int n;        // stages
+  int kind0;    // stage kind of stage 0 (kinds kind0 .. kind0 + n - 1; 0 = explicit)
+  int src_S;    // the supersonic-exit copy of stages > 0 reads the stage state
+  int lts_mode; // 0: per-stage rule of the reference (LTS in stage 1 only), 1: dt frozen per step
+};
+
+StagePlan stage_plan(const cfd_config &c, int consistent) {
+  if (c.integrator == CFD_INT_REFERENCE && !c.time_accurate) return {1, 0, 0, 0};
+  if (c.integrator == CFD_INT_RK4) return {4, 11, 1, 1};
+  if (c.integrator == CFD_INT_RK3_GPU_REF) return {3, 21, 1, 1};
+  if (c.integrator == CFD_INT_RK4_GPU_REF) return {4, 31, 1, 1};
+  if (c.integrator == CFD_INT_SSPRK3) return {3, 1, consistent, 1};
+  return {3, 1, consistent, 0};
+}
+
+// lts argument of the stage kernels for stage k (see k_stage).
+int stage_lts(const StagePlan &p, const cfd_config &c, int k) {
+  if (p.kind0 == 0) return 0;
+  if (p.lts_mode == 1) return c.local_time_stepping ? 2 : 3;
+  return (k == 0 && c.local_time_stepping) ? 1 : 0;
+}
+
+// Launch sequence of one pseudo-step (loop body of src/Solver.cpp:94-125): per stage the boundary
+// conditions, the residual (face-based forms: gradients, face fluxes, gather) and the update.
 int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
   const cfd_config &c = ctx->cfg;
   cudaStream_t s = ctx->stream;
   DevMesh &m = ctx->dm;
   DevState &st = ctx->ds;
   int n = 0;
-  const int cons = ctx->fp.consistent;
-  if (c.integrator == CFD_INT_REFERENCE && !c.time_accurate) {
-    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, 0); }
-    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, 0); }
-    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, 0, 0, fuse_final, ctx->keep_delu); }
-    return n;
-  }
-  if (c.integrator == CFD_INT_RK4) {
-    const int lts = c.local_time_stepping ? 2 : 3;
-    for (int k = 0; k < 4; k++) {
-      { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0); }
-      { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
-      { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, 11 + k, lts, k == 3 ? fuse_final : 0, ctx->keep_delu); }
-    }
-    return n;
-  }
-  // Three-stage forms: the reference's Runge_Kutta_Method (LTS in stage 1 only, Min_dt of the
-  // current evaluation in stages 2-3) or the stage-consistent SSP-RK3 (dt frozen per step).
-  const bool ssp = c.integrator == CFD_INT_SSPRK3;
+  const StagePlan p = stage_plan(c, ctx->fp.consistent);
   const bool faces = ctx->dm.NF > 0;
-  for (int k = 0; k < 3; k++) {
-    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0 && cons); }
-    int lts;
-    if (ssp) lts = c.local_time_stepping ? 2 : 3;
-    else lts = (k == 0 && c.local_time_stepping) ? 1 : 0;
+  for (int k = 0; k < p.n; k++) {
+    const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
+    const int lts = stage_lts(p, c, k);
+    const int fin = (k == p.n - 1) ? fuse_final : 0;
+    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0); }
     if (faces) {
       { TimedScope ts(ctx, TK_GRAD); n += launch_muscl_gradients(s, m, st); }
       { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
       if (ctx->fuse_gather && (lts == 1 || lts == 2)) {
         TimedScope ts(ctx, TK_GATHER_STAGE);
-        n += launch_gather_stage(s, m, st, ctx->fp, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu);
+        n += launch_gather_stage(s, m, st, ctx->fp, kind, lts, fin, ctx->keep_delu);
       } else {
         { TimedScope ts(ctx, TK_FLUX); n += launch_gather(s, m, st, ctx->fp); }
-        { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu); }
+        { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
       }
       continue;
     }
     { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
-    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, k + 1, lts, k == 2 ? fuse_final : 0, ctx->keep_delu); }
+    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
   }
   return n;
 }
@@ -402,14 +409,19 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       return fail(CFD_ERR_MESH, "invalid boundary entry " + std::to_string(e));
   }
   const int diss = cfg->dissipation_type;
-  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && diss != CFD_DISS_AUSM && diss != CFD_DISS_HLLC)
+  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && diss != CFD_DISS_AUSM && diss != CFD_DISS_HLLC &&
+      diss != CFD_DISS_AUSM_GPU)
     return fail(CFD_ERR_BAD_ARG, "dissipation type " + std::to_string(diss) + " is not available in this build");
+  if (diss == CFD_DISS_AUSM_GPU && !(cfg->is_second_order && cfg->muscl))
+    return fail(CFD_ERR_BAD_ARG, "the reference GPU AUSM face flux is available in the gradient-MUSCL form only");
+  if (cfg->integrator < CFD_INT_REFERENCE || cfg->integrator > CFD_INT_RK4_GPU_REF)
+    return fail(CFD_ERR_BAD_ARG, "bad integrator");
   if ((diss == CFD_DISS_AUSM || diss == CFD_DISS_HLLC) && cfg->is_second_order && !cfg->muscl)
     return fail(CFD_ERR_BAD_ARG, "second-order AUSM / HLLC use the gradient-MUSCL form (muscl = 1)");
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
-  if (cfg->inlet_bc < 0 || cfg->inlet_bc > 3 || cfg->exit_bc < 0 || cfg->exit_bc > 2)
+  if (cfg->inlet_bc < 0 || cfg->inlet_bc > CFD_INLET_FARFIELD || cfg->exit_bc < 0 || cfg->exit_bc > CFD_EXIT_FIXED_P_REF)
     return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
   if (cfg->precision != CFD_PREC_FP64 && !(cfg->precision == CFD_PREC_FP32_FLUX && cfg->muscl && cfg->is_second_order))
     return fail(CFD_ERR_BAD_ARG, "the FP32-flux form is available for the gradient-MUSCL scheme only");
@@ -770,7 +782,7 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info) {
 
 cfd_status cfd_apply_boundary_conditions(cfd_ctx *ctx) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
-  ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, 0);
+  ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, 0, 0);
   CUDA_TRY(cudaGetLastError());
   return sync_status(ctx, nullptr);
 }
@@ -796,13 +808,12 @@ cfd_status cfd_explicit_method(cfd_ctx *ctx) {
 cfd_status cfd_runge_kutta_method(cfd_ctx *ctx) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
   const cfd_config &c = ctx->cfg;
-  const int cons = ctx->fp.consistent;
-  const bool ssp = c.integrator == CFD_INT_SSPRK3;
-  for (int k = 0; k < 3; k++) {
-    if (k > 0) ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, cons);
+  StagePlan p = stage_plan(c, ctx->fp.consistent);
+  if (p.kind0 == 0) p = {3, 1, ctx->fp.consistent, 0};  // the reference's RK3 on an explicit config
+  for (int k = 0; k < p.n; k++) {
+    if (k > 0) ctx->launches += launch_bc(ctx->stream, ctx->dm, ctx->ds, ctx->bp, p.src_S, 1);
     ctx->launches += launch_flux(ctx->stream, ctx->dm, ctx->ds, ctx->fp, k > 0);
-    int lts = ssp ? (c.local_time_stepping ? 2 : 3) : ((k == 0 && c.local_time_stepping) ? 1 : 0);
-    ctx->launches += launch_stage(ctx->stream, ctx->dm, ctx->ds, k + 1, lts, 0, 1);
+    ctx->launches += launch_stage(ctx->stream, ctx->dm, ctx->ds, p.kind0 + k, stage_lts(p, c, k), 0, 1);
   }
   CUDA_TRY(cudaGetLastError());
   ctx->prim_from_S = true;
@@ -821,7 +832,8 @@ cfd_status cfd_estimate_error(cfd_ctx *ctx, double error[4]) {
 
 cfd_status cfd_update(cfd_ctx *ctx) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
-  ctx->launches += launch_update(ctx->stream, ctx->dm, ctx->ds);
+  const int direct = ctx->cfg.integrator == CFD_INT_RK3_GPU_REF || ctx->cfg.integrator == CFD_INT_RK4_GPU_REF;
+  ctx->launches += launch_update(ctx->stream, ctx->dm, ctx->ds, direct);
   CUDA_TRY(cudaGetLastError());
   ctx->prim_from_S = false;
   return sync_status(ctx, nullptr);
@@ -949,6 +961,65 @@ cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, dou
     if (indicator) indicator[ctx->perm[i]] = h[i];
     if (tags) tags[ctx->perm[i]] = ht[i];
   }
+  return CFD_OK;
+}
+
+namespace {
+// Device copies of host arrays for the pointwise entry points; freed on scope exit.
+struct DevBufs {
+  std::vector<void *> p;
+  ~DevBufs() {
+    for (void *q : p) cudaFree(q);
+  }
+  double *put(const double *h, size_t n) {
+    void *d = nullptr;
+    if (cudaMalloc(&d, n * sizeof(double) + 8) != cudaSuccess) return nullptr;
+    p.push_back(d);
+    if (h && cudaMemcpy(d, h, n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+    return static_cast<double *>(d);
+  }
+};
+
+cfd_status set_eval_device(int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CFD_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(CFD_ERR_BAD_ARG, "bad device ordinal");
+  CUDA_TRY(cudaSetDevice(device));
+  return CFD_OK;
+}
+}  // namespace
+
+cfd_status cfd_eval_limiter(int limiter, const double *a, const double *b, int n, double *out, int device) {
+  if (n < 0 || (n > 0 && (!a || !b || !out))) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  if (limiter < CFD_LIM_MINMOD || limiter > CFD_LIM_VANALBADA) return fail(CFD_ERR_BAD_ARG, "bad limiter");
+  if (n == 0) return CFD_OK;
+  cfd_status st = set_eval_device(device);
+  if (st != CFD_OK) return st;
+  DevBufs d;
+  double *da = d.put(a, n), *db = d.put(b, n), *dout = d.put(nullptr, n);
+  if (!da || !db || !dout) return fail(CFD_ERR_CUDA, "device buffers");
+  launch_eval_limiter(0, limiter, da, db, n, dout);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpy(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return CFD_OK;
+}
+
+cfd_status cfd_eval_face_flux(int scheme, int precision, const double *UL, const double *UR, const double *normals,
+                              const double *lengths, int n, double *F, int device) {
+  if (n < 0 || (n > 0 && (!UL || !UR || !normals || !lengths || !F))) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  if (scheme != CFD_DISS_ROE && scheme != CFD_DISS_AUSM && scheme != CFD_DISS_HLLC && scheme != CFD_DISS_AUSM_GPU)
+    return fail(CFD_ERR_BAD_ARG, "bad face-flux scheme");
+  if (precision != CFD_PREC_FP64 && precision != CFD_PREC_FP32_FLUX) return fail(CFD_ERR_BAD_ARG, "bad precision");
+  if (n == 0) return CFD_OK;
+  cfd_status st = set_eval_device(device);
+  if (st != CFD_OK) return st;
+  DevBufs d;
+  double *dl = d.put(UL, 4 * (size_t)n), *dr = d.put(UR, 4 * (size_t)n), *dn = d.put(normals, 2 * (size_t)n),
+         *dlen = d.put(lengths, n), *dF = d.put(nullptr, 4 * (size_t)n);
+  if (!dl || !dr || !dn || !dlen || !dF) return fail(CFD_ERR_CUDA, "device buffers");
+  launch_eval_face_flux(0, scheme, precision, dl, dr, dn, dlen, n, dF);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpy(F, dF, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
   return CFD_OK;
 }
 

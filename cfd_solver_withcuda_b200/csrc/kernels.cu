@@ -160,7 +160,11 @@ __global__ void k_prim_all(DevMesh m, DevState st) {
 //   supersonic exit  src/Exit_Boundary_Conditions.cpp:68-94 (copy of U_Cells of the interior cell)
 //   subsonic exit    src/Exit_Boundary_Conditions.cpp:83-85 (no-op in the reference)
 // Additive forms: total-(p, T) characteristic inflow and static-pressure outflow.
-__global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
+//   far field        CUDA_KERNELS/Boundary_Conditions_Cuda_Kernels.cu:257-325 (inlet kind 4)
+//   fixed-p exit     src/Exit_Boundary_Conditions.cpp:8-66 (exit kind 3)
+// src_is_S: the supersonic-exit copy reads the stage state (stage-consistent forms) instead of
+// U^n; cur_is_S: the state the primitives were last computed from is the stage state.
+__global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S, int cur_is_S) {
   const int e = item_index(m.bblk, m.NB);
   if (e >= m.NB || step_done(st.ctl)) return;
   const int4 b = m.bnd[e];
@@ -180,7 +184,17 @@ __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
     G2 = rho * v2g;
     G3 = ((p / kGM1) + rho * vmag);
   } else if (kind == 0) {
-    if (bp.inlet_bc == 3) {
+    if (bp.inlet_bc == 4) {
+      const double *Uc = cur_is_S ? st.S : st.U;
+      const int ld = cur_is_S ? NP : NT;
+      const double Ui[4] = {Uc[c], Uc[ld + c], Uc[2 * ld + c], Uc[3 * ld + c]};
+      double Gf[4];
+      farfield_state(Ui, m.nx[f * NP + c], m.ny[f * NP + c], bp.inlet_rho, bp.inlet_u, bp.inlet_v, bp.inlet_p, Gf);
+      G0 = Gf[0];
+      G1 = Gf[1];
+      G2 = Gf[2];
+      G3 = Gf[3];
+    } else if (bp.inlet_bc == 3) {
       // Fully prescribed inflow (rho, u, v, p), per boundary entry when given (batched solves).
       const double4 q = m.bstate ? m.bstate[e] : make_double4(bp.inlet_rho, bp.inlet_u, bp.inlet_v, bp.inlet_p);
       G0 = q.x;
@@ -235,6 +249,14 @@ __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S) {
       G1 = Us[ld + c];
       G2 = Us[2 * ld + c];
       G3 = Us[3 * ld + c];
+    } else if (bp.exit_bc == 3) {
+      const double rho_Et = cur_is_S ? st.S[3 * NP + c] : st.U[3 * NT + c];
+      double Gf[4];
+      fixed_p_exit_state(rho, u, v, p, rho_Et, m.nx[f * NP + c], m.ny[f * NP + c], bp.exit_p, Gf);
+      G0 = Gf[0];
+      G1 = Gf[1];
+      G2 = Gf[2];
+      G3 = Gf[3];
     } else {
       // Static-pressure outflow: rho, V extrapolated; p prescribed when the normal Mach
       // number is subsonic, extrapolated otherwise.
@@ -547,6 +569,8 @@ __global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, Flu
                      qR[3] / T(kGM1) + T(0.5) * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])};
     if (DISS == 6) {
       ausm_face<T>(UL, UR, nx, ny, dl, A);
+    } else if (DISS == 8) {
+      ausm_gpu_face<T>(UL, UR, nx, ny, dl, A);
     } else {
       const T q5L[5] = {qL[0], qL[1], qL[2], qL[3], aL}, q5R[5] = {qR[0], qR[1], qR[2], qR[3], aR};
       hllc_face<T>(q5L, UL, q5R, UR, nx, ny, dl, A);
@@ -653,6 +677,17 @@ __device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const doub
 // (:26-103) for one cell, written with the reference's association order.  kind: 1,2,3 RK3
 // stages, 0 explicit, 11..14 classical RK4.  The final kind writes dU and, with fuse_final,
 // applies Estimate_Error's terms (e[0..3]), the residual squares (e[4..7]) and Update().
+// Stage kinds: 0 explicit; 1-3 the three-stage forms (reference Runge_Kutta_Method or SSP-RK3);
+// 11-14 classical RK4; 21-23 the reference GPU TVD-RK3 kernel (21, 22 equal 1, 2); 31-34 the
+// reference GPU RK4 kernel.  Kinds 23 and 34 produce U^{n+1} itself, the others dU.
+__host__ __device__ __forceinline__ bool first_kind(int kind) {
+  return kind == 1 || kind == 11 || kind == 21 || kind == 31;
+}
+__host__ __device__ __forceinline__ bool final_kind(int kind) {
+  return kind == 0 || kind == 3 || kind == 14 || kind == 23 || kind == 34;
+}
+__host__ __device__ __forceinline__ bool direct_kind(int kind) { return kind == 23 || kind == 34; }
+
 // Inputs of one cell's stage update that do not depend on the residual: U^n, the stage state
 // (RK3 stages 2 and 3) and 1/A.  Loaded ahead of the residual gather so that both sets of loads
 // are in flight together.
@@ -665,7 +700,7 @@ __device__ __forceinline__ void load_stage_in(const DevMesh &m, const DevState &
   in.invA = m.inv_area[c];
 #pragma unroll
   for (int k = 0; k < 4; k++) in.Un[k] = st.U[k * NT + c];
-  if (kind == 2 || kind == 3) {
+  if (kind == 2 || kind == 3 || kind == 22 || kind == 23) {
 #pragma unroll
     for (int k = 0; k < 4; k++) in.Sk[k] = st.S[k * NP + c];
   }
@@ -680,10 +715,10 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
 #pragma unroll
   for (int k = 0; k < 4; k++) Un[k] = in.Un[k];
   bool final_stage = false;
-  if (kind == 1) {
+  if (kind == 1 || kind == 21) {
 #pragma unroll
     for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
-  } else if (kind == 2) {
+  } else if (kind == 2 || kind == 22) {
 #pragma unroll
     for (int k = 0; k < 4; k++) out[k] = 0.25 * (in.Sk[k] + 3.0 * Un[k] - dt * invA * Rk[k]);
   } else if (kind == 3) {
@@ -693,6 +728,26 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
   } else if (kind == 0) {
 #pragma unroll
     for (int k = 0; k < 4; k++) out[k] = -dt * invA * Rk[k];
+    final_stage = true;
+  } else if (kind == 23) {
+    // tvd_rk3_kernel stage 3 (CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu:125-130):
+    // U^{n+1} = (1/3)(U^n + 2 U2 - 2 dt/V R(U2)).
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = (1.0 / 3.0) * (Un[k] + 2.0 * in.Sk[k] - 2.0 * dt * invA * Rk[k]);
+    final_stage = true;
+  } else if (kind == 31 || kind == 32) {
+    // rk4_complete_kernel stages 1-2 (CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu:43-56): the
+    // stage state is U^n - dt/(2V) R of the previous stage state (its dissipation terms are zero
+    // for the inviscid path).
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = Un[k] - 0.5 * dt * invA * Rk[k];
+  } else if (kind == 33) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = Un[k] - dt * invA * Rk[k];
+  } else if (kind == 34) {
+    // Stage 4 (:64-72): U^{n+1} = U^n - dt/(6V) R(U3), the last stage's residual only.
+#pragma unroll
+    for (int k = 0; k < 4; k++) out[k] = Un[k] - (dt * invA / 6.0) * Rk[k];
     final_stage = true;
   } else if (kind == 11) {
 #pragma unroll
@@ -723,18 +778,30 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
     store_prim(st.prim, NT, c, q);
     if (!ok) flag_bad(st.status, c);
   } else {
+    // dU and U^{n+1}: the forms that produce U^{n+1} directly keep it exactly (dU = U^{n+1} - U^n
+    // is stored for Estimate_Error, and U^{n+1} is parked in the stage state for Update()).
+    const bool direct = direct_kind(kind);
+    double du[4], nu[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      du[k] = direct ? out[k] - Un[k] : out[k];
+      nu[k] = direct ? out[k] : Un[k] + out[k];
+    }
     if (keep_delu || !fuse_final) {
 #pragma unroll
-      for (int k = 0; k < 4; k++) st.dU[k * NP + c] = out[k];
+      for (int k = 0; k < 4; k++) st.dU[k * NP + c] = du[k];
+    }
+    if (direct && !fuse_final) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) st.S[k * NP + c] = nu[k];
     }
     if (fuse_final) {
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        e[k] = err_term(out[k], Un[k]);
+        e[k] = err_term(du[k], Un[k]);
         e[4 + k] = Rk[k] * Rk[k];
-        double nu = Un[k] + out[k];
-        st.U[k * NT + c] = nu;
-        Un[k] = nu;
+        st.U[k * NT + c] = nu[k];
+        Un[k] = nu[k];
       }
       Prim q;
       bool ok = eos_prim(Un[0], Un[1], Un[2], Un[3], q);
@@ -762,21 +829,22 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const double dtmin = st.ctl[CTL_DTMIN];
   if (active) {
-    if (kind == 1 || kind == 11) {
+    const bool first = first_kind(kind);
+    if (first) {
       if (lts == 2) st.dtk[c] = st.dtc[c];
     }
     double dt;
     if (lts == 0) dt = dtmin;
     else if (lts == 1) dt = st.dtc[c];
-    else if (lts == 2) dt = (kind == 1 || kind == 11) ? st.dtc[c] : st.dtk[c];
-    else dt = (kind == 1 || kind == 11) ? dtmin : st.ctl[CTL_DTSTEP];
+    else if (lts == 2) dt = first ? st.dtc[c] : st.dtk[c];
+    else dt = first ? dtmin : st.ctl[CTL_DTSTEP];
     double Rk[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) Rk[k] = st.R[k * NP + c];
     cell_update(m, st, c, kind, dt, Rk, fuse_final, keep_delu, e);
   }
-  if ((kind == 1 || kind == 11) && blockIdx.x == 0 && threadIdx.x == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
-  if (fuse_final && (kind == 3 || kind == 0 || kind == 14)) {
+  if (first_kind(kind) && blockIdx.x == 0 && threadIdx.x == 0 && !done) st.ctl[CTL_DTSTEP] = dtmin;
+  if (fuse_final && final_kind(kind)) {
     if (done) return;
     const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : dtmin;
     reduce_err_and_epilogue(st, e, true, dt_time);
@@ -793,8 +861,8 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
   const int NP = m.NP;
   const int c = item_index(m.cblk, NP);
   if (step_done(st.ctl)) return;
-  const bool first = (kind == 1 || kind == 11);
-  const bool final_kind = (kind == 3 || kind == 0 || kind == 14);
+  const bool first = first_kind(kind);
+  const bool is_final = final_kind(kind);
   double dtc = 1e308 * 10.0;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (c < NP) {
@@ -819,7 +887,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
   }
   const double bm = block_min(dtc, sh);
   if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
-  const bool do_err = fuse_final && final_kind;
+  const bool do_err = fuse_final && is_final;
   if (do_err) {
     __shared__ double sh8[8 * 32];
     const double sq = block_sums<8>(e, sh8);
@@ -870,14 +938,15 @@ __global__ void __launch_bounds__(kBlock) k_error(DevMesh m, DevState st) {
 }
 
 // Update() (src/Error_Estimate_Update.cpp:31-43): U += dU, primitives refreshed.
-__global__ void __launch_bounds__(kBlock) k_update(DevMesh m, DevState st) {
+// from_S: the integrator produced U^{n+1} itself (reference GPU forms), parked in the stage state.
+__global__ void __launch_bounds__(kBlock) k_update(DevMesh m, DevState st, int from_S) {
   const int NP = m.NP, NT = m.NT;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= NP) return;
   double u[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    u[k] = st.U[k * NT + c] + st.dU[k * NP + c];
+    u[k] = from_S ? st.S[k * NP + c] : st.U[k * NT + c] + st.dU[k * NP + c];
     st.U[k * NT + c] = u[k];
   }
   Prim q;
@@ -973,6 +1042,47 @@ __global__ void k_instance_residual(const double *R, const int *start, const int
   for (int c = start[i] + threadIdx.x; c < end[i]; c += blockDim.x) acc += R[c] * R[c];
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) out[i] = acc;
+}
+
+// ---- Pointwise evaluation of the face functions (checkers' entry points) ----
+// phi(a, b) of the limiter family for n pairs.
+__global__ void k_eval_limiter(int limiter, const double *a, const double *b, int n, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = phi_ab<double>(limiter, a[i], b[i]);
+}
+
+// Face flux of scheme `scheme` (3 Roe average + dissipation, 6 AUSM, 7 HLLC, 8 reference GPU AUSM)
+// for n conserved left/right states [n][4], outward normals [n][2] and lengths [n]; T is the
+// arithmetic precision (the states are rounded to T first, as in the FP32-flux form).  Primitive
+// variables for Roe and HLLC come from the reference EOS (eos_prim).
+template <typename T>
+__global__ void k_eval_face_flux(int scheme, const double *UL, const double *UR, const double *nrm, const double *len,
+                                 int n, double *F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const T nx = T(nrm[2 * i]), ny = T(nrm[2 * i + 1]), dl = T(len[i]);
+  T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
+  const T uL[4] = {T(UL[4 * i]), T(UL[4 * i + 1]), T(UL[4 * i + 2]), T(UL[4 * i + 3])};
+  const T uR[4] = {T(UR[4 * i]), T(UR[4 * i + 1]), T(UR[4 * i + 2]), T(UR[4 * i + 3])};
+  if (scheme == 6) {
+    ausm_face<T>(uL, uR, nx, ny, dl, A);
+  } else if (scheme == 8) {
+    ausm_gpu_face<T>(uL, uR, nx, ny, dl, A);
+  } else {
+    Prim pl, pr;
+    eos_prim(UL[4 * i], UL[4 * i + 1], UL[4 * i + 2], UL[4 * i + 3], pl);
+    eos_prim(UR[4 * i], UR[4 * i + 1], UR[4 * i + 2], UR[4 * i + 3], pr);
+    const T qL[5] = {T(pl.rho), T(pl.u), T(pl.v), T(pl.p), T(pl.a)};
+    const T qR[5] = {T(pr.rho), T(pr.u), T(pr.v), T(pr.p), T(pr.a)};
+    if (scheme == 7) {
+      hllc_face<T>(qL, uL, qR, uR, nx, ny, dl, A);
+    } else {
+      average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
+      roe_1o<T>(qL[0], qL[1], qL[2], qL[3], qL[4], qR[0], qR[1], qR[2], qR[3], qR[4], nx, ny, dl, false, D);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) F[4 * i + k] = double(A[k] - D[k]);
 }
 
 // ---- AMR tagging (TagRefinableCells, src/Grid_Refine_Functions.cpp:33-63) on the device ----
@@ -1089,13 +1199,13 @@ int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st) {
   return 1;
 }
 
-int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int src_is_S) {
+int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int src_is_S, int cur_is_S) {
   if (m.NB == 0) return 0;
   if (m.bblk) {
     if (m.n_bblk == 0) return 0;
-    k_bc<<<m.n_bblk, kWorkItemBlock, 0, s>>>(m, st, bp, src_is_S);
+    k_bc<<<m.n_bblk, kWorkItemBlock, 0, s>>>(m, st, bp, src_is_S, cur_is_S);
   } else {
-    k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S);
+    k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S, cur_is_S);
   }
   return 1;
 }
@@ -1154,6 +1264,7 @@ template <typename T, int MINB>
 void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st, const FluxParams &fp) {
   if (fp.dissipation == 6) k_faces<T, 6, MINB><<<g, b, 0, s>>>(m, st, fp);
   else if (fp.dissipation == 7) k_faces<T, 7, MINB><<<g, b, 0, s>>>(m, st, fp);
+  else if (fp.dissipation == 8) k_faces<T, 8, MINB><<<g, b, 0, s>>>(m, st, fp);
   else k_faces<T, 3, MINB><<<g, b, 0, s>>>(m, st, fp);
 }
 
@@ -1187,8 +1298,22 @@ int launch_error(cudaStream_t s, const DevMesh &m, DevState &st) {
   return 1;
 }
 
-int launch_update(cudaStream_t s, const DevMesh &m, DevState &st) {
-  k_update<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st);
+int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const double *b, int n, double *out) {
+  if (n <= 0) return 0;
+  k_eval_limiter<<<nblk(n, kBlock), kBlock, 0, s>>>(limiter, a, b, n, out);
+  return 1;
+}
+
+int launch_eval_face_flux(cudaStream_t s, int scheme, int precision, const double *UL, const double *UR,
+                          const double *nrm, const double *len, int n, double *F) {
+  if (n <= 0) return 0;
+  if (precision == 1) k_eval_face_flux<float><<<nblk(n, kBlock), kBlock, 0, s>>>(scheme, UL, UR, nrm, len, n, F);
+  else k_eval_face_flux<double><<<nblk(n, kBlock), kBlock, 0, s>>>(scheme, UL, UR, nrm, len, n, F);
+  return 1;
+}
+
+int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S) {
+  k_update<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, from_S);
   return 1;
 }
 

@@ -95,7 +95,7 @@ struct BcParams {
 // Kernel launchers (stream-ordered, no host synchronisation).  Each returns the number of
 // kernels launched.
 int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st);
-int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int stage_src_is_S);
+int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int stage_src_is_S, int cur_is_S);
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int stage_src_is_S);
 // kind: 1,2,3 = reference RK3 stages; 0 = Explicit; 11..14 = RK4 stages; fuse_final = apply
 // Estimate_Error + Update in the last stage's kernel.
@@ -107,7 +107,10 @@ int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxPara
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
                         int fuse_final, int keep_delu);
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
-int launch_update(cudaStream_t s, const DevMesh &m, DevState &st);
+int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S);
+int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const double *b, int n, double *out);
+int launch_eval_face_flux(cudaStream_t s, int scheme, int precision, const double *UL, const double *UR,
+                          const double *nrm, const double *len, int n, double *F);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
 int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);

@@ -330,4 +330,137 @@ __device__ __forceinline__ void hllc_face(const T qL[5], const T UL[4], const T 
   for (int i = 0; i < 4; i++) F[i] = flux[i] * area;
 }
 
+
+// AUSM face flux of the reference's GPU kernel ausm_flux_kernel
+// (CUDA_KERNELS/Flux_Calculations_Cuda_Kernels.cu:11-113), 2-D: its third velocity and normal
+// components are zero and kept in the expressions, so the arithmetic is the kernel's own.  Its
+// macros expand to gamma 1.4 and R 287.5; T = P/(rho R), a = sqrt(gamma R T); the interface Mach
+// number upwinds the convected part, the split pressures are added.
+template <typename T>
+__device__ __forceinline__ T ausm_gpu_mplus(T M) {
+  if (M >= T(1.0)) return M;
+  else if (M > T(-1.0) && M < T(1.0)) return T(0.25) * (M + T(1.0)) * (M + T(1.0));
+  else return T(0.0);
+}
+template <typename T>
+__device__ __forceinline__ T ausm_gpu_mminus(T M) {
+  if (M >= T(1.0)) return T(0.0);
+  else if (M > T(-1.0) && M < T(1.0)) return T(-0.25) * (M - T(1.0)) * (M - T(1.0));
+  else return M;
+}
+template <typename T>
+__device__ __forceinline__ T ausm_gpu_pplus(T P, T M) {
+  if (M >= T(1.0)) return P;
+  else if (M > T(-1.0) && M < T(1.0)) return (P * T(0.25)) * (M + T(1.0)) * (M + T(1.0)) * (T(2.0) - M);
+  else return T(0.0);
+}
+template <typename T>
+__device__ __forceinline__ T ausm_gpu_pminus(T P, T M) {
+  if (M >= T(1.0)) return T(0.0);
+  else if (M > T(-1.0) && M < T(1.0)) return (P * T(0.25)) * (M - T(1.0)) * (M - T(1.0)) * (T(2.0) + M);
+  else return P;
+}
+
+template <typename T>
+__device__ __forceinline__ void ausm_gpu_face(const T UL[4], const T UR[4], const T nx, const T ny, const T area,
+                                              T F[4]) {
+  const T g = T(1.4), Rg = T(287.5), gm1 = T(1.4 - 1.0), gR = T(1.4 * 287.5), zero = T(0.0);
+  const T rho_L = UL[0];
+  const T u_L = UL[1] / rho_L, v_L = UL[2] / rho_L, w_L = zero / rho_L;
+  const T E_L = UL[3];
+  const T P_L = gm1 * (E_L - T(0.5) * rho_L * (u_L * u_L + v_L * v_L + w_L * w_L));
+  const T T_L = P_L / (rho_L * Rg);
+  const T a_L = sqrt(gR * T_L);
+  const T rho_R = UR[0];
+  const T u_R = UR[1] / rho_R, v_R = UR[2] / rho_R, w_R = zero / rho_R;
+  const T E_R = UR[3];
+  const T P_R = gm1 * (E_R - T(0.5) * rho_R * (u_R * u_R + v_R * v_R + w_R * w_R));
+  const T T_R = P_R / (rho_R * Rg);
+  const T a_R = sqrt(gR * T_R);
+  (void)g;
+  const T nz = zero;
+  const T V_L = u_L * nx + v_L * ny + w_L * nz;
+  const T V_R = u_R * nx + v_R * ny + w_R * nz;
+  const T M_L = V_L / a_L, M_R = V_R / a_R;
+  const T Mi = ausm_gpu_mplus(M_L) + ausm_gpu_mminus(M_R);
+  const T Pi = ausm_gpu_pplus(P_L, M_L) + ausm_gpu_pminus(P_R, M_R);
+  const T H_L = (E_L + P_L) / rho_L, H_R = (E_R + P_R) / rho_R;
+  if (Mi > T(0)) {
+    F[0] = area * rho_L * a_L * Mi;
+    F[1] = area * (rho_L * a_L * Mi * u_L + Pi * nx);
+    F[2] = area * (rho_L * a_L * Mi * v_L + Pi * ny);
+    F[3] = area * rho_L * a_L * Mi * H_L;
+  } else {
+    F[0] = area * rho_R * a_R * Mi;
+    F[1] = area * (rho_R * a_R * Mi * u_R + Pi * nx);
+    F[2] = area * (rho_R * a_R * Mi * v_R + Pi * ny);
+    F[3] = area * rho_R * a_R * Mi * H_R;
+  }
+}
+
+// Far-field (Riemann-invariant) boundary state of the reference's GPU kernel farfield_bc_kernel
+// (CUDA_KERNELS/Boundary_Conditions_Cuda_Kernels.cu:257-325, with calculate_primitive_device
+// :28-49 and its GAMMA_VAL 1.4, GAMMA_M1 0.4): the interior conserved state Ui, the outward unit
+// normal (nx, ny) and the free stream give the conserved boundary state G, written to the ghost.
+__device__ __forceinline__ void farfield_state(const double Ui[4], double nx, double ny, double rho_inf,
+                                               double u_inf, double v_inf, double p_inf, double G[4]) {
+  const double GV = 1.4, GM = 0.4;
+  double rho = Ui[0];
+  if (rho < 1e-12) rho = 1e-12;
+  const double u = Ui[1] / rho, v = Ui[2] / rho, E = Ui[3];
+  const double kinetic_energy = 0.5 * rho * (u * u + v * v);
+  double p = GM * (E - kinetic_energy);
+  if (p < 1e-12) p = 1e-12;
+  const double rho_i = rho, u_i = u, v_i = v, p_i = p;
+  const double a_i = sqrt(GV * p_i / rho_i);
+  const double a_inf = sqrt(GV * p_inf / rho_inf);
+  const double v_n_i = u_i * nx + v_i * ny;
+  const double v_n_inf = u_inf * nx + v_inf * ny;
+  const double R_plus = v_n_i + 2.0 * a_i / GM;
+  const double R_minus = v_n_inf - 2.0 * a_inf / GM;
+  const double v_n_b = 0.5 * (R_plus + R_minus);
+  double a_b = 0.25 * GM * (R_plus - R_minus);
+  if (a_b < 1e-12) a_b = 1e-12;
+  double rho_b, u_b, v_b, p_b;
+  if (v_n_b >= 0.0) {
+    const double s_i = p_i / pow(rho_i, GV);
+    rho_b = pow(a_b * a_b / (GV * s_i), 1.0 / GM);
+    u_b = u_i + (v_n_b - v_n_i) * nx;
+    v_b = v_i + (v_n_b - v_n_i) * ny;
+    p_b = rho_b * a_b * a_b / GV;
+  } else {
+    const double s_inf = p_inf / pow(rho_inf, GV);
+    rho_b = pow(a_b * a_b / (GV * s_inf), 1.0 / GM);
+    u_b = u_inf + (v_n_b - v_n_inf) * nx;
+    v_b = v_inf + (v_n_b - v_n_inf) * ny;
+    p_b = rho_b * a_b * a_b / GV;
+  }
+  const double v_mag_sq = u_b * u_b + v_b * v_b;
+  G[0] = rho_b;
+  G[1] = rho_b * u_b;
+  G[2] = rho_b * v_b;
+  G[3] = p_b / GM + 0.5 * rho_b * v_mag_sq;
+}
+
+// Fixed-pressure exit of the reference (Subsonic_Exit_Boundary_Condition,
+// src/Exit_Boundary_Conditions.cpp:8-66; present in the reference but not called by its
+// Apply_Boundary_Conditions): linearised characteristic face state with the prescribed pressure
+// P_f and reference density and sound speed 1, mirrored into the ghost.  Inputs: the interior
+// cell's primitives (rho, u, v, p), its rho*E (primitive slot 6 = conserved energy of the state
+// the primitives were computed from) and the face's outward normal.
+__device__ __forceinline__ void fixed_p_exit_state(double Rho, double v1, double v2, double P, double rho_Et,
+                                                   double n1, double n2, double P_f, double G[4]) {
+  const double Rho_o = 1.0, C_o = 1.0;
+  const double temp = (P - P_f) / (Rho_o * C_o * C_o);
+  const double rho_f = Rho - temp * Rho_o;
+  const double u_f = v1 + n1 * temp * C_o;
+  const double v_f = v2 + n2 * temp * C_o;
+  const double v_mag_f = 0.5 * (u_f * u_f + v_f * v_f);
+  const double F0 = rho_f, F1 = rho_f * u_f, F2 = rho_f * v_f, F3 = ((P_f / (1.4 - 1.0)) + rho_f * v_mag_f);
+  G[0] = 2.0 * F0 - Rho;
+  G[1] = 2.0 * F1 - Rho * v1;
+  G[2] = 2.0 * F2 - Rho * v2;
+  G[3] = 2.0 * F3 - rho_Et;
+}
+
 }  // namespace cfdb

@@ -90,11 +90,23 @@ void cfd_mesh_destroy(cfd_mesh *m);
  * Solver configuration: the reference's Solver_Config keys (json_Files/Solver_Config.json:1-38,
  * read at src/Configuration_Read.cpp:23-87) plus additive keys.
  * ------------------------------------------------------------------------------------------ */
-enum { CFD_DISS_LLF = 1, CFD_DISS_ROE = 3, CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7 };
+/* Flux schemes.  CFD_DISS_AUSM_GPU: the face flux of the reference's GPU kernel ausm_flux_kernel
+ * (CUDA_KERNELS/Flux_Calculations_Cuda_Kernels.cu:37-113); gradient-MUSCL (face-based) form only. */
+enum { CFD_DISS_LLF = 1, CFD_DISS_ROE = 3, CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7, CFD_DISS_AUSM_GPU = 8 };
 enum { CFD_LIM_REF_MINMOD = 0, CFD_LIM_MINMOD = 1, CFD_LIM_VANLEER = 2, CFD_LIM_SUPERBEE = 3, CFD_LIM_VANALBADA = 4 };
-enum { CFD_INT_REFERENCE = 0, CFD_INT_RK4 = 1, CFD_INT_SSPRK3 = 2 };
-enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2, CFD_INLET_FIXED = 3 };
-enum { CFD_EXIT_SUPERSONIC = 0, CFD_EXIT_SUBSONIC_REF = 1, CFD_EXIT_STATIC_P = 2 };
+/* Integrators.  CFD_INT_RK3_GPU_REF / CFD_INT_RK4_GPU_REF: the stage updates of the reference's
+ * GPU kernels tvd_rk3_kernel and rk4_complete_kernel (CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu
+ * :94-131 and :11-73; the RK4 one is not the classical scheme: its last stage uses only the last
+ * residual), with dt taken at the first stage. */
+enum { CFD_INT_REFERENCE = 0, CFD_INT_RK4 = 1, CFD_INT_SSPRK3 = 2, CFD_INT_RK3_GPU_REF = 3, CFD_INT_RK4_GPU_REF = 4 };
+/* CFD_INLET_FARFIELD: Riemann-invariant far field of the reference's GPU kernel farfield_bc_kernel
+ * (CUDA_KERNELS/Boundary_Conditions_Cuda_Kernels.cu:257-325), free stream (inlet_rho, inlet_u,
+ * inlet_v, inlet_p).  CFD_EXIT_FIXED_P_REF: the reference's Subsonic_Exit_Boundary_Condition
+ * (src/Exit_Boundary_Conditions.cpp:8-66, not called by its own driver) with P_f = exit_p (the
+ * reference hard-codes 0.9/1.4). */
+enum { CFD_INLET_SUPERSONIC = 0, CFD_INLET_SUBSONIC_REF = 1, CFD_INLET_TOTAL_PT = 2, CFD_INLET_FIXED = 3,
+       CFD_INLET_FARFIELD = 4 };
+enum { CFD_EXIT_SUPERSONIC = 0, CFD_EXIT_SUBSONIC_REF = 1, CFD_EXIT_STATIC_P = 2, CFD_EXIT_FIXED_P_REF = 3 };
 enum { CFD_PREC_FP64 = 0, CFD_PREC_FP32_FLUX = 1 };
 enum { CFD_MUSCL_REFERENCE = 0, CFD_MUSCL_GRADIENT = 1 };
 
@@ -103,7 +115,8 @@ typedef struct {
   int is_second_order;       /* Is_Second_Order */
   int time_accurate;         /* Time_Accurate: 1 -> Runge_Kutta_Method, 0 -> Explicit_Method */
   int local_time_stepping;   /* Local_Time_Stepping */
-  int integrator;            /* CFD_INT_*: reference forms, classical RK4, standard SSP-RK3 */
+  int integrator;            /* CFD_INT_*: reference forms, classical RK4, standard SSP-RK3,
+                                reference GPU RK3 / RK4 kernels */
   int limiter;               /* CFD_LIM_*: 0 = reference 2-argument MinMod (src/Limiters.cpp:58-63) */
   int reconstruct_primitive; /* MUSCL on (rho,u,v,p) instead of conserved variables */
   int muscl;                 /* CFD_MUSCL_REFERENCE: the reference's directional stencil
@@ -203,6 +216,16 @@ cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad);
 /* AMR indicator [NP] and tags [NP] (Compute_Gradient_Refinement_Indicator / TagRefinableCells,
  * src/Grid_Refine_Functions.cpp:8-63).  Either output may be NULL. */
 cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags);
+
+/* Pointwise evaluation of the face functions on host arrays (runs on `device`): the limiter
+ * phi(a, b) of CFD_LIM_MINMOD..CFD_LIM_VANALBADA for n pairs (the phi(r) family of
+ * CUDA_KERNELS/Limiter_Cuda_Kernels.cu:89-154: r = a/b, phi = 0 when |b| < 1e-12 or r <= 0), and
+ * the face flux of scheme CFD_DISS_ROE / _AUSM / _HLLC / _AUSM_GPU for n conserved left/right
+ * states [n*4], outward unit normals [n*2] and face lengths [n], into F [n*4], in precision
+ * CFD_PREC_FP64 or CFD_PREC_FP32_FLUX.  The same device functions as the solver's face kernel. */
+cfd_status cfd_eval_limiter(int limiter, const double *a, const double *b, int n, double *out, int device);
+cfd_status cfd_eval_face_flux(int scheme, int precision, const double *UL, const double *UR, const double *normals,
+                              const double *lengths, int n, double *F, int device);
 
 /* Device arrays of one net-flux evaluation, in the device layout this library uses internally
  * (no renumbering): face-major [4][NP] per-face arrays, component-major state planes. */

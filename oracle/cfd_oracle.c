@@ -119,12 +119,61 @@ void orc_set_state(orc_state *s, const double *U, int n) {
 /* The conserved state the limiter, LLF and the exit BC read: U_Cells (U^n on physical rows,
  * boundary values on ghost rows) for the reference integrator; the current stage state for the
  * stage-consistent integrators. */
+/* The stage state of the current stage (> 0): RK4 forms keep it in S1, three-stage forms in
+ * S1 then S2. */
+static const double *stage_state(const orc_state *s) {
+  const int integ = s->c.integrator;
+  return (integ == 1 || integ == 4) ? s->S1 : (s->stage == 1 ? s->S1 : s->S2);
+}
+
 static const double *uread(orc_state *s) {
   if (s->c.integrator == 0 || s->stage == 0) return s->U;
   memcpy(s->Urd, s->U, 4 * (size_t)s->NT * sizeof(double));
-  const double *src = (s->c.integrator == 1) ? s->S1 : (s->stage == 1 ? s->S1 : s->S2);
-  memcpy(s->Urd, src, 4 * (size_t)s->NP * sizeof(double));
+  memcpy(s->Urd, stage_state(s), 4 * (size_t)s->NP * sizeof(double));
   return s->Urd;
+}
+
+/* Conserved state of cell c that the primitives were last computed from (U^n at stage 0, the
+ * stage state after). */
+static const double *ucur(const orc_state *s, int c) {
+  return (s->stage == 0 ? s->U : stage_state(s)) + 4 * (size_t)c;
+}
+
+/* farfield_bc_kernel, CUDA_KERNELS/Boundary_Conditions_Cuda_Kernels.cu:257-325, with
+ * calculate_primitive_device :28-49 (GAMMA_VAL 1.4, GAMMA_M1 0.4).  libm pow, so the result
+ * is compared with the device's within a relative tolerance. */
+static void farfield_state(const double *Ui, double nx, double ny, double rho_inf, double u_inf, double v_inf,
+                           double p_inf, double *G) {
+  const double GV = 1.4, GM = 0.4;
+  double rho = Ui[0];
+  if (rho < 1e-12) rho = 1e-12;
+  double u = Ui[1] / rho, v = Ui[2] / rho, E = Ui[3];
+  double kinetic_energy = 0.5 * rho * (u * u + v * v);
+  double p = GM * (E - kinetic_energy);
+  if (p < 1e-12) p = 1e-12;
+  double a_i = sqrt(GV * p / rho), a_inf = sqrt(GV * p_inf / rho_inf);
+  double v_n_i = u * nx + v * ny, v_n_inf = u_inf * nx + v_inf * ny;
+  double R_plus = v_n_i + 2.0 * a_i / GM, R_minus = v_n_inf - 2.0 * a_inf / GM;
+  double v_n_b = 0.5 * (R_plus + R_minus);
+  double a_b = 0.25 * GM * (R_plus - R_minus);
+  if (a_b < 1e-12) a_b = 1e-12;
+  double rho_b, u_b, v_b, p_b;
+  if (v_n_b >= 0.0) {
+    double s_i = p / pow(rho, GV);
+    rho_b = pow(a_b * a_b / (GV * s_i), 1.0 / GM);
+    u_b = u + (v_n_b - v_n_i) * nx;
+    v_b = v + (v_n_b - v_n_i) * ny;
+  } else {
+    double s_inf = p_inf / pow(rho_inf, GV);
+    rho_b = pow(a_b * a_b / (GV * s_inf), 1.0 / GM);
+    u_b = u_inf + (v_n_b - v_n_inf) * nx;
+    v_b = v_inf + (v_n_b - v_n_inf) * ny;
+  }
+  p_b = rho_b * a_b * a_b / GV;
+  G[0] = rho_b;
+  G[1] = rho_b * u_b;
+  G[2] = rho_b * v_b;
+  G[3] = p_b / GM + 0.5 * rho_b * (u_b * u_b + v_b * v_b);
 }
 
 /* Apply_Boundary_Conditions, src/Boundary_Conditions.cpp:12-61 and the per-kind functions:
@@ -151,7 +200,10 @@ void orc_apply_bc(orc_state *s) {
       G[3] = ((Pc[4] / GM1) + Pc[0] * vmag);
     } else if (kind == 0) {
       double u = Pc[1], v = Pc[2];
-      if (s->c.inlet_bc == 0) {
+      if (s->c.inlet_bc == 4) {
+        farfield_state(ucur(s, c), s->nrm[8 * c + 2 * f], s->nrm[8 * c + 2 * f + 1], s->c.inlet_rho, s->c.inlet_u,
+                       s->c.inlet_v, s->c.inlet_p, G);
+      } else if (s->c.inlet_bc == 0) {
         double vmag = (u * u + v * v) * 0.5;
         G[0] = s->c.inlet_rho;
         G[1] = s->c.inlet_rho * u;
@@ -187,6 +239,21 @@ void orc_apply_bc(orc_state *s) {
       if (s->c.exit_bc == 1) continue;
       if (s->c.exit_bc == 0) {
         for (int k = 0; k < 4; k++) G[k] = Ur[4 * (size_t)c + k];
+      } else if (s->c.exit_bc == 3) {
+        /* Subsonic_Exit_Boundary_Condition, src/Exit_Boundary_Conditions.cpp:8-66, P_f = exit_p. */
+        double Rho = Pc[0], v1 = Pc[1], v2 = Pc[2], P = Pc[4], rho_Et = Pc[6];
+        double n1 = s->nrm[8 * c + 2 * f], n2 = s->nrm[8 * c + 2 * f + 1];
+        double Rho_o = 1.0, C_o = 1.0, P_f = s->c.exit_p;
+        double temp = (P - P_f) / (Rho_o * C_o * C_o);
+        double rho_f = Rho - temp * Rho_o;
+        double u_f = v1 + n1 * temp * C_o;
+        double v_f = v2 + n2 * temp * C_o;
+        double v_mag_f = 0.5 * (u_f * u_f + v_f * v_f);
+        double UF[4] = {rho_f, rho_f * u_f, rho_f * v_f, ((P_f / GM1) + rho_f * v_mag_f)};
+        G[0] = 2.0 * UF[0] - Rho;
+        G[1] = 2.0 * UF[1] - Rho * v1;
+        G[2] = 2.0 * UF[2] - Rho * v2;
+        G[3] = 2.0 * UF[3] - rho_Et;
       } else {
         double n1 = s->nrm[8 * c + 2 * f], n2 = s->nrm[8 * c + 2 * f + 1];
         double vn = Pc[1] * n1 + Pc[2] * n2;
@@ -548,6 +615,44 @@ static void refresh_prims(orc_state *s, const double *src) {
  * with dt frozen per step (integrator 2); classical RK4 (integrator 1). */
 void orc_rk(orc_state *s) {
   const int NP = s->NP, integ = s->c.integrator, lts = s->c.local_time_stepping;
+  if (integ == 3 || integ == 4) {
+    /* The reference's GPU kernels tvd_rk3_kernel (integrator 3) and rk4_complete_kernel
+     * (integrator 4), CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu:94-131 and :11-73 (its
+     * dissipation terms are zero for the inviscid path), dt taken at the first stage.  The last
+     * stage produces U^{n+1}; dU = U^{n+1} - U^n, and U^{n+1} is kept for orc_update. */
+    const int ns = integ == 3 ? 3 : 4;
+    for (int st = 0; st < ns; st++) {
+      s->stage = st;
+      if (st > 0) orc_apply_bc(s);
+      orc_net_flux(s);
+      if (st == 0) {
+        s->dt_step = s->min_dt;
+        memcpy(s->dtk, s->dt, (size_t)NP * sizeof(double));
+      }
+      for (int c = 0; c < NP; c++) {
+        double dt = lts ? s->dtk[c] : s->dt_step, invA = s->inva[c];
+        for (int k = 0; k < 4; k++) {
+          size_t i = 4 * (size_t)c + k;
+          double Un = s->U[i], Rk = s->R[i], nu;
+          if (integ == 3) {
+            if (st == 0) { s->S1[i] = Un - dt * invA * Rk; continue; }
+            if (st == 1) { s->S2[i] = 0.25 * (3.0 * Un + s->S1[i] - dt * invA * Rk); continue; }
+            nu = (1.0 / 3.0) * (Un + 2.0 * s->S2[i] - 2.0 * dt * invA * Rk);
+          } else {
+            if (st < 2) { s->S1[i] = Un - 0.5 * dt * invA * Rk; continue; }
+            if (st == 2) { s->S1[i] = Un - dt * invA * Rk; continue; }
+            nu = Un - (dt * invA / 6.0) * Rk;
+          }
+          s->Racc[i] = nu;
+          s->dU[i] = nu - Un;
+        }
+      }
+      if (st < ns - 1) refresh_prims(s, (integ == 3 && st == 1) ? s->S2 : s->S1);
+    }
+    s->min_dt = s->dt_step;
+    s->stage = 0;
+    return;
+  }
   if (integ == 1) {
     const double w[3] = {0.5, 0.5, 1.0};
     for (int st = 0; st < 4; st++) {
@@ -623,10 +728,14 @@ void orc_estimate_error(orc_state *s) {
   for (int i = 0; i < 4; i++) s->err[i] = sqrt(e[i]);
 }
 
-/* Update(), src/Error_Estimate_Update.cpp:31-43. */
+/* Update(), src/Error_Estimate_Update.cpp:31-43 (the reference GPU integrators: U = U^{n+1}). */
 void orc_update(orc_state *s) {
+  const int direct = s->c.integrator == 3 || s->c.integrator == 4;
   for (int c = 0; c < s->NP; c++) {
-    for (int k = 0; k < 4; k++) s->U[4 * c + k] += s->dU[4 * c + k];
+    for (int k = 0; k < 4; k++) {
+      if (direct) s->U[4 * c + k] = s->Racc[4 * c + k];
+      else s->U[4 * c + k] += s->dU[4 * c + k];
+    }
     eos(s, c, s->U + 4 * (size_t)c, s->P + 11 * (size_t)c);
   }
 }

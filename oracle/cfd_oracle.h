@@ -7,7 +7,9 @@
  * from its sources (oracle/_ref, tests/test_oracle_vs_reference.py).  The additive forms with no
  * reference counterpart (phi(r) limiters inside the MUSCL stencil, MUSCL on primitives,
  * stage-consistent SSP-RK3, classical RK4, total-(p,T) inflow, static-pressure outflow) are
- * "parity unpinned": this restatement is their only oracle. */
+ * "parity unpinned": this restatement is their only oracle.  The forms restating the reference's
+ * GPU kernels (far-field BC, AUSM face flux, TVD-RK3 / RK4 stage updates) and its unused
+ * fixed-pressure exit are pinned separately against those kernels and that function. */
 #ifndef CFD_ORACLE_H
 #define CFD_ORACLE_H
 #ifdef __cplusplus
@@ -17,7 +19,7 @@ extern "C" {
 typedef struct {
   int dissipation_type, is_second_order, time_accurate, local_time_stepping, integrator, limiter,
       reconstruct_primitive, muscl, precision, inlet_bc, exit_bc;
-  double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas;
+  double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas, inlet_u, inlet_v;
 } orc_config;
 
 typedef struct orc_state orc_state;

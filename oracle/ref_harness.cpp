@@ -271,6 +271,11 @@ void refh_update() { Update(); }
 void refh_ausm_net_flux() {
   for (int c = 0; c < No_Physical_Cells; c++) Ausm_Flux(c);
 }
+// The reference's fixed-pressure exit (src/Exit_Boundary_Conditions.cpp:8-66, which its
+// Apply_Boundary_Conditions does not call) on every exit entry, from the current primitives.
+void refh_exit_fixed_p() {
+  for (unsigned int i = 0; i + 2 < Exit_Cells_List.size(); i += 3) Subsonic_Exit_Boundary_Condition(i);
+}
 
 // The loop body of Inviscid_Solver (src/Solver.cpp:94-125), n times or until t_end is reached
 // (t_end <= 0: no time limit).  Returns the number of iterations performed.

@@ -71,6 +71,66 @@ def refcuda_hllc(U, P6, nbr, normals, areas, flux, num_cells):
     return L.refcu_hllc_flux(U, P6, nbr, normals, areas, flux, num_cells)
 
 
+_refcu = []
+
+
+def _refcu_lib():
+    if not _refcu:
+        L = ctypes.CDLL(REFCUDA_LIB)
+        L.refcu_limiter.argtypes = [ctypes.c_int, _DP, _DP, ctypes.c_int, _DP]
+        L.refcu_ausm_flux.argtypes = [_DP, _DP, _DP, _DP, ctypes.c_int, _DP]
+        L.refcu_farfield.argtypes = [_DP, _DP, ctypes.c_int] + [ctypes.c_double] * 4
+        L.refcu_rk_stage.argtypes = [ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, ctypes.c_double,
+                                     ctypes.c_int]
+        for n in ("refcu_limiter", "refcu_ausm_flux", "refcu_farfield", "refcu_rk_stage"):
+            getattr(L, n).restype = ctypes.c_int
+        _refcu.append(L)
+    return _refcu[0]
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def refcuda_limiter(kind, a, b):
+    """phi(a, b) of the reference's vanleer/superbee/vanalbada_limiter_device (kind 2/3/4)."""
+    a, b = _c(a), _c(b)
+    out = np.zeros_like(a)
+    rc = _refcu_lib().refcu_limiter(kind, _dp(a), _dp(b), a.size, _dp(out))
+    if rc:
+        raise RuntimeError("refcu_limiter: CUDA error %d" % rc)
+    return out
+
+
+def refcuda_ausm_flux(UL5, UR5, normals3, areas):
+    """The reference's ausm_flux_kernel on 5-component states; returns fluxes [n, 5]."""
+    UL5, UR5, normals3, areas = _c(UL5), _c(UR5), _c(normals3), _c(areas)
+    out = np.zeros((UL5.shape[0], 5))
+    rc = _refcu_lib().refcu_ausm_flux(_dp(UL5), _dp(UR5), _dp(normals3), _dp(areas), UL5.shape[0], _dp(out))
+    if rc:
+        raise RuntimeError("refcu_ausm_flux: CUDA error %d" % rc)
+    return out
+
+
+def refcuda_farfield(U4, normals8, rho_inf, u_inf, v_inf, p_inf):
+    """The reference's farfield_bc_kernel: boundary states [n, 4] from interior states [n, 4]."""
+    U = _c(U4).copy()
+    normals8 = _c(normals8)
+    rc = _refcu_lib().refcu_farfield(_dp(U), _dp(normals8), U.shape[0], rho_inf, u_inf, v_inf, p_inf)
+    if rc:
+        raise RuntimeError("refcu_farfield: CUDA error %d" % rc)
+    return U
+
+
+def refcuda_rk_stage(which, stage, U5, T1, T2, net_flux5, volumes, dt):
+    """One stage of the reference's tvd_rk3_kernel (which 3) or rk4_complete_kernel (which 4);
+    U5, T1, T2 ([n, 5] float64 C arrays) are updated in place."""
+    F, V = _c(net_flux5), _c(volumes)
+    rc = _refcu_lib().refcu_rk_stage(which, stage, _dp(U5), _dp(T1), _dp(T2), _dp(F), _dp(V), dt, U5.shape[0])
+    if rc:
+        raise RuntimeError("refcu_rk_stage: CUDA error %d" % rc)
+
+
 _ref = {}
 DROPIN_LIB = os.path.join(HERE, "_ref", "libcfdref_dropin.so")
 
@@ -88,7 +148,7 @@ def reflib(path=REF_LIB):
     if path not in _ref:
         L = ctypes.CDLL(path)
         for n in ["refh_reset", "refh_clear_boundary_lists", "refh_apply_bc", "refh_net_flux", "refh_explicit",
-                  "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux"]:
+                  "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux", "refh_exit_fixed_p"]:
             getattr(L, n).restype = None
         L.refh_load_vtk.argtypes = [ctypes.c_char_p]
         L.refh_load_vtk.restype = ctypes.c_int
@@ -216,7 +276,7 @@ class _OrcConfig(ctypes.Structure):
                                             "local_time_stepping", "integrator", "limiter", "reconstruct_primitive",
                                             "muscl", "precision", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
-                                               "exit_p", "r_gas"]]
+                                               "exit_p", "r_gas", "inlet_u", "inlet_v"]]
 
 
 _orc = None
@@ -277,6 +337,8 @@ class OracleRun:
         c.inlet_t0 = params.get("inlet_t0", 0.0)
         c.exit_p = params.get("exit_p", 0.0)
         c.r_gas = params.get("r_gas", 287.0)
+        c.inlet_u = params.get("inlet_u", 0.0)
+        c.inlet_v = params.get("inlet_v", 0.0)
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,

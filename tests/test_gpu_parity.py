@@ -97,6 +97,15 @@ ADDITIVE = {
     "grad_muscl_ausm_fp32_ssp_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, dissipation_type=cb.DISS_AUSM,
                                          precision=cb.PREC_FP32_FLUX, integrator=cb.INT_SSPRK3,
                                          local_time_stepping=1),
+    "grad_muscl_ausm_gpu_minmod": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD,
+                                       dissipation_type=cb.DISS_AUSM_GPU),
+    "grad_muscl_ausm_gpu_fp32_ssp_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANLEER,
+                                             dissipation_type=cb.DISS_AUSM_GPU, precision=cb.PREC_FP32_FLUX,
+                                             integrator=cb.INT_SSPRK3, local_time_stepping=1),
+    "grad_muscl_rk3_gpu_ref": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANLEER, integrator=cb.INT_RK3_GPU_REF),
+    "grad_muscl_rk4_gpu_ref_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, integrator=cb.INT_RK4_GPU_REF,
+                                       local_time_stepping=1),
+    "rk3_gpu_ref_lts": dict(integrator=cb.INT_RK3_GPU_REF, local_time_stepping=1),
     "hllc_reference_1o": dict(dissipation_type=cb.DISS_HLLC, is_second_order=0),
     "ausm_reference_1o": dict(dissipation_type=cb.DISS_AUSM, is_second_order=0),
     "grad_muscl_vanalbada_fp32_ssp_lts": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANALBADA,

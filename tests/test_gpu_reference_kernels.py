@@ -1,0 +1,245 @@
+"""Forms restating the reference's GPU kernels (CUDA_KERNELS/ of the reference) and its unused
+fixed-pressure exit, pinned bit for bit against that code itself: the kernels are compiled from
+the reference's sources into oracle/_ref/librefcuda.so (oracle/Makefile, target refcuda) and the
+exit function runs inside the reference's CPU build (oracle/_ref/libcfdref.so).  Multi-step runs
+of the same forms are compared with the C restatement."""
+import numpy as np
+import pytest
+
+import cfd_solver_withcuda_b200 as cb
+from cases import CASES, make_mesh, initial_state, oracle_params, solver_config
+from conftest import assert_bits_equal
+
+pytestmark = pytest.mark.gpu
+GAMMA = 1.4
+
+
+def _refpy():
+    from oracle import refpy
+    return refpy
+
+
+def need_refcuda():
+    refpy = _refpy()
+    if not refpy.refcuda_available():
+        pytest.skip("oracle/_ref/librefcuda.so not built (reference sources absent at build time)")
+    return refpy
+
+
+def need_ref():
+    refpy = _refpy()
+    if not refpy.ref_available():
+        pytest.skip("oracle/_ref/libcfdref.so not built (reference sources absent at build time)")
+    return refpy
+
+
+def random_states(rng, n, mach_max=2.5, rho_range=(0.2, 2.0), p_range=(0.2, 2.0)):
+    rho = rng.uniform(*rho_range, n)
+    p = rng.uniform(*p_range, n)
+    a = np.sqrt(GAMMA * p / rho)
+    ang = rng.uniform(0.0, 2.0 * np.pi, n)
+    mach = rng.uniform(0.0, mach_max, n)
+    u, v = mach * a * np.cos(ang), mach * a * np.sin(ang)
+    return cb.conserved_from_primitive(rho, u, v, p)
+
+
+@pytest.mark.parametrize("limiter", [cb.LIM_VANLEER, cb.LIM_SUPERBEE, cb.LIM_VANALBADA])
+def test_limiter_phi_matches_reference_gpu_functions(limiter):
+    """phi(a, b) against vanleer/superbee/vanalbada_limiter_device
+    (CUDA_KERNELS/Limiter_Cuda_Kernels.cu:116-154), including |b| < 1e-12, r <= 0, r = 1 and
+    very large and very small ratios."""
+    refpy = need_refcuda()
+    rng = np.random.default_rng(7)
+    a = np.concatenate([rng.normal(size=4000), [0.0, 1.0, -1.0, 1e-13, 5e-13, 1e300, -0.0, 3.0, 1e-300, 2.0]])
+    b = np.concatenate([rng.normal(size=4000), [1.0, 1.0, 1.0, 1.0, 9e-13, 1e-3, 1.0, 1.5, 1.0, 1e-12]])
+    got = cb.eval_limiter(limiter, a, b)
+    want = refpy.refcuda_limiter(limiter, a, b)
+    assert_bits_equal(got, want, "phi limiter %d" % limiter)
+
+
+def test_ausm_gpu_face_flux_matches_reference_kernel():
+    """CFD_DISS_AUSM_GPU face flux against ausm_flux_kernel
+    (CUDA_KERNELS/Flux_Calculations_Cuda_Kernels.cu:37-113) on subsonic and supersonic states in
+    both directions; the kernel's 3-D slots carry w = 0, nz = 0."""
+    refpy = need_refcuda()
+    rng = np.random.default_rng(11)
+    n = 6000
+    UL, UR = random_states(rng, n), random_states(rng, n)
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    nrm = np.stack([np.cos(th), np.sin(th)], axis=1)
+    ln = rng.uniform(0.01, 1.0, n)
+    got = cb.eval_face_flux(cb.DISS_AUSM_GPU, UL, UR, nrm, ln)
+    UL5 = np.insert(UL, 3, 0.0, axis=1)
+    UR5 = np.insert(UR, 3, 0.0, axis=1)
+    n3 = np.concatenate([nrm, np.zeros((n, 1))], axis=1)
+    want = refpy.refcuda_ausm_flux(UL5, UR5, n3, ln)
+    assert_bits_equal(got, want[:, [0, 1, 2, 4]], "AUSM face flux vs ausm_flux_kernel")
+
+
+def farfield_case():
+    case = dict(CASES["cyl_roe2_lts"])
+    m = make_mesh(case)
+    rho, p = 1.0, 1.0 / GAMMA
+    u = case["mach"] * np.sqrt(GAMMA * p / rho)
+    over = dict(inlet_bc=cb.INLET_FARFIELD, inlet_u=u, inlet_v=0.0, reorder=1)
+    return case, m, over
+
+
+def test_farfield_bc_matches_reference_kernel():
+    """Ghost states of CFD_INLET_FARFIELD against farfield_bc_kernel
+    (CUDA_KERNELS/Boundary_Conditions_Cuda_Kernels.cu:257-325) on a perturbed state with inflow
+    and outflow faces (both branches of the kernel)."""
+    refpy = need_refcuda()
+    case, m, over = farfield_case()
+    rng = np.random.default_rng(3)
+    NP = m.n_physical
+    U0 = initial_state(case, m).copy()
+    U0[:NP] = random_states(rng, NP, mach_max=1.5)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.Apply_Boundary_Conditions()
+    got = s.download()["U"]
+    b = m.boundary[m.boundary[:, 0] == cb.BC_INLET]
+    cells, faces, ghosts = b[:, 1], b[:, 2], b[:, 3]
+    nrm8 = np.zeros((len(b), 8))
+    nrm8[:, 0] = m.face_normals[cells, 2 * faces]
+    nrm8[:, 1] = m.face_normals[cells, 2 * faces + 1]
+    cfg = s.config
+    want = refpy.refcuda_farfield(U0[cells], nrm8, cfg.inlet_rho, cfg.inlet_u, cfg.inlet_v, cfg.inlet_p)
+    vn = (U0[cells, 1] * nrm8[:, 0] + U0[cells, 2] * nrm8[:, 1]) / U0[cells, 0]
+    assert (vn > 0).any() and (vn < 0).any()
+    assert_bits_equal(got[ghosts], want, "far-field ghost states")
+
+
+def test_fixed_p_exit_matches_reference_function():
+    """Ghost states of CFD_EXIT_FIXED_P_REF against the reference's own
+    Subsonic_Exit_Boundary_Condition (src/Exit_Boundary_Conditions.cpp:8-66, P_f = 0.9/1.4 as it
+    hard-codes) run in the reference's CPU build."""
+    refpy = need_ref()
+    case = dict(CASES["bump_llf1_subsonic"])
+    m = make_mesh(case)
+    rng = np.random.default_rng(5)
+    NP = m.n_physical
+    U0 = initial_state(case, m).copy()
+    # States near the prescribed pressure: the linearised face state (density corrected by
+    # P - P_f with reference density and sound speed 1) mirrored into the ghost stays physical.
+    U0[:NP] = random_states(rng, NP, mach_max=0.9, rho_range=(0.8, 1.2), p_range=(0.55, 0.75))
+    s = cb.Solver(m, solver_config(case, exit_bc=cb.EXIT_FIXED_P_REF, exit_p=0.9 / 1.4))
+    s.upload_state(U0)
+    s.Apply_Boundary_Conditions()
+    got = s.download()["U"]
+    from cases import ref_params
+    r = refpy.RefRun(m, ref_params(case))
+    r.set_state(U0)
+    r.L.refh_exit_fixed_p()
+    want = r.state()["U"]
+    g = m.boundary[m.boundary[:, 0] == cb.BC_EXIT][:, 3]
+    assert len(g) > 0
+    assert_bits_equal(got[g], want[g], "fixed-p exit ghost states")
+
+
+@pytest.mark.parametrize("which", [3, 4])
+@pytest.mark.parametrize("form", ["roe1", "grad_muscl"])
+def test_gpu_reference_integrators_match_reference_kernels(which, form):
+    """One pseudo-step of CFD_INT_RK3_GPU_REF / CFD_INT_RK4_GPU_REF against a driver that
+    evaluates each stage's residual with this library and applies the reference's own
+    tvd_rk3_kernel / rk4_complete_kernel (CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu) for the
+    stage updates, global dt from the first stage."""
+    refpy = need_refcuda()
+    case = dict(CASES["cyl_roe2_lts"])
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    NP = m.n_physical
+    integ = cb.INT_RK3_GPU_REF if which == 3 else cb.INT_RK4_GPU_REF
+    over = dict(integrator=integ, local_time_stepping=0)
+    if form == "roe1":
+        over.update(is_second_order=0)
+    else:
+        over.update(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANLEER)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.step(1)
+    mine = s.download()["U"][:NP]
+
+    ev = cb.Solver(m, solver_config(case, **over))
+
+    def residual(state):
+        ev.upload_state(state)
+        ev.Apply_Boundary_Conditions()
+        ev.Evaluate_Cell_Net_Flux()
+        d = ev.download()
+        return d["net_flux"], d["U"]
+
+    R0, Ub = residual(U0)
+    dt = ev.get_Min_dt()
+    U5 = np.zeros((NP, 5))
+    U5[:, :4] = U0[:NP]
+    T1, T2 = np.zeros((NP, 5)), np.zeros((NP, 5))
+    F5 = np.zeros((NP, 5))
+    nst = 3 if which == 3 else 4
+    R = R0
+    for stage in range(1, nst + 1):
+        F5[:, :4] = R
+        refpy.refcuda_rk_stage(which, stage, U5, T1, T2, F5, m.area, dt)
+        if stage == nst:
+            break
+        nxt = T2 if (which == 3 and stage == 2) else T1
+        full = Ub.copy()
+        full[:NP] = nxt[:, :4]
+        R, Ub = residual(full)
+    assert_bits_equal(mine, U5[:, :4], "integrator %d vs reference kernels" % which)
+
+
+def check_close(a, b, rtol, what):
+    for k in ("U", "net_flux", "delU"):
+        np.testing.assert_allclose(a[k], b[k], rtol=rtol, atol=rtol * 1e-1, err_msg="%s %s" % (what, k))
+
+
+def test_farfield_runs_match_oracle(oracle_lib):
+    """Half cylinder with the far-field outer boundary, 20 steps, against the C restatement (libm
+    pow vs the device pow: relative 1e-11)."""
+    case, m, over = farfield_case()
+    U0 = initial_state(case, m)
+    over.update(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, integrator=cb.INT_SSPRK3)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.step(20)
+    o = oracle_lib.OracleRun(m, **oracle_params(case, **over))
+    o.set_state(U0)
+    o.iterate(20)
+    check_close(s.download(), o.state(), 1e-11, "far field")
+
+
+@pytest.mark.parametrize("integ", [cb.INT_REFERENCE, cb.INT_SSPRK3])
+def test_fixed_p_exit_runs_match_oracle(integ, oracle_lib):
+    """The bump channel with the fixed-pressure exit, 25 steps, bit for bit."""
+    case = dict(CASES["bump_llf1_subsonic"])
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    over = dict(exit_bc=cb.EXIT_FIXED_P_REF, exit_p=0.9 / 1.4, integrator=integ)
+    s = cb.Solver(m, solver_config(case, **over))
+    s.upload_state(U0)
+    s.step(25)
+    o = oracle_lib.OracleRun(m, **oracle_params(case, **over))
+    o.set_state(U0)
+    o.iterate(25)
+    a, b = s.download(), o.state()
+    for k in ("U", "net_flux", "delU", "dt"):
+        assert_bits_equal(a[k], b[k], k)
+
+
+def test_eval_face_flux_matches_solver_schemes():
+    """cfd_eval_face_flux of Roe / AUSM / HLLC on random states is finite and antisymmetric under
+    swapping the states and flipping the normal for the mass flux of the upwind schemes (a
+    property of the numerical flux, F(L, R, n) = -F(R, L, -n))."""
+    rng = np.random.default_rng(13)
+    n = 2000
+    UL, UR = random_states(rng, n), random_states(rng, n)
+    th = rng.uniform(0.0, 2.0 * np.pi, n)
+    nrm = np.stack([np.cos(th), np.sin(th)], axis=1)
+    ln = np.ones(n)
+    for scheme in (cb.DISS_ROE, cb.DISS_AUSM, cb.DISS_HLLC, cb.DISS_AUSM_GPU):
+        F = cb.eval_face_flux(scheme, UL, UR, nrm, ln)
+        G = cb.eval_face_flux(scheme, UR, UL, -nrm, ln)
+        assert np.all(np.isfinite(F))
+        np.testing.assert_allclose(F, -G, rtol=1e-12, atol=1e-12, err_msg="scheme %d" % scheme)
