@@ -98,6 +98,7 @@ SIGNATURES = {
     "cfd_step_async": (_I, [_P, _I]),
     "cfd_sync": (_I, [_P, ctypes.POINTER(StepInfo)]),
     "cfd_set_option": (_I, [_P, ctypes.c_char_p, _D]),
+    "cfd_autotune": (_I, [_P, _I, ctypes.c_char_p, ctypes.c_size_t]),
     "cfd_apply_boundary_conditions": (_I, [_P]),
     "cfd_evaluate_net_flux": (_I, [_P]),
     "cfd_explicit_method": (_I, [_P]),
@@ -329,6 +330,13 @@ class Solver:
     def sync(self):
         _check(lib().cfd_sync(self._h, ctypes.byref(self.info)))
         return self.info
+
+    def autotune(self, steps=20):
+        """Picks the fastest bit-identical launch options on this mesh (cfd_autotune); returns
+        the per-candidate report."""
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib().cfd_autotune(self._h, steps, buf, len(buf)))
+        return buf.value.decode()
 
     def set_option(self, name, value):
         _check(lib().cfd_set_option(self._h, name.encode(), float(value)))

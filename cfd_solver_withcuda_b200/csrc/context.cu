@@ -202,17 +202,31 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
   int n = 0;
   const StagePlan p = stage_plan(c, ctx->fp.consistent);
   const bool faces = ctx->dm.NF > 0;
+  bool ghosts_written = false;  // the previous stage's owner threads wrote this stage's ghosts
   for (int k = 0; k < p.n; k++) {
     const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
     const int lts = stage_lts(p, c, k);
     const int fin = (k == p.n - 1) ? fuse_final : 0;
-    { TimedScope ts(ctx, TK_BC); n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0); }
+    if (!ghosts_written) {
+      TimedScope ts(ctx, TK_BC);
+      n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
+    }
+    ghosts_written = false;
     if (faces) {
-      { TimedScope ts(ctx, TK_GRAD); n += launch_muscl_gradients(s, m, st); }
+      // Fused form (per-cell dt): del_t and Min_dt come from the gradient pass, and the stage
+      // kernel writes the next stage's ghost states from the owner cells.
+      const bool fused = ctx->fuse_gather && (lts == 1 || lts == 2);
+      {
+        TimedScope ts(ctx, TK_GRAD);
+        n += launch_muscl_gradients(s, m, st, ctx->fp, fused ? 1 : 0, k == 0 || lts == 1);
+      }
       { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
-      if (ctx->fuse_gather && (lts == 1 || lts == 2)) {
+      if (fused) {
         TimedScope ts(ctx, TK_GATHER_STAGE);
-        n += launch_gather_stage(s, m, st, ctx->fp, kind, lts, fin, ctx->keep_delu);
+        const bool bc_next = k < p.n - 1;
+        const int flags = 1 | (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+        n += launch_gather_stage(s, m, st, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags);
+        ghosts_written = bc_next;
       } else {
         { TimedScope ts(ctx, TK_FLUX); n += launch_gather(s, m, st, ctx->fp); }
         { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
@@ -575,6 +589,14 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     const int *b = d->boundary + 4 * e;
     bnd[e] = make_int4(b[0], dev_of(ctx, b[1]), b[2], b[3]);
   }
+  // Boundary entries grouped by (device) owner cell, in entry order within a cell.
+  std::vector<int> bptr(NP + 1, 0), bidx(NB > 0 ? NB : 1, 0);
+  for (int e = 0; e < NB; e++) bptr[bnd[e].y + 1]++;
+  for (int i = 0; i < NP; i++) bptr[i + 1] += bptr[i];
+  {
+    std::vector<int> fill(bptr.begin(), bptr.end() - 1);
+    for (int e = 0; e < NB; e++) bidx[fill[bnd[e].y]++] = e;
+  }
 
   DevMesh &m = ctx->dm;
   m.NP = NP;
@@ -595,6 +617,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvx), cvx)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.cvy), cvy)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.bnd), bnd)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<int **>(&m.bptr), bptr)) != CFD_OK) return bail(s);
+  if ((s = ctx_upload(ctx, const_cast<int **>(&m.bidx), bidx)) != CFD_OK) return bail(s);
   m.NF = static_cast<int>(fo.size());
   if (m.NF > 0) {
     if ((s = ctx_upload(ctx, const_cast<int **>(&m.fo), fo)) != CFD_OK) return bail(s);
@@ -960,6 +984,103 @@ cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, dou
   for (int i = 0; i < NP; i++) {
     if (indicator) indicator[ctx->perm[i]] = h[i];
     if (tags) tags[ctx->perm[i]] = ht[i];
+  }
+  return CFD_OK;
+}
+
+// Autotuner: times each combination of the launch options that never change a result bit
+// (face-kernel shape, fused gather + stage, per-cell flux lanes) over `steps` graph-replayed
+// pseudo-steps of this context's own mesh and state, keeps the fastest, and restores the state
+// (every candidate starts from the same state; the solve is not advanced).
+cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len) {
+  if (!ctx || steps < 1) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  DevState &st = ctx->ds;
+  const size_t NT = ctx->NT, NP = ctx->NP;
+  struct Part {
+    double *p;
+    size_t n;
+  };
+  std::vector<Part> parts = {{st.U, 4 * NT}, {st.S, 4 * NP}, {st.prim, 5 * NT}, {st.R, 4 * NP}, {st.dtc, NP},
+                             {st.dtk, NP},    {st.dU, 4 * NP}, {st.ctl, (size_t)CTL_SIZE}};
+  if (st.Racc) parts.push_back({st.Racc, 4 * NP});
+  size_t total = 0;
+  for (const Part &q : parts) total += q.n;
+  double *snap = nullptr;
+  CUDA_TRY(cudaMalloc(&snap, total * sizeof(double)));
+  auto copy_all = [&](bool save) {
+    size_t off = 0;
+    for (const Part &q : parts) {
+      if (save) cudaMemcpyAsync(snap + off, q.p, q.n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+      else cudaMemcpyAsync(q.p, snap + off, q.n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+      off += q.n;
+    }
+  };
+  struct Cand {
+    int faces_shape, fuse, lanes;
+    double ms;
+  };
+  std::vector<Cand> cands;
+  if (ctx->dm.NF > 0) {
+    for (int f = 0; f < 3; f++)
+      for (int g = 0; g < 2; g++) cands.push_back({f, g, ctx->fp.lanes, 0.0});
+  } else {
+    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, 0.0});
+  }
+  const int prof = ctx->profile, graph_on = ctx->use_graph;
+  ctx->profile = 0;
+  ctx->use_graph = 1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  copy_all(true);
+  cfd_status status = CFD_OK;
+  for (Cand &cd : cands) {
+    ctx->fp.faces_shape = cd.faces_shape;
+    ctx->fuse_gather = cd.fuse;
+    ctx->fp.lanes = cd.lanes;
+    if (ctx->graph) {
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+    ctx->launches += launch_set_ctl(ctx->stream, st, CTL_TEND, 0.0);
+    ctx->launches += launch_set_ctl(ctx->stream, st, CTL_DONE, 0.0);
+    if ((status = enqueue_steps(ctx, 2)) != CFD_OK) break;
+    cudaEventRecord(e0, ctx->stream);
+    if ((status = enqueue_steps(ctx, steps)) != CFD_OK) break;
+    cudaEventRecord(e1, ctx->stream);
+    if ((status = sync_status(ctx, nullptr)) != CFD_OK) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cd.ms = ms / steps;
+    copy_all(false);
+  }
+  copy_all(false);
+  cudaStreamSynchronize(ctx->stream);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(snap);
+  ctx->profile = prof;
+  ctx->use_graph = graph_on;
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  if (status != CFD_OK) return status;
+  const Cand *best = &cands[0];
+  for (const Cand &cd : cands)
+    if (cd.ms < best->ms) best = &cd;
+  ctx->fp.faces_shape = best->faces_shape;
+  ctx->fuse_gather = best->fuse;
+  ctx->fp.lanes = best->lanes;
+  if (report && report_len > 0) {
+    std::string r;
+    char line[160];
+    for (const Cand &cd : cands) {
+      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d: %.4f ms/step%s\n", cd.faces_shape,
+               cd.fuse, cd.lanes, cd.ms, &cd == best ? " (chosen)" : "");
+      r += line;
+    }
+    snprintf(report, report_len, "%s", r.c_str());
   }
   return CFD_OK;
 }

@@ -87,21 +87,41 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return v;
 }
 
-// Block sums of NQ per-thread values with one pair of barriers: a shuffle tree per warp, then the
-// warps in order.  The sum of quantity q is returned in thread q (q < NQ).
-template <int NQ>
-__device__ __forceinline__ double block_sums(double v[NQ], double *sh /* NQ * 32 */) {
+// Warp sums of 8 per-lane values in 9 shuffles: three halving exchanges leave each lane one
+// quantity q = 4*bit4 + 2*bit3 + bit2 of its lane id summed over 8 lanes, two more sum the 4
+// lanes that share it.  Fixed order, so deterministic.
+__device__ __forceinline__ double warp_sums8(const double v[8], int &q) {
+  const int lane = threadIdx.x & 31;
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+  double a[4], b[2];
 #pragma unroll
-  for (int q = 0; q < NQ; q++) v[q] = warp_sum(v[q]);
+  for (int i = 0; i < 4; i++) {
+    const double send = h16 ? v[i] : v[i + 4], keep = h16 ? v[i + 4] : v[i];
+    a[i] = keep + __shfl_xor_sync(kFull, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const double send = h8 ? a[i] : a[i + 2], keep = h8 ? a[i + 2] : a[i];
+    b[i] = keep + __shfl_xor_sync(kFull, send, 8);
+  }
+  const double send = h4 ? b[0] : b[1], keep = h4 ? b[1] : b[0];
+  double c = keep + __shfl_xor_sync(kFull, send, 4);
+  c += __shfl_xor_sync(kFull, c, 2);
+  c += __shfl_xor_sync(kFull, c, 1);
+  q = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0);
+  return c;
+}
+
+// Block sums of 8 per-thread values; the sum of quantity q is returned in thread q (q < 8).
+__device__ __forceinline__ double block_sums8(const double v[8], double *sh /* 8 * 32 */) {
+  int q;
+  const double c = warp_sums8(v, q);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; q++) sh[q * 32 + w] = v[q];
-  }
+  if ((lane & 3) == 0) sh[q * 32 + w] = c;
   __syncthreads();
   double s = 0.0;
-  if (threadIdx.x < NQ)
+  if (threadIdx.x < 8)
     for (int i = 0; i < nw; i++) s += sh[threadIdx.x * 32 + i];
   return s;
 }
@@ -128,10 +148,13 @@ __device__ __forceinline__ void sum_partials(const double *partial, int nb, Stor
   }
 }
 
-// Returns true in every thread of the block that finished last among the grid's blocks.
+// Returns true in every thread of the block that finished last among the grid's blocks.  The
+// only data the last block reads from other blocks are their partials, which every caller writes
+// from threads of warp 0; only that warp fences (a fence in every warp would hold each warp until
+// all of its state stores were acknowledged).
 __device__ __forceinline__ bool last_block(unsigned int *counter) {
   __shared__ bool is_last;
-  __threadfence();
+  if (threadIdx.x < 32) __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned t = atomicAdd(counter, 1u);
@@ -164,9 +187,8 @@ __global__ void k_prim_all(DevMesh m, DevState st) {
 //   fixed-p exit     src/Exit_Boundary_Conditions.cpp:8-66 (exit kind 3)
 // src_is_S: the supersonic-exit copy reads the stage state (stage-consistent forms) instead of
 // U^n; cur_is_S: the state the primitives were last computed from is the stage state.
-__global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S, int cur_is_S) {
-  const int e = item_index(m.bblk, m.NB);
-  if (e >= m.NB || step_done(st.ctl)) return;
+__device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const BcParams &bp, int e, int src_is_S,
+                                         int cur_is_S) {
   const int4 b = m.bnd[e];
   const int kind = b.x, c = b.y, f = b.z, g = b.w;
   const int NT = m.NT, NP = m.NP;
@@ -279,6 +301,12 @@ __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S, int cur_
   bool ok = eos_prim(G0, G1, G2, G3, q);
   store_prim(st.prim, NT, g, q);
   if (!ok) flag_bad(st.status, g);
+}
+
+__global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S, int cur_is_S) {
+  const int e = item_index(m.bblk, m.NB);
+  if (e >= m.NB || step_done(st.ctl)) return;
+  bc_entry(m, st, bp, e, src_is_S, cur_is_S);
 }
 
 // Conserved state of cell n for the limiter / LLF: U_Cells (U^n on physical rows, boundary
@@ -582,9 +610,11 @@ __global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, Flu
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
 // side) and the del_t denominator.  The four slots are unrolled and predicated, so every face's
 // id and flux loads are in flight together.
+template <bool DEN = true>
 __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &st, int c, double R[4], double &den) {
   const int NP = m.NP, NT = m.NT;
-  const double uc = st.prim[NT + c], vc = st.prim[2 * NT + c], ac = st.prim[4 * NT + c];
+  const double uc = DEN ? st.prim[NT + c] : 0.0, vc = DEN ? st.prim[2 * NT + c] : 0.0,
+               ac = DEN ? st.prim[4 * NT + c] : 0.0;
   const int nf = m.nf[c];
   int e[4];
 #pragma unroll
@@ -611,9 +641,11 @@ __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &s
         R[2] += F[f].z;
         R[3] += F[f].w;
       }
-      const int idx = f * NP + c;
-      const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
-      den += (fabs(vnf) + ac) * m.dl[idx];
+      if (DEN) {
+        const int idx = f * NP + c;
+        const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
+        den += (fabs(vnf) + ac) * m.dl[idx];
+      }
     }
   }
 }
@@ -641,7 +673,9 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather(DevMesh m, DevState st, F
 // Estimate_Error (src/Error_Estimate_Update.cpp:10-28) terms of one cell; dU < 1e-9 is the
 // reference's signed test.
 __device__ __forceinline__ double err_term(double du, double u) {
-  double t = (du < 1e-9) ? fabs(du) : (fabs(du) / u);
+  double t;
+  if (du < 1e-9) t = fabs(du);
+  else t = fabs(du) / u;
   return t * t;
 }
 
@@ -653,7 +687,7 @@ __device__ __forceinline__ void reduce_err_and_epilogue(DevState &st, const doub
   double v[8];
 #pragma unroll
   for (int q = 0; q < 8; q++) v[q] = e[q];
-  const double s = block_sums<8>(v, sh);
+  const double s = block_sums8(v, sh);
   if (threadIdx.x < 8) st.partial[threadIdx.x * gridDim.x + blockIdx.x] = s;
   if (last_block(st.counter)) {
     double *ctl = st.ctl;
@@ -855,8 +889,10 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
 // update of k_stage in one pass, so the residual never leaves registers on its way to the update
 // (it is still stored for downloads).  The last block finishes Min_dt (and the step's frozen dt at
 // the first stage), and at the final stage the error norms and the Total_Time epilogue.
-__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, int kind, int lts,
-                                                             int fuse_final, int keep_delu) {
+template <bool DTPRE>
+__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
+                                                             int kind, int lts, int fuse_final, int keep_delu,
+                                                             int flags) {
   __shared__ double sh[32];
   const int NP = m.NP;
   const int c = item_index(m.cblk, NP);
@@ -868,15 +904,19 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
   if (c < NP) {
     // The residual gather is issued first; loading the state rows ahead of it (more registers,
     // fewer resident warps) measured slower on B200.
-    double R[4], den;
-    gather_faces(m, st, c, R, den);
+    double R[4], den = 0.0;
+    gather_faces<!DTPRE>(m, st, c, R, den);
     StageIn in;
     load_stage_in(m, st, c, kind, in);
     const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
-    dtc = cell_dt(m, fp, c, den);
+    if (DTPRE) {
+      dtc = st.dtc[c];
+    } else {
+      dtc = cell_dt(m, fp, c, den);
+      st.dtc[c] = dtc;
+    }
 #pragma unroll
     for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
-    st.dtc[c] = dtc;
     double dt;
     if (lts == 1) dt = dtc;
     else {
@@ -884,32 +924,46 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
       dt = first ? dtc : dt_frozen;
     }
     cell_update_in(m, st, c, kind, dt, R, in, fuse_final, keep_delu, e);
+    if ((flags & 2) && !is_final) {
+      // Boundary conditions of the next stage: every ghost depends only on its owner cell's
+      // new state, so the owner writes them (Apply_Boundary_Conditions at the next stage).
+      const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+      for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], (flags & 4) ? 1 : 0, 1);
+    }
   }
-  const double bm = block_min(dtc, sh);
-  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
   const bool do_err = fuse_final && is_final;
+  if (DTPRE && !do_err) return;
+  if (!DTPRE) {
+    const double bm = block_min(dtc, sh);
+    if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
+  }
   if (do_err) {
     __shared__ double sh8[8 * 32];
-    const double sq = block_sums<8>(e, sh8);
+    const double sq = block_sums8(e, sh8);
     if (threadIdx.x < 8) st.partial[(1 + threadIdx.x) * gridDim.x + blockIdx.x] = sq;
   }
   if (last_block(st.counter)) {
-    double v = 1e308 * 10.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-      double w = __ldcg(&st.partial[i]);
-      v = w < v ? w : v;
+    double v = 0.0;
+    if (!DTPRE) {
+      v = 1e308 * 10.0;
+      for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+        double w = __ldcg(&st.partial[i]);
+        v = w < v ? w : v;
+      }
+      v = block_min(v, sh);
     }
-    v = block_min(v, sh);
     if (do_err) {
       double *ctl = st.ctl;
       sum_partials<8>(st.partial + gridDim.x, (int)gridDim.x,
                       [ctl](int q, double a) { ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(a); });
     }
     if (threadIdx.x == 0) {
-      st.ctl[CTL_DTMIN] = v;
-      if (first) st.ctl[CTL_DTSTEP] = v;
+      if (!DTPRE) {
+        st.ctl[CTL_DTMIN] = v;
+        if (first) st.ctl[CTL_DTSTEP] = v;
+      }
       if (do_err) {
-        const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : v;
+        const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : st.ctl[CTL_DTMIN];
         double t = st.ctl[CTL_TOTAL_TIME] + dt_time;
         st.ctl[CTL_TOTAL_TIME] = t;
         st.ctl[CTL_ITER] += 1.0;
@@ -979,32 +1033,68 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // Records of the face-based forms: (rho, u, v, p) and their Green-Gauss gradients, the face
 // value being the mean of the two cell values, ghost cells included (their values carry the
 // boundary state).  Ghost rows get (rho, u, v, p) only.
-__global__ void k_muscl_gradients(DevMesh m, DevState st) {
+// DT: also del_t of each physical cell; MIN: also Min_dt and the step's frozen dt (first stage).
+template <bool DT, bool MIN>
+__global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevState st, FluxParams fp) {
+  __shared__ double sh[32];
   const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
-  if (c >= NT || step_done(st.ctl)) return;
-  double qc[4];
+  if (step_done(st.ctl)) return;
+  double dt = 1e308 * 10.0;
+  if (c < NT) {
+    double qc[4];
 #pragma unroll
-  for (int k = 0; k < 4; k++) qc[k] = st.prim[k * NT + c];
-  double4 *r = reinterpret_cast<double4 *>(st.rec + 12 * (size_t)c);
-  r[0] = make_double4(qc[0], qc[1], qc[2], qc[3]);
-  if (c >= NP) return;
-  const int nf = m.nf[c];
-  const double ia = m.inv_area[c];
-  double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int f = 0; f < nf; f++) {
-    const int idx = f * NP + c;
-    const int N = m.nbr[idx];
-    const double wx = m.nx[idx] * m.dl[idx], wy = m.ny[idx] * m.dl[idx];
+    for (int k = 0; k < 4; k++) qc[k] = st.prim[k * NT + c];
+    double4 *r = reinterpret_cast<double4 *>(st.rec + 12 * (size_t)c);
+    r[0] = make_double4(qc[0], qc[1], qc[2], qc[3]);
+    if (c < NP) {
+      const int nf = m.nf[c];
+      const double ia = m.inv_area[c];
+      const double ac = DT ? st.prim[4 * NT + c] : 0.0;
+      double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double den = 0.0;
+      for (int f = 0; f < nf; f++) {
+        const int idx = f * NP + c;
+        const int N = m.nbr[idx];
+        const double nxf = m.nx[idx], nyf = m.ny[idx], dlf = m.dl[idx];
+        const double wx = nxf * dlf, wy = nyf * dlf;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const double qf = 0.5 * (qc[k] + st.prim[k * NT + N]);
-      g[2 * k] += qf * wx;
-      g[2 * k + 1] += qf * wy;
+        for (int k = 0; k < 4; k++) {
+          const double qf = 0.5 * (qc[k] + st.prim[k * NT + N]);
+          g[2 * k] += qf * wx;
+          g[2 * k + 1] += qf * wy;
+        }
+        if (DT) {
+          // Inviscid_Time_Step's denominator (src/Time_Step.cpp:293-329), faces in order.
+          const double vnf = qc[1] * nxf + qc[2] * nyf;
+          den += (fabs(vnf) + ac) * dlf;
+        }
+      }
+      r[1] = make_double4(g[0] * ia, g[1] * ia, g[2] * ia, g[3] * ia);
+      r[2] = make_double4(g[4] * ia, g[5] * ia, g[6] * ia, g[7] * ia);
+      if (DT) {
+        dt = cell_dt(m, fp, c, den);
+        st.dtc[c] = dt;
+      }
     }
   }
-  r[1] = make_double4(g[0] * ia, g[1] * ia, g[2] * ia, g[3] * ia);
-  r[2] = make_double4(g[4] * ia, g[5] * ia, g[6] * ia, g[7] * ia);
+  if (!MIN) return;
+  // Min_dt (get_Min_dt, src/Numerical_Method.cpp:322-330) and the step's dt.
+  const double bm = block_min(dt, sh);
+  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
+  if (last_block(st.counter)) {
+    double v = 1e308 * 10.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+      double w = __ldcg(&st.partial[i]);
+      v = w < v ? w : v;
+    }
+    v = block_min(v, sh);
+    if (threadIdx.x == 0) {
+      st.ctl[CTL_DTMIN] = v;
+      st.ctl[CTL_DTSTEP] = v;
+      *st.counter = 0u;
+    }
+  }
 }
 
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
@@ -1223,7 +1313,7 @@ void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const
 
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
-  if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st);
+  if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st, fp, 0, 0);
   if (fp.second_order && fp.muscl && m.NF > 0) {
     if (fp.precision == 1) launch_faces_t<float>(s, nblk(m.NF, 256), m, st, fp);
     else launch_faces_t<double>(s, nblk(m.NF, 256), m, st, fp);
@@ -1286,10 +1376,11 @@ int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParam
   return 1;
 }
 
-int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
-                        int fuse_final, int keep_delu) {
+int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                        int kind, int lts, int fuse_final, int keep_delu, int flags) {
   const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
-  k_gather_stage<<<g, kFluxBlock, 0, s>>>(m, st, fp, kind, lts, fuse_final, keep_delu);
+  if (flags & 1) k_gather_stage<true><<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  else k_gather_stage<false><<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
   return 1;
 }
 
@@ -1322,9 +1413,13 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
   return 1;
 }
 
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st) {
-  if (m.rblk) k_muscl_gradients<<<m.n_rblk, kWorkItemBlock, 0, s>>>(m, st);
-  else k_muscl_gradients<<<nblk(m.NT, kBlock), kBlock, 0, s>>>(m, st);
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
+                           int first) {
+  const int g = m.rblk ? m.n_rblk : nblk(m.NT, kBlock);
+  if (m.rblk && g == 0) return 0;
+  if (with_dt && first) k_muscl_gradients<true, true><<<g, kBlock, 0, s>>>(m, st, fp);
+  else if (with_dt) k_muscl_gradients<true, false><<<g, kBlock, 0, s>>>(m, st, fp);
+  else k_muscl_gradients<false, false><<<g, kBlock, 0, s>>>(m, st, fp);
   return 1;
 }
 

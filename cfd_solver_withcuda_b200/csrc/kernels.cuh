@@ -24,6 +24,7 @@ struct DevMesh {
   const double *cvx, *cvy;  // [4][NP] centre-to-centre vectors (gradient MUSCL)
   const uint8_t *degen;
   const int4 *bnd;  // kind, cell, face, ghost
+  const int *bptr, *bidx;  // boundary entries of each cell: bidx[bptr[c] .. bptr[c + 1]) (CSR)
   // Unique faces (face-based forms): owner and neighbour cell, owner-side geometry, and for each
   // cell slot the face id (owner side) or -(id + 1) (neighbour side).
   int NF;
@@ -104,15 +105,21 @@ int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int l
 // gather + stage update.
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
-int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int kind, int lts,
-                        int fuse_final, int keep_delu);
+// flags: bit 0 del_t and Min_dt come from the gradient pass (launch_muscl_gradients with
+// with_dt); bit 1 the owner thread writes its ghosts for the next stage (non-final stages), bit 2
+// that next stage's supersonic-exit copy reads the stage state.
+int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                        int kind, int lts, int fuse_final, int keep_delu, int flags);
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S);
 int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const double *b, int n, double *out);
 int launch_eval_face_flux(cudaStream_t s, int scheme, int precision, const double *UL, const double *UR,
                           const double *nrm, const double *len, int n, double *F);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st);
+// with_dt: also del_t of every physical cell; with first as well: Min_dt and the step's frozen dt
+// (the per-cell-dt forms use no later Min_dt of the step).
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
+                           int first);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
 // TagRefinableCells on the device; scratch holds >= 2 x 32 + 1024 bytes.

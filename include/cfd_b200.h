@@ -186,6 +186,10 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1).
  * None of the options changes a result bit. */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
+/* Times every combination of the options above that applies to this configuration over `steps`
+ * pseudo-steps of the context's own mesh and state, keeps the fastest and restores the state
+ * (the solve is not advanced).  report (may be NULL) receives one line per candidate. */
+cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len);
 
 /* Entry points of the reference path, one call each, same semantics and post-conditions. */
 cfd_status cfd_apply_boundary_conditions(cfd_ctx *ctx); /* Apply_Boundary_Conditions, src/Boundary_Conditions.cpp:12 */

@@ -325,3 +325,25 @@ def test_nonphysical_state_is_reported():
         s.upload_state(U0)
     assert e.value.status == 3
     assert "37" in str(e.value)
+
+
+def test_autotune_keeps_state_and_bits():
+    """cfd_autotune times the launch-option candidates on the context's own state and restores
+    it: the state right after tuning is bit-identical to before, and a run after tuning equals a
+    run of an untuned context."""
+    case = CASES["cyl_roe2_lts"]
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    cfg = solver_config(case, **ADDITIVE["grad_muscl_minmod_ssp_lts"])
+    a = cb.Solver(m, cfg)
+    a.upload_state(U0)
+    a.step(3)
+    before = a.download()
+    report = a.autotune(steps=5)
+    assert report.count("ms/step") == 6 and "(chosen)" in report
+    check_state(a.download(), before, "after autotune")
+    a.step(10)
+    b = cb.Solver(m, cfg)
+    b.upload_state(U0)
+    b.step(13)
+    check_state(a.download(), b.download(), "tuned vs untuned")
