@@ -213,18 +213,19 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
     }
     ghosts_written = false;
     if (faces) {
-      // Fused form (per-cell dt): del_t and Min_dt come from the gradient pass, and the stage
-      // kernel writes the next stage's ghost states from the owner cells.
+      // Fused form (per-cell dt): del_t comes from the gradient pass, the stage kernel writes
+      // the next stage's ghost states from the owner cells, and the last stage forms the step's
+      // Min_dt from the per-cell dt frozen at the first stage.
       const bool fused = ctx->fuse_gather && (lts == 1 || lts == 2);
       {
         TimedScope ts(ctx, TK_GRAD);
-        n += launch_muscl_gradients(s, m, st, ctx->fp, fused ? 1 : 0, k == 0 || lts == 1);
+        n += launch_muscl_gradients(s, m, st, ctx->fp, fused ? 1 : 0);
       }
       { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
       if (fused) {
         TimedScope ts(ctx, TK_GATHER_STAGE);
         const bool bc_next = k < p.n - 1;
-        const int flags = 1 | (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+        const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
         n += launch_gather_stage(s, m, st, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags);
         ghosts_written = bc_next;
       } else {
@@ -651,13 +652,15 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
-  if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)nblk * dsz)) != CFD_OK) return bail(s);
-  if ((s = ctx_alloc(ctx, (void **)&st.counter, 64)) != CFD_OK) return bail(s);
+  if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)(nblk + kMaxGroups) * dsz)) != CFD_OK) return bail(s);
+  const size_t counter_bytes = 64 + 4 * (size_t)(kMaxGroups + 1);
+  if ((s = ctx_alloc(ctx, (void **)&st.counter, counter_bytes)) != CFD_OK) return bail(s);
+  st.gcount = st.counter + 16;
   if ((s = ctx_alloc(ctx, (void **)&st.status, 64)) != CFD_OK) return bail(s);
   if (cudaMemset(st.U, 0, 4 * (size_t)NT * dsz) != cudaSuccess || cudaMemset(st.S, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
       cudaMemset(st.prim, 0, 5 * (size_t)NT * dsz) != cudaSuccess || cudaMemset(st.R, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
       cudaMemset(st.dtc, 0, (size_t)NP * dsz) != cudaSuccess || cudaMemset(st.dU, 0, 4 * (size_t)NP * dsz) != cudaSuccess ||
-      cudaMemset(st.ctl, 0, CTL_SIZE * dsz) != cudaSuccess || cudaMemset(st.counter, 0, 64) != cudaSuccess)
+      cudaMemset(st.ctl, 0, CTL_SIZE * dsz) != cudaSuccess || cudaMemset(st.counter, 0, counter_bytes) != cudaSuccess)
     return bail(fail(CFD_ERR_CUDA, "memset failed"));
   int hs[2] = {0, INT_MAX};
   if (cudaMemcpy(st.status, hs, sizeof(hs), cudaMemcpyHostToDevice) != cudaSuccess)

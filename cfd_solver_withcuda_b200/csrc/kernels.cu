@@ -148,6 +148,48 @@ __device__ __forceinline__ void sum_partials(const double *partial, int nb, Stor
   }
 }
 
+// Reduces nq quantities of n values each, src[q * stride + i] for i < n: the minimum for quantity
+// 0 when has_min, sums otherwise.  Warp w takes quantities w, w + nw, ... (at most 3 per warp);
+// every lane issues its strided loads of all its quantities before any arithmetic, then a fixed
+// shuffle tree, so the result is deterministic.  store(q, v) runs in lane 0 of q's warp.
+template <typename Store>
+__device__ __forceinline__ void reduce_rows(const double *src, int stride, int n, int nq, bool has_min, Store store) {
+  constexpr int kMaxQ = 3, kPer = 4;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double kInf = 1e308 * 10.0;
+  int qs[kMaxQ];
+  double acc[kMaxQ];
+#pragma unroll
+  for (int j = 0; j < kMaxQ; j++) {
+    qs[j] = w + j * nw;
+    acc[j] = (has_min && qs[j] == 0) ? kInf : 0.0;
+  }
+  for (int base = 0; base < n; base += 32 * kPer) {
+    double v[kMaxQ][kPer];
+#pragma unroll
+    for (int j = 0; j < kMaxQ; j++)
+#pragma unroll
+      for (int k = 0; k < kPer; k++) {
+        const int i = base + k * 32 + lane;
+        const bool mn = has_min && qs[j] == 0;
+        v[j][k] = (qs[j] < nq && i < n) ? __ldcg(src + (size_t)qs[j] * stride + i) : (mn ? kInf : 0.0);
+      }
+#pragma unroll
+    for (int j = 0; j < kMaxQ; j++)
+#pragma unroll
+      for (int k = 0; k < kPer; k++) {
+        if (has_min && qs[j] == 0) acc[j] = v[j][k] < acc[j] ? v[j][k] : acc[j];
+        else acc[j] += v[j][k];
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < kMaxQ; j++) {
+    if (qs[j] >= nq) continue;  // uniform across the warp
+    const double r = (has_min && qs[j] == 0) ? warp_min(acc[j]) : warp_sum(acc[j]);
+    if (lane == 0) store(qs[j], r);
+  }
+}
+
 // Returns true in every thread of the block that finished last among the grid's blocks.  The
 // only data the last block reads from other blocks are their partials, which every caller writes
 // from threads of warp 0; only that warp fences (a fence in every warp would hold each warp until
@@ -162,6 +204,39 @@ __device__ __forceinline__ bool last_block(unsigned int *counter) {
   }
   __syncthreads();
   return is_last;
+}
+
+// Two-level grid reduction of 9 per-block values, written at partial[q * nb + blockIdx.x] by
+// threads of warp 0 (q = 0: a minimum, q = 1..8: sums).  Blocks form groups of G consecutive
+// blocks; the last block of a group to finish reduces the group's partials in block order into
+// partial[9 nb + q * ngroups + group], and the last group to finish reduces those in group order
+// into out[9] (shared memory).  Both rounds are a single set of independent loads, and the group
+// rounds run while other blocks are still working.  Returns true in the block that wrote out.
+__device__ __forceinline__ bool grid_reduce9(DevState &st, double *out) {
+  __shared__ bool flag;
+  const int nb = gridDim.x;
+  const int G = max(32, (nb + kMaxGroups - 1) / kMaxGroups);
+  const int ngroups = (nb + G - 1) / G;
+  const int grp = blockIdx.x / G;
+  const int gsize = min(G, nb - grp * G);
+  if (threadIdx.x < 32) __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) flag = (atomicAdd(&st.gcount[grp], 1u) == (unsigned)(gsize - 1));
+  __syncthreads();
+  if (!flag) return false;
+  double *gp = st.partial + 9 * (size_t)nb;
+  reduce_rows(st.partial + (size_t)grp * G, nb, gsize, 9, true,
+              [&](int q, double v) { gp[(size_t)q * ngroups + grp] = v; });
+  if (threadIdx.x == 0) st.gcount[grp] = 0u;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) flag = (atomicAdd(&st.gcount[kMaxGroups], 1u) == (unsigned)(ngroups - 1));
+  __syncthreads();
+  if (!flag) return false;
+  reduce_rows(gp, ngroups, ngroups, 9, true, [&](int q, double v) { out[q] = v; });
+  if (threadIdx.x == 0) st.gcount[kMaxGroups] = 0u;
+  __syncthreads();
+  return true;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -889,32 +964,25 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
 // update of k_stage in one pass, so the residual never leaves registers on its way to the update
 // (it is still stored for downloads).  The last block finishes Min_dt (and the step's frozen dt at
 // the first stage), and at the final stage the error norms and the Total_Time epilogue.
-template <bool DTPRE>
 __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
                                                              int kind, int lts, int fuse_final, int keep_delu,
                                                              int flags) {
-  __shared__ double sh[32];
   const int NP = m.NP;
   const int c = item_index(m.cblk, NP);
   if (step_done(st.ctl)) return;
   const bool first = first_kind(kind);
   const bool is_final = final_kind(kind);
-  double dtc = 1e308 * 10.0;
+  double dtu = 1e308 * 10.0;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (c < NP) {
     // The residual gather is issued first; loading the state rows ahead of it (more registers,
     // fewer resident warps) measured slower on B200.
     double R[4], den = 0.0;
-    gather_faces<!DTPRE>(m, st, c, R, den);
+    gather_faces<false>(m, st, c, R, den);
     StageIn in;
     load_stage_in(m, st, c, kind, in);
+    const double dtc = st.dtc[c];
     const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
-    if (DTPRE) {
-      dtc = st.dtc[c];
-    } else {
-      dtc = cell_dt(m, fp, c, den);
-      st.dtc[c] = dtc;
-    }
 #pragma unroll
     for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
     double dt;
@@ -923,6 +991,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
       if (first) st.dtk[c] = dtc;
       dt = first ? dtc : dt_frozen;
     }
+    dtu = dt;
     cell_update_in(m, st, c, kind, dt, R, in, fuse_final, keep_delu, e);
     if ((flags & 2) && !is_final) {
       // Boundary conditions of the next stage: every ghost depends only on its owner cell's
@@ -931,47 +1000,26 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
       for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], (flags & 4) ? 1 : 0, 1);
     }
   }
-  const bool do_err = fuse_final && is_final;
-  if (DTPRE && !do_err) return;
-  if (!DTPRE) {
-    const double bm = block_min(dtc, sh);
-    if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
-  }
-  if (do_err) {
-    __shared__ double sh8[8 * 32];
-    const double sq = block_sums8(e, sh8);
-    if (threadIdx.x < 8) st.partial[(1 + threadIdx.x) * gridDim.x + blockIdx.x] = sq;
-  }
-  if (last_block(st.counter)) {
-    double v = 0.0;
-    if (!DTPRE) {
-      v = 1e308 * 10.0;
-      for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-        double w = __ldcg(&st.partial[i]);
-        v = w < v ? w : v;
-      }
-      v = block_min(v, sh);
-    }
-    if (do_err) {
-      double *ctl = st.ctl;
-      sum_partials<8>(st.partial + gridDim.x, (int)gridDim.x,
-                      [ctl](int q, double a) { ctl[(q < 4 ? CTL_ERR + q : CTL_RES + q - 4)] = sqrt(a); });
-    }
-    if (threadIdx.x == 0) {
-      if (!DTPRE) {
-        st.ctl[CTL_DTMIN] = v;
-        if (first) st.ctl[CTL_DTSTEP] = v;
-      }
-      if (do_err) {
-        const double dt_time = (lts >= 2) ? st.ctl[CTL_DTSTEP] : st.ctl[CTL_DTMIN];
-        double t = st.ctl[CTL_TOTAL_TIME] + dt_time;
-        st.ctl[CTL_TOTAL_TIME] = t;
-        st.ctl[CTL_ITER] += 1.0;
-        double te = st.ctl[CTL_TEND];
-        if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
-      }
-      *st.counter = 0u;
-    }
+  if (!(fuse_final && is_final)) return;
+  // Last stage: Estimate_Error's terms, the residual squares and the step's dt (the minimum of
+  // the per-cell dt frozen at the first stage, i.e. that stage's Min_dt), then the Total_Time
+  // epilogue of the loop body.
+  __shared__ double sh[32];
+  __shared__ double sh8[8 * 32];
+  __shared__ double red[9];
+  const double sq = block_sums8(e, sh8);
+  if (threadIdx.x < 8) st.partial[(1 + threadIdx.x) * gridDim.x + blockIdx.x] = sq;
+  const double bm = block_min(dtu, sh);
+  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
+  if (grid_reduce9(st, red) && threadIdx.x == 0) {
+    st.ctl[CTL_DTMIN] = red[0];
+    st.ctl[CTL_DTSTEP] = red[0];
+    for (int q = 0; q < 8; q++) st.ctl[q < 4 ? CTL_ERR + q : CTL_RES + q - 4] = sqrt(red[1 + q]);
+    double t = st.ctl[CTL_TOTAL_TIME] + red[0];
+    st.ctl[CTL_TOTAL_TIME] = t;
+    st.ctl[CTL_ITER] += 1.0;
+    double te = st.ctl[CTL_TEND];
+    if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
   }
 }
 
@@ -1033,14 +1081,13 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // Records of the face-based forms: (rho, u, v, p) and their Green-Gauss gradients, the face
 // value being the mean of the two cell values, ghost cells included (their values carry the
 // boundary state).  Ghost rows get (rho, u, v, p) only.
-// DT: also del_t of each physical cell; MIN: also Min_dt and the step's frozen dt (first stage).
-template <bool DT, bool MIN>
+// DT: also del_t of each physical cell (the fused per-cell-dt forms; their Min_dt is formed in
+// the last stage's reduction).
+template <bool DT>
 __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevState st, FluxParams fp) {
-  __shared__ double sh[32];
   const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
   if (step_done(st.ctl)) return;
-  double dt = 1e308 * 10.0;
   if (c < NT) {
     double qc[4];
 #pragma unroll
@@ -1072,27 +1119,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
       }
       r[1] = make_double4(g[0] * ia, g[1] * ia, g[2] * ia, g[3] * ia);
       r[2] = make_double4(g[4] * ia, g[5] * ia, g[6] * ia, g[7] * ia);
-      if (DT) {
-        dt = cell_dt(m, fp, c, den);
-        st.dtc[c] = dt;
-      }
-    }
-  }
-  if (!MIN) return;
-  // Min_dt (get_Min_dt, src/Numerical_Method.cpp:322-330) and the step's dt.
-  const double bm = block_min(dt, sh);
-  if (threadIdx.x == 0) st.partial[blockIdx.x] = bm;
-  if (last_block(st.counter)) {
-    double v = 1e308 * 10.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
-      double w = __ldcg(&st.partial[i]);
-      v = w < v ? w : v;
-    }
-    v = block_min(v, sh);
-    if (threadIdx.x == 0) {
-      st.ctl[CTL_DTMIN] = v;
-      st.ctl[CTL_DTSTEP] = v;
-      *st.counter = 0u;
+      if (DT) st.dtc[c] = cell_dt(m, fp, c, den);
     }
   }
 }
@@ -1313,7 +1340,7 @@ void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const
 
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
-  if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st, fp, 0, 0);
+  if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st, fp, 0);
   if (fp.second_order && fp.muscl && m.NF > 0) {
     if (fp.precision == 1) launch_faces_t<float>(s, nblk(m.NF, 256), m, st, fp);
     else launch_faces_t<double>(s, nblk(m.NF, 256), m, st, fp);
@@ -1379,8 +1406,7 @@ int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParam
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                         int kind, int lts, int fuse_final, int keep_delu, int flags) {
   const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
-  if (flags & 1) k_gather_stage<true><<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
-  else k_gather_stage<false><<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  k_gather_stage<<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
   return 1;
 }
 
@@ -1413,13 +1439,11 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
   return 1;
 }
 
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
-                           int first) {
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt) {
   const int g = m.rblk ? m.n_rblk : nblk(m.NT, kBlock);
   if (m.rblk && g == 0) return 0;
-  if (with_dt && first) k_muscl_gradients<true, true><<<g, kBlock, 0, s>>>(m, st, fp);
-  else if (with_dt) k_muscl_gradients<true, false><<<g, kBlock, 0, s>>>(m, st, fp);
-  else k_muscl_gradients<false, false><<<g, kBlock, 0, s>>>(m, st, fp);
+  if (with_dt) k_muscl_gradients<true><<<g, kBlock, 0, s>>>(m, st, fp);
+  else k_muscl_gradients<false><<<g, kBlock, 0, s>>>(m, st, fp);
   return 1;
 }
 

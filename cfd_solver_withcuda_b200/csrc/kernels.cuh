@@ -41,6 +41,7 @@ struct DevMesh {
 };
 
 constexpr int kWorkCellBlock = 128;
+constexpr int kMaxGroups = 256;  // block groups of the two-level grid reductions
 constexpr int kWorkItemBlock = 256;
 
 struct DevState {
@@ -57,8 +58,9 @@ struct DevState {
   double4 *F;    // [NF] face fluxes (face-based forms)
   // reduction / control block (see CtrlIdx)
   double *ctl;
-  double *partial;     // [nblk_max * 9]
+  double *partial;     // [(nblk_max + kMaxGroups) * 9]
   unsigned int *counter;
+  unsigned int *gcount;  // [kMaxGroups + 1] group and top counters of two-level reductions
   int *status;         // [0] status code, [1] first bad cell (device order)
 };
 
@@ -105,9 +107,9 @@ int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int l
 // gather + stage update.
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
-// flags: bit 0 del_t and Min_dt come from the gradient pass (launch_muscl_gradients with
-// with_dt); bit 1 the owner thread writes its ghosts for the next stage (non-final stages), bit 2
-// that next stage's supersonic-exit copy reads the stage state.
+// Fused gather + stage update of the per-cell-dt forms; del_t comes from the gradient pass
+// (launch_muscl_gradients with with_dt).  flags: bit 1 the owner thread writes its ghosts for the
+// next stage (non-final stages), bit 2 that next stage's supersonic-exit copy reads the stage state.
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                         int kind, int lts, int fuse_final, int keep_delu, int flags);
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
@@ -116,10 +118,8 @@ int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const doub
 int launch_eval_face_flux(cudaStream_t s, int scheme, int precision, const double *UL, const double *UR,
                           const double *nrm, const double *len, int n, double *F);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
-// with_dt: also del_t of every physical cell; with first as well: Min_dt and the step's frozen dt
-// (the per-cell-dt forms use no later Min_dt of the step).
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
-                           int first);
+// with_dt: also del_t of every physical cell (the fused per-cell-dt forms).
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
 // TagRefinableCells on the device; scratch holds >= 2 x 32 + 1024 bytes.
