@@ -81,6 +81,35 @@ std::vector<int> rcm_from_arrays(int NP, const int *nf, const int *nbr) {
   return order;
 }
 
+// Patch ordering: cells grouped into patches of `patch` cells grown breadth-first from seeds
+// taken in RCM order, so a thread block of `patch` cells covers a compact piece of the mesh and
+// most of its neighbours lie inside the same block (cache reuse for the gather kernels).
+std::vector<int> patch_from_arrays(int NP, const int *nf, const int *nbr, int patch) {
+  const std::vector<int> rcm = rcm_from_arrays(NP, nf, nbr);
+  std::vector<char> used(NP, 0);
+  std::vector<int> order, q;
+  order.reserve(NP);
+  q.reserve(patch);
+  for (int seed : rcm) {
+    if (used[seed]) continue;
+    q.clear();
+    q.push_back(seed);
+    used[seed] = 1;
+    for (size_t head = 0; head < q.size(); head++) {
+      const int c = q[head];
+      order.push_back(c);
+      for (int f = 0; f < nf[c]; f++) {
+        const int n = nbr[4 * c + f];
+        if (n >= 0 && n < NP && !used[n] && (int)q.size() < patch) {
+          used[n] = 1;
+          q.push_back(n);
+        }
+      }
+    }
+  }
+  return order;
+}
+
 template <typename T>
 cfd_status dev_upload(T **dst, const std::vector<T> &v) {
   CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), std::max<size_t>(1, v.size()) * sizeof(T)));
@@ -467,7 +496,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     return bail(fail(CFD_ERR_CUDA, "pinned allocation failed"));
 
   // Renumbering (reverse Cuthill-McKee over physical cells; ghosts keep their ids).
-  if (cfg->reorder) ctx->perm = rcm_from_arrays(NP, d->n_faces, d->neighbours);
+  if (cfg->reorder == 2) ctx->perm = patch_from_arrays(NP, d->n_faces, d->neighbours, 128);
+  else if (cfg->reorder) ctx->perm = rcm_from_arrays(NP, d->n_faces, d->neighbours);
   else {
     ctx->perm.resize(NP);
     for (int i = 0; i < NP; i++) ctx->perm[i] = i;

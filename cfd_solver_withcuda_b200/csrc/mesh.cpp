@@ -486,42 +486,5 @@ std::string write_vtk(const Mesh &m, const std::string &path) {
 // ---------------------------------------------------------------------------------------------
 // Reverse Cuthill-McKee over the physical-cell adjacency (ghosts excluded).
 // ---------------------------------------------------------------------------------------------
-std::vector<int> rcm_order(const Mesh &m) {
-  const int NP = m.n_physical;
-  std::vector<int> deg(NP, 0);
-  for (int c = 0; c < NP; c++)
-    for (int f = 0; f < m.n_faces[c]; f++)
-      if (m.nbr[4 * c + f] < NP) deg[c]++;
-  std::vector<int> order;
-  order.reserve(NP);
-  std::vector<char> seen(NP, 0);
-  std::vector<int> by_deg(NP);
-  for (int i = 0; i < NP; i++) by_deg[i] = i;
-  std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-  std::vector<int> nb;
-  for (int start : by_deg) {
-    if (seen[start]) continue;
-    std::queue<int> q;
-    q.push(start);
-    seen[start] = 1;
-    while (!q.empty()) {
-      int c = q.front();
-      q.pop();
-      order.push_back(c);
-      nb.clear();
-      for (int f = 0; f < m.n_faces[c]; f++) {
-        int n = m.nbr[4 * c + f];
-        if (n < NP && !seen[n]) nb.push_back(n);
-      }
-      std::stable_sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b]; });
-      for (int n : nb) {
-        seen[n] = 1;
-        q.push(n);
-      }
-    }
-  }
-  std::reverse(order.begin(), order.end());
-  return order;
-}
 
 }  // namespace cfdb

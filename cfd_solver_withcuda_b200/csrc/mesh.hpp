@@ -53,6 +53,5 @@ std::string read_vtk(Mesh &m, const std::string &path);
 std::string write_vtk(const Mesh &m, const std::string &path);
 
 // Reverse Cuthill-McKee order of the physical cells (perm[new] = old).
-std::vector<int> rcm_order(const Mesh &m);
 
 }  // namespace cfdb

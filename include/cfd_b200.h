@@ -126,7 +126,8 @@ typedef struct {
   int inlet_bc;              /* CFD_INLET_* (reference: Is_Inlet_SubSonic) */
   int exit_bc;               /* CFD_EXIT_*  (reference: Is_Exit_SubSonic) */
   int precision;             /* CFD_PREC_* */
-  int reorder;               /* 1: reverse Cuthill-McKee renumbering on the device */
+  int reorder;               /* device cell numbering: 0 as given, 1 reverse Cuthill-McKee,
+                                2 patches of 128 cells grown breadth-first in RCM seed order */
   double cfl;                /* CFL */
   double limiter_zeta;       /* Limiter_Zeta */
   double limiter_zeta1;      /* Limiter_Zeta1 */

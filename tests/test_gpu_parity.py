@@ -19,7 +19,7 @@ def check_state(st, ref, what, keys=("U", "prim", "dt", "net_flux", "delU")):
         assert_bits_equal(st[k], ref[k], what + ":" + k)
 
 
-@pytest.mark.parametrize("reorder", [0, 1])
+@pytest.mark.parametrize("reorder", [0, 1, 2])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_cuda_matches_reference_fixture(name, reorder):
     case = CASES[name]
@@ -148,7 +148,7 @@ def test_ausm_reference_form_matches_reference():
     g = load_golden("ausm_reference")
     case = CASES["bump_roe2_rk3"]
     m = make_mesh(case)
-    for reorder in (0, 1):
+    for reorder in (0, 1, 2):
         s = cb.Solver(m, solver_config(case, dissipation_type=cb.DISS_AUSM, is_second_order=0, reorder=reorder))
         s.upload_state(g["U"])
         s.Evaluate_Cell_Net_Flux()
@@ -266,7 +266,7 @@ def test_amr_tags_with_ties_match_oracle(frac, oracle_lib):
     o = oracle_lib.OracleRun(m, **oracle_params(case))
     o.set_state(g["U"])
     want_ind, want = o.amr(thr, frac)
-    for reorder in (0, 1):
+    for reorder in (0, 1, 2):
         s = cb.Solver(m, solver_config(case, reorder=reorder))
         s.upload_state(g["U"])
         ind, tags = s.amr_tags(thr, frac)

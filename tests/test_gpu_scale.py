@@ -42,7 +42,7 @@ def test_c2_full_size_matches_oracle(oracle_lib):
 def test_c2_renumbering_invariant():
     m, U0, kw = c2_setup()
     res = []
-    for reorder in (0, 1):
+    for reorder in (0, 1, 2):
         s = cb.Solver(m, cb.default_config(reorder=reorder, **kw))
         s.upload_state(U0)
         s.step(10)
