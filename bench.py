@@ -375,6 +375,27 @@ def run_bump(args, rank, world):
     print(json.dumps(out))
 
 
+def run_warmstart(args, rank, world):
+    """--workload warmstart: learned warm start on the morphed bump family (seeded draws of
+    thickness, inlet Mach and back-pressure ratio); train members solved by the FP64 solver, a
+    message-passing surrogate trained on them, held-out members solved from the freestream and
+    from the predicted start to the same absolute residual."""
+    import torch
+    from cfd_solver_withcuda_b200 import warmstart as ws
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    r = ws.run_experiment(nx=args.ws_nx, ny=args.ws_ny, n_train=args.ws_train, n_test=args.ws_test,
+                          tol=args.ws_tol, max_steps=args.max_steps, check_every=args.check_every,
+                          epochs=args.ws_epochs, seed=args.seed)
+    out = {"metric": "pseudo-steps to tolerance, warm start vs freestream (median ratio)",
+           "value": r["steps_ratio_median"], "unit": "ratio", "n_gpus": world, "higher_is_better": False,
+           "data": "synthetic (seeded morphed-bump family)", "dtype": "f64 solver, bf16/fp32 surrogate",
+           "config": {"workload": "warm_start_bump_family_%s" % r["mesh"]}, "warmstart": r}
+    print(json.dumps(out))
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -406,7 +427,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump"])
+    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart"])
+    ap.add_argument("--ws-nx", type=int, default=64)
+    ap.add_argument("--ws-ny", type=int, default=32)
+    ap.add_argument("--ws-train", type=int, default=192)
+    ap.add_argument("--ws-test", type=int, default=64)
+    ap.add_argument("--ws-tol", type=float, default=1e-4)
+    ap.add_argument("--ws-epochs", type=int, default=200)
     ap.add_argument("--bump-nx", type=int, default=2520)
     ap.add_argument("--bump-ny", type=int, default=840)
     ap.add_argument("--steady-nx", type=int, default=120)
@@ -426,6 +453,8 @@ def main():
         return run_ramps(args, rank, world)
     if args.workload == "bump":
         return run_bump(args, rank, world)
+    if args.workload == "warmstart":
+        return run_warmstart(args, rank, world)
 
     import torch
     import torch.distributed as dist

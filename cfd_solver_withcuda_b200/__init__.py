@@ -122,6 +122,12 @@ SIGNATURES = {
     "cfd_batch_run": (_I, [_P, _I, _D, _I, ctypes.POINTER(_I), _DP, _DP, ctypes.POINTER(ctypes.c_longlong),
                            ctypes.POINTER(_I)]),
     "cfd_batch_destroy": (None, [_P]),
+    "cfd_batch_set_boundary_values": (_I, [_P, _DP, _DP]),
+    "cfd_mpnn_segment_sum": (_I, [_P, _P, _P, _I, _I, _P, _P]),
+    "cfd_mpnn_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _I,
+                           _P]),
+    "cfd_batch_set_reference_residual": (_I, [_P, _DP]),
+    "cfd_batch_residuals": (_I, [_P, _DP]),
     "cfd_kernel_launches": (ctypes.c_longlong, [_P]),
     "cfd_device_bytes": (ctypes.c_size_t, [_P]),
 }
@@ -398,6 +404,25 @@ class Batch:
     def upload_state(self, states):
         U = np.ascontiguousarray(np.concatenate(states, axis=0), dtype=np.float64)
         _check(lib().cfd_batch_upload_state(self._h, _dp(U)))
+
+    def set_boundary_values(self, inlet=None, exit_p=None):
+        """Per-instance inlet values [n, 4] (read by the inlet kind) and exit pressures [n]."""
+        n = len(self.meshes)
+        self._bv = [None if inlet is None else np.ascontiguousarray(inlet, dtype=np.float64).reshape(n, 4),
+                    None if exit_p is None else np.ascontiguousarray(exit_p, dtype=np.float64).reshape(n)]
+        _check(lib().cfd_batch_set_boundary_values(self._h, None if self._bv[0] is None else _dp(self._bv[0]),
+                                                   None if self._bv[1] is None else _dp(self._bv[1])))
+
+    def set_reference_residual(self, r0=None):
+        """Per-instance residual normalisers for run()'s tolerance (None: first-step residual)."""
+        self._r0 = None if r0 is None else np.ascontiguousarray(r0, dtype=np.float64)
+        _check(lib().cfd_batch_set_reference_residual(self._h, None if self._r0 is None else _dp(self._r0)))
+
+    def residuals(self):
+        """||R_rho||_2 of each instance's last residual evaluation."""
+        r = np.zeros(len(self.meshes))
+        _check(lib().cfd_batch_residuals(self._h, _dp(r)))
+        return r
 
     def download_state(self):
         U = np.zeros((sum(self.rows), 4))

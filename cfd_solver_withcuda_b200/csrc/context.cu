@@ -1211,6 +1211,8 @@ struct cfd_batch {
   double *d_res = nullptr;
   int table_cap[4] = {0, 0, 0, 0};
   double4 *d_bstate = nullptr;
+  double *d_bexit = nullptr;
+  std::vector<double> r0_fixed;  // per-instance residual normalisers (empty: first-step residual)
 };
 
 static cfd_status batch_tables(cfd_batch *b) {
@@ -1380,7 +1382,46 @@ cfd_status cfd_batch_upload_state(cfd_batch *b, const double *U) {
     for (int g = b->gs[i]; g < b->ge[i]; g++, row++)
       for (int k = 0; k < 4; k++) u[4 * (size_t)g + k] = U[4 * row + k];
   }
-  return cfd_upload_state(b->ctx, u.data(), ctx->NT);
+  cfd_status s = cfd_upload_state(b->ctx, u.data(), ctx->NT);
+  if (s != CFD_OK) return s;
+  // A new state restarts every instance.
+  b->active.assign(b->n, 1);
+  return batch_tables(b);
+}
+
+cfd_status cfd_batch_set_boundary_values(cfd_batch *b, const double *inlet, const double *exit_p) {
+  if (!b) return fail(CFD_ERR_BAD_ARG, "null argument");
+  cfd_ctx *ctx = b->ctx;
+  cfd_status s;
+  if (inlet) {
+    std::vector<double4> v;
+    for (int i = 0; i < b->n; i++)
+      for (int e = b->bs[i]; e < b->be[i]; e++)
+        v.push_back(make_double4(inlet[4 * i], inlet[4 * i + 1], inlet[4 * i + 2], inlet[4 * i + 3]));
+    if (!b->d_bstate && (s = ctx_alloc(ctx, (void **)&b->d_bstate, sizeof(double4) * v.size())) != CFD_OK) return s;
+    CUDA_TRY(cudaMemcpy(b->d_bstate, v.data(), sizeof(double4) * v.size(), cudaMemcpyHostToDevice));
+    ctx->dm.bstate = b->d_bstate;
+  }
+  if (exit_p) {
+    std::vector<double> v;
+    for (int i = 0; i < b->n; i++)
+      for (int e = b->bs[i]; e < b->be[i]; e++) v.push_back(exit_p[i]);
+    if (!b->d_bexit && (s = ctx_alloc(ctx, (void **)&b->d_bexit, sizeof(double) * v.size())) != CFD_OK) return s;
+    CUDA_TRY(cudaMemcpy(b->d_bexit, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    ctx->dm.bexit = b->d_bexit;
+  }
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_set_reference_residual(cfd_batch *b, const double *r0) {
+  if (!b) return fail(CFD_ERR_BAD_ARG, "null argument");
+  if (r0) b->r0_fixed.assign(r0, r0 + b->n);
+  else b->r0_fixed.clear();
+  return CFD_OK;
 }
 
 cfd_status cfd_batch_download_state(cfd_batch *b, double *U) {
@@ -1409,6 +1450,15 @@ static cfd_status batch_residuals(cfd_batch *b, std::vector<double> &res) {
   return CFD_OK;
 }
 
+cfd_status cfd_batch_residuals(cfd_batch *b, double *res) {
+  if (!b || !res) return fail(CFD_ERR_BAD_ARG, "null argument");
+  std::vector<double> r;
+  cfd_status s = batch_residuals(b, r);
+  if (s != CFD_OK) return s;
+  for (int i = 0; i < b->n; i++) res[i] = r[i];
+  return CFD_OK;
+}
+
 cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,
                          double *time_to_tol, double *res_ratio, long long *cell_updates, int *steps_done) {
   if (!b || max_steps < 1 || check_every < 1) return fail(CFD_ERR_BAD_ARG, "bad argument");
@@ -1430,6 +1480,7 @@ cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_ever
   for (int i = 0; i < n; i++)
     if (b->active[i]) cu += b->ce[i] - b->cs[i];
   if ((s = batch_residuals(b, r0)) != CFD_OK) return s;
+  if (!b->r0_fixed.empty()) r0 = b->r0_fixed;
   int steps = 1;
   while (steps < max_steps) {
     bool any = false;

@@ -286,7 +286,8 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
       const int ld = cur_is_S ? NP : NT;
       const double Ui[4] = {Uc[c], Uc[ld + c], Uc[2 * ld + c], Uc[3 * ld + c]};
       double Gf[4];
-      farfield_state(Ui, m.nx[f * NP + c], m.ny[f * NP + c], bp.inlet_rho, bp.inlet_u, bp.inlet_v, bp.inlet_p, Gf);
+      const double4 fs = m.bstate ? m.bstate[e] : make_double4(bp.inlet_rho, bp.inlet_u, bp.inlet_v, bp.inlet_p);
+      farfield_state(Ui, m.nx[f * NP + c], m.ny[f * NP + c], fs.x, fs.y, fs.z, fs.w, Gf);
       G0 = Gf[0];
       G1 = Gf[1];
       G2 = Gf[2];
@@ -322,14 +323,15 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
       const double a_i = prim[4 * NT + c];
       const double vn_i = u * n1 + v * n2;
       const double Rp = vn_i + 2.0 * a_i / kGM1;
-      const double a0sq = kGamma * bp.r_gas * bp.inlet_t0;
+      const double p0 = m.bstate ? m.bstate[e].x : bp.inlet_p0, t0 = m.bstate ? m.bstate[e].y : bp.inlet_t0;
+      const double a0sq = kGamma * bp.r_gas * t0;
       const double qa = (kGamma + 1.0) / kGM1, qb = -2.0 * Rp, qc = 0.5 * kGM1 * Rp * Rp - a0sq;
       const double disc = qb * qb - 4.0 * qa * qc;
       const double ab = (-qb + sqrt(disc > 0.0 ? disc : 0.0)) / (2.0 * qa);
       double vn = Rp - 2.0 * ab / kGM1;
       if (vn > 0.0) vn = 0.0;
       const double Tb = ab * ab / (kGamma * bp.r_gas);
-      const double pb = bp.inlet_p0 * pow(Tb / bp.inlet_t0, kGamma / kGM1);
+      const double pb = p0 * pow(Tb / t0, kGamma / kGM1);
       const double rb = pb / (bp.r_gas * Tb);
       const double ub = vn * n1, vb = vn * n2;
       G0 = rb;
@@ -349,7 +351,8 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
     } else if (bp.exit_bc == 3) {
       const double rho_Et = cur_is_S ? st.S[3 * NP + c] : st.U[3 * NT + c];
       double Gf[4];
-      fixed_p_exit_state(rho, u, v, p, rho_Et, m.nx[f * NP + c], m.ny[f * NP + c], bp.exit_p, Gf);
+      fixed_p_exit_state(rho, u, v, p, rho_Et, m.nx[f * NP + c], m.ny[f * NP + c], m.bexit ? m.bexit[e] : bp.exit_p,
+                         Gf);
       G0 = Gf[0];
       G1 = Gf[1];
       G2 = Gf[2];
@@ -360,7 +363,7 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
       const double n1 = m.nx[f * NP + c], n2 = m.ny[f * NP + c];
       const double a_i = prim[4 * NT + c];
       const double vn = u * n1 + v * n2;
-      const double pb = (vn < a_i) ? bp.exit_p : p;
+      const double pb = (vn < a_i) ? (m.bexit ? m.bexit[e] : bp.exit_p) : p;
       G0 = rho;
       G1 = rho * u;
       G2 = rho * v;

@@ -36,8 +36,11 @@ struct DevMesh {
   // ghost rows); null = all items.
   const int2 *cblk, *fblk, *bblk, *rblk;
   int n_cblk, n_fblk, n_bblk, n_rblk;
-  // Prescribed inflow state (rho, u, v, p) per boundary entry (CFD_INLET_FIXED), or null.
+  // Per boundary entry (batched solves), or null: inlet values read by the inlet kind
+  // (CFD_INLET_FIXED and CFD_INLET_FARFIELD: rho, u, v, p; CFD_INLET_TOTAL_PT: p0, T0) and the
+  // exit pressure (CFD_EXIT_STATIC_P, CFD_EXIT_FIXED_P_REF).
   const double4 *bstate;
+  const double *bexit;
 };
 
 constexpr int kWorkCellBlock = 128;

@@ -274,17 +274,39 @@ cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_con
 typedef struct cfd_batch cfd_batch;
 cfd_status cfd_batch_create(int n, const cfd_mesh_desc *meshes, const double *inflow, const cfd_config *cfg,
                             cfd_batch **out);
-/* U: for each instance in order, its NP_i + NG_i rows in reference order. */
+/* U: for each instance in order, its NP_i + NG_i rows in reference order.  Uploading restarts
+ * every instance (all active again). */
 cfd_status cfd_batch_upload_state(cfd_batch *b, const double *U);
+/* Per-instance boundary values (either pointer may be NULL): inlet [n*4] read by the configured
+ * inlet kind (CFD_INLET_FIXED / CFD_INLET_FARFIELD: rho, u, v, p; CFD_INLET_TOTAL_PT: p0, T0, -, -),
+ * exit_p [n] the exit pressure of CFD_EXIT_STATIC_P / CFD_EXIT_FIXED_P_REF. */
+cfd_status cfd_batch_set_boundary_values(cfd_batch *b, const double *inlet, const double *exit_p);
+/* Per-instance residual normalisers r0 [n] for cfd_batch_run's tolerance test (NULL: each
+ * instance's first-step residual), so that runs from different starts share one absolute target. */
+cfd_status cfd_batch_set_reference_residual(cfd_batch *b, const double *r0);
+/* ||R_rho||_2 of each instance's last residual evaluation, [n]. */
+cfd_status cfd_batch_residuals(cfd_batch *b, double *res);
 cfd_status cfd_batch_download_state(cfd_batch *b, double *U);
 /* Runs until every instance's plain residual ||R_rho||_2 has dropped by the factor tol from its
- * first-step value, or max_steps; the residuals are checked every check_every steps (each check
+ * first-step value (or from the normaliser set by cfd_batch_set_reference_residual), or
+ * max_steps; the residuals are checked every check_every steps (each check
  * synchronises).  Per instance: steps_to_tol (-1 if not reached), time_to_tol (seconds since the
  * call, -1 if not reached), res_ratio (last ||R_rho|| / first).  cell_updates counts the cells
  * actually advanced.  Any output pointer may be NULL. */
 cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,
                          double *time_to_tol, double *res_ratio, long long *cell_updates, int *steps_done);
 void cfd_batch_destroy(cfd_batch *b);
+
+/* ------------------------------------------------------------------------------------------
+ * Kernels of the warm-start surrogate (message passing on the cell graph of a mesh; no reference
+ * counterpart).  Device pointers, float32, launched on `stream` (cudaStream_t, NULL = default).
+ * Segment sum: out[r, :] = sum over j in [ptr[r], ptr[r+1]) of x[idx[j], :] in list order
+ * (deterministic; width columns).  Adam: one bias-corrected step (`step` counts from 1).
+ * ------------------------------------------------------------------------------------------ */
+cfd_status cfd_mpnn_segment_sum(const float *x, const int *ptr, const int *idx, int n_rows, int width, float *out,
+                                void *stream);
+cfd_status cfd_mpnn_adam(float *param, const float *grad, float *m, float *v, int n, float lr, float beta1,
+                         float beta2, float eps, int step, void *stream);
 
 /* Accumulated device time of one kernel family ("flux", "stage", "bc", and for the face-based
  * forms "gradients", "faces", "gather_stage") over the launches made while option "profile" was
