@@ -54,7 +54,8 @@ class Config(ctypes.Structure):
                 ("limiter_zeta1", ctypes.c_double), ("inlet_rho", ctypes.c_double), ("inlet_p", ctypes.c_double),
                 ("inlet_u", ctypes.c_double), ("inlet_v", ctypes.c_double), ("inlet_p0", ctypes.c_double),
                 ("inlet_t0", ctypes.c_double), ("exit_p", ctypes.c_double), ("r_gas", ctypes.c_double),
-                ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+                ("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("weno", ctypes.c_int),
+                ("weno_characteristic", ctypes.c_int)]
 
 
 class FluxArrays(ctypes.Structure):

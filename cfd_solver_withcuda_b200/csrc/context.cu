@@ -460,6 +460,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     return fail(CFD_ERR_BAD_ARG, "the reference GPU AUSM face flux is available in the gradient-MUSCL form only");
   if (cfg->integrator < CFD_INT_REFERENCE || cfg->integrator > CFD_INT_RK4_GPU_REF)
     return fail(CFD_ERR_BAD_ARG, "bad integrator");
+  if (cfg->weno && cfg->muscl && cfg->is_second_order)
+    return fail(CFD_ERR_BAD_ARG, "the WENO path replaces the MUSCL reconstruction (muscl = 0 with weno = 1)");
+  if (cfg->weno && cfg->precision != CFD_PREC_FP64) return fail(CFD_ERR_BAD_ARG, "the WENO path is FP64");
   if ((diss == CFD_DISS_AUSM || diss == CFD_DISS_HLLC) && cfg->is_second_order && !cfg->muscl)
     return fail(CFD_ERR_BAD_ARG, "second-order AUSM / HLLC use the gradient-MUSCL form (muscl = 1)");
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
@@ -706,6 +709,15 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.muscl = cfg->muscl && cfg->is_second_order;
   fp.lanes = 1;
   fp.faces_shape = 2;
+  // WENO (Is_WENO): Explicit_Method falls back to the 1O/2O residual when any cell is not a quad
+  // (src/Numerical_Method.cpp:31-55); Runge_Kutta_Method keeps WENO (zero flux on those cells).
+  {
+    bool all_quads = true;
+    for (int c = 0; c < NP; c++) all_quads = all_quads && d->n_faces[c] == 4;
+    const bool explicit_form = cfg->integrator == CFD_INT_REFERENCE && !cfg->time_accurate;
+    fp.weno = cfg->weno && (all_quads || !explicit_form) ? 1 : 0;
+    fp.weno_char = cfg->weno_characteristic ? 1 : 0;
+  }
   fp.consistent = (cfg->integrator != CFD_INT_REFERENCE) ? 1 : 0;
   fp.precision = cfg->precision;
   fp.cfl = cfg->cfl;

@@ -220,18 +220,21 @@ std::string config_from_json(const std::string &text, cfd_config *cfg) {
     as_bool(sol->get("Is_Second_Order"), cfg->is_second_order);
     as_bool(sol->get("Time_Accurate"), cfg->time_accurate);
     as_bool(sol->get("Local_Time_Stepping"), cfg->local_time_stepping);
+    as_bool(sol->get("Is_WENO"), cfg->weno);
+    as_bool(sol->get("Is_Char"), cfg->weno_characteristic);
     const JVal *fs = sol->get("Flux_Scheme");
     if (fs && fs->kind == JVal::STR) {
-      int k = enum_from(fs, {"llf", "roe", "ausm", "hllc"}, -1);
-      const int map[4] = {CFD_DISS_LLF, CFD_DISS_ROE, CFD_DISS_AUSM, CFD_DISS_HLLC};
+      int k = enum_from(fs, {"llf", "roe", "ausm", "hllc", "ausm_gpu"}, -1);
+      const int map[5] = {CFD_DISS_LLF, CFD_DISS_ROE, CFD_DISS_AUSM, CFD_DISS_HLLC, CFD_DISS_AUSM_GPU};
       if (k >= 0) cfg->dissipation_type = map[k];
     }
     cfg->limiter = enum_from(sol->get("Limiter_Type"), {"minmod_reference", "minmod", "vanleer", "superbee", "vanalbada"},
                              cfg->limiter);
-    cfg->integrator = enum_from(sol->get("Integrator"), {"reference", "rk4", "ssprk3"}, cfg->integrator);
+    cfg->integrator = enum_from(sol->get("Integrator"), {"reference", "rk4", "ssprk3", "rk3_gpu_ref", "rk4_gpu_ref"},
+                                cfg->integrator);
     cfg->precision = enum_from(sol->get("Precision"), {"fp64", "fp32_flux"}, cfg->precision);
     cfg->reconstruct_primitive = enum_from(sol->get("Reconstruction"), {"conserved", "primitive"}, cfg->reconstruct_primitive);
-    as_bool(sol->get("Reorder"), cfg->reorder);
+    as_int(sol->get("Reorder"), cfg->reorder);
     cfg->muscl = enum_from(sol->get("MUSCL"), {"reference", "gradient"}, cfg->muscl);
   }
   if (lim) {

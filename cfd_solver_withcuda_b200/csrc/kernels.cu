@@ -618,6 +618,139 @@ __global__ void __launch_bounds__(kFlux4Block) k_flux4(DevMesh m, DevState st, F
   min_dt_epilogue(st, dt, sh);
 }
 
+// Evaluate_Cell_Net_Flux_WENO, src/WENO2D.cpp:395-456, one thread per cell.  Quad cells only
+// (others get a zero net flux and their del_t, as in the reference).  Stencils walk the neighbour
+// slots as the reference does (WENO_Reconstruction_X, :245-393): slot 0 / 1 for the "i" walks and
+// 2 / 3 for the "j" walks, a ghost repeated when the walk leaves the domain.  The stencil values
+// are the conserved variables the reference rebuilds from the primitives
+// (Calculate_Computational_Variables, src/Basic_Functions.cpp:156-163): rho, rho*u, rho*v and the
+// energy the primitives were computed from (cur_is_S: the stage state for physical cells).
+__device__ __forceinline__ void weno_cons(const DevMesh &m, const DevState &st, int i, int cur_is_S, double U[4]) {
+  const int NP = m.NP, NT = m.NT;
+  const double rho = st.prim[i];
+  U[0] = rho;
+  U[1] = rho * st.prim[NT + i];
+  U[2] = rho * st.prim[2 * NT + i];
+  U[3] = (i < NP && cur_is_S) ? st.S[3 * NP + i] : st.U[3 * NT + i];
+}
+
+// Get_Reconstructed_U, src/WENO2D.cpp:216-243.
+__device__ __forceinline__ bool weno_recon(const DevMesh &m, const DevState &st, int cur_is_S, bool chr,
+                                           const double Lm[16], const double ILm[16], int i1, int i2, int i3, int i4,
+                                           int i5, int lr, double U[4]) {
+  double s[5][4];
+  weno_cons(m, st, i1, cur_is_S, s[0]);
+  weno_cons(m, st, i2, cur_is_S, s[1]);
+  weno_cons(m, st, i3, cur_is_S, s[2]);
+  weno_cons(m, st, i4, cur_is_S, s[3]);
+  weno_cons(m, st, i5, cur_is_S, s[4]);
+  if (chr) {
+    double w[5][4], W[4];
+#pragma unroll
+    for (int k = 0; k < 5; k++) weno_matvec(Lm, s[k], w[k]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) W[i] = weno5(w[0][i], w[1][i], w[2][i], w[3][i], w[4][i], lr);
+    weno_matvec(ILm, W, U);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; i++) U[i] = weno5(s[0][i], s[1][i], s[2][i], s[3][i], s[4][i], lr);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, FluxParams fp, int cur_is_S) {
+  __shared__ double sh[32];
+  const int NP = m.NP, NT = m.NT;
+  const int c = item_index(m.cblk, NP);
+  const bool done = step_done(st.ctl);
+  double dt = 1e308 * 10.0;
+  if (c < NP && !done) {
+    const int nf = m.nf[c];
+    double R[4] = {0.0, 0.0, 0.0, 0.0};
+    bool ok = true;
+    if (nf == 4) {
+      const int im1 = m.nbr[c], ip1 = m.nbr[NP + c], jm1 = m.nbr[2 * NP + c], jp1 = m.nbr[3 * NP + c];
+      int im2, im3, ip2, ip3, jm2, jm3, jp2, jp3;
+      if (im1 >= NP) {
+        im2 = im1;
+        im3 = im1;
+      } else {
+        im2 = m.nbr[im1];
+        if (im2 >= NP || im2 < 0) {
+          im3 = im2;
+        } else {
+          im3 = m.nbr[im2];
+          if (im3 < 0) im3 = im2;
+        }
+      }
+      if (ip1 >= NP) {
+        ip2 = ip1;
+        ip3 = ip1;
+      } else {
+        ip2 = m.nbr[NP + ip1];
+        if (ip2 >= NP || ip2 < 0) {
+          ip3 = ip2;
+        } else {
+          ip3 = m.nbr[NP + ip2];
+          if (ip3 < 0) ip3 = ip2;
+        }
+      }
+      if (jm1 >= NP) {
+        jm2 = jm1;
+        jm3 = jm1;
+      } else {
+        jm2 = m.nbr[2 * NP + jm1];
+        jm3 = (jm2 >= NP) ? jm2 : m.nbr[2 * NP + jm2];
+      }
+      if (jp1 >= NP) {
+        jp2 = jp1;
+        jp3 = jp1;
+      } else {
+        jp2 = m.nbr[3 * NP + jp1];
+        jp3 = (jp2 >= NP) ? jp2 : m.nbr[3 * NP + jp2];
+      }
+      // Face stencils (left: shift 0, right: shift 1) of WENO_Reconstruction_X's switch.
+      const int st5[4][2][5] = {{{im3, im2, im1, c, ip1}, {im2, im1, c, ip1, ip2}},
+                                {{jm3, jm2, jm1, c, jp1}, {jm2, jm1, c, jp1, jp2}},
+                                {{im2, im1, c, ip1, ip2}, {im1, c, ip1, ip2, ip3}},
+                                {{jm2, jm1, c, jp1, jp2}, {jm1, c, jp1, jp2, jp3}}};
+      const int nb[4] = {im1, ip1, jm1, jp1};
+#pragma unroll 1
+      for (int f = 0; f < 4; f++) {
+        const int idx = f * NP + c;
+        const double nx = m.nx[idx], ny = m.ny[idx], dl = m.dl[idx];
+        double Lm[16], ILm[16];
+        if (fp.weno_char) {
+          const int N = nb[f];
+          ok = weno_lr(st.prim[c], st.prim[NT + c], st.prim[2 * NT + c], st.prim[4 * NT + c], st.prim[N],
+                       st.prim[NT + N], st.prim[2 * NT + N], st.prim[4 * NT + N], nx, ny, Lm, ILm) && ok;
+        }
+        double UL[4], UR[4], F[4];
+        const int *a = st5[f][0], *b = st5[f][1];
+        weno_recon(m, st, cur_is_S, fp.weno_char, Lm, ILm, a[0], a[1], a[2], a[3], a[4], 0, UL);
+        weno_recon(m, st, cur_is_S, fp.weno_char, Lm, ILm, b[0], b[1], b[2], b[3], b[4], 1, UR);
+        ok = weno_face_flux(UL, UR, nx, ny, dl, F) && ok;
+#pragma unroll
+        for (int k = 0; k < 4; k++) R[k] += F[k];
+      }
+    }
+    if (!ok) flag_bad(st.status, c);
+    // Evaluate_Time_Step (src/Time_Step.cpp:293-329) from the cell's own state.
+    const double uc = st.prim[NT + c], vc = st.prim[2 * NT + c], ac = st.prim[4 * NT + c];
+    double den = 0.0;
+    for (int f = 0; f < nf; f++) {
+      const int idx = f * NP + c;
+      const double vnf = uc * m.nx[idx] + vc * m.ny[idx];
+      den += (fabs(vnf) + ac) * m.dl[idx];
+    }
+    dt = cell_dt(m, fp, c, den);
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
+    st.dtc[c] = dt;
+  }
+  min_dt_epilogue(st, dt, sh);
+}
+
 // Face-based evaluation (the Green-Gauss-gradient MUSCL form; no reference counterpart): one
 // thread per unique face computes the flux once from its owner's side, in precision T (double,
 // or float for the FP32-flux form); the neighbour receives exactly the negated flux, so the
@@ -1349,6 +1482,10 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
     else launch_faces_t<double>(s, nblk(m.NF, 256), m, st, fp);
     k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
     return n + 2;
+  }
+  if (fp.weno) {
+    k_weno<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    return n + 1;
   }
   if (fp.lanes == 1) {
     const int g = nblk(m.NP, kFluxBlock);

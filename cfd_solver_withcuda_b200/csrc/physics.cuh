@@ -463,4 +463,154 @@ __device__ __forceinline__ void fixed_p_exit_state(double Rho, double v1, double
   G[3] = 2.0 * F3 - rho_Et;
 }
 
+
+// ---- WENO path (src/WENO2D.cpp), double precision, the reference's association order ----
+
+// WENO_Reconstruction, src/WENO2D.cpp:9-85: fifth-order WENO value at a face from five cell
+// values, shift 0 for the left and 1 for the right state.  The reference's pow(x, 2) calls are
+// x*x here (its libm returns exactly that, checked on 2e8 samples); non-finite inputs or result
+// fall back to the central value.
+__device__ __forceinline__ double weno5(double a, double b, double c, double d, double e, int shift) {
+  if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(d) || !isfinite(e)) return c;
+  const double epsilon = 1e-6;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0;
+  if (shift == 0) {
+    d0 = 3.0 / 10.0;
+    d1 = 6.0 / 10.0;
+    d2 = 1.0 / 10.0;
+    v2 = (2.0 * a - 7.0 * b + 11.0 * c) / 6.0;
+    v1 = (-1.0 * b + 5.0 * c + 2.0 * d) / 6.0;
+    v0 = (2.0 * c + 5.0 * d - 1.0 * e) / 6.0;
+  } else if (shift == 1) {
+    d0 = 1.0 / 10.0;
+    d1 = 6.0 / 10.0;
+    d2 = 3.0 / 10.0;
+    v2 = (-1.0 * a + 5.0 * b + 2.0 * c) / 6.0;
+    v1 = (2.0 * b + 5.0 * c - 1.0 * d) / 6.0;
+    v0 = (11.0 * c - 7.0 * d + 2.0 * e) / 6.0;
+  }
+  const double s2a = a - 2.0 * b + c, s2b = a - 4.0 * b + 3.0 * c;
+  const double s1a = b - 2.0 * c + d, s1b = b - d;
+  const double s0a = c - 2.0 * d + e, s0b = 3.0 * c - 4.0 * d + e;
+  const double b2 = (13.0 / 12.0) * (s2a * s2a) + (1.0 / 4.0) * (s2b * s2b);
+  const double b1 = (13.0 / 12.0) * (s1a * s1a) + (1.0 / 4.0) * (s1b * s1b);
+  const double b0 = (13.0 / 12.0) * (s0a * s0a) + (1.0 / 4.0) * (s0b * s0b);
+  const double q0 = epsilon + b0, q1 = epsilon + b1, q2 = epsilon + b2;
+  const double a0 = d0 / (q0 * q0);
+  const double a1 = d1 / (q1 * q1);
+  const double a2 = d2 / (q2 * q2);
+  const double sum = a0 + a1 + a2;
+  double U;
+  if (sum < epsilon) {
+    U = (v0 + v1 + v2) / 3.0;
+  } else {
+    const double w0 = a0 / sum, w1 = a1 / sum, w2 = a2 / sum;
+    U = w0 * v0 + w1 * v1 + w2 * v2;
+  }
+  if (!isfinite(U)) U = c;
+  return U;
+}
+
+// Get_LR, src/WENO2D.cpp:87-199: conserved-to-characteristic matrix L and its inverse IL (column
+// major, [i + 4 j]) from the Roe-type average of the two face cells' (rho, u, v, a).  Returns
+// false where the reference would stop on a NaN entry.
+__device__ __forceinline__ bool weno_lr(double dL, double uL, double vL, double aL, double dR, double uR, double vR,
+                                        double aR, double nx, double ny, double L[16], double IL[16]) {
+  const double sqrt_dL = sqrt(fmax(dL, 1e-14)), sqrt_dR = sqrt(fmax(dR, 1e-14));
+  const double denom = sqrt_dL + sqrt_dR;
+  double u_RL, v_RL, a_RL;
+  if (denom < 1e-14) {
+    u_RL = 0.5 * (uL + uR);
+    v_RL = 0.5 * (vL + vR);
+    a_RL = 0.5 * (aL + aR);
+  } else {
+    u_RL = (uL * sqrt_dL + uR * sqrt_dR) / denom;
+    v_RL = (vL * sqrt_dL + vR * sqrt_dR) / denom;
+    a_RL = (aL * sqrt_dL + aR * sqrt_dR) / denom;
+  }
+  const double vn = (u_RL * nx + v_RL * ny);
+  const double ek = 0.5 * (u_RL * u_RL + v_RL * v_RL);
+  const double h = (a_RL * a_RL / kGM1) + ek;
+  if (a_RL < 1e-14) a_RL = 1e-14;
+  const double t1 = 0.5 / (a_RL * a_RL);
+  const double t2 = kGM1 * t1;
+  L[0] = 1.0 - 2.0 * t2 * ek;
+  L[4] = 2.0 * t2 * u_RL;
+  L[8] = 2.0 * t2 * v_RL;
+  L[12] = -2.0 * t2;
+  L[1] = v_RL * nx - u_RL * ny;
+  L[5] = ny;
+  L[9] = -nx;
+  L[13] = 0.0;
+  L[2] = t2 * ek - a_RL * vn * t1;
+  L[6] = -t2 * u_RL + a_RL * t1 * nx;
+  L[10] = -t2 * v_RL + a_RL * t1 * ny;
+  L[14] = t2;
+  L[3] = t2 * ek + a_RL * vn * t1;
+  L[7] = -t2 * u_RL - a_RL * t1 * nx;
+  L[11] = -t2 * v_RL - a_RL * t1 * ny;
+  L[15] = t2;
+  IL[0] = 1.0;
+  IL[4] = 0.0;
+  IL[8] = 1.0;
+  IL[12] = 1.0;
+  IL[1] = u_RL;
+  IL[5] = ny;
+  IL[9] = u_RL + a_RL * nx;
+  IL[13] = u_RL - a_RL * nx;
+  IL[2] = v_RL;
+  IL[6] = -nx;
+  IL[10] = v_RL + a_RL * ny;
+  IL[14] = v_RL - a_RL * ny;
+  IL[3] = ek;
+  IL[7] = u_RL * ny - v_RL * nx;
+  IL[11] = h + a_RL * vn;
+  IL[15] = h - a_RL * vn;
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < 16; i++) ok = ok && !(L[i] != L[i]) && !(IL[i] != IL[i]);
+  return ok;
+}
+
+// MatVecMul, src/WENO2D.cpp:201-214: B = A x with A column major, each row summed from 0.0.
+__device__ __forceinline__ void weno_matvec(const double A[16], const double x[4], double B[4]) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += A[i + 4 * j] * x[j];
+    B[i] = s;
+  }
+}
+
+// Calculate_Face_WENO_Flux, src/WENO2D.cpp:458-562 (the wall-face flag is never set on the
+// reference path): average of the two face states' fluxes minus 0.5 * max|lambda| dl (UR - UL).
+// F receives Average - Dissipative; returns false when a face state has a NaN sound speed.
+__device__ __forceinline__ bool weno_face_flux(const double UL[4], const double UR[4], double nx, double ny, double dl,
+                                               double F[4]) {
+  Prim L, R;
+  const bool okL = eos_prim(UL[0], UL[1], UL[2], UL[3], L);
+  const bool okR = eos_prim(UR[0], UR[1], UR[2], UR[3], R);
+  const double Vdotn_L = (L.u * nx + L.v * ny), Vdotn_R = (R.u * nx + R.v * ny);
+  const double Vmag_L = 0.5 * (L.u * L.u + L.v * L.v), Vmag_R = 0.5 * (R.u * R.u + R.v * R.v);
+  double FL[4], FR[4];
+  FL[0] = L.rho * Vdotn_L * dl;
+  FL[1] = L.rho * L.u * Vdotn_L * dl + L.p * nx * dl;
+  FL[2] = L.rho * L.v * Vdotn_L * dl + L.p * ny * dl;
+  FL[3] = (kGamma1 * L.p + L.rho * Vmag_L) * Vdotn_L * dl;
+  FR[0] = R.rho * Vdotn_R * dl;
+  FR[1] = R.rho * R.u * Vdotn_R * dl + R.p * nx * dl;
+  FR[2] = R.rho * R.v * Vdotn_R * dl + R.p * ny * dl;
+  FR[3] = (kGamma1 * R.p + R.rho * Vmag_R) * Vdotn_R * dl;
+  double C_L = L.a, C_R = R.a;
+  if (C_L < 1e-14) C_L = 1e-14;
+  if (C_R < 1e-14) C_R = 1e-14;
+  const double S0 = fabs(Vdotn_L - C_L) * dl, S1 = fabs(Vdotn_L + C_L) * dl, S2 = fabs(Vdotn_L) * dl;
+  const double S3 = fabs(Vdotn_R - C_R) * dl, S4 = fabs(Vdotn_R + C_R) * dl, S5 = fabs(Vdotn_R) * dl;
+  const double mx = max2_ref<double>(max3_ref<double>(S0, S1, S2), max3_ref<double>(S3, S4, S5));
+#pragma unroll
+  for (int i = 0; i < 4; i++) F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * mx * (UR[i] - UL[i]);
+  return okL && okR;
+}
+
 }  // namespace cfdb

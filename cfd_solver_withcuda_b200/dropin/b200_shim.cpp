@@ -75,6 +75,8 @@ void b200_init() {
   cfg.cfl = CFL;
   cfg.limiter_zeta = Limiter_Zeta;
   cfg.limiter_zeta1 = Limiter_Zeta1;
+  cfg.weno = Is_WENO ? 1 : 0;
+  cfg.weno_characteristic = Is_Char ? 1 : 0;
   cfg.inlet_bc = Is_Inlet_SubSonic ? CFD_INLET_SUBSONIC_REF : CFD_INLET_SUPERSONIC;
   cfg.exit_bc = Is_Exit_SubSonic ? CFD_EXIT_SUBSONIC_REF : CFD_EXIT_SUPERSONIC;
   cfg.inlet_rho = inletCond.Rho;

@@ -137,6 +137,9 @@ typedef struct {
   double r_gas;                                /* gas constant for total-temperature inflow */
   int device;                /* CUDA device ordinal */
   void *stream;              /* cudaStream_t to launch on (NULL: the context creates its own) */
+  int weno;                  /* Is_WENO: the reference's WENO path (Evaluate_Cell_Net_Flux_WENO,
+                                src/WENO2D.cpp:395-456; quad cells; replaces the MUSCL forms) */
+  int weno_characteristic;   /* Is_Char: WENO on characteristic variables (src/WENO2D.cpp:228-236) */
 } cfd_config;
 
 /* Defaults of json_Files/Solver_Config.json with Dissipation_Type = ROE. */

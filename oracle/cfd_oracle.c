@@ -543,18 +543,179 @@ static void muscl_net_flux(orc_state *s) {
   }
 }
 
+/* ---- WENO path, src/WENO2D.cpp ---- */
+
+/* WENO_Reconstruction, src/WENO2D.cpp:9-85 (pow(x, 2) written x*x, which libm returns). */
+static double weno5(double a, double b, double c, double d, double e, int shift) {
+  if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(d) || !isfinite(e)) return c;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, v0 = 0.0, v1 = 0.0, v2 = 0.0, epsilon = 1e-6;
+  if (shift == 0) {
+    d0 = 3.0 / 10.0; d1 = 6.0 / 10.0; d2 = 1.0 / 10.0;
+    v2 = (2.0 * a - 7.0 * b + 11.0 * c) / 6.0;
+    v1 = (-1.0 * b + 5.0 * c + 2.0 * d) / 6.0;
+    v0 = (2.0 * c + 5.0 * d - 1.0 * e) / 6.0;
+  } else if (shift == 1) {
+    d0 = 1.0 / 10.0; d1 = 6.0 / 10.0; d2 = 3.0 / 10.0;
+    v2 = (-1.0 * a + 5.0 * b + 2.0 * c) / 6.0;
+    v1 = (2.0 * b + 5.0 * c - 1.0 * d) / 6.0;
+    v0 = (11.0 * c - 7.0 * d + 2.0 * e) / 6.0;
+  }
+  double s2a = a - 2.0 * b + c, s2b = a - 4.0 * b + 3.0 * c;
+  double s1a = b - 2.0 * c + d, s1b = b - d;
+  double s0a = c - 2.0 * d + e, s0b = 3.0 * c - 4.0 * d + e;
+  double b2 = (13.0 / 12.0) * (s2a * s2a) + (1.0 / 4.0) * (s2b * s2b);
+  double b1 = (13.0 / 12.0) * (s1a * s1a) + (1.0 / 4.0) * (s1b * s1b);
+  double b0 = (13.0 / 12.0) * (s0a * s0a) + (1.0 / 4.0) * (s0b * s0b);
+  double q0 = epsilon + b0, q1 = epsilon + b1, q2 = epsilon + b2;
+  double a0 = d0 / (q0 * q0), a1 = d1 / (q1 * q1), a2 = d2 / (q2 * q2);
+  double sum = a0 + a1 + a2, U;
+  if (sum < epsilon) U = (v0 + v1 + v2) / 3.0;
+  else U = (a0 / sum) * v0 + (a1 / sum) * v1 + (a2 / sum) * v2;
+  if (!isfinite(U)) U = c;
+  return U;
+}
+
+/* Get_LR, src/WENO2D.cpp:87-199 (column-major L and its inverse). */
+static void weno_lr(const double *PL, const double *PR, double nx, double ny, double *L, double *IL) {
+  double dL = PL[0], uL = PL[1], vL = PL[2], aL = PL[5], dR = PR[0], uR = PR[1], vR = PR[2], aR = PR[5];
+  double sqrt_dL = sqrt(fmax(dL, 1e-14)), sqrt_dR = sqrt(fmax(dR, 1e-14)), denom = sqrt_dL + sqrt_dR;
+  double u_RL, v_RL, a_RL;
+  if (denom < 1e-14) {
+    u_RL = 0.5 * (uL + uR); v_RL = 0.5 * (vL + vR); a_RL = 0.5 * (aL + aR);
+  } else {
+    u_RL = (uL * sqrt_dL + uR * sqrt_dR) / denom;
+    v_RL = (vL * sqrt_dL + vR * sqrt_dR) / denom;
+    a_RL = (aL * sqrt_dL + aR * sqrt_dR) / denom;
+  }
+  double vn = (u_RL * nx + v_RL * ny), ek = 0.5 * (u_RL * u_RL + v_RL * v_RL), h = (a_RL * a_RL / GM1) + ek;
+  if (a_RL < 1e-14) a_RL = 1e-14;
+  double t1 = 0.5 / (a_RL * a_RL), t2 = GM1 * t1;
+  L[0] = 1.0 - 2.0 * t2 * ek; L[4] = 2.0 * t2 * u_RL; L[8] = 2.0 * t2 * v_RL; L[12] = -2.0 * t2;
+  L[1] = v_RL * nx - u_RL * ny; L[5] = ny; L[9] = -nx; L[13] = 0.0;
+  L[2] = t2 * ek - a_RL * vn * t1; L[6] = -t2 * u_RL + a_RL * t1 * nx; L[10] = -t2 * v_RL + a_RL * t1 * ny; L[14] = t2;
+  L[3] = t2 * ek + a_RL * vn * t1; L[7] = -t2 * u_RL - a_RL * t1 * nx; L[11] = -t2 * v_RL - a_RL * t1 * ny; L[15] = t2;
+  IL[0] = 1.0; IL[4] = 0.0; IL[8] = 1.0; IL[12] = 1.0;
+  IL[1] = u_RL; IL[5] = ny; IL[9] = u_RL + a_RL * nx; IL[13] = u_RL - a_RL * nx;
+  IL[2] = v_RL; IL[6] = -nx; IL[10] = v_RL + a_RL * ny; IL[14] = v_RL - a_RL * ny;
+  IL[3] = ek; IL[7] = u_RL * ny - v_RL * nx; IL[11] = h + a_RL * vn; IL[15] = h - a_RL * vn;
+}
+
+static void weno_matvec(const double *A, const double *x, double *B) {
+  for (int i = 0; i < 4; i++) {
+    B[i] = 0.0;
+    for (int j = 0; j < 4; j++) B[i] += A[i + 4 * j] * x[j];
+  }
+}
+
+/* Calculate_Computational_Variables(cell, U), src/Basic_Functions.cpp:156-163. */
+static void weno_cons(const orc_state *s, int i, double *U) {
+  const double *P = s->P + 11 * (size_t)i;
+  U[0] = P[0];
+  U[1] = P[0] * P[1];
+  U[2] = P[0] * P[2];
+  U[3] = P[6];
+}
+
+/* Get_Reconstructed_U, src/WENO2D.cpp:216-243. */
+static void weno_recon(const orc_state *s, int chr, const double *L, const double *IL, const int *ix, int lr,
+                       double *U) {
+  double v[5][4];
+  for (int k = 0; k < 5; k++) weno_cons(s, ix[k], v[k]);
+  if (chr) {
+    double w[5][4], W[4];
+    for (int k = 0; k < 5; k++) weno_matvec(L, v[k], w[k]);
+    for (int i = 0; i < 4; i++) W[i] = weno5(w[0][i], w[1][i], w[2][i], w[3][i], w[4][i], lr);
+    weno_matvec(IL, W, U);
+  } else {
+    for (int i = 0; i < 4; i++) U[i] = weno5(v[0][i], v[1][i], v[2][i], v[3][i], v[4][i], lr);
+  }
+}
+
+/* Calculate_Face_WENO_Flux, src/WENO2D.cpp:458-562; F = Average - Dissipative. */
+static void weno_face_flux(orc_state *s, int c, int N, const double *UL, const double *UR, double nx, double ny,
+                           double dl, double *F) {
+  double GL[11], GR[11];
+  eos(s, c, UL, GL);
+  eos(s, N, UR, GR);
+  double Rho_L = GL[0], P_L = GL[4], u_L = GL[1], v_L = GL[2], C_L = GL[5];
+  double Rho_R = GR[0], P_R = GR[4], u_R = GR[1], v_R = GR[2], C_R = GR[5];
+  double Vdotn_L = (u_L * nx + v_L * ny), Vdotn_R = (u_R * nx + v_R * ny);
+  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L), Vmag_R = 0.5 * (u_R * u_R + v_R * v_R);
+  double FL[4], FR[4];
+  FL[0] = Rho_L * Vdotn_L * dl;
+  FL[1] = Rho_L * u_L * Vdotn_L * dl + P_L * nx * dl;
+  FL[2] = Rho_L * v_L * Vdotn_L * dl + P_L * ny * dl;
+  FL[3] = (G1 * P_L + Rho_L * Vmag_L) * Vdotn_L * dl;
+  FR[0] = Rho_R * Vdotn_R * dl;
+  FR[1] = Rho_R * u_R * Vdotn_R * dl + P_R * nx * dl;
+  FR[2] = Rho_R * v_R * Vdotn_R * dl + P_R * ny * dl;
+  FR[3] = (G1 * P_R + Rho_R * Vmag_R) * Vdotn_R * dl;
+  if (C_L < 1e-14) C_L = 1e-14;
+  if (C_R < 1e-14) C_R = 1e-14;
+  double S0 = fabs(Vdotn_L - C_L) * dl, S1 = fabs(Vdotn_L + C_L) * dl, S2 = fabs(Vdotn_L) * dl;
+  double S3 = fabs(Vdotn_R - C_R) * dl, S4 = fabs(Vdotn_R + C_R) * dl, S5 = fabs(Vdotn_R) * dl;
+  double mx = max3(S0, S1, S2), m2 = max3(S3, S4, S5);
+  if (!(mx >= m2)) mx = m2;
+  for (int i = 0; i < 4; i++) F[i] = 0.5 * (FL[i] + FR[i]) - 0.5 * mx * (UR[i] - UL[i]);
+}
+
+/* Evaluate_Cell_Net_Flux_WENO, src/WENO2D.cpp:395-456 with the stencils of
+ * WENO_Reconstruction_X (:245-393). */
+static void weno_net_flux(orc_state *s, int c, double *net) {
+  const int NP = s->NP, *nb = s->nbr + 4 * c;
+  for (int k = 0; k < 4; k++) net[k] = 0.0;
+  if (s->nf[c] != 4) return;
+  int im1 = nb[0], ip1 = nb[1], jm1 = nb[2], jp1 = nb[3], im2, im3, ip2, ip3, jm2, jm3, jp2, jp3;
+  if (im1 >= NP) { im2 = im1; im3 = im1; }
+  else {
+    im2 = s->nbr[4 * im1 + 0];
+    if (im2 >= NP || im2 < 0) im3 = im2;
+    else { im3 = s->nbr[4 * im2 + 0]; if (im3 < 0) im3 = im2; }
+  }
+  if (ip1 >= NP) { ip2 = ip1; ip3 = ip1; }
+  else {
+    ip2 = s->nbr[4 * ip1 + 1];
+    if (ip2 >= NP || ip2 < 0) ip3 = ip2;
+    else { ip3 = s->nbr[4 * ip2 + 1]; if (ip3 < 0) ip3 = ip2; }
+  }
+  if (jm1 >= NP) { jm2 = jm1; jm3 = jm1; }
+  else { jm2 = s->nbr[4 * jm1 + 2]; jm3 = (jm2 >= NP) ? jm2 : s->nbr[4 * jm2 + 2]; }
+  if (jp1 >= NP) { jp2 = jp1; jp3 = jp1; }
+  else { jp2 = s->nbr[4 * jp1 + 3]; jp3 = (jp2 >= NP) ? jp2 : s->nbr[4 * jp2 + 3]; }
+  const int st[4][2][5] = {{{im3, im2, im1, c, ip1}, {im2, im1, c, ip1, ip2}},
+                           {{jm3, jm2, jm1, c, jp1}, {jm2, jm1, c, jp1, jp2}},
+                           {{im2, im1, c, ip1, ip2}, {im1, c, ip1, ip2, ip3}},
+                           {{jm2, jm1, c, jp1, jp2}, {jm1, c, jp1, jp2, jp3}}};
+  const int N4[4] = {im1, ip1, jm1, jp1};
+  for (int f = 0; f < 4; f++) {
+    double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+    double L[16], IL[16], UL[4], UR[4], F[4];
+    if (s->c.weno_char) weno_lr(s->P + 11 * (size_t)c, s->P + 11 * (size_t)N4[f], nx, ny, L, IL);
+    weno_recon(s, s->c.weno_char, L, IL, st[f][0], 0, UL);
+    weno_recon(s, s->c.weno_char, L, IL, st[f][1], 1, UR);
+    weno_face_flux(s, c, N4[f], UL, UR, nx, ny, dl, F);
+    for (int k = 0; k < 4; k++) net[k] += F[k];
+  }
+}
+
 /* Evaluate_Cell_Net_Flux_1O/2O + Calculate_Flux_For_All_Faces, src/Net_Flux.cpp:7-129;
  * Inviscid_Time_Step, src/Time_Step.cpp:293-329. */
 void orc_net_flux(orc_state *s) {
   const double *Ur = uread(s);
-  const int gmuscl = s->c.muscl && s->c.is_second_order;
+  int all_quads = 1;
+  for (int c = 0; c < s->NP; c++) all_quads = all_quads && s->nf[c] == 4;
+  /* Explicit_Method falls back to the 1O/2O residual on meshes with non-quad cells
+   * (src/Numerical_Method.cpp:31-55); Runge_Kutta_Method does not. */
+  const int weno = s->c.weno && (all_quads || s->c.time_accurate || s->c.integrator != 0);
+  const int gmuscl = s->c.muscl && s->c.is_second_order && !weno;
   if (gmuscl) {
     muscl_gradients(s);
     muscl_net_flux(s);
   }
   for (int c = 0; c < s->NP; c++) {
     double net[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int f = 0; f < s->nf[c] && !gmuscl; f++) {
+    if (weno) weno_net_flux(s, c, net);
+    for (int f = 0; f < s->nf[c] && !gmuscl && !weno; f++) {
       int N = s->nbr[4 * c + f];
       if (N < 0) continue;
       double A[4], D[4];

@@ -20,6 +20,7 @@ typedef struct {
   int dissipation_type, is_second_order, time_accurate, local_time_stepping, integrator, limiter,
       reconstruct_primitive, muscl, precision, inlet_bc, exit_bc;
   double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas, inlet_u, inlet_v;
+  int weno, weno_char;
 } orc_config;
 
 typedef struct orc_state orc_state;

@@ -31,6 +31,7 @@
 #include "Initialize.h"
 #include "Primitive_Computational.h"
 #include "Gradients.h"
+#include "Weno.h"
 
 #include <unistd.h>
 #include <fcntl.h>
@@ -45,7 +46,10 @@ extern "C" void b200_shim_reset() __attribute__((weak));
 
 namespace {
 int g_saved_stdout = -1;
+// The reference prints per-call diagnostics on stdout; they are discarded unless REFH_VERBOSE is
+// set in the environment.
 void quiet_begin() {
+  if (getenv("REFH_VERBOSE")) return;
   fflush(stdout);
   std::cout.flush();
   g_saved_stdout = dup(1);
@@ -98,6 +102,7 @@ void refh_reset() {
   NUM_FLUX_COMPONENTS = 4;
   Is_Viscous_Wall = false;
   Is_WENO = false;
+  Is_Char = false;
   Is_Implicit_Method = false;
   Non_Dimensional_Form = false;
   Is_Inlet_SubSonic = false;
@@ -198,6 +203,8 @@ int refh_set_param(const char *name, double v) {
   else if (n == "Inlet_P") inletCond.P = v;
   else if (n == "Inlet_u") inletCond.u = v;
   else if (n == "Inlet_v") inletCond.v = v;
+  else if (n == "Is_WENO") Is_WENO = v != 0.0;
+  else if (n == "Is_Char") Is_Char = v != 0.0;
   else if (n == "Enable_AMR") Enable_AMR = v != 0.0;
   else if (n == "AMR_Period") AMR_Period = (int)v;
   else if (n == "AMR_Gradient_Threshold") AMR_Gradient_Threshold = v;
@@ -257,9 +264,14 @@ int refh_iterations() { return iterations; }
 
 // Individual entry points of the path.
 void refh_apply_bc() { Apply_Boundary_Conditions(); }
+// The residual the configured method evaluates: WENO when Is_WENO (Runge_Kutta_Method always;
+// Explicit_Method only on all-quad meshes, src/Numerical_Method.cpp:31-55), else 1O / 2O.
 void refh_net_flux() {
   quiet_begin();
-  if (Is_Second_Order) Evaluate_Cell_Net_Flux_2O();
+  bool all_quads = true;
+  for (int c = 0; c < No_Physical_Cells; c++) all_quads = all_quads && Cells[c].numFaces == 4;
+  if (Is_WENO && (Time_Accurate || all_quads)) Evaluate_Cell_Net_Flux_WENO();
+  else if (Is_Second_Order) Evaluate_Cell_Net_Flux_2O();
   else Evaluate_Cell_Net_Flux_1O();
   quiet_end();
 }

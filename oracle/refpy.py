@@ -276,7 +276,8 @@ class _OrcConfig(ctypes.Structure):
                                             "local_time_stepping", "integrator", "limiter", "reconstruct_primitive",
                                             "muscl", "precision", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
-                                               "exit_p", "r_gas", "inlet_u", "inlet_v"]]
+                                               "exit_p", "r_gas", "inlet_u", "inlet_v"]] + \
+               [(n, ctypes.c_int) for n in ["weno", "weno_char"]]
 
 
 _orc = None
@@ -339,6 +340,8 @@ class OracleRun:
         c.r_gas = params.get("r_gas", 287.0)
         c.inlet_u = params.get("inlet_u", 0.0)
         c.inlet_v = params.get("inlet_v", 0.0)
+        c.weno = params.get("weno", 0)
+        c.weno_char = params.get("weno_characteristic", 0)
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,

@@ -34,6 +34,20 @@ CASES = {
     "bump_roe2_rk3": dict(mesh=("bump", 40, 16, 3.0, 1.0, 0.1, 3, 0.3, 11, 1), ic="freestream", mach=1.6,
                           dissipation_type=3, is_second_order=1, time_accurate=1, cfl=0.5, inlet_rho=1.0,
                           inlet_p=1.0 / GAMMA, steps=30, amr=(0.1, 0.2)),
+    # WENO path (src/WENO2D.cpp): component-wise on Sod with RK3, characteristic (Is_Char) on the
+    # O-grid with local dt, and the explicit method on the mixed bump, where the reference falls
+    # back to the 1O/2O residual because the mesh has triangles.
+    "sod_weno_rk3": dict(mesh=("box", 100, 4, 0.0, 1.0, 0.0, 0.01), ic="sod", dissipation_type=3, is_second_order=0,
+                         time_accurate=1, cfl=0.4, inlet_rho=1.0, inlet_p=1.0, steps=6, weno=1),
+    "pulse_weno_rk3": dict(mesh=("box", 40, 20, 0.0, 2.0, 0.0, 1.0), ic="pulse", mach=1.5, dissipation_type=3,
+                           is_second_order=0, time_accurate=1, cfl=0.4, inlet_rho=1.0, inlet_p=1.0 / GAMMA, steps=18,
+                           weno=1),
+    "sod_weno_char_rk3": dict(mesh=("box", 100, 4, 0.0, 1.0, 0.0, 0.01), ic="sod", dissipation_type=3,
+                              is_second_order=0, time_accurate=1, local_time_stepping=1, cfl=0.4, inlet_rho=1.0,
+                              inlet_p=1.0, steps=10, weno=1, weno_characteristic=1),
+    "bump_weno_explicit_fallback": dict(mesh=("bump", 40, 16, 3.0, 1.0, 0.1, 3, 0.3, 11, 1), ic="freestream",
+                                        mach=1.6, dissipation_type=3, is_second_order=1, time_accurate=0, cfl=0.4,
+                                        inlet_rho=1.0, inlet_p=1.0 / GAMMA, steps=20, weno=1),
     # Reference subsonic inlet (energy form of src/Inlet_Boundary_Conditions.cpp:32) and the
     # empty subsonic exit, LLF.
     "bump_llf1_subsonic": dict(mesh=("bump", 30, 12, 3.0, 1.0, 0.05, 2, 0.2, 5, 0), ic="freestream", mach=0.5,
@@ -64,6 +78,13 @@ def initial_state(case, mesh):
     if case["ic"] == "sod":
         left = xc < 0.5
         U = cb.conserved_from_primitive(np.where(left, 1.0, 0.125), 0 * xc, 0 * xc, np.where(left, 1.0, 0.1))
+    elif case["ic"] == "pulse":
+        # Uniform stream at the inlet state with a smooth density pulse at uniform pressure.
+        rho0, p = case["inlet_rho"], case["inlet_p"]
+        u = case["mach"] * np.sqrt(GAMMA * p / rho0)
+        yc = mesh.centers[:NP, 1]
+        rho = rho0 + 0.2 * np.exp(-((xc - 0.6) ** 2 + (yc - 0.5) ** 2) / 0.02)
+        U = cb.conserved_from_primitive(rho, np.full(NP, u), np.zeros(NP), np.full(NP, p))
     else:
         rho, p = case["inlet_rho"], case["inlet_p"]
         a = np.sqrt(GAMMA * p / rho)
@@ -81,7 +102,8 @@ def solver_config(case, **over):
               time_accurate=case["time_accurate"], local_time_stepping=case.get("local_time_stepping", 0),
               cfl=case["cfl"], limiter_zeta=case.get("limiter_zeta", 0.5), limiter_zeta1=case.get("limiter_zeta1", 0.5),
               inlet_rho=case["inlet_rho"], inlet_p=case["inlet_p"], inlet_bc=case.get("inlet_bc", 0),
-              exit_bc=case.get("exit_bc", 0))
+              exit_bc=case.get("exit_bc", 0), weno=case.get("weno", 0),
+              weno_characteristic=case.get("weno_characteristic", 0))
     kw.update(over)
     return cb.default_config(**kw)
 
@@ -91,7 +113,8 @@ def oracle_params(case, **over):
               time_accurate=case["time_accurate"], local_time_stepping=case.get("local_time_stepping", 0),
               cfl=case["cfl"], limiter_zeta=case.get("limiter_zeta", 0.5), limiter_zeta1=case.get("limiter_zeta1", 0.5),
               inlet_rho=case["inlet_rho"], inlet_p=case["inlet_p"], inlet_bc=case.get("inlet_bc", 0),
-              exit_bc=case.get("exit_bc", 0))
+              exit_bc=case.get("exit_bc", 0), weno=case.get("weno", 0),
+              weno_characteristic=case.get("weno_characteristic", 0))
     kw.update(over)
     return kw
 
@@ -103,5 +126,6 @@ def ref_params(case):
          "Limiter_Zeta": case.get("limiter_zeta", 0.5), "Limiter_Zeta1": case.get("limiter_zeta1", 0.5),
          "Inlet_Rho": case["inlet_rho"], "Inlet_P": case["inlet_p"],
          "Is_Inlet_SubSonic": 1 if case.get("inlet_bc", 0) == 1 else 0,
-         "Is_Exit_SubSonic": 1 if case.get("exit_bc", 0) == 1 else 0}
+         "Is_Exit_SubSonic": 1 if case.get("exit_bc", 0) == 1 else 0,
+         "Is_WENO": case.get("weno", 0), "Is_Char": case.get("weno_characteristic", 0)}
     return p
