@@ -112,6 +112,10 @@ SIGNATURES = {
     "cfd_download_U": (_I, [_P, _DP]),
     "cfd_gradient": (_I, [_P, _I, _DP]),
     "cfd_eval_limiter": (_I, [_I, _DP, _DP, _I, _DP, _I]),
+    "cfd_write_solution": (_I, [_P, ctypes.c_char_p, ctypes.POINTER(_I), _I]),
+    "cfd_read_solution": (_I, [_P, ctypes.c_char_p, _I]),
+    "cfd_vtk_copy_grid": (_I, [ctypes.c_char_p, ctypes.c_char_p]),
+    "cfd_vtk_append_solution": (_I, [ctypes.c_char_p, ctypes.c_char_p, _I]),
     "cfd_eval_face_flux": (_I, [_I, _I, _DP, _DP, _DP, _DP, _I, _DP, _I]),
     "cfd_amr_tags": (_I, [_P, _D, _D, _DP, ctypes.POINTER(ctypes.c_uint8)]),
     "cfd_kernel_time": (_I, [_P, ctypes.c_char_p, _DP, ctypes.POINTER(ctypes.c_longlong)]),
@@ -338,6 +342,15 @@ class Solver:
         _check(lib().cfd_sync(self._h, ctypes.byref(self.info)))
         return self.info
 
+    def write_solution(self, path, header=(0, 0, 0)):
+        """Solution file in the reference's Write_Solution format (cfd_write_solution)."""
+        h = (ctypes.c_int * len(header))(*header)
+        _check(lib().cfd_write_solution(self._h, str(path).encode(), h, len(header)))
+
+    def read_solution(self, path, n_header=3):
+        """Restart from a solution file (cfd_read_solution)."""
+        _check(lib().cfd_read_solution(self._h, str(path).encode(), n_header))
+
     def autotune(self, steps=20):
         """Picks the fastest bit-identical launch options on this mesh (cfd_autotune); returns
         the per-candidate report."""
@@ -456,6 +469,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def vtk_copy_grid(grid_vtk, out_vtk):
+    """The grid part of a VTK file, copied as the reference's Read_Write_Grid does."""
+    _check(lib().cfd_vtk_copy_grid(str(grid_vtk).encode(), str(out_vtk).encode()))
+
+
+def vtk_append_solution(solution_txt, out_vtk, n_header=3):
+    """Cell data of a solution file appended to a VTK file (the reference's Append_Solution)."""
+    _check(lib().cfd_vtk_append_solution(str(solution_txt).encode(), str(out_vtk).encode(), n_header))
 
 
 def eval_limiter(limiter, a, b, device=0):

@@ -908,6 +908,71 @@ cfd_status cfd_update(cfd_ctx *ctx) {
   return sync_status(ctx, nullptr);
 }
 
+// Write_Solution type 1 (src/output_files.cpp:492-556): the header integers, No_Physical_Cells,
+// iterations, then per cell its id, del_t, rho, p, T, u, v, M and p0 with the reference's stream
+// formatting (default precision, its separators) in reference cell order.
+cfd_status cfd_write_solution(cfd_ctx *ctx, const char *path, const int *header, int n_header) {
+  if (!ctx || !path || n_header < 0 || (n_header > 0 && !header)) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  const int NP = ctx->NP, NT = ctx->NT;
+  std::vector<double> P(11 * (size_t)NT), dt(NP);
+  cfd_status s = cfd_download(ctx, nullptr, P.data(), dt.data(), nullptr, nullptr);
+  if (s != CFD_OK) return s;
+  if ((s = sync_status(ctx, nullptr)) != CFD_OK) return s;
+  std::ofstream out(path);
+  if (!out.is_open()) return fail(CFD_ERR_IO, std::string("cannot write ") + path);
+  for (int k = 0; k < n_header; k++) out << header[k] << (k + 1 < n_header ? "\t" : "");
+  out << std::endl;
+  out << NP << std::endl;
+  out << static_cast<int>(ctx->h_ctl[CTL_ITER]) << std::endl;
+  for (int c = 0; c < NP; c++) {
+    const double *q = P.data() + 11 * (size_t)c;
+    out << c << "\t\t" << dt[c] << "\t" << q[0] << "\t" << q[4] << "\t" << q[3] << "\t\t\t\t" << q[1] << "\t\t\t\t"
+        << q[2] << "\t\t\t\t" << q[7] << "\t\t\t\t" << q[10] << std::endl;
+  }
+  if (!out.good()) return fail(CFD_ERR_IO, std::string("write failed: ") + path);
+  return CFD_OK;
+}
+
+// Initialize(const string &), src/Initialize.cpp:125-176: the state of the physical cells from a
+// solution file (rho, p, u, v of each row; U = (rho, rho u, rho v, p/(gamma-1) + rho |V|^2/2) as
+// Calculate_Computational_Variables(P, V, Rho, 2) forms it) and the iteration count; ghost rows
+// keep the context's current values.  A cell-count mismatch changes nothing (the reference
+// reports it and carries on) and returns CFD_ERR_MESH.
+cfd_status cfd_read_solution(cfd_ctx *ctx, const char *path, int n_header) {
+  if (!ctx || !path || n_header < 0) return fail(CFD_ERR_BAD_ARG, "bad argument");
+  std::ifstream in(path);
+  if (!in.is_open()) return fail(CFD_ERR_IO, std::string("cannot open ") + path);
+  const int NP = ctx->NP, NT = ctx->NT;
+  for (int k = 0; k < n_header; k++) {
+    int h;
+    in >> h;
+  }
+  int n_cells = -1, iters = 0;
+  in >> n_cells >> iters;
+  if (!in.good()) return fail(CFD_ERR_IO, std::string("bad solution file header: ") + path);
+  if (n_cells != NP) return fail(CFD_ERR_MESH, "solution file has " + std::to_string(n_cells) + " cells, mesh " +
+                                                   std::to_string(NP));
+  std::vector<double> U(4 * (size_t)NT);
+  cfd_status s = cfd_download_U(ctx, U.data());
+  if (s != CFD_OK) return s;
+  for (int c = 0; c < NP; c++) {
+    int idx;
+    double dtc, Rho, P, T, v1, v2, M, P0;
+    in >> idx >> dtc >> Rho >> P >> T >> v1 >> v2 >> M >> P0;
+    if (in.fail()) return fail(CFD_ERR_IO, "bad solution row " + std::to_string(c));
+    const double vmag = 0.5 * (v1 * v1 + v2 * v2);
+    double *u = U.data() + 4 * (size_t)c;
+    u[0] = Rho;
+    u[1] = Rho * v1;
+    u[2] = Rho * v2;
+    u[3] = ((P / kGM1) + Rho * vmag);
+  }
+  if ((s = cfd_upload_state(ctx, U.data(), NT)) != CFD_OK) return s;
+  ctx->launches += launch_set_ctl(ctx->stream, ctx->ds, CTL_ITER, static_cast<double>(iters));
+  CUDA_TRY(cudaGetLastError());
+  return sync_status(ctx, nullptr);
+}
+
 cfd_status cfd_get_min_dt(cfd_ctx *ctx, double *min_dt) {
   if (!ctx || !min_dt) return fail(CFD_ERR_BAD_ARG, "null argument");
   cfd_status s = sync_status(ctx, nullptr);

@@ -225,6 +225,23 @@ cfd_status cfd_gradient(cfd_ctx *ctx, int var, double *grad);
  * src/Grid_Refine_Functions.cpp:8-63).  Either output may be NULL. */
 cfd_status cfd_amr_tags(cfd_ctx *ctx, double threshold, double max_fraction, double *indicator, uint8_t *tags);
 
+/* ------------------------------------------------------------------------------------------
+ * Solution files in the reference's formats.
+ * cfd_write_solution: Write_Solution type 1 (src/output_files.cpp:492-556): the header integers
+ *   (the reference writes nx_c ny_c nz_c for Grid_Type 0), No_Physical_Cells, iterations, then
+ *   one row per cell: id, del_t, rho, p, T, u, v, M, p0 (default stream precision).
+ * cfd_read_solution: the restart Initialize(const string &) (src/Initialize.cpp:125-176): physical
+ *   cells' U from the rows' rho, p, u, v, and the iteration count; n_header integers are skipped.
+ * cfd_vtk_copy_grid / cfd_vtk_append_solution: Read_Write_Grid and Append_Solution
+ *   (src/Create_Vtk_File.cpp:5-157): the grid of a VTK file copied, then the cell data of a
+ *   solution file appended (pressure, temperature, density, velocities, total pressure, entropy,
+ *   Mach number, velocity vectors).  Host only.
+ * ------------------------------------------------------------------------------------------ */
+cfd_status cfd_write_solution(cfd_ctx *ctx, const char *path, const int *header, int n_header);
+cfd_status cfd_read_solution(cfd_ctx *ctx, const char *path, int n_header);
+cfd_status cfd_vtk_copy_grid(const char *grid_vtk, const char *out_vtk);
+cfd_status cfd_vtk_append_solution(const char *solution_txt, const char *out_vtk, int n_header);
+
 /* Pointwise evaluation of the face functions on host arrays (runs on `device`): the limiter
  * phi(a, b) of CFD_LIM_MINMOD..CFD_LIM_VANALBADA for n pairs (the phi(r) family of
  * CUDA_KERNELS/Limiter_Cuda_Kernels.cu:89-154: r = a/b, phi = 0 when |b| < 1e-12 or r <= 0), and

@@ -32,6 +32,7 @@
 #include "Primitive_Computational.h"
 #include "Gradients.h"
 #include "Weno.h"
+#include "IO_Write.h"
 
 #include <unistd.h>
 #include <fcntl.h>
@@ -280,6 +281,17 @@ void refh_explicit() { quiet_begin(); Explicit_Method(); quiet_end(); }
 void refh_rk3() { quiet_begin(); Runge_Kutta_Method(); quiet_end(); }
 void refh_estimate_error() { Estimate_Error(); }
 void refh_update() { Update(); }
+// The reference's solution writers (src/output_files.cpp:492-556, src/Create_Vtk_File.cpp).
+void refh_write_solution(const char *path) {
+  Grid_Type = 0;
+  nx_c = ny_c = nz_c = 0;
+  Write_Solution(string(path), 1);
+}
+void refh_read_write_grid(const char *grid, const char *out) { Read_Write_Grid(string(grid), string(out)); }
+void refh_append_solution(const char *sol, const char *out) {
+  Grid_Type = 0;
+  Append_Solution(string(sol), string(out));
+}
 void refh_ausm_net_flux() {
   for (int c = 0; c < No_Physical_Cells; c++) Ausm_Flux(c);
 }

@@ -171,6 +171,11 @@ def reflib(path=REF_LIB):
         L.refh_iterate.restype = ctypes.c_int
         L.refh_gradient.argtypes = [ctypes.c_int, _DP]
         L.refh_amr.argtypes = [ctypes.c_double, ctypes.c_double, _DP, ctypes.POINTER(ctypes.c_uint8)]
+        L.refh_write_solution.argtypes = [ctypes.c_char_p]
+        L.refh_read_write_grid.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.refh_append_solution.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        for n in ("refh_write_solution", "refh_read_write_grid", "refh_append_solution"):
+            getattr(L, n).restype = None
         _ref[path] = L
     return _ref[path]
 
