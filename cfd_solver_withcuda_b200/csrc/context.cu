@@ -751,6 +751,7 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
     if (value != 0.0 && value != 1.0 && value != 2.0) return fail(CFD_ERR_BAD_ARG, "faces_shape must be 0, 1 or 2");
     ctx->fp.faces_shape = static_cast<int>(value);
   }
+  else if (n == "pdl") ctx->dm.pdl = value != 0.0;
   else if (n == "profile") ctx->profile = value != 0.0;
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
@@ -1126,15 +1127,16 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     }
   };
   struct Cand {
-    int faces_shape, fuse, lanes;
+    int faces_shape, fuse, lanes, pdl;
     double ms;
   };
   std::vector<Cand> cands;
   if (ctx->dm.NF > 0) {
     for (int f = 0; f < 3; f++)
-      for (int g = 0; g < 2; g++) cands.push_back({f, g, ctx->fp.lanes, 0.0});
+      for (int g = 0; g < 2; g++)
+        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0.0});
   } else {
-    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, 0.0});
+    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, ctx->dm.pdl, 0.0});
   }
   const int prof = ctx->profile, graph_on = ctx->use_graph;
   ctx->profile = 0;
@@ -1148,6 +1150,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     ctx->fp.faces_shape = cd.faces_shape;
     ctx->fuse_gather = cd.fuse;
     ctx->fp.lanes = cd.lanes;
+    ctx->dm.pdl = cd.pdl;
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
       ctx->graph = nullptr;
@@ -1182,12 +1185,13 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   ctx->fp.faces_shape = best->faces_shape;
   ctx->fuse_gather = best->fuse;
   ctx->fp.lanes = best->lanes;
+  ctx->dm.pdl = best->pdl;
   if (report && report_len > 0) {
     std::string r;
     char line[160];
     for (const Cand &cd : cands) {
-      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d: %.4f ms/step%s\n", cd.faces_shape,
-               cd.fuse, cd.lanes, cd.ms, &cd == best ? " (chosen)" : "");
+      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d: %.4f ms/step%s\n",
+               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.ms, &cd == best ? " (chosen)" : "");
       r += line;
     }
     snprintf(report, report_len, "%s", r.c_str());

@@ -21,6 +21,35 @@ constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ bool step_done(const double *ctl) { return ctl[CTL_DONE] != 0.0; }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
+// start while its predecessor grid drains; it allows its own dependents to launch at entry and
+// waits for the predecessor's completion (and memory) before its first global access.  Both are
+// no-ops for a normal launch.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launches kernel k, with programmatic stream serialization when m.pdl is set.
+template <typename... KArgs, typename... Args>
+void launch_k(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+  if (!m.pdl) {
+    k<<<grid, block, 0, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Item handled by this thread: from the block's work-list range when a list is given (n when the
 // thread is past the range's end), else the plain global index.
 __device__ __forceinline__ int item_index(const int2 *blk, int n) {
@@ -382,6 +411,7 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
 }
 
 __global__ void k_bc(DevMesh m, DevState st, BcParams bp, int src_is_S, int cur_is_S) {
+  pdl_enter();
   const int e = item_index(m.bblk, m.NB);
   if (e >= m.NB || step_done(st.ctl)) return;
   bc_entry(m, st, bp, e, src_is_S, cur_is_S);
@@ -762,6 +792,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, Flu
 // face states plus Roe dissipation between them.
 template <typename T, int DISS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
+  pdl_enter();
   const int i = item_index(m.fblk, m.NF);
   if (i >= m.NF || step_done(st.ctl)) return;
   const int NP = m.NP;
@@ -1103,6 +1134,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
 __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
                                                              int kind, int lts, int fuse_final, int keep_delu,
                                                              int flags) {
+  pdl_enter();
   const int NP = m.NP;
   const int c = item_index(m.cblk, NP);
   if (step_done(st.ctl)) return;
@@ -1221,6 +1253,7 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // the last stage's reduction).
 template <bool DT>
 __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevState st, FluxParams fp) {
+  pdl_enter();
   const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
   if (step_done(st.ctl)) return;
@@ -1456,9 +1489,9 @@ int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp
   if (m.NB == 0) return 0;
   if (m.bblk) {
     if (m.n_bblk == 0) return 0;
-    k_bc<<<m.n_bblk, kWorkItemBlock, 0, s>>>(m, st, bp, src_is_S, cur_is_S);
+    launch_k(m, k_bc, m.n_bblk, kWorkItemBlock, s, m, st, bp, src_is_S, cur_is_S);
   } else {
-    k_bc<<<nblk(m.NB, kBlock), kBlock, 0, s>>>(m, st, bp, src_is_S, cur_is_S);
+    launch_k(m, k_bc, nblk(m.NB, kBlock), kBlock, s, m, st, bp, src_is_S, cur_is_S);
   }
   return 1;
 }
@@ -1519,10 +1552,10 @@ int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxPara
 
 template <typename T, int MINB>
 void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  if (fp.dissipation == 6) k_faces<T, 6, MINB><<<g, b, 0, s>>>(m, st, fp);
-  else if (fp.dissipation == 7) k_faces<T, 7, MINB><<<g, b, 0, s>>>(m, st, fp);
-  else if (fp.dissipation == 8) k_faces<T, 8, MINB><<<g, b, 0, s>>>(m, st, fp);
-  else k_faces<T, 3, MINB><<<g, b, 0, s>>>(m, st, fp);
+  if (fp.dissipation == 6) launch_k(m, k_faces<T, 6, MINB>, g, b, s, m, st, fp);
+  else if (fp.dissipation == 7) launch_k(m, k_faces<T, 7, MINB>, g, b, s, m, st, fp);
+  else if (fp.dissipation == 8) launch_k(m, k_faces<T, 8, MINB>, g, b, s, m, st, fp);
+  else launch_k(m, k_faces<T, 3, MINB>, g, b, s, m, st, fp);
 }
 
 // Launch shapes of the face kernel (identical results).  The double Roe kernel needs 86
@@ -1546,7 +1579,7 @@ int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParam
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                         int kind, int lts, int fuse_final, int keep_delu, int flags) {
   const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
-  k_gather_stage<<<g, kFluxBlock, 0, s>>>(m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  launch_k(m, k_gather_stage, g, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
   return 1;
 }
 
@@ -1582,8 +1615,8 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
 int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt) {
   const int g = m.rblk ? m.n_rblk : nblk(m.NT, kBlock);
   if (m.rblk && g == 0) return 0;
-  if (with_dt) k_muscl_gradients<true><<<g, kBlock, 0, s>>>(m, st, fp);
-  else k_muscl_gradients<false><<<g, kBlock, 0, s>>>(m, st, fp);
+  if (with_dt) launch_k(m, k_muscl_gradients<true>, g, kBlock, s, m, st, fp);
+  else launch_k(m, k_muscl_gradients<false>, g, kBlock, s, m, st, fp);
   return 1;
 }
 

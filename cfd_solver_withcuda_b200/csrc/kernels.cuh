@@ -36,6 +36,9 @@ struct DevMesh {
   // ghost rows); null = all items.
   const int2 *cblk, *fblk, *bblk, *rblk;
   int n_cblk, n_fblk, n_bblk, n_rblk;
+  // Launch policy: 1 = the kernels of a pseudo-step are launched with programmatic stream
+  // serialization (each waits on its predecessor grid before touching memory).
+  int pdl;
   // Per boundary entry (batched solves), or null: inlet values read by the inlet kind
   // (CFD_INLET_FIXED and CFD_INLET_FARFIELD: rho, u, v, p; CFD_INLET_TOTAL_PT: p0, T0) and the
   // exit pressure (CFD_EXIT_STATIC_P, CFD_EXIT_FIXED_P_REF).

@@ -187,7 +187,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "profile" (time every launch with CUDA events; disables graph replay, default 0),
  * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
  * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0/1/2, default 2),
- * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1).
+ * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1),
+ * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0).
  * None of the options changes a result bit. */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
 /* Times every combination of the options above that applies to this configuration over `steps`
