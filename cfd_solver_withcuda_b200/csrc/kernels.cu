@@ -3,8 +3,8 @@
 // One thread per physical cell gathers its own faces in the reference's face order 0..nF-1,
 // so every per-cell sum is formed in the same order as the reference's serial loop and the
 // result is deterministic and bit-identical; there are no atomics on data.  Reductions (min dt,
-// residual norms) use a fixed-shape warp-shuffle tree per block and a last-block pass over the
-// per-block partials in block order.
+// residual and error norms) use a fixed-shape warp-shuffle tree per block and a fixed-order pass
+// over the per-block partials (a last-block pass, or the two-level group pass of the last stage).
 #include <climits>
 
 #include "kernels.cuh"

@@ -1,12 +1,14 @@
 // Device data layout and kernel declarations of the residual/update path.
 //
-// HBM layout (all arrays in device cell order; physical cells 0..NP-1 possibly RCM-renumbered,
-// ghost cells NP..NT-1 in the reference's ghost order):
-//   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l
-//   per cell [NP]: nf, area, inv_area, degenerate-face mask
+// HBM layout (all arrays in device cell order; physical cells 0..NP-1 possibly renumbered (RCM or
+// patches), ghost cells NP..NT-1 in the reference's ghost order):
+//   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l; centre vectors
+//   per cell [NP]: nf, area, inv_area, degenerate-face mask; boundary entries per cell (CSR)
+//   unique faces [NF] (face-based forms): owner, neighbour, owner-side geometry; cell slot -> face
 //   state, component-major SoA: U[4][NT] (U^n on physical rows, boundary values on ghost rows),
 //   S[4][NP] (RK stage state), prim[5][NT] (rho, u, v, p, a), R[4][NP] (net flux),
-//   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU)
+//   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU); records rec[NT][12] and face fluxes F[NF]
+//   (face-based forms)
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
