@@ -446,6 +446,8 @@ def main():
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--vl-steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--launch-options", default="auto",
+                    help="'auto' (the library's autotuner picks) or e.g. 'faces_shape=1,fuse_gather=1,pdl=1'")
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--max-steps", type=int, default=20000)
     ap.add_argument("--check-every", type=int, default=100)
@@ -485,8 +487,14 @@ def main():
 
     # Launch options (all bit-identical) chosen by the library's autotuner on this mesh; the
     # state is restored afterwards.  Then warm-up (graph capture on the first multi-step call).
-    tune_report = s.autotune(steps=20)
-    tuned = [l.split(":")[0] for l in tune_report.splitlines() if "(chosen)" in l]
+    if args.launch_options == "auto":
+        tune_report = s.autotune(steps=20)
+        tuned = [l.split(":")[0] for l in tune_report.splitlines() if "(chosen)" in l]
+    else:
+        pinned = [kv.split("=") for kv in args.launch_options.split(",") if kv]
+        for k, v in pinned:
+            s.set_option(k.strip(), float(v))
+        tuned = [" ".join(f"{k.strip()}={v.strip()}" for k, v in pinned) + " (pinned)"]
     s.step_async(max(args.warmup, 3))
     s.sync()
     barrier()

@@ -850,8 +850,9 @@ __global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, Flu
 }
 
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
-// side) and the del_t denominator.  The four slots are unrolled and predicated, so every face's
-// id and flux loads are in flight together.
+// side) and the del_t denominator.  All four slots of the [4][NP] face table are loaded without
+// waiting for the face count (an unused slot holds face 0), so the id loads and then the flux
+// loads of every face are in flight together; only the sums are predicated on the count.
 template <bool DEN = true>
 __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &st, int c, double R[4], double &den) {
   const int NP = m.NP, NT = m.NT;
@@ -860,12 +861,12 @@ __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &s
   const int nf = m.nf[c];
   int e[4];
 #pragma unroll
-  for (int f = 0; f < 4; f++) e[f] = (f < nf) ? m.cface[f * NP + c] : 0;
+  for (int f = 0; f < 4; f++) e[f] = m.cface[f * NP + c];
   double4 F[4];
 #pragma unroll
   for (int f = 0; f < 4; f++) {
     const int id = e[f] < 0 ? -e[f] - 1 : e[f];
-    F[f] = (f < nf) ? st.F[id] : make_double4(0.0, 0.0, 0.0, 0.0);
+    F[f] = st.F[id];
   }
   R[0] = R[1] = R[2] = R[3] = 0.0;
   den = 0.0;
@@ -1267,16 +1268,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
       const int nf = m.nf[c];
       const double ia = m.inv_area[c];
       const double ac = DT ? st.prim[4 * NT + c] : 0.0;
+      // All four slots of the [4][NP] neighbour table are read without waiting for the face
+      // count (an unused slot reads the cell itself), so every neighbour's loads are in flight
+      // together; the sums run over the cell's faces in order.
+      int nb[4];
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        const int N = m.nbr[f * NP + c];
+        nb[f] = (N >= 0 && N < NT) ? N : c;
+      }
+      double qn[4][4];
+#pragma unroll
+      for (int f = 0; f < 4; f++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) qn[f][k] = st.prim[k * NT + nb[f]];
       double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       double den = 0.0;
-      for (int f = 0; f < nf; f++) {
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        if (f >= nf) break;
         const int idx = f * NP + c;
-        const int N = m.nbr[idx];
         const double nxf = m.nx[idx], nyf = m.ny[idx], dlf = m.dl[idx];
         const double wx = nxf * dlf, wy = nyf * dlf;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-          const double qf = 0.5 * (qc[k] + st.prim[k * NT + N]);
+          const double qf = 0.5 * (qc[k] + qn[f][k]);
           g[2 * k] += qf * wx;
           g[2 * k + 1] += qf * wy;
         }
