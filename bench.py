@@ -46,7 +46,7 @@ def workload_state(cb):
     full[:NP] = U
     full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
     kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
-              limiter=2, muscl=1, integrator=2, inlet_rho=rho, inlet_p=p)
+              limiter=2, muscl=1, integrator=2, inlet_rho=rho, inlet_p=p, reorder=3)
     return m, full, kw
 
 
@@ -138,6 +138,24 @@ def gather_stage_bytes_per_cell():
     stage 3 reads the stage state 32 and the frozen dt 8 and writes U 32.  Per stage 184, 216
     and 212 B (the ghost rows the owner threads write are < 0.1 % and left out)."""
     return (184 + 216 + 212) / 3.0
+
+
+def patch_bytes_per_cell():
+    """Algorithmic DRAM bytes per cell of the one-kernel patch stage k_patch_stage, averaged over
+    the three TVD-RK3 stages with frozen local dt.  Records: the cell's primitives 40, nf 4,
+    neighbour ids 16, face normals and lengths 96, 1/area and area 16, del_t written 8 (180 B;
+    halo cells and neighbours re-read these, which is not algorithmic).  Stage update: U^n 32,
+    R written 32, primitives written 40, boundary-entry offsets 4, plus at stage 1 the frozen dt
+    written 8 and the stage state written 32, at stage 2 the stage state and frozen dt read 40 and
+    the stage state written 32, at stage 3 the stage state and frozen dt read 40 and U written 32
+    (148, 180, 180 B)."""
+    return 180 + (148 + 180 + 180) / 3.0
+
+
+def patch_bytes_per_face():
+    """Per unique face: owner-side normal, length and centre vector 40 B and its patch-table entry
+    16 B (faces between two patches have one entry in each; counted once)."""
+    return 56
 
 
 def gather_stage_bytes_per_face():
@@ -527,16 +545,38 @@ def main():
     st_ms, st_n = s.kernel_time("stage")
     bc_ms, bc_n = s.kernel_time("bc")
     gs_ms, gs_n = s.kernel_time("gather_stage")
+    pa_ms, pa_n = s.kernel_time("patch")
     peaks, peak_kind = measured_peaks()
-    face_avg_ms = face_ms / max(face_n, 1)
     NF = s.n_faces
-    bytes_launch = face_bytes_per_face() * NF + face_bytes_per_cell() * NP
-    achieved = bytes_launch / (face_avg_ms * 1e-3) / 1e9
-    traffic = profile_figure("k_faces_traffic.json")
-    gs_avg_ms = gs_ms / max(gs_n, 1)
-    gs_bytes = gather_stage_bytes_per_cell() * NP + gather_stage_bytes_per_face() * NF
-    gs_achieved = gs_bytes / (gs_avg_ms * 1e-3) / 1e9 if gs_n else None
-    gs_traffic = profile_figure("k_gather_stage_traffic.json")
+
+    def roofline(kernel, ms, n, bytes_launch, traffic_file, **extra):
+        avg = ms / n
+        achieved = bytes_launch / (avg * 1e-3) / 1e9
+        r = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+             "frac": achieved / peaks["hbm_gbs"], "traffic": profile_figure(traffic_file),
+             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+             "bytes_per_launch": bytes_launch, "avg_launch_ms": avg, "cells": NP, "faces": NF}
+        r.update(extra)
+        return r
+
+    # The dominant kernel of the chosen launch options: the one-kernel patch stage, else the fused
+    # gather + stage kernel (the face kernel reported beside it).
+    rl_patch = rl_gs = rl_faces = None
+    if pa_n:
+        rl_patch = roofline("k_patch_stage<Roe> (records, face fluxes, gather and RK stage update of one "
+                            "128-cell patch per block; all of the pseudo-step but the first-stage BCs)",
+                            pa_ms, pa_n, patch_bytes_per_cell() * NP + patch_bytes_per_face() * NF,
+                            "k_patch_stage_traffic.json",
+                            fp64_pipe_active_pct=profile_figure("k_patch_stage_traffic.json", "fp64_pipe_active_pct"))
+    if gs_n:
+        rl_gs = roofline("k_gather_stage (face-flux gather + RK stage update)", gs_ms, gs_n,
+                         gather_stage_bytes_per_cell() * NP + gather_stage_bytes_per_face() * NF,
+                         "k_gather_stage_traffic.json")
+    if face_n:
+        rl_faces = roofline("k_faces<double> (face fluxes, gradient MUSCL + Roe)", face_ms, face_n,
+                            face_bytes_per_face() * NF + face_bytes_per_cell() * NP, "k_faces_traffic.json",
+                            fp64_pipe_active_pct=profile_figure("k_faces_traffic.json", "fp64_pipe_active_pct"),
+                            note="FP64 issue rather than HBM limits this kernel (ncu)")
 
     # The other forms on the same mesh: FP32 fluxes with FP64 state (north-star precision form,
     # its error against the all-FP64 run stated), and the reference-parity second-order Roe path
@@ -604,23 +644,11 @@ def main():
                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps},
                "gpu_launches": int(launches),
-               "roofline": {"kernel": "k_gather_stage (face-flux gather + RK stage update, the largest "
-                                      "time share)", "bound": "hbm",
-                            "achieved": gs_achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                            "frac": gs_achieved / peaks["hbm_gbs"] if gs_achieved else None,
-                            "traffic": gs_traffic,
-                            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-                            "bytes_per_launch": gs_bytes, "avg_launch_ms": gs_avg_ms, "cells": NP, "faces": NF},
-               "roofline_faces": {"kernel": "k_faces<double> (face fluxes, gradient MUSCL + Roe)", "bound": "hbm",
-                                  "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                                  "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                                  "bytes_per_launch": bytes_launch, "avg_launch_ms": face_avg_ms, "faces": NF,
-                                  "fp64_pipe_active_pct": profile_figure("k_faces_traffic.json",
-                                                                         "fp64_pipe_active_pct"),
-                                  "note": "FP64 issue rather than HBM limits this kernel (ncu)"},
+               "roofline": rl_patch or rl_gs,
+               "roofline_faces": rl_faces,
                "kernel_ms_per_step": {"faces": face_ms / nprof, "gradients": grad_ms / nprof,
                                       "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof,
-                                      "gather_stage": gs_ms / nprof},
+                                      "gather_stage": gs_ms / nprof, "patch": pa_ms / nprof},
                "forms": forms,
                "clocks": clk.summary(),
                "final_residual_rho": info.error[0]}

@@ -110,6 +110,66 @@ std::vector<int> patch_from_arrays(int NP, const int *nf, const int *nbr, int pa
   return order;
 }
 
+// Patch ordering by recursive coordinate bisection, for the one-block-per-patch stage kernel.
+// Cell centres are recovered (up to a shift per connected piece of the mesh) by walking the face
+// graph with the centre-to-centre vectors; each piece is then cut at the median of its longer
+// extent until every part has at most `patch` cells, the cuts chosen so that all parts of a piece
+// but the last hold exactly `patch` cells.  Parts are numbered depth-first (neighbouring parts get
+// nearby numbers); the cells of a part keep their given order.  starts[b] = first cell of part b.
+void rcb_patches(int NP, const int *nf, const int *nbr, const double *cvec, int patch, std::vector<int> &order,
+                 std::vector<int> &starts) {
+  std::vector<double> x(NP, 0.0), y(NP, 0.0);
+  std::vector<char> seen(NP, 0);
+  std::vector<int> comp, q;
+  order.clear();
+  starts.clear();
+  order.reserve(NP);
+  q.reserve(NP);
+  auto split = [&](auto &&self, int lo, int hi) -> void {
+    const int n = hi - lo;
+    if (n <= patch) {
+      std::sort(comp.begin() + lo, comp.begin() + hi);
+      starts.push_back(static_cast<int>(order.size()));
+      order.insert(order.end(), comp.begin() + lo, comp.begin() + hi);
+      return;
+    }
+    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+    for (int i = lo; i < hi; i++) {
+      const int c = comp[i];
+      xmin = std::min(xmin, x[c]);
+      xmax = std::max(xmax, x[c]);
+      ymin = std::min(ymin, y[c]);
+      ymax = std::max(ymax, y[c]);
+    }
+    const std::vector<double> &a = (xmax - xmin >= ymax - ymin) ? x : y;
+    const int k = (n + patch - 1) / patch;
+    const int left = (k / 2) * patch;
+    std::nth_element(comp.begin() + lo, comp.begin() + lo + left, comp.begin() + hi,
+                     [&](int u, int v) { return a[u] < a[v] || (a[u] == a[v] && u < v); });
+    self(self, lo, lo + left);
+    self(self, lo + left, hi);
+  };
+  for (int s0 = 0; s0 < NP; s0++) {
+    if (seen[s0]) continue;
+    q.clear();
+    q.push_back(s0);
+    seen[s0] = 1;
+    for (size_t h = 0; h < q.size(); h++) {
+      const int c = q[h];
+      for (int f = 0; f < nf[c]; f++) {
+        const int n = nbr[4 * c + f];
+        if (n < 0 || n >= NP || seen[n]) continue;
+        seen[n] = 1;
+        x[n] = x[c] + cvec[8 * c + 2 * f];
+        y[n] = y[c] + cvec[8 * c + 2 * f + 1];
+        q.push_back(n);
+      }
+    }
+    comp = q;
+    split(split, 0, static_cast<int>(comp.size()));
+  }
+}
+
 template <typename T>
 cfd_status dev_upload(T **dst, const std::vector<T> &v) {
   CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), std::max<size_t>(1, v.size()) * sizeof(T)));
@@ -140,6 +200,9 @@ struct cfd_ctx {
   int keep_delu = 1;
   int use_graph = 1;
   int fuse_gather = 1;  // face-based forms with per-cell dt: fused gather + stage update
+  int patch_stage = 0;  // ... or, with patch tables (reorder 3), the one-kernel patch stage
+  std::vector<int> patch_starts;  // first device cell of each patch (reorder 3)
+  double *pbuf[2] = {nullptr, nullptr};  // stage primitives of the patch form ([5][NT] each)
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
@@ -152,8 +215,8 @@ struct cfd_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Timed> timed;
-  double kind_ms[6] = {0, 0, 0, 0, 0, 0};
-  long long kind_n[6] = {0, 0, 0, 0, 0, 0};
+  double kind_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long kind_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
   void *d_amr = nullptr;      // AMR indicator, tags and selection scratch (allocated on first use)
   int2 *d_tables = nullptr;   // work lists of batched solves (cells, faces, entries, records)
@@ -178,7 +241,7 @@ cfd_status ctx_upload(cfd_ctx *ctx, T **dst, const std::vector<T> &v) {
 
 int dev_of(const cfd_ctx *ctx, int ref) { return ref < ctx->NP ? ctx->inv[ref] : ref; }
 
-enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_N = 6 };
+enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_PATCH = 6, TK_N = 7 };
 
 struct TimedScope {
   cfd_ctx *ctx;
@@ -232,6 +295,12 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
   const StagePlan p = stage_plan(c, ctx->fp.consistent);
   const bool faces = ctx->dm.NF > 0;
   bool ghosts_written = false;  // the previous stage's owner threads wrote this stage's ghosts
+  // Patch form: one kernel per stage.  Stage k reads the primitives of buffer in(k) and writes
+  // out(k): in(0) = st.prim, out(k) = pbuf[k % 2] for the other stages and st.prim for the last,
+  // in(k + 1) = out(k), so every stage writes a buffer that no block of it reads.
+  const bool patch = faces && ctx->patch_stage && m.npatch > 0 && !m.cblk && !m.fblk && fuse_final &&
+                     ctx->fp.precision == CFD_PREC_FP64 && !ctx->fp.weno && p.kind0 != 0 && p.lts_mode == 1 &&
+                     c.local_time_stepping;
   for (int k = 0; k < p.n; k++) {
     const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
     const int lts = stage_lts(p, c, k);
@@ -241,6 +310,17 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
       n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
     }
     ghosts_written = false;
+    if (patch) {
+      TimedScope ts(ctx, TK_PATCH);
+      const bool bc_next = k < p.n - 1;
+      const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+      DevState sk = st;
+      sk.prim = bc_next ? ctx->pbuf[k % 2] : st.prim;
+      const double *pin = k == 0 ? st.prim : ctx->pbuf[(k - 1) % 2];
+      n += launch_patch_stage(s, m, sk, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags, pin);
+      ghosts_written = bc_next;
+      continue;
+    }
     if (faces) {
       // Fused form (per-cell dt): del_t comes from the gradient pass, the stage kernel writes
       // the next stage's ghost states from the owner cells, and the last stage forms the step's
@@ -468,6 +548,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
+  if (cfg->reorder < 0 || cfg->reorder > 3) return fail(CFD_ERR_BAD_ARG, "reorder must be 0, 1, 2 or 3");
   if (cfg->inlet_bc < 0 || cfg->inlet_bc > CFD_INLET_FARFIELD || cfg->exit_bc < 0 || cfg->exit_bc > CFD_EXIT_FIXED_P_REF)
     return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
   if (cfg->precision != CFD_PREC_FP64 && !(cfg->precision == CFD_PREC_FP32_FLUX && cfg->muscl && cfg->is_second_order))
@@ -499,7 +580,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     return bail(fail(CFD_ERR_CUDA, "pinned allocation failed"));
 
   // Renumbering (reverse Cuthill-McKee over physical cells; ghosts keep their ids).
-  if (cfg->reorder == 2) ctx->perm = patch_from_arrays(NP, d->n_faces, d->neighbours, 128);
+  if (cfg->reorder == 3 && d->center_vectors)
+    rcb_patches(NP, d->n_faces, d->neighbours, d->center_vectors, kPatchCells, ctx->perm, ctx->patch_starts);
+  else if (cfg->reorder == 2) ctx->perm = patch_from_arrays(NP, d->n_faces, d->neighbours, 128);
   else if (cfg->reorder) ctx->perm = rcm_from_arrays(NP, d->n_faces, d->neighbours);
   else {
     ctx->perm.resize(NP);
@@ -618,6 +701,79 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       }
     }
   }
+  // Patch tables of the one-kernel stage form (reorder 3): per patch its halo cells and the faces
+  // touching its cells, each with the shared-memory rows of its two cells and the face slots they
+  // fill.  Any inconsistency leaves the patch form off (the three-kernel form is always there).
+  std::vector<int2> patches;
+  std::vector<int> phptr(1, 0), phcell, pfptr(1, 0);
+  std::vector<PatchFace> pface;
+  int patch_rows = 0;
+  if (!ctx->patch_starts.empty() && !fo.empty()) {
+    const int npatch = static_cast<int>(ctx->patch_starts.size());
+    std::vector<int> seen(NP, -1), loc(NP, 0);
+    bool ok = true;
+    auto slot_of = [&](int cell, int code) {
+      for (int g = 0; g < nf[cell]; g++)
+        if (cface[(size_t)g * NP + cell] == code) return g;
+      return -1;
+    };
+    for (int b = 0; b < npatch && ok; b++) {
+      const int c0 = ctx->patch_starts[b], c1 = b + 1 < npatch ? ctx->patch_starts[b + 1] : NP, P = c1 - c0;
+      auto own = [&](int x) { return x >= c0 && x < c1; };
+      if (P <= 0 || P > kPatchCells) {
+        ok = false;
+        break;
+      }
+      int H = 0;
+      for (int c = c0; c < c1; c++)
+        for (int f = 0; f < nf[c]; f++) {
+          const int N = nbr[(size_t)f * NP + c];
+          if (N < 0 || N >= NP || own(N) || seen[N] == b) continue;
+          seen[N] = b;
+          loc[N] = P + H++;
+          phcell.push_back(N);
+        }
+      const int rows = P + H;
+      if (rows >= 0xFFFF) {
+        ok = false;
+        break;
+      }
+      auto pack = [](int lo, int hi) { return static_cast<int>(static_cast<unsigned>(lo) | (static_cast<unsigned>(hi) << 16)); };
+      for (int c = c0; c < c1 && ok; c++)
+        for (int f = 0; f < nf[c]; f++) {
+          const int e = cface[(size_t)f * NP + c];
+          const int l = c - c0;
+          if (e >= 0) {
+            const int N = fn[e];
+            int ln, sn = 0xFF;
+            if (N >= NP) ln = 0xFFFF;
+            else if (own(N)) {
+              ln = N - c0;
+              sn = slot_of(N, -(e + 1));
+            } else ln = seen[N] == b ? loc[N] : -1;
+            if (ln < 0 || sn < 0 || fo[e] != c || N >= NT) ok = false;
+            pface.push_back({N, pack(l, ln), f | (sn << 8), e, fnx[e], fny[e], fdl[e], fdx[e], fdy[e], 0.0});
+          } else {
+            const int i = -e - 1, o = fo[i];
+            if (own(o)) continue;  // listed from its owner's side
+            if (o < 0 || o >= NP || seen[o] != b || fn[i] != c) ok = false;
+            pface.push_back({c, pack(ok ? loc[o] : 0, l), 0xFF | (f << 8), i, fnx[i], fny[i], fdl[i], fdx[i], fdy[i], 0.0});
+          }
+        }
+      patches.push_back(make_int2(c0, P));
+      phptr.push_back(static_cast<int>(phcell.size()));
+      pfptr.push_back(static_cast<int>(pface.size()));
+      patch_rows = std::max(patch_rows, rows);
+    }
+    if (!ok) {
+      patches.clear();
+      phcell.clear();
+      pface.clear();
+      phptr.assign(1, 0);
+      pfptr.assign(1, 0);
+      patch_rows = 0;
+    }
+  }
   std::vector<int4> bnd(NB);
   for (int e = 0; e < NB; e++) {
     const int *b = d->boundary + 4 * e;
@@ -665,9 +821,22 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_upload(ctx, const_cast<int **>(&m.cface), cface)) != CFD_OK) return bail(s);
   }
 
+  if (!patches.empty()) {
+    m.npatch = static_cast<int>(patches.size());
+    m.patch_rows = patch_rows;
+    if (!patch_prepare(m)) m.npatch = 0;
+  }
+  if (m.npatch > 0) {
+    if ((s = ctx_upload(ctx, const_cast<int2 **>(&m.patch), patches)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.phptr), phptr)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.phcell), phcell)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&m.pfptr), pfptr)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<PatchFace **>(&m.pface), pface)) != CFD_OK) return bail(s);
+  }
+
   DevState &st = ctx->ds;
   const size_t dsz = sizeof(double);
-  const int nblk = flux_block_count(NP);
+  const int nblk = std::max(flux_block_count(NP), m.npatch);
   if ((s = ctx_alloc(ctx, (void **)&st.U, 4 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.S, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.prim, 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
@@ -685,6 +854,10 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
+  for (int q = 0; q < 2 && m.npatch > 0; q++) {
+    if ((s = ctx_alloc(ctx, (void **)&ctx->pbuf[q], 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
+    if (cudaMemset(ctx->pbuf[q], 0, 5 * (size_t)NT * dsz) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
+  }
   if ((s = ctx_alloc(ctx, (void **)&st.partial, 9 * (size_t)(nblk + kMaxGroups) * dsz)) != CFD_OK) return bail(s);
   const size_t counter_bytes = 64 + 4 * (size_t)(kMaxGroups + 1);
   if ((s = ctx_alloc(ctx, (void **)&st.counter, counter_bytes)) != CFD_OK) return bail(s);
@@ -754,6 +927,7 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "pdl") ctx->dm.pdl = value != 0.0;
   else if (n == "profile") ctx->profile = value != 0.0;
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
+  else if (n == "patch_stage") ctx->patch_stage = value != 0.0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);
@@ -1127,16 +1301,18 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     }
   };
   struct Cand {
-    int faces_shape, fuse, lanes, pdl;
+    int faces_shape, fuse, lanes, pdl, patch;
     double ms;
   };
   std::vector<Cand> cands;
   if (ctx->dm.NF > 0) {
     for (int f = 0; f < 3; f++)
       for (int g = 0; g < 2; g++)
-        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0.0});
+        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, 0.0});
+    if (ctx->dm.npatch > 0)
+      for (int p = 0; p < 2; p++) cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, 0.0});
   } else {
-    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, ctx->dm.pdl, 0.0});
+    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, ctx->dm.pdl, 0, 0.0});
   }
   const int prof = ctx->profile, graph_on = ctx->use_graph;
   ctx->profile = 0;
@@ -1151,6 +1327,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     ctx->fuse_gather = cd.fuse;
     ctx->fp.lanes = cd.lanes;
     ctx->dm.pdl = cd.pdl;
+    ctx->patch_stage = cd.patch;
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
       ctx->graph = nullptr;
@@ -1186,12 +1363,13 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   ctx->fuse_gather = best->fuse;
   ctx->fp.lanes = best->lanes;
   ctx->dm.pdl = best->pdl;
+  ctx->patch_stage = best->patch;
   if (report && report_len > 0) {
     std::string r;
     char line[160];
     for (const Cand &cd : cands) {
-      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d: %.4f ms/step%s\n",
-               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.ms, &cd == best ? " (chosen)" : "");
+      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d patch_stage=%d: %.4f ms/step%s\n",
+               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.patch, cd.ms, &cd == best ? " (chosen)" : "");
       r += line;
     }
     snprintf(report, report_len, "%s", r.c_str());
@@ -1262,7 +1440,7 @@ cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, l
   if (!ctx || !kernel || !total_ms || !launches) return fail(CFD_ERR_BAD_ARG, "null argument");
   std::string k(kernel);
   int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : k == "gradients" ? TK_GRAD
-           : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : -1;
+           : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : k == "patch" ? TK_PATCH : -1;
   if (kind < 0) return fail(CFD_ERR_BAD_ARG, "unknown kernel " + k);
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   for (auto &t : ctx->timed) {

@@ -30,17 +30,19 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-// Launches kernel k, with programmatic stream serialization when m.pdl is set.
+// Launches kernel k (smem bytes of dynamic shared memory), with programmatic stream
+// serialization when m.pdl is set.
 template <typename... KArgs, typename... Args>
-void launch_k(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+void launch_ks(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+               Args... args) {
   if (!m.pdl) {
-    k<<<grid, block, 0, s>>>(args...);
+    k<<<grid, block, smem, s>>>(args...);
     return;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(block);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -48,6 +50,11 @@ void launch_k(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned blo
   cfg.attrs = at;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, k, args...);
+}
+
+template <typename... KArgs, typename... Args>
+void launch_k(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+  launch_ks(m, k, grid, block, 0, s, args...);
 }
 
 // Item handled by this thread: from the block's work-list range when a list is given (n when the
@@ -790,21 +797,12 @@ __global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, Flu
 // (phi(a, b), r = a/b).  A ghost neighbour uses the owner's gradient.  A non-positive
 // reconstructed density or pressure falls back to the cell-centre state.  Flux: average of the two
 // face states plus Roe dissipation between them.
-template <typename T, int DISS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
-  pdl_enter();
-  const int i = item_index(m.fblk, m.NF);
-  if (i >= m.NF || step_done(st.ctl)) return;
-  const int NP = m.NP;
-  const int c = m.fo[i], N = m.fn[i];
-  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
-  const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
-  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)c);
-  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)N);
-  const double4 c0 = rc[0], c1 = rc[1], c2 = rc[2];
-  const double4 n0 = rn[0];
-  const bool nphys = N < NP;
-  const double4 n1 = nphys ? rn[1] : c1, n2 = nphys ? rn[2] : c2;
+// Flux of one unique face from the owner's record (c0: rho, u, v, p; c1, c2: gradients) and the
+// neighbour's (n0, n1, n2), face normal (nx, ny), length dl and centre-to-centre vector (dx, dy).
+template <typename T, int DISS>
+__device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, const double4 c1, const double4 c2,
+                                                 const double4 n0, const double4 n1, const double4 n2, const T nx,
+                                                 const T ny, const T dl, const T dx, const T dy) {
   const T qc[4] = {T(c0.x), T(c0.y), T(c0.z), T(c0.w)};
   const T qn[4] = {T(n0.x), T(n0.y), T(n0.z), T(n0.w)};
   const T gc[8] = {T(c1.x), T(c1.y), T(c1.z), T(c1.w), T(c2.x), T(c2.y), T(c2.z), T(c2.w)};
@@ -846,7 +844,25 @@ __global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, Flu
       hllc_face<T>(q5L, UL, q5R, UR, nx, ny, dl, A);
     }
   }
-  st.F[i] = make_double4(double(A[0] - D[0]), double(A[1] - D[1]), double(A[2] - D[2]), double(A[3] - D[3]));
+  return make_double4(double(A[0] - D[0]), double(A[1] - D[1]), double(A[2] - D[2]), double(A[3] - D[3]));
+}
+
+template <typename T, int DISS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
+  pdl_enter();
+  const int i = item_index(m.fblk, m.NF);
+  if (i >= m.NF || step_done(st.ctl)) return;
+  const int NP = m.NP;
+  const int c = m.fo[i], N = m.fn[i];
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+  const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
+  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)c);
+  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)N);
+  const double4 c0 = rc[0], c1 = rc[1], c2 = rc[2];
+  const double4 n0 = rn[0];
+  const bool nphys = N < NP;
+  const double4 n1 = nphys ? rn[1] : c1, n2 = nphys ? rn[2] : c2;
+  st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy);
 }
 
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
@@ -1128,51 +1144,39 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
   }
 }
 
-// Face-based forms with a per-cell time step (lts 1 or 2): the gather of k_gather and the stage
-// update of k_stage in one pass, so the residual never leaves registers on its way to the update
-// (it is still stored for downloads).  The last block finishes Min_dt (and the step's frozen dt at
-// the first stage), and at the final stage the error norms and the Total_Time epilogue.
-__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
-                                                             int kind, int lts, int fuse_final, int keep_delu,
-                                                             int flags) {
-  pdl_enter();
+// Stage update of cell c from its residual R, shared by the gather and patch forms: stores R,
+// takes the stage dt (lts 1: del_t of this evaluation; else del_t frozen at the first stage),
+// updates the cell, and with flags bit 1 writes the next stage's ghost states from the owner
+// thread (every ghost depends only on its owner cell's new state: Apply_Boundary_Conditions of the
+// next stage).  Returns the dt used.
+__device__ __forceinline__ double stage_cell(const DevMesh &m, DevState &st, const BcParams &bp, int c,
+                                             const double R[4], double dtc, int kind, int lts, int fuse_final,
+                                             int keep_delu, int flags, double e[8]) {
   const int NP = m.NP;
-  const int c = item_index(m.cblk, NP);
-  if (step_done(st.ctl)) return;
   const bool first = first_kind(kind);
-  const bool is_final = final_kind(kind);
-  double dtu = 1e308 * 10.0;
-  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (c < NP) {
-    // The residual gather is issued first; loading the state rows ahead of it (more registers,
-    // fewer resident warps) measured slower on B200.
-    double R[4], den = 0.0;
-    gather_faces<false>(m, st, c, R, den);
-    StageIn in;
-    load_stage_in(m, st, c, kind, in);
-    const double dtc = st.dtc[c];
-    const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
+  StageIn in;
+  load_stage_in(m, st, c, kind, in);
+  const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
-    double dt;
-    if (lts == 1) dt = dtc;
-    else {
-      if (first) st.dtk[c] = dtc;
-      dt = first ? dtc : dt_frozen;
-    }
-    dtu = dt;
-    cell_update_in(m, st, c, kind, dt, R, in, fuse_final, keep_delu, e);
-    if ((flags & 2) && !is_final) {
-      // Boundary conditions of the next stage: every ghost depends only on its owner cell's
-      // new state, so the owner writes them (Apply_Boundary_Conditions at the next stage).
-      const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
-      for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], (flags & 4) ? 1 : 0, 1);
-    }
+  for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
+  double dt;
+  if (lts == 1) dt = dtc;
+  else {
+    if (first) st.dtk[c] = dtc;
+    dt = first ? dtc : dt_frozen;
   }
-  if (!(fuse_final && is_final)) return;
-  // Last stage: Estimate_Error's terms, the residual squares and the step's dt (the minimum of
-  // the per-cell dt frozen at the first stage, i.e. that stage's Min_dt), then the Total_Time
-  // epilogue of the loop body.
+  cell_update_in(m, st, c, kind, dt, R, in, fuse_final, keep_delu, e);
+  if ((flags & 2) && !final_kind(kind)) {
+    const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+    for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], (flags & 4) ? 1 : 0, 1);
+  }
+  return dt;
+}
+
+// Last stage of the fused forms: Estimate_Error's terms, the residual squares and the step's dt
+// (the minimum of the per-cell dt frozen at the first stage, i.e. that stage's Min_dt), reduced
+// over the grid, then the Total_Time epilogue of the loop body.  Called by every thread.
+__device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[8], double dtu) {
   __shared__ double sh[32];
   __shared__ double sh8[8 * 32];
   __shared__ double red[9];
@@ -1190,6 +1194,29 @@ __global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState
     double te = st.ctl[CTL_TEND];
     if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
   }
+}
+
+// Face-based forms with a per-cell time step (lts 1 or 2): the gather of k_gather and the stage
+// update of k_stage in one pass, so the residual never leaves registers on its way to the update
+// (it is still stored for downloads).  At the final stage the error norms, the step's Min_dt and
+// the Total_Time epilogue.
+__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
+                                                             int kind, int lts, int fuse_final, int keep_delu,
+                                                             int flags) {
+  pdl_enter();
+  const int NP = m.NP;
+  const int c = item_index(m.cblk, NP);
+  if (step_done(st.ctl)) return;
+  double dtu = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (c < NP) {
+    // The residual gather is issued first; loading the state rows ahead of it (more registers,
+    // fewer resident warps) measured slower on B200.
+    double R[4], den = 0.0;
+    gather_faces<false>(m, st, c, R, den);
+    dtu = stage_cell(m, st, bp, c, R, st.dtc[c], kind, lts, fuse_final, keep_delu, flags, e);
+  }
+  if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
 
 // Estimate_Error alone (src/Error_Estimate_Update.cpp:10-28).
@@ -1247,6 +1274,54 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
   g1 *= m.inv_area[c];
 }
 
+// Green-Gauss gradients of (rho, u, v, p) of physical cell c from the primitive planes `prim`
+// ([5][NT]), multiplied by 1/A (g[2k], g[2k+1]: d/dx, d/dy of variable k), and with DT the
+// denominator of del_t (Inviscid_Time_Step, src/Time_Step.cpp:293-329, faces in order).  All four
+// slots of the [4][NP] neighbour table are read without waiting for the face count (an unused
+// slot reads the cell itself), so every neighbour's loads are in flight together; the sums run
+// over the cell's faces in order.
+template <bool DT>
+__device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *__restrict__ prim, int c,
+                                               const double qc[4], double g[8], double &den) {
+  const int NP = m.NP, NT = m.NT;
+  const int nf = m.nf[c];
+  const double ia = m.inv_area[c];
+  const double ac = DT ? prim[4 * NT + c] : 0.0;
+  int nb[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const int N = m.nbr[f * NP + c];
+    nb[f] = (N >= 0 && N < NT) ? N : c;
+  }
+  double qn[4][4];
+#pragma unroll
+  for (int f = 0; f < 4; f++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) qn[f][k] = prim[k * NT + nb[f]];
+#pragma unroll
+  for (int k = 0; k < 8; k++) g[k] = 0.0;
+  den = 0.0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    if (f >= nf) break;
+    const int idx = f * NP + c;
+    const double nxf = m.nx[idx], nyf = m.ny[idx], dlf = m.dl[idx];
+    const double wx = nxf * dlf, wy = nyf * dlf;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double qf = 0.5 * (qc[k] + qn[f][k]);
+      g[2 * k] += qf * wx;
+      g[2 * k + 1] += qf * wy;
+    }
+    if (DT) {
+      const double vnf = qc[1] * nxf + qc[2] * nyf;
+      den += (fabs(vnf) + ac) * dlf;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; k++) g[k] = g[k] * ia;
+}
+
 // Records of the face-based forms: (rho, u, v, p) and their Green-Gauss gradients, the face
 // value being the mean of the two cell values, ghost cells included (their values carry the
 // boundary state).  Ghost rows get (rho, u, v, p) only.
@@ -1265,48 +1340,136 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
     double4 *r = reinterpret_cast<double4 *>(st.rec + 12 * (size_t)c);
     r[0] = make_double4(qc[0], qc[1], qc[2], qc[3]);
     if (c < NP) {
-      const int nf = m.nf[c];
-      const double ia = m.inv_area[c];
-      const double ac = DT ? st.prim[4 * NT + c] : 0.0;
-      // All four slots of the [4][NP] neighbour table are read without waiting for the face
-      // count (an unused slot reads the cell itself), so every neighbour's loads are in flight
-      // together; the sums run over the cell's faces in order.
-      int nb[4];
-#pragma unroll
-      for (int f = 0; f < 4; f++) {
-        const int N = m.nbr[f * NP + c];
-        nb[f] = (N >= 0 && N < NT) ? N : c;
-      }
-      double qn[4][4];
-#pragma unroll
-      for (int f = 0; f < 4; f++)
-#pragma unroll
-        for (int k = 0; k < 4; k++) qn[f][k] = st.prim[k * NT + nb[f]];
-      double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      double den = 0.0;
-#pragma unroll
-      for (int f = 0; f < 4; f++) {
-        if (f >= nf) break;
-        const int idx = f * NP + c;
-        const double nxf = m.nx[idx], nyf = m.ny[idx], dlf = m.dl[idx];
-        const double wx = nxf * dlf, wy = nyf * dlf;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const double qf = 0.5 * (qc[k] + qn[f][k]);
-          g[2 * k] += qf * wx;
-          g[2 * k + 1] += qf * wy;
-        }
-        if (DT) {
-          // Inviscid_Time_Step's denominator (src/Time_Step.cpp:293-329), faces in order.
-          const double vnf = qc[1] * nxf + qc[2] * nyf;
-          den += (fabs(vnf) + ac) * dlf;
-        }
-      }
-      r[1] = make_double4(g[0] * ia, g[1] * ia, g[2] * ia, g[3] * ia);
-      r[2] = make_double4(g[4] * ia, g[5] * ia, g[6] * ia, g[7] * ia);
+      double g[8], den;
+      cell_gradients<DT>(m, st.prim, c, qc, g, den);
+      r[1] = make_double4(g[0], g[1], g[2], g[3]);
+      r[2] = make_double4(g[4], g[5], g[6], g[7]);
       if (DT) st.dtc[c] = cell_dt(m, fp, c, den);
     }
   }
+}
+
+// Patch form of one stage of the face-based per-cell-dt forms: one thread block per patch of up
+// to kPatchCells cells does the work of k_muscl_gradients, k_faces and k_gather_stage for its
+// cells, with the records and face fluxes in shared memory instead of HBM.
+//   1. records (rho, u, v, p and gradients) of its own cells and of its halo cells (the cells
+//      across its faces), from the stage's primitives `pin`; del_t of its own cells;
+//   2. every face of its own cells (a face to a halo cell is evaluated by both patches, from the
+//      owner's side, so both get the same bits), +F into the owner's slot and -F into the
+//      neighbour's slot when that cell is its own;
+//   3. per own cell: the slots summed in face order and the stage update (stage_cell), which
+//      writes the new primitives and the next stage's ghosts to st.prim (a different buffer from
+//      `pin`: other blocks are still reading their halo primitives from it).
+// Every operation on a value is the one the three-kernel form does, in the same order.
+template <int DISS>
+__global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
+                                                                int kind, int lts, int fuse_final, int keep_delu,
+                                                                int flags, const double *__restrict__ pin) {
+  pdl_enter();
+  if (step_done(st.ctl)) return;
+  extern __shared__ double smem[];
+  const int NP = m.NP, NT = m.NT, rows = m.patch_rows;
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int2 pr = m.patch[b];
+  const int c0 = pr.x, P = min(pr.y, kPatchCells);
+  const int h0 = m.phptr[b], H = m.phptr[b + 1] - h0;
+  double *srec = smem;             // [12][rows]: rho, u, v, p, then the 8 gradient terms
+  double *sF = smem + 12 * rows;   // [4 slots][4][kPatchCells]
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+
+  // The tables are checked on the host; an entry that would still leave its buffer is skipped and
+  // reported as a mesh error instead of being used.
+  double dtc = 0.0;
+  const int nrow = min(P + H, rows);
+  for (int l = tid; l < nrow; l += kPatchCells) {
+    const int c = l < P ? c0 + l : m.phcell[h0 + l - P];
+    if (c < 0 || c >= NP) {
+      atomicCAS(&st.status[0], 0, 7 /* CFD_ERR_MESH */);
+      continue;
+    }
+    double qc[4], g[8], den;
+#pragma unroll
+    for (int k = 0; k < 4; k++) qc[k] = pin[k * NT + c];
+    cell_gradients<true>(m, pin, c, qc, g, den);
+#pragma unroll
+    for (int k = 0; k < 4; k++) srec[k * rows + l] = qc[k];
+#pragma unroll
+    for (int k = 0; k < 8; k++) srec[(4 + k) * rows + l] = g[k];
+    if (l < P) {
+      dtc = cell_dt(m, fp, c, den);
+      st.dtc[c] = dtc;
+    }
+  }
+  __syncthreads();
+
+  const int f0 = m.pfptr[b], f1 = m.pfptr[b + 1];
+  for (int j = f0 + tid; j < f1; j += kPatchCells) {
+    const PatchFace fe = m.pface[j];
+    const int N = fe.N;
+    const int lo = fe.rows & 0xFFFF, ln = (int)((unsigned)fe.rows >> 16);
+    const int so = fe.slots & 0xFF, sn = (fe.slots >> 8) & 0xFF;
+    const bool bad = lo >= nrow || (ln == 0xFFFF ? (N < NP || N >= NT) : ln >= nrow) ||
+                     (so != 0xFF && (so > 3 || lo >= P)) || (sn != 0xFF && (sn > 3 || ln >= P));
+    if (bad) {
+      atomicCAS(&st.status[0], 0, 7 /* CFD_ERR_MESH */);
+      continue;
+    }
+    const double4 c0r = make_double4(srec[lo], srec[rows + lo], srec[2 * rows + lo], srec[3 * rows + lo]);
+    const double4 c1r =
+        make_double4(srec[4 * rows + lo], srec[5 * rows + lo], srec[6 * rows + lo], srec[7 * rows + lo]);
+    const double4 c2r =
+        make_double4(srec[8 * rows + lo], srec[9 * rows + lo], srec[10 * rows + lo], srec[11 * rows + lo]);
+    double4 n0r, n1r, n2r;
+    if (ln == 0xFFFF) {
+      // Ghost neighbour: its state, with the owner's gradient.
+      n0r = make_double4(pin[N], pin[NT + N], pin[2 * NT + N], pin[3 * NT + N]);
+      n1r = c1r;
+      n2r = c2r;
+    } else {
+      n0r = make_double4(srec[ln], srec[rows + ln], srec[2 * rows + ln], srec[3 * rows + ln]);
+      n1r = make_double4(srec[4 * rows + ln], srec[5 * rows + ln], srec[6 * rows + ln], srec[7 * rows + ln]);
+      n2r = make_double4(srec[8 * rows + ln], srec[9 * rows + ln], srec[10 * rows + ln], srec[11 * rows + ln]);
+    }
+    const double4 F = face_flux_rec<double, DISS>(glim, c0r, c1r, c2r, n0r, n1r, n2r, fe.nx, fe.ny, fe.dl, fe.dx, fe.dy);
+    if (so < 4) {
+      sF[(so * 4 + 0) * kPatchCells + lo] = F.x;
+      sF[(so * 4 + 1) * kPatchCells + lo] = F.y;
+      sF[(so * 4 + 2) * kPatchCells + lo] = F.z;
+      sF[(so * 4 + 3) * kPatchCells + lo] = F.w;
+    }
+    if (sn < 4) {
+      sF[(sn * 4 + 0) * kPatchCells + ln] = -F.x;
+      sF[(sn * 4 + 1) * kPatchCells + ln] = -F.y;
+      sF[(sn * 4 + 2) * kPatchCells + ln] = -F.z;
+      sF[(sn * 4 + 3) * kPatchCells + ln] = -F.w;
+    }
+  }
+  __syncthreads();
+
+  double dtu = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (tid < P && c0 + tid < NP) {
+    const int c = c0 + tid;
+    const int nf = m.nf[c];
+    double R[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      if (f < nf) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) R[k] += sF[(f * 4 + k) * kPatchCells + tid];
+      }
+    }
+    // Ghost rows move to the output buffer with their owner (the final stage, and boundary kinds
+    // that leave a ghost unchanged, keep its current state); non-final stages overwrite them.
+    const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+    for (int q = b0; q < b1; q++) {
+      const int g = m.bnd[m.bidx[q]].w;
+#pragma unroll
+      for (int k = 0; k < 5; k++) st.prim[k * NT + g] = pin[k * NT + g];
+    }
+    dtu = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
+  }
+  if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
 
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
@@ -1596,6 +1759,44 @@ int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Fl
                         int kind, int lts, int fuse_final, int keep_delu, int flags) {
   const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
   launch_k(m, k_gather_stage, g, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  return 1;
+}
+
+size_t patch_smem_bytes(const DevMesh &m) {
+  return sizeof(double) * (12 * (size_t)m.patch_rows + 16 * (size_t)kPatchCells);
+}
+
+int patch_prepare(const DevMesh &m) {
+  const size_t bytes = patch_smem_bytes(m);
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  if (bytes + 4096 > (size_t)optin) return 0;
+  const int n = static_cast<int>(bytes);
+  if (cudaFuncSetAttribute(k_patch_stage<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
+      cudaFuncSetAttribute(k_patch_stage<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
+      cudaFuncSetAttribute(k_patch_stage<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
+      cudaFuncSetAttribute(k_patch_stage<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess)
+    return 0;
+  return 1;
+}
+
+int launch_patch_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                       int kind, int lts, int fuse_final, int keep_delu, int flags, const double *prim_in) {
+  const size_t sm = patch_smem_bytes(m);
+  const int g = m.npatch;
+  if (fp.dissipation == 6)
+    launch_ks(m, k_patch_stage<6>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
+              prim_in);
+  else if (fp.dissipation == 7)
+    launch_ks(m, k_patch_stage<7>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
+              prim_in);
+  else if (fp.dissipation == 8)
+    launch_ks(m, k_patch_stage<8>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
+              prim_in);
+  else
+    launch_ks(m, k_patch_stage<3>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
+              prim_in);
   return 1;
 }
 

@@ -15,6 +15,15 @@
 
 namespace cfdb {
 
+// One face of a patch (64 B, so one record is one aligned load set): the neighbour cell, the
+// shared-memory rows of its two cells (owner | neighbour << 16; 0xFFFF = ghost neighbour), the
+// face slots it fills (owner | neighbour << 8; 0xFF = not a cell of the patch), and the face's
+// owner-side normal, length and centre-to-centre vector.
+struct PatchFace {
+  int N, rows, slots, face;
+  double nx, ny, dl, dx, dy, pad;
+};
+
 struct DevMesh {
   int NP, NT, NB;
   const int *nf;
@@ -46,7 +55,18 @@ struct DevMesh {
   // exit pressure (CFD_EXIT_STATIC_P, CFD_EXIT_FIXED_P_REF).
   const double4 *bstate;
   const double *bexit;
+  // Patch form (face-based, per-cell dt; single solves): thread block b owns the cells
+  // [patch[b].x, patch[b].x + patch[b].y) (at most kPatchCells, contiguous in device order),
+  // recomputes the records of its halo cells phcell[phptr[b] .. phptr[b + 1]) and evaluates the
+  // faces pface[pfptr[b] .. pfptr[b + 1]) that touch its cells (rows: own cells first, then
+  // halo).  patch_rows = the largest own + halo row count (row stride of the shared records).
+  int npatch, patch_rows;
+  const int2 *patch;
+  const int *phptr, *phcell, *pfptr;
+  const PatchFace *pface;
 };
+
+constexpr int kPatchCells = 128;
 
 constexpr int kWorkCellBlock = 128;
 constexpr int kMaxGroups = 256;  // block groups of the two-level grid reductions
@@ -122,6 +142,16 @@ int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxPara
 // next stage (non-final stages), bit 2 that next stage's supersonic-exit copy reads the stage state.
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                         int kind, int lts, int fuse_final, int keep_delu, int flags);
+// Patch form of one stage (gradients, face fluxes, gather and stage update in one kernel): reads
+// the primitives `prim_in` and writes the stage's primitives and ghosts to st.prim, which must be a
+// different buffer (blocks read their halo cells' primitives while others write theirs).  Same
+// flags as launch_gather_stage; ghost rows are carried to st.prim at every stage.
+int launch_patch_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                       int kind, int lts, int fuse_final, int keep_delu, int flags, const double *prim_in);
+// Dynamic shared memory of the patch kernel for m.patch_rows, and the opt-in to it (0 if the
+// device cannot give it).
+size_t patch_smem_bytes(const DevMesh &m);
+int patch_prepare(const DevMesh &m);
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S);
 int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const double *b, int n, double *out);

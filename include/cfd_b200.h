@@ -127,7 +127,10 @@ typedef struct {
   int exit_bc;               /* CFD_EXIT_*  (reference: Is_Exit_SubSonic) */
   int precision;             /* CFD_PREC_* */
   int reorder;               /* device cell numbering: 0 as given, 1 reverse Cuthill-McKee,
-                                2 patches of 128 cells grown breadth-first in RCM seed order */
+                                2 patches of 128 cells grown breadth-first in RCM seed order,
+                                3 patches of 128 cells by recursive coordinate bisection (needs
+                                centre vectors; face-based per-cell-dt forms then run each
+                                stage as one kernel per patch, option "patch_stage") */
   double cfl;                /* CFL */
   double limiter_zeta;       /* Limiter_Zeta */
   double limiter_zeta1;      /* Limiter_Zeta1 */
@@ -188,7 +191,10 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
  * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0/1/2, default 2),
  * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1),
- * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0).
+ * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0),
+ * "patch_stage" (with reorder 3, the face-based forms with a per-cell dt frozen per step run each
+ * stage as one kernel: a thread block per 128-cell patch computes the records, face fluxes, gather
+ * and update of its cells in shared memory; default 0, tried by cfd_autotune).
  * None of the options changes a result bit. */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
 /* Times every combination of the options above that applies to this configuration over `steps`
@@ -330,7 +336,7 @@ cfd_status cfd_mpnn_adam(float *param, const float *grad, float *m, float *v, in
                          float beta2, float eps, int step, void *stream);
 
 /* Accumulated device time of one kernel family ("flux", "stage", "bc", and for the face-based
- * forms "gradients", "faces", "gather_stage") over the launches made while option "profile" was
+ * forms "gradients", "faces", "gather_stage", "patch") over the launches made while option "profile" was
  * set (CUDA events on the context's stream around each launch). */
 cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, long long *launches);
 /* Number of unique faces of the face-based forms (0 for the per-cell reference forms). */
