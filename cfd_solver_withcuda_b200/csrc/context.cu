@@ -881,7 +881,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.recon_prim = cfg->reconstruct_primitive;
   fp.muscl = cfg->muscl && cfg->is_second_order;
   fp.lanes = 1;
-  fp.faces_shape = 2;
+  fp.faces_shape = 3;
   // WENO (Is_WENO): Explicit_Method falls back to the 1O/2O residual when any cell is not a quad
   // (src/Numerical_Method.cpp:31-55); Runge_Kutta_Method keeps WENO (zero flux on those cells).
   {
@@ -921,7 +921,8 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
     ctx->fp.lanes = static_cast<int>(value);
   }
   else if (n == "faces_shape") {
-    if (value != 0.0 && value != 1.0 && value != 2.0) return fail(CFD_ERR_BAD_ARG, "faces_shape must be 0, 1 or 2");
+    if (value != 0.0 && value != 1.0 && value != 2.0 && value != 3.0 && value != 4.0)
+      return fail(CFD_ERR_BAD_ARG, "faces_shape must be 0, 1, 2, 3 or 4");
     ctx->fp.faces_shape = static_cast<int>(value);
   }
   else if (n == "pdl") ctx->dm.pdl = value != 0.0;
@@ -1306,7 +1307,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   };
   std::vector<Cand> cands;
   if (ctx->dm.NF > 0) {
-    for (int f = 0; f < 3; f++)
+    for (int f = 0; f < 5; f++)
       for (int g = 0; g < 2; g++)
         for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, 0.0});
     if (ctx->dm.npatch > 0)

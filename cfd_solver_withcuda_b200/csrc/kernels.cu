@@ -848,7 +848,7 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
 }
 
 template <typename T, int DISS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
+__global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m, DevState st, FluxParams fp) {
   pdl_enter();
   const int i = item_index(m.fblk, m.NF);
   if (i >= m.NF || step_done(st.ctl)) return;
@@ -1200,7 +1200,9 @@ __device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[
 // update of k_stage in one pass, so the residual never leaves registers on its way to the update
 // (it is still stored for downloads).  At the final stage the error norms, the step's Min_dt and
 // the Total_Time epilogue.
-__global__ void __launch_bounds__(kFluxBlock) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
+// 80 registers (6 blocks of 128 per SM, 24 warps) without spilling; the unbounded build takes 84
+// (5 blocks) and measured 9 % slower on B200.
+__global__ void __launch_bounds__(kFluxBlock, 6) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
                                                              int kind, int lts, int fuse_final, int keep_delu,
                                                              int flags) {
   pdl_enter();
@@ -1738,12 +1740,16 @@ void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st
 }
 
 // Launch shapes of the face kernel (identical results).  The double Roe kernel needs 86
-// registers: 256-thread blocks then fit 2 per SM (16 warps), 256-thread blocks capped at 80
-// registers fit 3 (24 warps, a few bytes of spill), 128-thread blocks fit 5 (20 warps).  Work
-// lists fix 256 faces per block, so shape 2 falls back to shape 1 there.
+// registers: 256-thread blocks then fit 2 per SM (16 warps, shape 0), 256-thread blocks capped
+// at 80 registers fit 3 (24 warps, a few bytes of spill; shape 1), 128-thread blocks fit 5 (20
+// warps; shape 2), 128-thread blocks capped at 72 or 64 registers fit 7 or 8 (28 or 32 warps,
+// 44 or 88 bytes of spill held in L1; shapes 3 and 4).  Work lists fix 256 faces per block, so
+// shapes 2-4 fall back to shape 1 there.
 template <typename T>
 void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  if (fp.faces_shape == 2 && !m.fblk) launch_faces_b<T, 1>(s, nblk(m.NF, 128), 128, m, st, fp);
+  if (fp.faces_shape == 4 && !m.fblk) launch_faces_b<T, 8>(s, nblk(m.NF, 128), 128, m, st, fp);
+  else if (fp.faces_shape == 3 && !m.fblk) launch_faces_b<T, 7>(s, nblk(m.NF, 128), 128, m, st, fp);
+  else if (fp.faces_shape == 2 && !m.fblk) launch_faces_b<T, 1>(s, nblk(m.NF, 128), 128, m, st, fp);
   else if (fp.faces_shape >= 1) launch_faces_b<T, 3>(s, g, 256, m, st, fp);
   else launch_faces_b<T, 1>(s, g, 256, m, st, fp);
 }

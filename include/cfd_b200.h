@@ -189,7 +189,7 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "use_graph" (replay pseudo-steps from a captured CUDA graph, default 1),
  * "profile" (time every launch with CUDA events; disables graph replay, default 0),
  * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
- * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0/1/2, default 2),
+ * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0-4, default 3),
  * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1),
  * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0),
  * "patch_stage" (with reorder 3, the face-based forms with a per-cell dt frozen per step run each

@@ -293,7 +293,8 @@ def test_deterministic_and_graph_equivalent():
 
 OPTION_SETS = [dict(fuse_gather=0, faces_shape=0), dict(fuse_gather=1, faces_shape=1),
                dict(fuse_gather=1, faces_shape=2, use_graph=0), dict(fuse_gather=0, faces_shape=2),
-               dict(pdl=1), dict(pdl=1, use_graph=0, fuse_gather=0)]
+               dict(pdl=1), dict(pdl=1, use_graph=0, fuse_gather=0), dict(faces_shape=4, pdl=1),
+               dict(faces_shape=4, fuse_gather=0), dict(faces_shape=2)]
 
 
 @pytest.mark.parametrize("form", ["grad_muscl_minmod_ssp_lts", "grad_muscl_ausm_fp32_ssp_lts", "grad_muscl_hllc_minmod"])
@@ -341,7 +342,7 @@ def test_autotune_keeps_state_and_bits():
     a.step(3)
     before = a.download()
     report = a.autotune(steps=5)
-    assert report.count("ms/step") == 12 and "(chosen)" in report
+    assert report.count("ms/step") == 20 and "(chosen)" in report
     check_state(a.download(), before, "after autotune")
     a.step(10)
     b = cb.Solver(m, cfg)

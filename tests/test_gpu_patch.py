@@ -106,7 +106,7 @@ def test_patch_option_and_autotune():
     a.step(3)
     before = a.download()
     report = a.autotune(steps=5)
-    assert report.count("ms/step") == 14 and report.count("patch_stage=1") == 2, report
+    assert report.count("ms/step") == 22 and report.count("patch_stage=1") == 2, report
     check_state(a.download(), before, "after autotune")
     a.step(10)
     b = cb.Solver(m, cfg)
