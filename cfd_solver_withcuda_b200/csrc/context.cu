@@ -328,7 +328,10 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
       const bool fused = ctx->fuse_gather && (lts == 1 || lts == 2);
       {
         TimedScope ts(ctx, TK_GRAD);
-        n += launch_muscl_gradients(s, m, st, ctx->fp, fused ? 1 : 0);
+        // del_t is formed where a stage uses it (lts 1, or the first stage, which freezes it) and
+        // at the last stage, whose value is the Cells[].del_t a download returns.
+        const bool with_dt = fused && (lts == 1 || k == 0 || k == p.n - 1);
+        n += launch_muscl_gradients(s, m, st, ctx->fp, with_dt ? 1 : 0);
       }
       { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
       if (fused) {

@@ -1216,7 +1216,8 @@ __global__ void __launch_bounds__(kFluxBlock, 6) k_gather_stage(DevMesh m, DevSt
     // fewer resident warps) measured slower on B200.
     double R[4], den = 0.0;
     gather_faces<false>(m, st, c, R, den);
-    dtu = stage_cell(m, st, bp, c, R, st.dtc[c], kind, lts, fuse_final, keep_delu, flags, e);
+    const double dtc = (lts == 1 || first_kind(kind)) ? st.dtc[c] : 0.0;  // the only stages that use it
+    dtu = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
   }
   if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
