@@ -851,7 +851,9 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.Racc, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   }
   if (cfg->muscl) {
-    if ((s = ctx_alloc(ctx, (void **)&st.rec, 12 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
+    if ((s = ctx_alloc(ctx, (void **)&st.rec, 8 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+    if ((s = ctx_alloc(ctx, (void **)&st.q4, (size_t)NT * sizeof(double4))) != CFD_OK) return bail(s);
+    if (cudaMemset(st.q4, 0, (size_t)NT * sizeof(double4)) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
   }
   if (m.NF > 0) {
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
@@ -1292,6 +1294,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   std::vector<Part> parts = {{st.U, 4 * NT}, {st.S, 4 * NP}, {st.prim, 5 * NT}, {st.R, 4 * NP}, {st.dtc, NP},
                              {st.dtk, NP},    {st.dU, 4 * NP}, {st.ctl, (size_t)CTL_SIZE}};
   if (st.Racc) parts.push_back({st.Racc, 4 * NP});
+  if (st.q4) parts.push_back({reinterpret_cast<double *>(st.q4), 4 * NT});
   size_t total = 0;
   for (const Part &q : parts) total += q.n;
   double *snap = nullptr;

@@ -73,12 +73,13 @@ __device__ __forceinline__ void flag_bad(int *status, int cell) {
   atomicCAS(&status[0], 0, 3 /* CFD_ERR_NONPHYSICAL */);
 }
 
-__device__ __forceinline__ void store_prim(double *prim, int NT, int c, const Prim &q) {
+__device__ __forceinline__ void store_prim(double *prim, double4 *q4, int NT, int c, const Prim &q) {
   prim[c] = q.rho;
   prim[NT + c] = q.u;
   prim[2 * NT + c] = q.v;
   prim[3 * NT + c] = q.p;
   prim[4 * NT + c] = q.a;
+  if (q4) q4[c] = make_double4(q.rho, q.u, q.v, q.p);
 }
 
 __device__ __forceinline__ double warp_min(double v) {
@@ -282,7 +283,7 @@ __global__ void k_prim_all(DevMesh m, DevState st) {
   const double *U = st.U;
   Prim q;
   bool ok = eos_prim(U[c], U[m.NT + c], U[2 * m.NT + c], U[3 * m.NT + c], q);
-  store_prim(st.prim, m.NT, c, q);
+  store_prim(st.prim, st.q4, m.NT, c, q);
   if (!ok) flag_bad(st.status, c);
 }
 
@@ -413,7 +414,7 @@ __device__ __forceinline__ void bc_entry(const DevMesh &m, DevState &st, const B
   U[3 * NT + g] = G3;
   Prim q;
   bool ok = eos_prim(G0, G1, G2, G3, q);
-  store_prim(st.prim, NT, g, q);
+  store_prim(st.prim, st.q4, NT, g, q);
   if (!ok) flag_bad(st.status, g);
 }
 
@@ -856,12 +857,12 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
   const int c = m.fo[i], N = m.fn[i];
   const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
   const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
-  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)c);
-  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 12 * (size_t)N);
-  const double4 c0 = rc[0], c1 = rc[1], c2 = rc[2];
-  const double4 n0 = rn[0];
+  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)c);
+  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)N);
+  const double4 c0 = st.q4[c], c1 = rc[0], c2 = rc[1];
+  const double4 n0 = st.q4[N];
   const bool nphys = N < NP;
-  const double4 n1 = nphys ? rn[1] : c1, n2 = nphys ? rn[2] : c2;
+  const double4 n1 = nphys ? rn[0] : c1, n2 = nphys ? rn[1] : c2;
   st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy);
 }
 
@@ -1068,7 +1069,7 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
     for (int k = 0; k < 4; k++) st.S[k * NP + c] = out[k];
     Prim q;
     bool ok = eos_prim(out[0], out[1], out[2], out[3], q);
-    store_prim(st.prim, NT, c, q);
+    store_prim(st.prim, st.q4, NT, c, q);
     if (!ok) flag_bad(st.status, c);
   } else {
     // dU and U^{n+1}: the forms that produce U^{n+1} directly keep it exactly (dU = U^{n+1} - U^n
@@ -1098,7 +1099,7 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
       }
       Prim q;
       bool ok = eos_prim(Un[0], Un[1], Un[2], Un[3], q);
-      store_prim(st.prim, NT, c, q);
+      store_prim(st.prim, st.q4, NT, c, q);
       if (!ok) flag_bad(st.status, c);
     }
   }
@@ -1252,7 +1253,7 @@ __global__ void __launch_bounds__(kBlock) k_update(DevMesh m, DevState st, int f
   }
   Prim q;
   bool ok = eos_prim(u[0], u[1], u[2], u[3], q);
-  store_prim(st.prim, NT, c, q);
+  store_prim(st.prim, st.q4, NT, c, q);
   if (!ok) flag_bad(st.status, c);
 }
 
@@ -1283,9 +1284,10 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // slots of the [4][NP] neighbour table are read without waiting for the face count (an unused
 // slot reads the cell itself), so every neighbour's loads are in flight together; the sums run
 // over the cell's faces in order.
-template <bool DT>
-__device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *__restrict__ prim, int c,
-                                               const double qc[4], double g[8], double &den) {
+template <bool DT, bool Q4 = false>
+__device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *__restrict__ prim,
+                                               const double4 *__restrict__ q4, int c, const double qc[4], double g[8],
+                                               double &den) {
   const int NP = m.NP, NT = m.NT;
   const int nf = m.nf[c];
   const double ia = m.inv_area[c];
@@ -1298,9 +1300,18 @@ __device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *_
   }
   double qn[4][4];
 #pragma unroll
-  for (int f = 0; f < 4; f++)
+  for (int f = 0; f < 4; f++) {
+    if (Q4) {
+      const double4 v = q4[nb[f]];
+      qn[f][0] = v.x;
+      qn[f][1] = v.y;
+      qn[f][2] = v.z;
+      qn[f][3] = v.w;
+    } else {
 #pragma unroll
-    for (int k = 0; k < 4; k++) qn[f][k] = prim[k * NT + nb[f]];
+      for (int k = 0; k < 4; k++) qn[f][k] = prim[k * NT + nb[f]];
+    }
+  }
 #pragma unroll
   for (int k = 0; k < 8; k++) g[k] = 0.0;
   den = 0.0;
@@ -1325,9 +1336,10 @@ __device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *_
   for (int k = 0; k < 8; k++) g[k] = g[k] * ia;
 }
 
-// Records of the face-based forms: (rho, u, v, p) and their Green-Gauss gradients, the face
-// value being the mean of the two cell values, ghost cells included (their values carry the
-// boundary state).  Ghost rows get (rho, u, v, p) only.
+// Gradient records of the face-based forms: the Green-Gauss gradients of (rho, u, v, p) of every
+// physical cell, the face value being the mean of the two cell values (a ghost neighbour's value
+// carries the boundary state); the states themselves are read from q4.  Work-list entries cover
+// record rows NP..NT-1 too (ghost rows), which have nothing to do.
 // DT: also del_t of each physical cell (the fused per-cell-dt forms; their Min_dt is formed in
 // the last stage's reduction).
 template <bool DT>
@@ -1336,20 +1348,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
   const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
   if (step_done(st.ctl)) return;
-  if (c < NT) {
-    double qc[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) qc[k] = st.prim[k * NT + c];
-    double4 *r = reinterpret_cast<double4 *>(st.rec + 12 * (size_t)c);
-    r[0] = make_double4(qc[0], qc[1], qc[2], qc[3]);
-    if (c < NP) {
-      double g[8], den;
-      cell_gradients<DT>(m, st.prim, c, qc, g, den);
-      r[1] = make_double4(g[0], g[1], g[2], g[3]);
-      r[2] = make_double4(g[4], g[5], g[6], g[7]);
-      if (DT) st.dtc[c] = cell_dt(m, fp, c, den);
-    }
+  if (c < NP) {
+    const double4 v = st.q4[c];
+    const double qc[4] = {v.x, v.y, v.z, v.w};
+    double4 *r = reinterpret_cast<double4 *>(st.rec + 8 * (size_t)c);
+    double g[8], den;
+    cell_gradients<DT, true>(m, st.prim, st.q4, c, qc, g, den);
+    r[0] = make_double4(g[0], g[1], g[2], g[3]);
+    r[1] = make_double4(g[4], g[5], g[6], g[7]);
+    if (DT) st.dtc[c] = cell_dt(m, fp, c, den);
   }
+  (void)NT;
 }
 
 // Patch form of one stage of the face-based per-cell-dt forms: one thread block per patch of up
@@ -1393,7 +1402,7 @@ __global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevSt
     double qc[4], g[8], den;
 #pragma unroll
     for (int k = 0; k < 4; k++) qc[k] = pin[k * NT + c];
-    cell_gradients<true>(m, pin, c, qc, g, den);
+    cell_gradients<true>(m, pin, nullptr, c, qc, g, den);
 #pragma unroll
     for (int k = 0; k < 4; k++) srec[k * rows + l] = qc[k];
 #pragma unroll
@@ -1469,6 +1478,7 @@ __global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevSt
       const int g = m.bnd[m.bidx[q]].w;
 #pragma unroll
       for (int k = 0; k < 5; k++) st.prim[k * NT + g] = pin[k * NT + g];
+      if (st.q4) st.q4[g] = make_double4(pin[g], pin[NT + g], pin[2 * NT + g], pin[3 * NT + g]);
     }
     dtu = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
   }

@@ -7,8 +7,8 @@
 //   unique faces [NF] (face-based forms): owner, neighbour, owner-side geometry; cell slot -> face
 //   state, component-major SoA: U[4][NT] (U^n on physical rows, boundary values on ghost rows),
 //   S[4][NP] (RK stage state), prim[5][NT] (rho, u, v, p, a), R[4][NP] (net flux),
-//   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU); records rec[NT][12] and face fluxes F[NF]
-//   (face-based forms)
+//   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU); face-based forms: the primitives again as
+//   q4[NT] (rho, u, v, p), gradients rec[NP][8] and face fluxes F[NF]
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -81,8 +81,10 @@ struct DevState {
   double *dtc;   // [NP]
   double *dtk;   // [NP] dt kept for the whole step (RK4 / SSP with LTS)
   double *dU;    // [4][NP]
-  double *rec;   // [NT][12] per-cell records of the face-based forms: rho, u, v, p and the
-                 // Green-Gauss gradients (x, y) of each (physical cells), 96 B = 3 x 32 B
+  double *rec;   // [NP][8] Green-Gauss gradients (x, y) of rho, u, v, p (face-based forms),
+                 // 64 B = 2 x 32 B per cell
+  double4 *q4;   // [NT] (rho, u, v, p) of every row, written wherever the primitives are, so the
+                 // face-based kernels fetch a neighbour's state with one 32-byte load (or null)
   double4 *F;    // [NF] face fluxes (face-based forms)
   // reduction / control block (see CtrlIdx)
   double *ctl;
