@@ -137,13 +137,13 @@ def face_bytes_per_cell():
 def gather_stage_bytes_per_cell():
     """Algorithmic DRAM bytes per cell of the fused gather + stage kernel k_gather_stage, averaged
     over the three TVD-RK3 stages with frozen local dt (face fluxes counted per face in
-    gather_stage_bytes_per_face; del_t comes from the gradient pass).  Every stage reads nf 4,
-    face ids 16, del_t 8, 1/area 8, U^n 32 and writes R 32 and the primitives 40; stage 1 also
-    reads the boundary-entry offsets 4 and writes the frozen dt 8 and the stage state 32; stage 2
-    reads the offsets 4, the stage state 32 and the frozen dt 8 and writes the stage state 32;
-    stage 3 reads the stage state 32 and the frozen dt 8 and writes U 32.  Per stage 184, 216
-    and 212 B (the ghost rows the owner threads write are < 0.1 % and left out)."""
-    return (184 + 216 + 212) / 3.0
+    gather_stage_bytes_per_face).  Every stage reads nf 4, face ids 16, 1/area 8, U^n 32 and writes
+    R 32, the primitive planes 40 and the (rho, u, v, p) row 32; stage 1 also reads del_t 8 and the
+    boundary-entry offsets 4 and writes the frozen dt 8 and the stage state 32; stage 2 reads the
+    offsets 4, the stage state 32 and the frozen dt 8 and writes the stage state 32; stage 3 reads
+    the stage state 32 and the frozen dt 8 and writes U 32.  Per stage 216, 240 and 236 B (the
+    ghost rows the owner threads write are < 0.1 % and left out)."""
+    return (216 + 240 + 236) / 3.0
 
 
 def patch_bytes_per_cell():
