@@ -110,6 +110,8 @@ SIGNATURES = {
     "cfd_download": (_I, [_P, _DP, _DP, _DP, _DP, _DP]),
     "cfd_download_stage_state": (_I, [_P, _DP]),
     "cfd_download_U": (_I, [_P, _DP]),
+    "cfd_upload_state_async": (_I, [_P, _DP, _I]),
+    "cfd_download_U_async": (_I, [_P, _DP]),
     "cfd_gradient": (_I, [_P, _I, _DP]),
     "cfd_eval_limiter": (_I, [_I, _DP, _DP, _I, _DP, _I]),
     "cfd_write_solution": (_I, [_P, ctypes.c_char_p, ctypes.POINTER(_I), _I]),
@@ -266,6 +268,7 @@ class Solver:
         _check(lib().cfd_create(ctypes.byref(mesh.desc), ctypes.byref(config), ctypes.byref(h)))
         self._h = h
         self.info = StepInfo()
+        self._pending = []  # host arrays of enqueued asynchronous copies, kept alive until sync()
 
     def close(self):
         if getattr(self, "_h", None):
@@ -338,8 +341,26 @@ class Solver:
     def step_async(self, n):
         _check(lib().cfd_step_async(self._h, n))
 
+    def upload_state_async(self, U):
+        """Enqueues the upload of all NP+NG rows (cfd_upload_state_async) and returns; U (float64,
+        C order, best page-locked) is kept alive until sync()."""
+        if not (isinstance(U, np.ndarray) and U.dtype == np.float64 and U.flags.c_contiguous):
+            raise ValueError("upload_state_async needs a C-contiguous float64 array")
+        _check(lib().cfd_upload_state_async(self._h, _dp(U), U.shape[0]))
+        self._pending.append(U)
+
+    def download_U_async(self, out):
+        """Enqueues the download of U_Cells into `out` ([NP+NG, 4] float64, best page-locked),
+        which holds the result after sync()."""
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous and
+                out.size >= 4 * self.mesh.n_total):
+            raise ValueError("download_U_async needs a C-contiguous float64 array of NP+NG rows")
+        _check(lib().cfd_download_U_async(self._h, _dp(out)))
+        self._pending.append(out)
+
     def sync(self):
         _check(lib().cfd_sync(self._h, ctypes.byref(self.info)))
+        self._pending = []
         return self.info
 
     def write_solution(self, path, header=(0, 0, 0)):

@@ -963,6 +963,25 @@ cfd_status cfd_upload_state(cfd_ctx *ctx, const double *U, int n) {
   return sync_status(ctx, nullptr);
 }
 
+cfd_status cfd_upload_state_async(cfd_ctx *ctx, const double *U, int n) {
+  if (!ctx || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  if (n != ctx->NT) return fail(CFD_ERR_BAD_ARG, "the asynchronous upload takes all NP+NG rows");
+  CUDA_TRY(cudaMemcpyAsync(ctx->d_stage, U, 4 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->launches += launch_import_aos(ctx->stream, ctx->d_stage, ctx->d_perm, ctx->NP, ctx->NT, ctx->ds.U);
+  ctx->launches += launch_prim_all(ctx->stream, ctx->dm, ctx->ds);
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = false;
+  return CFD_OK;
+}
+
+cfd_status cfd_download_U_async(cfd_ctx *ctx, double *U) {
+  if (!ctx || !U) return fail(CFD_ERR_BAD_ARG, "null argument");
+  ctx->launches += launch_export_aos(ctx->stream, ctx->ds.U, ctx->d_perm, ctx->NP, ctx->NT, ctx->NT, ctx->d_stage);
+  CUDA_TRY(cudaMemcpyAsync(U, ctx->d_stage, 4 * (size_t)ctx->NT * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaGetLastError());
+  return CFD_OK;
+}
+
 // Conserved rows U_Cells [(NP+NG)*4] in reference order, gathered on the device.
 cfd_status cfd_download_U(cfd_ctx *ctx, double *U) {
   if (!ctx || !U) return fail(CFD_ERR_BAD_ARG, "null argument");

@@ -221,6 +221,14 @@ cfd_status cfd_download(cfd_ctx *ctx, double *U, double *prim, double *dt, doubl
 /* Conserved rows U_Cells [(NP+NG)*4] only (gathered into reference order on the device; a
  * pinned destination gives full PCIe/C2C bandwidth). */
 cfd_status cfd_download_U(cfd_ctx *ctx, double *U);
+/* Asynchronous forms of cfd_upload_state (all NP+NG rows) and cfd_download_U for pipelines of
+ * independent solves: the copy and its gather kernels are enqueued on the context's stream and the
+ * call returns at once; cfd_sync waits and reports the status (a non-physical uploaded state
+ * included).  U must stay valid, and unchanged for an upload, until then, and must be page-locked
+ * for the copy to overlap other work: with two contexts on two streams, one solve's copies run
+ * while the other computes.  No reference counterpart (the reference keeps its state on the host). */
+cfd_status cfd_upload_state_async(cfd_ctx *ctx, const double *U, int n);
+cfd_status cfd_download_U_async(cfd_ctx *ctx, double *U);
 /* Stage state [NP*4]: after Runge_Kutta_Method it holds U_Cells_RK_2 (the stage buffer is
  * shared by U_Cells_RK_1 and U_Cells_RK_2, src/Numerical_Method.cpp:372-416). */
 cfd_status cfd_download_stage_state(cfd_ctx *ctx, double *S);

@@ -349,3 +349,40 @@ def test_autotune_keeps_state_and_bits():
     b.upload_state(U0)
     b.step(13)
     check_state(a.download(), b.download(), "tuned vs untuned")
+
+
+def test_async_upload_download_pipeline():
+    """cfd_upload_state_async / cfd_download_U_async on two contexts taking alternate one-step jobs
+    from different start states give the same bits as the blocking calls on one context."""
+    import torch
+    case = CASES["cyl_roe2_lts"]
+    m = make_mesh(case)
+    U0 = initial_state(case, m)
+    cfg = solver_config(case, **ADDITIVE["grad_muscl_minmod_ssp_lts"])
+    starts = [U0]
+    ref = cb.Solver(m, cfg)
+    ref.upload_state(U0)
+    for _ in range(3):
+        ref.step(7)
+        starts.append(ref.download_U())
+    want = []
+    for U in starts:
+        ref.upload_state(U)
+        ref.step(1)
+        want.append(ref.download_U())
+    pinned = [torch.from_numpy(U).pin_memory().numpy() for U in starts]
+    outs = [torch.empty(U0.shape, dtype=torch.float64).pin_memory().numpy() for _ in starts]
+    ctxs = [cb.Solver(m, cfg), cb.Solver(m, cfg)]
+    for j, U in enumerate(pinned):
+        c = ctxs[j % 2]
+        if j >= 2:
+            c.sync()
+        c.upload_state_async(U)
+        c.step_async(1)
+        c.download_U_async(outs[j])
+    for c in ctxs:
+        c.sync()
+    for j in range(len(starts)):
+        assert_bits_equal(outs[j], want[j], "job %d" % j)
+    with pytest.raises(RuntimeError):
+        ctxs[0].upload_state_async(np.ascontiguousarray(U0[:m.n_physical]))
