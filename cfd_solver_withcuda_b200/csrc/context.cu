@@ -201,6 +201,7 @@ struct cfd_ctx {
   int use_graph = 1;
   int fuse_gather = 1;  // face-based forms with per-cell dt: fused gather + stage update
   int patch_stage = 0;  // ... or, with patch tables (reorder 3), the one-kernel patch stage
+  bool ghost_private = false;  // every ghost row has one boundary entry and neighbours only its owner
   std::vector<int> patch_starts;  // first device cell of each patch (reorder 3)
   double *pbuf[2] = {nullptr, nullptr};  // stage primitives of the patch form ([5][NT] each)
   cudaGraphExec_t graph = nullptr;
@@ -305,7 +306,11 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
     const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
     const int lts = stage_lts(p, c, k);
     const int fin = (k == p.n - 1) ? fuse_final : 0;
-    if (!ghosts_written) {
+    // Fused face-based stages take the first stage's boundary conditions into the gradient pass
+    // (each cell applies its own entries before its gradient) when no ghost is shared.
+    const bool fused_faces = faces && ctx->fuse_gather && (lts == 1 || lts == 2);
+    const bool bc_in_grad = fused_faces && !patch && k == 0 && ctx->ghost_private;
+    if (!ghosts_written && !bc_in_grad) {
       TimedScope ts(ctx, TK_BC);
       n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
     }
@@ -331,7 +336,7 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
         // del_t is formed where a stage uses it (lts 1, or the first stage, which freezes it) and
         // at the last stage, whose value is the Cells[].del_t a download returns.
         const bool with_dt = fused && (lts == 1 || k == 0 || k == p.n - 1);
-        n += launch_muscl_gradients(s, m, st, ctx->fp, with_dt ? 1 : 0);
+        n += launch_muscl_gradients(s, m, st, ctx->fp, with_dt ? 1 : 0, bc_in_grad ? &ctx->bp : nullptr);
       }
       { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
       if (fused) {
@@ -781,6 +786,23 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   for (int e = 0; e < NB; e++) {
     const int *b = d->boundary + 4 * e;
     bnd[e] = make_int4(b[0], dev_of(ctx, b[1]), b[2], b[3]);
+  }
+  // A ghost row is private when it has exactly one boundary entry and only its owner cell lists it
+  // as a neighbour; then the owner's thread may apply that entry's boundary condition itself.
+  {
+    std::vector<int> owner(NT > NP ? NT - NP : 1, -1);
+    bool priv = true;
+    for (int e = 0; e < NB && priv; e++) {
+      const int g = bnd[e].w - NP;
+      if (owner[g] != -1) priv = false;
+      owner[g] = bnd[e].y;
+    }
+    for (int c = 0; c < NP && priv; c++)
+      for (int f = 0; f < nf[c]; f++) {
+        const int N = nbr[(size_t)f * NP + c];
+        if (N >= NP && owner[N - NP] != c) priv = false;
+      }
+    ctx->ghost_private = priv;
   }
   // Boundary entries grouped by (device) owner cell, in entry order within a cell.
   std::vector<int> bptr(NP + 1, 0), bidx(NB > 0 ? NB : 1, 0);

@@ -1284,10 +1284,10 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 // slots of the [4][NP] neighbour table are read without waiting for the face count (an unused
 // slot reads the cell itself), so every neighbour's loads are in flight together; the sums run
 // over the cell's faces in order.
+// q4 is not __restrict__: the first-stage gradient pass writes the ghost rows it then reads.
 template <bool DT, bool Q4 = false>
-__device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *__restrict__ prim,
-                                               const double4 *__restrict__ q4, int c, const double qc[4], double g[8],
-                                               double &den) {
+__device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *prim, const double4 *q4, int c,
+                                               const double qc[4], double g[8], double &den) {
   const int NP = m.NP, NT = m.NT;
   const int nf = m.nf[c];
   const double ia = m.inv_area[c];
@@ -1342,13 +1342,21 @@ __device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *_
 // record rows NP..NT-1 too (ghost rows), which have nothing to do.
 // DT: also del_t of each physical cell (the fused per-cell-dt forms; their Min_dt is formed in
 // the last stage's reduction).
+// with_bc: first stage of a step; each thread first applies the boundary conditions of its own
+// cell's boundary entries (Apply_Boundary_Conditions, as k_bc does), which is exact because a
+// ghost row depends only on its owner cell and is read by no other cell's gradient.
 template <bool DT>
-__global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevState st, FluxParams fp) {
+__global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevState st, FluxParams fp, BcParams bp,
+                                                               int with_bc) {
   pdl_enter();
   const int c = item_index(m.rblk, m.NT);
   const int NP = m.NP, NT = m.NT;
   if (step_done(st.ctl)) return;
   if (c < NP) {
+    if (with_bc) {
+      const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+      for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], 0, 0);
+    }
     const double4 v = st.q4[c];
     const double qc[4] = {v.x, v.y, v.z, v.w};
     double4 *r = reinterpret_cast<double4 *>(st.rec + 8 * (size_t)c);
@@ -1846,11 +1854,14 @@ int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, dou
   return 1;
 }
 
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt) {
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
+                           const BcParams *bc) {
   const int g = m.rblk ? m.n_rblk : nblk(m.NT, kBlock);
   if (m.rblk && g == 0) return 0;
-  if (with_dt) launch_k(m, k_muscl_gradients<true>, g, kBlock, s, m, st, fp);
-  else launch_k(m, k_muscl_gradients<false>, g, kBlock, s, m, st, fp);
+  const BcParams bp = bc ? *bc : BcParams{};
+  const int with_bc = bc ? 1 : 0;
+  if (with_dt) launch_k(m, k_muscl_gradients<true>, g, kBlock, s, m, st, fp, bp, with_bc);
+  else launch_k(m, k_muscl_gradients<false>, g, kBlock, s, m, st, fp, bp, with_bc);
   return 1;
 }
 

@@ -160,8 +160,11 @@ int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const doub
 int launch_eval_face_flux(cudaStream_t s, int scheme, int precision, const double *UL, const double *UR,
                           const double *nrm, const double *len, int n, double *F);
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad);
-// with_dt: also del_t of every physical cell (the fused per-cell-dt forms).
-int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt);
+// with_dt: also del_t of every physical cell (the fused per-cell-dt forms).  bc (or null): apply
+// the boundary conditions of each cell's boundary entries first (the first stage of a step, in
+// place of launch_bc; needs every ghost to neighbour only its owner cell).
+int launch_muscl_gradients(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int with_dt,
+                           const BcParams *bc = nullptr);
 int launch_amr_indicator(cudaStream_t s, const DevMesh &m, DevState &st, double *ind);
 int launch_set_ctl(cudaStream_t s, DevState &st, int idx, double v);
 // TagRefinableCells on the device; scratch holds >= 2 x 32 + 1024 bytes.
