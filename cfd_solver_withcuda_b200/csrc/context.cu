@@ -846,6 +846,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_upload(ctx, const_cast<int **>(&m.cface), cface)) != CFD_OK) return bail(s);
   }
 
+  m.wave_blocks = gather_stage_wave_blocks();
   if (!patches.empty()) {
     m.npatch = static_cast<int>(patches.size());
     m.patch_rows = patch_rows;

@@ -1203,22 +1203,41 @@ __device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[
 // the Total_Time epilogue.
 // 80 registers (6 blocks of 128 per SM, 24 warps) without spilling; the unbounded build takes 84
 // (5 blocks) and measured 9 % slower on B200.
-__global__ void __launch_bounds__(kFluxBlock, 6) k_gather_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp,
-                                                             int kind, int lts, int fuse_final, int keep_delu,
-                                                             int flags) {
+// STRIDED (the reducing last stage without work lists): a grid of one wave strides over the
+// cells, so the per-block fence and arrival count of the grid reduction is paid once per resident
+// block instead of once per 128 cells; each thread sums its cells' terms in cell order and the
+// grid is fixed per device, so the sums are reproducible.  Its accumulators take more registers
+// (5 blocks per SM).
+template <bool STRIDED>
+__global__ void __launch_bounds__(kFluxBlock, STRIDED ? 5 : 6) k_gather_stage(DevMesh m, DevState st, FluxParams fp,
+                                                                             BcParams bp, int kind, int lts,
+                                                                             int fuse_final, int keep_delu, int flags) {
   pdl_enter();
   const int NP = m.NP;
-  const int c = item_index(m.cblk, NP);
   if (step_done(st.ctl)) return;
   double dtu = 1e308 * 10.0;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (c < NP) {
-    // The residual gather is issued first; loading the state rows ahead of it (more registers,
-    // fewer resident warps) measured slower on B200.
-    double R[4], den = 0.0;
-    gather_faces<false>(m, st, c, R, den);
-    const double dtc = (lts == 1 || first_kind(kind)) ? st.dtc[c] : 0.0;  // the only stages that use it
-    dtu = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
+  if (!STRIDED) {
+    const int c = item_index(m.cblk, NP);
+    if (c < NP) {
+      // The residual gather is issued first; loading the state rows ahead of it (more registers,
+      // fewer resident warps) measured slower on B200.
+      double R[4], den = 0.0;
+      gather_faces<false>(m, st, c, R, den);
+      const double dtc = (lts == 1 || first_kind(kind)) ? st.dtc[c] : 0.0;  // the only stages that use it
+      dtu = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
+    }
+  } else {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < NP; c += gridDim.x * blockDim.x) {
+      double R[4], den = 0.0;
+      gather_faces<false>(m, st, c, R, den);
+      const double dtc = (lts == 1 || first_kind(kind)) ? st.dtc[c] : 0.0;
+      double ec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      const double dt = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, ec);
+#pragma unroll
+      for (int k = 0; k < 8; k++) e[k] += ec[k];
+      dtu = dt < dtu ? dt : dtu;
+    }
   }
   if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
@@ -1780,10 +1799,23 @@ int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParam
   return 1;
 }
 
+int gather_stage_wave_blocks() {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_stage<true>, kFluxBlock, 0) != cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
 int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                         int kind, int lts, int fuse_final, int keep_delu, int flags) {
   const int g = m.cblk ? m.n_cblk : nblk(m.NP, kFluxBlock);
-  launch_k(m, k_gather_stage, g, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  if (!m.cblk && fuse_final && final_kind(kind) && m.wave_blocks > 0 && g > m.wave_blocks)
+    launch_k(m, k_gather_stage<true>, m.wave_blocks, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu,
+             flags);
+  else
+    launch_k(m, k_gather_stage<false>, g, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
   return 1;
 }
 

@@ -62,6 +62,9 @@ struct DevMesh {
   // halo).  patch_rows = the largest own + halo row count (row stride of the shared records).
   int npatch, patch_rows;
   const int2 *patch;
+  // Blocks of k_gather_stage resident on the whole device at once (SMs x blocks per SM): the grid
+  // of its reducing stage (0 = one block per 128 cells).
+  int wave_blocks;
   const int *phptr, *phcell, *pfptr;
   const PatchFace *pface;
 };
@@ -154,6 +157,8 @@ int launch_patch_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Flu
 // device cannot give it).
 size_t patch_smem_bytes(const DevMesh &m);
 int patch_prepare(const DevMesh &m);
+// SMs x resident blocks of k_gather_stage on the current device (0 if unknown).
+int gather_stage_wave_blocks();
 int launch_error(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S);
 int launch_eval_limiter(cudaStream_t s, int limiter, const double *a, const double *b, int n, double *out);
