@@ -1092,8 +1092,8 @@ __device__ __forceinline__ void cell_update_in(const DevMesh &m, DevState &st, i
     if (fuse_final) {
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        e[k] = err_term(du[k], Un[k]);
-        e[4 + k] = Rk[k] * Rk[k];
+        e[k] += err_term(du[k], Un[k]);  // callers start e at 0 (strided callers sum their cells)
+        e[4 + k] += Rk[k] * Rk[k];
         st.U[k * NT + c] = nu[k];
         Un[k] = nu[k];
       }
@@ -1206,10 +1206,10 @@ __device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[
 // STRIDED (the reducing last stage without work lists): a grid of one wave strides over the
 // cells, so the per-block fence and arrival count of the grid reduction is paid once per resident
 // block instead of once per 128 cells; each thread sums its cells' terms in cell order and the
-// grid is fixed per device, so the sums are reproducible.  Its accumulators take more registers
-// (5 blocks per SM).
+// grid is fixed per device, so the sums are reproducible.  Its accumulators spill 64 bytes at the
+// same 80-register cap, which measured faster than 96 registers at 5 blocks per SM.
 template <bool STRIDED>
-__global__ void __launch_bounds__(kFluxBlock, STRIDED ? 5 : 6) k_gather_stage(DevMesh m, DevState st, FluxParams fp,
+__global__ void __launch_bounds__(kFluxBlock, 6) k_gather_stage(DevMesh m, DevState st, FluxParams fp,
                                                                              BcParams bp, int kind, int lts,
                                                                              int fuse_final, int keep_delu, int flags) {
   pdl_enter();
@@ -1232,10 +1232,7 @@ __global__ void __launch_bounds__(kFluxBlock, STRIDED ? 5 : 6) k_gather_stage(De
       double R[4], den = 0.0;
       gather_faces<false>(m, st, c, R, den);
       const double dtc = (lts == 1 || first_kind(kind)) ? st.dtc[c] : 0.0;
-      double ec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      const double dt = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, ec);
-#pragma unroll
-      for (int k = 0; k < 8; k++) e[k] += ec[k];
+      const double dt = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
       dtu = dt < dtu ? dt : dtu;
     }
   }
