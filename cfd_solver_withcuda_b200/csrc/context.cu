@@ -1531,7 +1531,7 @@ static cfd_status batch_tables(cfd_batch *b) {
   for (int i = 0; i < b->n; i++) {
     if (!b->active[i]) continue;
     chunks(t[0], b->cs[i], b->ce[i], kWorkCellBlock);
-    chunks(t[1], b->fs[i], b->fe[i], kWorkItemBlock);
+    chunks(t[1], b->fs[i], b->fe[i], kWorkFaceBlock);
     chunks(t[2], b->bs[i], b->be[i], kWorkItemBlock);
     chunks(t[3], b->cs[i], b->ce[i], kWorkItemBlock);
     chunks(t[3], b->gs[i], b->ge[i], kWorkItemBlock);
@@ -1660,7 +1660,7 @@ cfd_status cfd_batch_create(int n, const cfd_mesh_desc *meshes, const double *in
   long long cap[4] = {0, 0, 0, 0};
   for (int i = 0; i < n; i++) {
     cap[0] += (b->ce[i] - b->cs[i] + kWorkCellBlock - 1) / kWorkCellBlock;
-    cap[1] += (b->fe[i] - b->fs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
+    cap[1] += (b->fe[i] - b->fs[i] + kWorkFaceBlock - 1) / kWorkFaceBlock;
     cap[2] += (b->be[i] - b->bs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
     cap[3] += (b->ce[i] - b->cs[i] + kWorkItemBlock - 1) / kWorkItemBlock + (b->ge[i] - b->gs[i] + kWorkItemBlock - 1) / kWorkItemBlock;
   }

@@ -1721,14 +1721,14 @@ int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const i
 }
 
 template <typename T>
-void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const FluxParams &fp);
+void launch_faces_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
   if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st, fp, 0);
   if (fp.second_order && fp.muscl && m.NF > 0) {
-    if (fp.precision == 1) launch_faces_t<float>(s, nblk(m.NF, 256), m, st, fp);
-    else launch_faces_t<double>(s, nblk(m.NF, 256), m, st, fp);
+    if (fp.precision == 1) launch_faces_t<float>(s, m, st, fp);
+    else launch_faces_t<double>(s, m, st, fp);
     k_gather<<<nblk(m.NP, kFluxBlock), kFluxBlock, 0, s>>>(m, st, fp);
     return n + 2;
   }
@@ -1778,21 +1778,24 @@ void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st
 // registers: 256-thread blocks then fit 2 per SM (16 warps, shape 0), 256-thread blocks capped
 // at 80 registers fit 3 (24 warps, a few bytes of spill; shape 1), 128-thread blocks fit 5 (20
 // warps; shape 2), 128-thread blocks capped at 72 or 64 registers fit 7 or 8 (28 or 32 warps,
-// 44 or 88 bytes of spill held in L1; shapes 3 and 4).  Work lists fix 256 faces per block, so
-// shapes 2-4 fall back to shape 1 there.
+// 44 or 88 bytes of spill held in L1; shapes 3 and 4).  Work lists hold kWorkFaceBlock (128)
+// faces per block, so with them every shape runs 128-thread blocks.
 template <typename T>
-void launch_faces_t(cudaStream_t s, int g, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  if (fp.faces_shape == 4 && !m.fblk) launch_faces_b<T, 8>(s, nblk(m.NF, 128), 128, m, st, fp);
-  else if (fp.faces_shape == 3 && !m.fblk) launch_faces_b<T, 7>(s, nblk(m.NF, 128), 128, m, st, fp);
-  else if (fp.faces_shape == 2 && !m.fblk) launch_faces_b<T, 1>(s, nblk(m.NF, 128), 128, m, st, fp);
-  else if (fp.faces_shape >= 1) launch_faces_b<T, 3>(s, g, 256, m, st, fp);
-  else launch_faces_b<T, 1>(s, g, 256, m, st, fp);
+void launch_faces_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
+  const bool wl = m.fblk != nullptr;
+  const int g128 = wl ? m.n_fblk : nblk(m.NF, 128);
+  const int g = wl ? m.n_fblk : nblk(m.NF, 256), b = wl ? 128 : 256;
+  if (fp.faces_shape == 4) launch_faces_b<T, 8>(s, g128, 128, m, st, fp);
+  else if (fp.faces_shape == 3) launch_faces_b<T, 7>(s, g128, 128, m, st, fp);
+  else if (fp.faces_shape == 2) launch_faces_b<T, 1>(s, g128, 128, m, st, fp);
+  else if (fp.faces_shape == 1) launch_faces_b<T, 3>(s, g, b, m, st, fp);
+  else launch_faces_b<T, 1>(s, g, b, m, st, fp);
 }
 
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  const int g = m.fblk ? m.n_fblk : nblk(m.NF, 256);
-  if (fp.precision == 1) launch_faces_t<float>(s, g, m, st, fp);
-  else launch_faces_t<double>(s, g, m, st, fp);
+  if (m.fblk && m.n_fblk == 0) return 0;
+  if (fp.precision == 1) launch_faces_t<float>(s, m, st, fp);
+  else launch_faces_t<double>(s, m, st, fp);
   return 1;
 }
 

@@ -43,7 +43,7 @@ struct DevMesh {
   const double *fnx, *fny, *fdl, *fdx, *fdy;
   const int *cface;  // [4][NP]
   // Optional work lists (batched solves): each entry is one thread block's [start, end) range of
-  // cells (128 per block), faces (256), boundary entries (256) or record rows (256, physical and
+  // cells (128 per block), faces (128), boundary entries (256) or record rows (256, physical and
   // ghost rows); null = all items.
   const int2 *cblk, *fblk, *bblk, *rblk;
   int n_cblk, n_fblk, n_bblk, n_rblk;
@@ -74,6 +74,7 @@ constexpr int kPatchCells = 128;
 constexpr int kWorkCellBlock = 128;
 constexpr int kMaxGroups = 256;  // block groups of the two-level grid reductions
 constexpr int kWorkItemBlock = 256;
+constexpr int kWorkFaceBlock = 128;  // faces per work-list entry (the face kernel's 128-thread shapes)
 
 struct DevState {
   double *U;     // [4][NT]
