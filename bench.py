@@ -455,6 +455,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady leg of the default workload")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart"])
     ap.add_argument("--ws-nx", type=int, default=64)
@@ -619,6 +620,29 @@ def main():
                                                        np.linalg.norm(finals[0]))
     forms["fp32_flux"]["error_steps"] = nform
 
+    # Time to steady state on the same case (the configuration's stopping rule: the L2 density
+    # residual 1e-8 below its first-step value, or --max-steps pseudo-steps), FP64, the tuned
+    # launch options, residual checked every 500 steps; device time by CUDA events.
+    steady = None
+    if not args.no_steady:
+        f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **kw))
+        f.set_option("keep_delu", 0)
+        for kv in (tuned[0].split(" (")[0].split() if tuned else []):
+            k, v = kv.split("=")
+            f.set_option(k, float(v))
+        f.upload_state(U0)
+        r0 = f.step(1).res_l2[0]
+        done, ratio, dev_ms = 1, 1.0, 0.0
+        while done < args.max_steps and ratio > args.tol:
+            n = min(500, args.max_steps - done)
+            ms_chunk, inf = timed_steps(f, stream, n, torch)
+            dev_ms += ms_chunk
+            done += n
+            ratio = inf.res_l2[0] / r0
+        steady = {"steps": done, "seconds": dev_ms * 1e-3, "res_ratio": ratio, "tol": args.tol,
+                  "converged": bool(ratio <= args.tol), "max_steps": args.max_steps}
+        f.close()
+
     # End to end through the public C ABI with host buffers, as a stream of independent one-step
     # solves: every job uploads its state U from pinned host memory, runs one pseudo-step and reads
     # back U and the residual norm.  Three contexts on three streams take the jobs in turn, so a
@@ -692,7 +716,8 @@ def main():
                                       "gather_stage": gs_ms / nprof, "patch": pa_ms / nprof},
                "forms": forms,
                "clocks": clk.summary(),
-               "final_residual_rho": info.error[0]}
+               "final_residual_rho": info.error[0],
+               "time_to_steady": steady}
         if not args.no_cpu_baseline and world == 1:
             try:
                 base = cpu_baseline()
