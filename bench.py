@@ -623,13 +623,14 @@ def main():
     # Time to steady state on the same case (the configuration's stopping rule: the L2 density
     # residual 1e-8 below its first-step value, or --max-steps pseudo-steps), FP64, the tuned
     # launch options, residual checked every 500 steps; device time by CUDA events.
-    steady = None
-    if not args.no_steady:
-        f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **kw))
+    def time_to_steady(over):
+        k = dict(kw)
+        k.update(over)
+        f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
         f.set_option("keep_delu", 0)
         for kv in (tuned[0].split(" (")[0].split() if tuned else []):
-            k, v = kv.split("=")
-            f.set_option(k, float(v))
+            name, v = kv.split("=")
+            f.set_option(name, float(v))
         f.upload_state(U0)
         r0 = f.step(1).res_l2[0]
         done, ratio, dev_ms = 1, 1.0, 0.0
@@ -639,9 +640,15 @@ def main():
             dev_ms += ms_chunk
             done += n
             ratio = inf.res_l2[0] / r0
-        steady = {"steps": done, "seconds": dev_ms * 1e-3, "res_ratio": ratio, "tol": args.tol,
-                  "converged": bool(ratio <= args.tol), "max_steps": args.max_steps}
         f.close()
+        return {"steps": done, "seconds": dev_ms * 1e-3, "res_ratio": ratio, "tol": args.tol,
+                "converged": bool(ratio <= args.tol), "max_steps": args.max_steps}
+
+    steady = None
+    if not args.no_steady:
+        # The configured Van Leer form, and the same run with the minmod limiter beside it.
+        steady = time_to_steady({})
+        steady["minmod"] = time_to_steady({"limiter": 1})
 
     # End to end through the public C ABI with host buffers, as a stream of independent one-step
     # solves: every job uploads its state U from pinned host memory, runs one pseudo-step and reads
