@@ -146,6 +146,15 @@ def gather_stage_bytes_per_cell():
     return (216 + 240 + 236) / 3.0
 
 
+def gradient_bytes_per_cell():
+    """Algorithmic DRAM bytes per cell of k_muscl_gradients, averaged over the three stages: the
+    cell's (rho, u, v, p) row 32, nf 4, neighbour ids 16, face normals and lengths 96, 1/area 8,
+    the gradient records written 64 (220 B), plus at the stages that form del_t (first and last)
+    the sound speed 8, the area 8 and del_t written 8 (244 B).  Neighbour rows are re-reads, and
+    the first stage's ghost rows (< 0.1 %) are left out."""
+    return (244 + 220 + 244) / 3.0
+
+
 def patch_bytes_per_cell():
     """Algorithmic DRAM bytes per cell of the one-kernel patch stage k_patch_stage, averaged over
     the three TVD-RK3 stages with frozen local dt.  Records: the cell's primitives 40, nf 4,
@@ -566,24 +575,34 @@ def main():
         r.update(extra)
         return r
 
-    # The dominant kernel of the chosen launch options: the one-kernel patch stage, else the fused
-    # gather + stage kernel (the face kernel reported beside it).
-    rl_patch = rl_gs = rl_faces = None
+    # Per-kernel rooflines of the chosen launch options; the one with the largest device time per
+    # pseudo-step is the line's `roofline`, the others are listed beside it.
+    rl = {}
     if pa_n:
-        rl_patch = roofline("k_patch_stage<Roe> (records, face fluxes, gather and RK stage update of one "
-                            "128-cell patch per block; all of the pseudo-step but the first-stage BCs)",
-                            pa_ms, pa_n, patch_bytes_per_cell() * NP + patch_bytes_per_face() * NF,
-                            "k_patch_stage_traffic.json",
-                            fp64_pipe_active_pct=profile_figure("k_patch_stage_traffic.json", "fp64_pipe_active_pct"))
+        rl["k_patch_stage"] = (pa_ms, roofline(
+            "k_patch_stage<Roe> (records, face fluxes, gather and RK stage update of one 128-cell patch per "
+            "block)", pa_ms, pa_n, patch_bytes_per_cell() * NP + patch_bytes_per_face() * NF,
+            "k_patch_stage_traffic.json",
+            fp64_pipe_active_pct=profile_figure("k_patch_stage_traffic.json", "fp64_pipe_active_pct")))
     if gs_n:
-        rl_gs = roofline("k_gather_stage (face-flux gather + RK stage update)", gs_ms, gs_n,
-                         gather_stage_bytes_per_cell() * NP + gather_stage_bytes_per_face() * NF,
-                         "k_gather_stage_traffic.json")
+        rl["k_gather_stage"] = (gs_ms, roofline(
+            "k_gather_stage (face-flux gather + RK stage update)", gs_ms, gs_n,
+            gather_stage_bytes_per_cell() * NP + gather_stage_bytes_per_face() * NF, "k_gather_stage_traffic.json"))
     if face_n:
-        rl_faces = roofline("k_faces<double> (face fluxes, gradient MUSCL + Roe)", face_ms, face_n,
-                            face_bytes_per_face() * NF + face_bytes_per_cell() * NP, "k_faces_traffic.json",
-                            fp64_pipe_active_pct=profile_figure("k_faces_traffic.json", "fp64_pipe_active_pct"),
-                            note="FP64 issue rather than HBM limits this kernel (ncu)")
+        rl["k_faces"] = (face_ms, roofline(
+            "k_faces<double> (face fluxes, gradient MUSCL + Roe)", face_ms, face_n,
+            face_bytes_per_face() * NF + face_bytes_per_cell() * NP, "k_faces_traffic.json",
+            fp64_pipe_active_pct=profile_figure("k_faces_traffic.json", "fp64_pipe_active_pct"),
+            note="FP64 issue and load latency rather than HBM bandwidth limit this kernel (ncu)"))
+    if grad_n:
+        rl["k_muscl_gradients"] = (grad_ms, roofline(
+            "k_muscl_gradients (Green-Gauss gradient records, del_t, first-stage BCs)", grad_ms, grad_n,
+            gradient_bytes_per_cell() * NP, "k_muscl_gradients_traffic.json"))
+    dominant = max(rl, key=lambda k: rl[k][0]) if rl else None
+    rl_main = rl[dominant][1] if dominant else None
+    if rl_main:
+        rl_main["share_of_step"] = rl[dominant][0] / max(sum(v[0] for v in rl.values()) + bc_ms, 1e-30)
+    rl_others = {k: v[1] for k, v in rl.items() if k != dominant}
 
     # The other forms on the same mesh: FP32 fluxes with FP64 state (north-star precision form,
     # its error against the all-FP64 run stated), and the reference-parity second-order Roe path
@@ -716,8 +735,8 @@ def main():
                                "copies overlap the others' kernels)",
                        "sequential_value": e2e_seq},
                "gpu_launches": int(launches),
-               "roofline": rl_patch or rl_gs,
-               "roofline_faces": rl_faces,
+               "roofline": rl_main,
+               "roofline_others": rl_others,
                "kernel_ms_per_step": {"faces": face_ms / nprof, "gradients": grad_ms / nprof,
                                       "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof,
                                       "gather_stage": gs_ms / nprof, "patch": pa_ms / nprof},
