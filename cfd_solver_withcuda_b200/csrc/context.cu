@@ -874,7 +874,11 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.Racc, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   }
   if (cfg->muscl) {
-    if ((s = ctx_alloc(ctx, (void **)&st.rec, 8 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
+    if (cfg->precision == CFD_PREC_FP32_FLUX) {
+      if ((s = ctx_alloc(ctx, (void **)&st.recf, 2 * (size_t)NP * sizeof(float4))) != CFD_OK) return bail(s);
+    } else if ((s = ctx_alloc(ctx, (void **)&st.rec, 8 * (size_t)NP * dsz)) != CFD_OK) {
+      return bail(s);
+    }
     if ((s = ctx_alloc(ctx, (void **)&st.q4, (size_t)NT * sizeof(double4))) != CFD_OK) return bail(s);
     if (cudaMemset(st.q4, 0, (size_t)NT * sizeof(double4)) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
   }

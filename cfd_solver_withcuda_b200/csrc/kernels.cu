@@ -857,12 +857,31 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
   const int c = m.fo[i], N = m.fn[i];
   const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
   const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
-  const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)c);
-  const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)N);
-  const double4 c0 = st.q4[c], c1 = rc[0], c2 = rc[1];
-  const double4 n0 = st.q4[N];
+  const double4 c0 = st.q4[c], n0 = st.q4[N];
   const bool nphys = N < NP;
-  const double4 n1 = nphys ? rn[0] : c1, n2 = nphys ? rn[1] : c2;
+  double4 c1, c2, n1, n2;
+  if (sizeof(T) == sizeof(float)) {
+    // FP32-flux form: 32-byte float records (the values face_flux_rec would round to anyway).
+    const float4 *rc = st.recf + 2 * (size_t)c, *rn = st.recf + 2 * (size_t)N;
+    const float4 a = rc[0], b = rc[1];
+    c1 = make_double4(a.x, a.y, a.z, a.w);
+    c2 = make_double4(b.x, b.y, b.z, b.w);
+    if (nphys) {
+      const float4 p = rn[0], q = rn[1];
+      n1 = make_double4(p.x, p.y, p.z, p.w);
+      n2 = make_double4(q.x, q.y, q.z, q.w);
+    } else {
+      n1 = c1;
+      n2 = c2;
+    }
+  } else {
+    const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)c);
+    const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)N);
+    c1 = rc[0];
+    c2 = rc[1];
+    n1 = nphys ? rn[0] : c1;
+    n2 = nphys ? rn[1] : c2;
+  }
   st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy);
 }
 
@@ -1375,11 +1394,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
     }
     const double4 v = st.q4[c];
     const double qc[4] = {v.x, v.y, v.z, v.w};
-    double4 *r = reinterpret_cast<double4 *>(st.rec + 8 * (size_t)c);
     double g[8], den;
     cell_gradients<DT, true>(m, st.prim, st.q4, c, qc, g, den);
-    r[0] = make_double4(g[0], g[1], g[2], g[3]);
-    r[1] = make_double4(g[4], g[5], g[6], g[7]);
+    if (st.recf) {
+      float4 *r = st.recf + 2 * (size_t)c;
+      r[0] = make_float4(float(g[0]), float(g[1]), float(g[2]), float(g[3]));
+      r[1] = make_float4(float(g[4]), float(g[5]), float(g[6]), float(g[7]));
+    } else {
+      double4 *r = reinterpret_cast<double4 *>(st.rec + 8 * (size_t)c);
+      r[0] = make_double4(g[0], g[1], g[2], g[3]);
+      r[1] = make_double4(g[4], g[5], g[6], g[7]);
+    }
     if (DT) st.dtc[c] = cell_dt(m, fp, c, den);
   }
   (void)NT;

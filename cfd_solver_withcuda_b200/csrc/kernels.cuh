@@ -89,6 +89,8 @@ struct DevState {
                  // 64 B = 2 x 32 B per cell
   double4 *q4;   // [NT] (rho, u, v, p) of every row, written wherever the primitives are, so the
                  // face-based kernels fetch a neighbour's state with one 32-byte load (or null)
+  float4 *recf;  // [NP][2] the gradients rounded to float, in place of rec, for the FP32-flux form
+                 // (whose face kernel rounds them to float anyway), or null
   double4 *F;    // [NF] face fluxes (face-based forms)
   // reduction / control block (see CtrlIdx)
   double *ctl;
