@@ -820,6 +820,12 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   cfd_status s;
   if ((s = ctx_upload(ctx, const_cast<int **>(&m.nf), nf)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<int **>(&m.nbr), nbr)) != CFD_OK) return bail(s);
+  {
+    std::vector<int4> n4(NP);
+    for (int i = 0; i < NP; i++)
+      n4[i] = make_int4(nbr[i], nbr[(size_t)NP + i], nbr[2 * (size_t)NP + i], nbr[3 * (size_t)NP + i]);
+    if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.nbr4), n4)) != CFD_OK) return bail(s);
+  }
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.nx), nx)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.ny), ny)) != CFD_OK) return bail(s);
   if ((s = ctx_upload(ctx, const_cast<double **>(&m.dl), dl)) != CFD_OK) return bail(s);
@@ -844,6 +850,10 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdx), fdx)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdy), fdy)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<int **>(&m.cface), cface)) != CFD_OK) return bail(s);
+    std::vector<int4> c4(NP);
+    for (int i = 0; i < NP; i++)
+      c4[i] = make_int4(cface[i], cface[(size_t)NP + i], cface[2 * (size_t)NP + i], cface[3 * (size_t)NP + i]);
+    if ((s = ctx_upload(ctx, const_cast<int4 **>(&m.cface4), c4)) != CFD_OK) return bail(s);
   }
 
   m.wave_blocks = gather_stage_wave_blocks();

@@ -886,18 +886,17 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
 }
 
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
-// side) and the del_t denominator.  All four slots of the [4][NP] face table are loaded without
-// waiting for the face count (an unused slot holds face 0), so the id loads and then the flux
-// loads of every face are in flight together; only the sums are predicated on the count.
+// side) and the del_t denominator.  The cell's four face-table slots come in one 16-byte load
+// without waiting for the face count (an unused slot holds face 0), so the flux loads of every
+// face are in flight together; only the sums are predicated on the count.
 template <bool DEN = true>
 __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &st, int c, double R[4], double &den) {
   const int NP = m.NP, NT = m.NT;
   const double uc = DEN ? st.prim[NT + c] : 0.0, vc = DEN ? st.prim[2 * NT + c] : 0.0,
                ac = DEN ? st.prim[4 * NT + c] : 0.0;
   const int nf = m.nf[c];
-  int e[4];
-#pragma unroll
-  for (int f = 0; f < 4; f++) e[f] = m.cface[f * NP + c];
+  const int4 e4 = m.cface4[c];
+  const int e[4] = {e4.x, e4.y, e4.z, e4.w};
   double4 F[4];
 #pragma unroll
   for (int f = 0; f < 4; f++) {
@@ -1315,8 +1314,8 @@ __device__ __forceinline__ void gg_gradient(const DevMesh &m, const double *q, i
 
 // Green-Gauss gradients of (rho, u, v, p) of physical cell c from the primitive planes `prim`
 // ([5][NT]), multiplied by 1/A (g[2k], g[2k+1]: d/dx, d/dy of variable k), and with DT the
-// denominator of del_t (Inviscid_Time_Step, src/Time_Step.cpp:293-329, faces in order).  All four
-// slots of the [4][NP] neighbour table are read without waiting for the face count (an unused
+// denominator of del_t (Inviscid_Time_Step, src/Time_Step.cpp:293-329, faces in order).  The
+// four neighbour slots come in one 16-byte load without waiting for the face count (an unused
 // slot reads the cell itself), so every neighbour's loads are in flight together; the sums run
 // over the cell's faces in order.
 // q4 is not __restrict__: the first-stage gradient pass writes the ghost rows it then reads.
@@ -1327,12 +1326,11 @@ __device__ __forceinline__ void cell_gradients(const DevMesh &m, const double *p
   const int nf = m.nf[c];
   const double ia = m.inv_area[c];
   const double ac = DT ? prim[4 * NT + c] : 0.0;
+  const int4 n4 = m.nbr4[c];
+  const int nr[4] = {n4.x, n4.y, n4.z, n4.w};
   int nb[4];
 #pragma unroll
-  for (int f = 0; f < 4; f++) {
-    const int N = m.nbr[f * NP + c];
-    nb[f] = (N >= 0 && N < NT) ? N : c;
-  }
+  for (int f = 0; f < 4; f++) nb[f] = (nr[f] >= 0 && nr[f] < NT) ? nr[f] : c;
   double qn[4][4];
 #pragma unroll
   for (int f = 0; f < 4; f++) {

@@ -2,7 +2,8 @@
 //
 // HBM layout (all arrays in device cell order; physical cells 0..NP-1 possibly renumbered (RCM or
 // patches), ghost cells NP..NT-1 in the reference's ghost order):
-//   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l; centre vectors
+//   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l; centre vectors;
+//   the neighbour and face-table slots again as one int4 per cell (nbr4, cface4)
 //   per cell [NP]: nf, area, inv_area, degenerate-face mask; boundary entries per cell (CSR)
 //   unique faces [NF] (face-based forms): owner, neighbour, owner-side geometry; cell slot -> face
 //   state, component-major SoA: U[4][NT] (U^n on physical rows, boundary values on ghost rows),
@@ -42,6 +43,8 @@ struct DevMesh {
   const int *fo, *fn;
   const double *fnx, *fny, *fdl, *fdx, *fdy;
   const int *cface;  // [4][NP]
+  const int4 *cface4;  // [NP] the same four slots per cell (one 16-byte load)
+  const int4 *nbr4;    // [NP] the four neighbour slots per cell
   // Optional work lists (batched solves): each entry is one thread block's [start, end) range of
   // cells (128 per block), faces (128), boundary entries (256) or record rows (256, physical and
   // ghost rows); null = all items.
