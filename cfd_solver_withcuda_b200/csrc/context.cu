@@ -849,6 +849,16 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdl), fdl)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdx), fdx)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<double **>(&m.fdy), fdy)) != CFD_OK) return bail(s);
+    {
+      std::vector<int2> on(fo.size());
+      std::vector<double4> g4(fo.size());
+      for (size_t i = 0; i < fo.size(); i++) {
+        on[i] = make_int2(fo[i], fn[i]);
+        g4[i] = make_double4(fnx[i], fny[i], fdl[i], fdx[i]);
+      }
+      if ((s = ctx_upload(ctx, const_cast<int2 **>(&m.fon), on)) != CFD_OK) return bail(s);
+      if ((s = ctx_upload(ctx, const_cast<double4 **>(&m.fg4), g4)) != CFD_OK) return bail(s);
+    }
     if ((s = ctx_upload(ctx, const_cast<int **>(&m.cface), cface)) != CFD_OK) return bail(s);
     std::vector<int4> c4(NP);
     for (int i = 0; i < NP; i++)

@@ -854,9 +854,11 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
   const int i = item_index(m.fblk, m.NF);
   if (i >= m.NF || step_done(st.ctl)) return;
   const int NP = m.NP;
-  const int c = m.fo[i], N = m.fn[i];
+  const int2 on = m.fon[i];
+  const int c = on.x, N = on.y;
   const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
-  const T nx = T(m.fnx[i]), ny = T(m.fny[i]), dl = T(m.fdl[i]), dx = T(m.fdx[i]), dy = T(m.fdy[i]);
+  const double4 gq = m.fg4[i];
+  const T nx = T(gq.x), ny = T(gq.y), dl = T(gq.z), dx = T(gq.w), dy = T(m.fdy[i]);
   const double4 c0 = st.q4[c], n0 = st.q4[N];
   const bool nphys = N < NP;
   double4 c1, c2, n1, n2;

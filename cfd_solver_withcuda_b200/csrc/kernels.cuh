@@ -3,7 +3,8 @@
 // HBM layout (all arrays in device cell order; physical cells 0..NP-1 possibly renumbered (RCM or
 // patches), ghost cells NP..NT-1 in the reference's ghost order):
 //   geometry, face-major SoA [4][NP]: nbr, nx, ny, dl; limiter stencil n2, d1l, d2l; centre vectors;
-//   the neighbour and face-table slots again as one int4 per cell (nbr4, cface4)
+//   the neighbour and face-table slots again as one int4 per cell (nbr4, cface4); per unique face
+//   also its owner and neighbour as one int2 (fon) and nx, ny, dl, dx as one double4 (fg4)
 //   per cell [NP]: nf, area, inv_area, degenerate-face mask; boundary entries per cell (CSR)
 //   unique faces [NF] (face-based forms): owner, neighbour, owner-side geometry; cell slot -> face
 //   state, component-major SoA: U[4][NT] (U^n on physical rows, boundary values on ghost rows),
@@ -43,6 +44,8 @@ struct DevMesh {
   const int *fo, *fn;
   const double *fnx, *fny, *fdl, *fdx, *fdy;
   const int *cface;  // [4][NP]
+  const int2 *fon;     // [NF] owner, neighbour of each face (one load)
+  const double4 *fg4;  // [NF] nx, ny, dl, dx of each face (dy stays in fdy)
   const int4 *cface4;  // [NP] the same four slots per cell (one 16-byte load)
   const int4 *nbr4;    // [NP] the four neighbour slots per cell
   // Optional work lists (batched solves): each entry is one thread block's [start, end) range of
