@@ -202,6 +202,7 @@ struct cfd_ctx {
   int fuse_gather = 1;  // face-based forms with per-cell dt: fused gather + stage update
   int patch_stage = 0;  // ... or, with patch tables (reorder 3), the one-kernel patch stage
   bool ghost_private = false;  // every ghost row has one boundary entry and neighbours only its owner
+  size_t l2_window = 0;        // bytes of the face-flux L2 window (option "l2_persist" turns it on/off)
   std::vector<int> patch_starts;  // first device cell of each patch (reorder 3)
   double *pbuf[2] = {nullptr, nullptr};  // stage primitives of the patch form ([5][NT] each)
   cudaGraphExec_t graph = nullptr;
@@ -906,6 +907,27 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
+  // Face-based forms: the face fluxes (written by the face kernel, read by the gather right after)
+  // are kept in L2 as persisting lines.  The device's persisting set-aside is raised to hold them
+  // (up to the device maximum; never lowered; it lasts as long as this process's CUDA context).
+  if (m.NF > 0) {
+    int maxp = 0, maxw = 0;
+    size_t cur = 0;
+    const size_t fb = 4 * (size_t)m.NF * dsz;
+    if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, cfg->device) == cudaSuccess &&
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, cfg->device) == cudaSuccess &&
+        maxp > 0 && maxw > 0 && cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
+      const size_t want = std::min<size_t>((size_t)maxp, fb);
+      if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) cur = want;
+      if (cur > 0) {
+        m.l2_base = st.F;
+        m.l2_bytes = std::min<size_t>(fb, (size_t)maxw);
+        m.l2_hit = std::min(1.0f, (float)cur / (float)m.l2_bytes);
+        ctx->l2_window = m.l2_bytes;
+      }
+    }
+    cudaGetLastError();
+  }
   for (int q = 0; q < 2 && m.npatch > 0; q++) {
     if ((s = ctx_alloc(ctx, (void **)&ctx->pbuf[q], 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
     if (cudaMemset(ctx->pbuf[q], 0, 5 * (size_t)NT * dsz) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
@@ -981,6 +1003,7 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "profile") ctx->profile = value != 0.0;
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
   else if (n == "patch_stage") ctx->patch_stage = value != 0.0;
+  else if (n == "l2_persist") ctx->dm.l2_bytes = value != 0.0 ? ctx->l2_window : 0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   if (ctx->graph) {
     cudaGraphExecDestroy(ctx->graph);

@@ -31,11 +31,11 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 // Launches kernel k (smem bytes of dynamic shared memory), with programmatic stream
-// serialization when m.pdl is set.
+// serialization when m.pdl is set and the L2 access-policy window of m when it has one.
 template <typename... KArgs, typename... Args>
 void launch_ks(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
                Args... args) {
-  if (!m.pdl) {
+  if (!m.pdl && !m.l2_bytes) {
     k<<<grid, block, smem, s>>>(args...);
     return;
   }
@@ -44,11 +44,24 @@ void launch_ks(const DevMesh &m, void (*k)(KArgs...), unsigned grid, unsigned bl
   cfg.blockDim = dim3(block);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  int na = 0;
+  if (m.pdl) {
+    at[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[na].val.programmaticStreamSerializationAllowed = 1;
+    na++;
+  }
+  if (m.l2_bytes) {
+    at[na].id = cudaLaunchAttributeAccessPolicyWindow;
+    at[na].val.accessPolicyWindow.base_ptr = m.l2_base;
+    at[na].val.accessPolicyWindow.num_bytes = m.l2_bytes;
+    at[na].val.accessPolicyWindow.hitRatio = m.l2_hit;
+    at[na].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    at[na].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    na++;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = na;
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
