@@ -294,7 +294,8 @@ def test_deterministic_and_graph_equivalent():
 OPTION_SETS = [dict(fuse_gather=0, faces_shape=0), dict(fuse_gather=1, faces_shape=1),
                dict(fuse_gather=1, faces_shape=2, use_graph=0), dict(fuse_gather=0, faces_shape=2),
                dict(pdl=1), dict(pdl=1, use_graph=0, fuse_gather=0), dict(faces_shape=4, pdl=1),
-               dict(faces_shape=4, fuse_gather=0), dict(faces_shape=2)]
+               dict(faces_shape=4, fuse_gather=0), dict(faces_shape=2), dict(l2_persist=0),
+               dict(l2_persist=0, pdl=1, use_graph=0)]
 
 
 @pytest.mark.parametrize("form", ["grad_muscl_minmod_ssp_lts", "grad_muscl_ausm_fp32_ssp_lts", "grad_muscl_hllc_minmod"])
