@@ -900,27 +900,30 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     } else if ((s = ctx_alloc(ctx, (void **)&st.rec, 8 * (size_t)NP * dsz)) != CFD_OK) {
       return bail(s);
     }
-    if ((s = ctx_alloc(ctx, (void **)&st.q4, (size_t)NT * sizeof(double4))) != CFD_OK) return bail(s);
+    if ((s = ctx_alloc(ctx, (void **)&st.q4, ((size_t)NT + (size_t)m.NF) * sizeof(double4))) != CFD_OK) return bail(s);
     if (cudaMemset(st.q4, 0, (size_t)NT * sizeof(double4)) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
+    if (m.NF > 0) st.F = st.q4 + NT;
   }
-  if (m.NF > 0) {
+  if (m.NF > 0 && !st.F) {
     if ((s = ctx_alloc(ctx, (void **)&st.F, 4 * (size_t)m.NF * dsz)) != CFD_OK) return bail(s);
   }
   if ((s = ctx_alloc(ctx, (void **)&st.ctl, CTL_SIZE * dsz)) != CFD_OK) return bail(s);
-  // Face-based forms: the face fluxes (written by the face kernel, read by the gather right after)
-  // are kept in L2 as persisting lines.  The device's persisting set-aside is raised to hold them
-  // (up to the device maximum; never lowered; it lasts as long as this process's CUDA context).
+  // Face-based forms: the (rho, u, v, p) rows and the face fluxes, one allocation (rows first), are
+  // kept in L2 as persisting lines: the gather writes the rows that the gradient and face kernels
+  // read next, and the face kernel writes the fluxes the gather reads right after.  The device's
+  // persisting set-aside is raised to hold them (up to the device maximum; never lowered; it lasts
+  // as long as this process's CUDA context).
   if (m.NF > 0) {
     int maxp = 0, maxw = 0;
     size_t cur = 0;
-    const size_t fb = 4 * (size_t)m.NF * dsz;
+    const size_t fb = 4 * ((size_t)m.NF + (st.q4 ? (size_t)NT : 0)) * dsz;
     if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, cfg->device) == cudaSuccess &&
         cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, cfg->device) == cudaSuccess &&
         maxp > 0 && maxw > 0 && cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
       const size_t want = std::min<size_t>((size_t)maxp, fb);
       if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) cur = want;
       if (cur > 0) {
-        m.l2_base = st.F;
+        m.l2_base = st.q4 ? (void *)st.q4 : (void *)st.F;
         m.l2_bytes = std::min<size_t>(fb, (size_t)maxw);
         m.l2_hit = std::min(1.0f, (float)cur / (float)m.l2_bytes);
         ctx->l2_window = m.l2_bytes;

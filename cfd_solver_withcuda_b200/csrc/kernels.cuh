@@ -71,8 +71,8 @@ struct DevMesh {
   // Blocks of k_gather_stage resident on the whole device at once (SMs x blocks per SM): the grid
   // of its reducing stage (0 = one block per 128 cells).
   int wave_blocks;
-  // L2 access-policy window given to every launch (null / 0: none): the face-flux array, which the
-  // face kernel writes and the gather kernel reads right after, kept as persisting lines.
+  // L2 access-policy window given to every launch (null / 0: none): the (rho, u, v, p) rows and the
+  // face-flux array that follows them, kept as persisting lines between the kernels of a stage.
   void *l2_base;
   size_t l2_bytes;
   float l2_hit;

@@ -195,10 +195,10 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "patch_stage" (with reorder 3, the face-based forms with a per-cell dt frozen per step run each
  * stage as one kernel: a thread block per 128-cell patch computes the records, face fluxes, gather
  * and update of its cells in shared memory; default 0, tried by cfd_autotune),
- * "l2_persist" (face-based forms: the face-flux array is kept in L2 as persisting lines between the
- * face kernel and the gather; default 1.  Creating such a context raises the device's persisting-L2
- * set-aside, cudaLimitPersistingL2CacheSize, to hold that array, up to the device maximum; it is
- * never lowered and lasts as long as the process's CUDA context).
+ * "l2_persist" (face-based forms: the per-cell (rho, u, v, p) rows and the face-flux array are kept
+ * in L2 as persisting lines between the kernels of a stage; default 1.  Creating such a context
+ * raises the device's persisting-L2 set-aside, cudaLimitPersistingL2CacheSize, to hold them, up to
+ * the device maximum; it is never lowered and lasts as long as the process's CUDA context).
  * None of the options changes a result bit. */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
 /* Times every combination of the options above that applies to this configuration over `steps`
