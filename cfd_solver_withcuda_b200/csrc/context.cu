@@ -912,14 +912,17 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   // kept in L2 as persisting lines: the gather writes the rows that the gradient and face kernels
   // read next, and the face kernel writes the fluxes the gather reads right after.  The device's
   // persisting set-aside is raised to hold them (up to the device maximum; never lowered; it lasts
-  // as long as this process's CUDA context).
+  // as long as this process's CUDA context).  Only when the whole region fits in the largest
+  // set-aside the device allows (meshes up to about a million cells on B200); a partial window was
+  // not measured to help.
   if (m.NF > 0) {
     int maxp = 0, maxw = 0;
     size_t cur = 0;
     const size_t fb = 4 * ((size_t)m.NF + (st.q4 ? (size_t)NT : 0)) * dsz;
     if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, cfg->device) == cudaSuccess &&
         cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, cfg->device) == cudaSuccess &&
-        maxp > 0 && maxw > 0 && cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
+        maxp > 0 && maxw > 0 && fb <= (size_t)maxp && fb <= (size_t)maxw &&
+        cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
       const size_t want = std::min<size_t>((size_t)maxp, fb);
       if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) cur = want;
       if (cur > 0) {

@@ -196,7 +196,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * stage as one kernel: a thread block per 128-cell patch computes the records, face fluxes, gather
  * and update of its cells in shared memory; default 0, tried by cfd_autotune),
  * "l2_persist" (face-based forms: the per-cell (rho, u, v, p) rows and the face-flux array are kept
- * in L2 as persisting lines between the kernels of a stage; default 1.  Creating such a context
+ * in L2 as persisting lines between the kernels of a stage, when they fit in the device's largest
+ * persisting set-aside; default 1.  Creating such a context
  * raises the device's persisting-L2 set-aside, cudaLimitPersistingL2CacheSize, to hold them, up to
  * the device maximum; it is never lowered and lasts as long as the process's CUDA context).
  * None of the options changes a result bit. */
