@@ -913,7 +913,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   // read next, and the face kernel writes the fluxes the gather reads right after.  The device's
   // persisting set-aside is raised to hold them (up to the device maximum; never lowered; it lasts
   // as long as this process's CUDA context).  Only when the whole region fits in the largest
-  // set-aside the device allows (meshes up to about a million cells on B200); a partial window was
+  // set-aside the device allows (quad meshes up to about 0.86 M cells on B200); a partial window was
   // not measured to help.
   if (m.NF > 0) {
     int maxp = 0, maxw = 0;
