@@ -483,9 +483,12 @@ def main():
     ap.add_argument("--launch-options", default="auto",
                     help="'auto' (the library's autotuner picks) or e.g. 'faces_shape=1,fuse_gather=1,pdl=1'")
     ap.add_argument("--tol", type=float, default=1e-8)
-    ap.add_argument("--max-steps", type=int, default=20000)
+    ap.add_argument("--max-steps", type=int, default=None,
+                    help="pseudo-step cap of the steady runs (default 20000; 150000 for --workload warmstart)")
     ap.add_argument("--check-every", type=int, default=100)
     args = ap.parse_args()
+    if args.max_steps is None:
+        args.max_steps = 150000 if args.workload == "warmstart" else 20000
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
