@@ -466,6 +466,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady leg of the default workload")
     ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-contexts", type=int, default=3, help="contexts the end-to-end jobs rotate over")
     ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart"])
     ap.add_argument("--ws-nx", type=int, default=64)
     ap.add_argument("--ws-ny", type=int, default=32)
@@ -681,7 +682,7 @@ def main():
     pin = torch.empty((m.n_total, 4), dtype=torch.float64, pin_memory=True)
     pin.copy_(torch.from_numpy(U0))
     host_U = pin.numpy()
-    NCTX = 3
+    NCTX = max(1, args.e2e_contexts)
     out_pin = [torch.empty((m.n_total, 4), dtype=torch.float64, pin_memory=True).numpy() for _ in range(NCTX)]
     s.set_option("use_graph", 0)
     barrier()
@@ -734,8 +735,8 @@ def main():
                           "cuda_graph": True, "launch_options": tuned[0] if tuned else None},
                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
-                       "mode": "independent one-step solves, three contexts on three streams (a solve's "
-                               "copies overlap the others' kernels)",
+                       "mode": "independent one-step solves, %d contexts on %d streams (a solve's copies "
+                               "overlap the others' kernels)" % (NCTX, NCTX),
                        "sequential_value": e2e_seq},
                "gpu_launches": int(launches),
                "roofline": rl_main,
