@@ -34,6 +34,11 @@ NTHETA, NR, R_BODY, R_OUTER, RATIO = 1024, 512, 1.0, 4.0, 1.005
 MACH = 3.0
 WORKLOAD = "half_cylinder_M3_ogrid_1024x512_roe_gg_muscl_vanleer_prim_tvdrk3_lts_cfl0.8"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# Compulsory HBM bytes per cell-update of the second-order, local-time-step path on quads: per
+# stage the state reads (U^n at stage 1, U^n and the stage state at stages 2-3), the state write,
+# 1/area, and per face the normal times length (16 B), the neighbour id (4 B) and the centre
+# distance (8 B): 160 + 96 + 3 x (8 + 4 x 28) = 616 B.
+BYTES_PER_CELL_UPDATE = 616
 
 
 def workload_state(cb):
@@ -60,56 +65,78 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks, power and clock-event (throttle) reasons sampled through NVML every 20 ms while
+    the timed region runs (read-only queries).  The CUDA device is matched to its NVML handle by
+    UUID, so a CUDA_VISIBLE_DEVICES remap is followed."""
 
-    def __init__(self, index):
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, index, period=0.02):
         self.index = index
+        self.period = period
         self.samples = []
-        self.proc = None
+        self.error = None
+        self._stop = threading.Event()
+        self.t = None
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-            # nvidia-smi takes a moment to start: wait for its first line so the samples cover the
-            # timed region, then keep only what comes after it.
-            t0 = time.time()
-            while not self.samples and time.time() - t0 < 5.0 and self.proc.poll() is None:
-                time.sleep(0.01)
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            self.nv = nv
+            try:
+                uuid = "GPU-" + str(torch.cuda.get_device_properties(self.index).uuid)
+                self.h = nv.nvmlDeviceGetHandleByUUID(uuid)
+            except Exception:
+                self.h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS if hasattr(nv, attr)]
+            self._sample()
             self.samples.clear()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+        except Exception as e:  # no NVML: the line says so
+            self.error = str(e)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) == 7:
-                self.samples.append(parts)
+    def _sample(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.samples.append((sm, pw, [name for name, m in self.masks if rs & m]))
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception as e:
+                self.error = str(e)
+                return
+            time.sleep(self.period)
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self.t:
+            self.t.join(timeout=2)
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._sample()  # one sample at the end of the region
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "error": self.error}
+        sm = [s[0] for s in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": min(sm), "sm_max_mhz": self.max_mhz,
+                "power_w_max": max(s[1] for s in self.samples),
+                "reasons": sorted({r for s in self.samples for r in s[2]}), "samples": len(self.samples),
+                "source": "NVML, every %d ms during the timed region" % int(self.period * 1000)}
 
 
 def profile_figure(name, key="bytes_per_launch"):
@@ -193,18 +220,18 @@ def timed_steps(s, stream, steps, torch):
 
 def cpu_baseline(steps=3):
     """The reference's own CPU code (oracle/_ref, single-threaded as the reference is) timed on a
-    bounded sample: `steps` pseudo-steps of the full workload mesh, mesh load excluded.  The
-    reference's CPU path has no Van Leer / gradient MUSCL, so it runs its own ROE_2O with the
-    2-argument MinMod stencil (src/Limiters.cpp:97-200) and its Runge_Kutta_Method with local dt,
-    otherwise the same mesh, state and CFL."""
-    import cfd_solver_withcuda_b200 as cb
-    from oracle import refpy
+    bounded sample: `steps` pseudo-steps of the full workload mesh from the freestream, mesh load
+    excluded.  The O-grid is written and set up by oracle/ogrid.py with numpy and the reference's
+    own VTK reader, so this leg maps none of the product's libraries.  The reference's CPU path has
+    no Van Leer / gradient MUSCL: it runs its own ROE_2O with the two-slope MinMod stencil
+    (src/Limiters.cpp:97-200) and its Runge_Kutta_Method with local dt (the scheme of the GPU form
+    `reference_roe2_minmod_rk3`), otherwise the same mesh, state and CFL."""
+    from oracle import ogrid, refpy
     if not refpy.ref_available():
         return None
-    m, U0, kw = workload_state(cb)
-    r = refpy.RefRun(m, {"CFL": kw["cfl"], "Time_Accurate": 1, "Dissipation_Type": 3, "Is_Second_Order": 1,
-                         "Local_Time_Stepping": 1, "Inlet_Rho": kw["inlet_rho"], "Inlet_P": kw["inlet_p"]})
-    r.set_state(U0)
+    params = {"CFL": 0.8, "Time_Accurate": 1, "Dissipation_Type": 3, "Is_Second_Order": 1, "Local_Time_Stepping": 1,
+              "Inlet_Rho": 1.0, "Inlet_P": 1.0 / GAMMA}
+    r = ogrid.reference_half_cylinder(NTHETA, NR, R_BODY, R_OUTER, RATIO, params, mach=MACH)
     r.iterate(1)
     t = time.perf_counter()
     r.iterate(steps)
@@ -215,10 +242,11 @@ def cpu_baseline(steps=3):
             cpu = next(l.split(":", 1)[1].strip() for l in f if l.startswith("model name"))
     except (OSError, StopIteration):
         pass
-    return {"value": m.n_physical * steps / el, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-            "sample": "%d pseudo-steps (3 RK stages each) of the full %d-cell mesh, mesh load excluded; "
-                      "reference MinMod limiter (its CPU path has no Van Leer); CPU: %s" % (steps, m.n_physical, cpu),
-            "seconds": el}
+    return {"value": r.NP * steps / el, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "sample": "%d pseudo-steps (3 RK stages each) of the full %d-cell mesh after one untimed step, mesh "
+                      "load excluded; the reference's ROE_2O + MinMod stencil + Runge_Kutta_Method with local dt "
+                      "(its CPU path has no Van Leer); CPU: %s" % (steps, r.NP, cpu),
+            "scheme": "reference_roe2_minmod_rk3", "seconds": el}
 
 
 def ramp_instances(n, seed):
@@ -434,8 +462,45 @@ def run_warmstart(args, rank, world):
     print(json.dumps(out))
 
 
+def _reference_replica(steps, ready, go, out):
+    """One single-threaded reference solve of the workload (a spawned process): set-up and one
+    untimed step, then `steps` timed pseudo-steps once every replica is ready."""
+    sys.path.insert(0, ROOT)
+    from oracle import ogrid
+    params = {"CFL": 0.8, "Time_Accurate": 1, "Dissipation_Type": 3, "Is_Second_Order": 1, "Local_Time_Stepping": 1,
+              "Inlet_Rho": 1.0, "Inlet_P": 1.0 / GAMMA}
+    r = ogrid.reference_half_cylinder(NTHETA, NR, R_BODY, R_OUTER, RATIO, params, mach=MACH)
+    r.iterate(1)
+    ready.put(r.NP)
+    go.wait()
+    t = time.perf_counter()
+    r.iterate(steps)
+    out.put(time.perf_counter() - t)
+
+
+def reference_replica_count():
+    """Host cores the reference arm uses: one single-threaded replica per core, bounded by half the
+    available memory at about 1.5 GB per replica (1.0 GB measured peak RSS on the full O-grid) and
+    by 32."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    by_mem = int(0.5 * avail / 1.5e9) if avail else 1
+    return max(1, min(cores, by_mem, 32))
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own CPU path on the host cores (rank 0 only)."""
+    """--impl reference: the reference's own CPU path on the host cores (rank 0 only).  The
+    reference solves one mesh on one thread (its loop and globals are single-threaded), so the host
+    runs one independent replica of the workload per core (spawned processes, each set up from the
+    O-grid file by the reference's own reader; no product library is loaded) and the line's value
+    is their aggregate cell-updates/s; the per-replica rates are listed beside it."""
     if rank != 0:
         return
     from oracle import refpy
@@ -443,18 +508,47 @@ def run_reference(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcfdref.so was not built "
                           "(the reference sources were absent when build() ran)"}))
         return
-    steps = max(1, min(args.steps, 20))
-    base = cpu_baseline(steps=steps)
-    v = base["value"]
-    out = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": steps,
-           "warmup": 1, "ms_per_step": 1e3 * base["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic (in-repo O-grid generator, freestream start)",
-           "impl": "reference",
-           "config": {"workload": WORKLOAD, "cells": NTHETA * NR, "limiter": "reference MinMod (conserved)",
-                      "parallelism": "single-threaded reference CPU code"},
-           "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
-           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out))
+    import multiprocessing as mp
+    steps = max(1, min(args.steps, 10))
+    nproc = args.ref_procs or reference_replica_count()
+    ctx = mp.get_context("spawn")
+    ready, out, go = ctx.Queue(), ctx.Queue(), ctx.Event()
+    procs = [ctx.Process(target=_reference_replica, args=(steps, ready, go, out)) for _ in range(nproc)]
+    t0 = time.perf_counter()
+    for p in procs:
+        p.start()
+    NP = [ready.get(timeout=900) for _ in procs][0]
+    setup_s = time.perf_counter() - t0
+    go.set()
+    secs = [out.get(timeout=900) for _ in procs]
+    for p in procs:
+        p.join()
+    el = max(secs)
+    v = nproc * NP * steps / el
+    per = [NP * steps / x for x in secs]
+    cpu = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            cpu = next(l.split(":", 1)[1].strip() for l in f if l.startswith("model name"))
+    except (OSError, StopIteration):
+        pass
+    sample = ("%d replicas x %d timed pseudo-steps (after one untimed step) of the full %d-cell O-grid, one "
+              "single-threaded reference process per core, mesh set-up excluded (%.0f s); the reference's ROE_2O + "
+              "MinMod stencil + Runge_Kutta_Method with local dt (its CPU path has no Van Leer); CPU: %s"
+              % (nproc, steps, NP, setup_s, cpu))
+    out_line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+                "steps": steps, "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (O-grid written by oracle/ogrid.py, freestream start)", "impl": "reference",
+                "config": {"workload": WORKLOAD, "cells": NP, "scheme": "reference_roe2_minmod_rk3",
+                           "scheme_note": "the reference's own second-order scheme; the GPU arm reports the same "
+                                          "scheme as forms.reference_roe2_minmod_rk3 and same_scheme_vs_reference",
+                           "parallelism": "%d single-threaded reference replicas (one per host core)" % nproc},
+                "per_replica_value": {"median": float(np.median(per)), "min": min(per), "max": max(per)},
+                "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": nproc, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out_line))
 
 
 def main():
@@ -464,6 +558,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=0, help="reference replicas (default: one per host core, "
+                    "bounded by memory)")
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady leg of the default workload")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--e2e-contexts", type=int, default=3, help="contexts the end-to-end jobs rotate over")
@@ -569,13 +665,26 @@ def main():
     peaks, peak_kind = measured_peaks()
     NF = s.n_faces
 
-    def roofline(kernel, ms, n, bytes_launch, traffic_file, **extra):
+    # Roofline accounting on the per-unit figure of the path: BYTES_PER_CELL_UPDATE compulsory HBM
+    # bytes per cell-update (one pseudo-step of one cell, 3 RK stages).  Each kernel of the default
+    # step launches once per stage over all cells, so one launch's algorithmic bytes are a third of
+    # that figure times the cells.  The kernels' own traffic models (every array they touch, once)
+    # are kept beside it as kernel_model_*; ncu's DRAM bytes of one launch are `traffic`.
+    alg_launch = BYTES_PER_CELL_UPDATE / 3.0 * NP
+
+    def roofline(kernel, ms, n, model_bytes, traffic_file, **extra):
         avg = ms / n
-        achieved = bytes_launch / (avg * 1e-3) / 1e9
+        achieved = alg_launch / (avg * 1e-3) / 1e9
+        traffic = profile_figure(traffic_file)
         r = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-             "frac": achieved / peaks["hbm_gbs"], "traffic": profile_figure(traffic_file),
+             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+             "traffic_over_algorithmic": traffic / alg_launch if traffic else None,
              "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-             "bytes_per_launch": bytes_launch, "avg_launch_ms": avg, "cells": NP, "faces": NF}
+             "bytes_per_launch": alg_launch,
+             "bytes_basis": "%d B per cell-update / 3 stages x %d cells" % (BYTES_PER_CELL_UPDATE, NP),
+             "avg_launch_ms": avg, "launches": n, "cells": NP, "faces": NF,
+             "kernel_model_bytes_per_launch": model_bytes,
+             "kernel_model_frac": model_bytes / (avg * 1e-3) / 1e9 / peaks["hbm_gbs"]}
         r.update(extra)
         return r
 
@@ -604,9 +713,18 @@ def main():
             gradient_bytes_per_cell() * NP, "k_muscl_gradients_traffic.json"))
     dominant = max(rl, key=lambda k: rl[k][0]) if rl else None
     rl_main = rl[dominant][1] if dominant else None
-    if rl_main:
-        rl_main["share_of_step"] = rl[dominant][0] / max(sum(v[0] for v in rl.values()) + bc_ms, 1e-30)
+    total_kernel_ms = max(sum(v[0] for v in rl.values()) + bc_ms, 1e-30)
+    for k, v in rl.items():
+        v[1]["share_of_step"] = v[0] / total_kernel_ms
     rl_others = {k: v[1] for k, v in rl.items() if k != dominant}
+    # The whole pseudo-step against the same figure, and the ncu DRAM bytes of its kernels.
+    step_achieved = BYTES_PER_CELL_UPDATE * NP / (ms_per_step * 1e-3) / 1e9
+    step_traffic = sum(3 * v[1]["traffic"] for v in rl.values() if v[1]["traffic"]) if rl else None
+    step_roofline = {"achieved": step_achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": step_achieved / peaks["hbm_gbs"],
+                     "bytes_per_step": BYTES_PER_CELL_UPDATE * NP, "ms_per_step": ms_per_step,
+                     "ncu_traffic_per_step": step_traffic,
+                     "traffic_over_algorithmic": step_traffic / (BYTES_PER_CELL_UPDATE * NP) if step_traffic else None}
 
     # The other forms on the same mesh: FP32 fluxes with FP64 state (north-star precision form,
     # its error against the all-FP64 run stated), and the reference-parity second-order Roe path
@@ -740,6 +858,7 @@ def main():
                        "sequential_value": e2e_seq},
                "gpu_launches": int(launches),
                "roofline": rl_main,
+               "roofline_step": step_roofline,
                "roofline_others": rl_others,
                "kernel_ms_per_step": {"faces": face_ms / nprof, "gradients": grad_ms / nprof,
                                       "gather": ga_ms / nprof, "stage": st_ms / nprof, "bc": bc_ms / nprof,

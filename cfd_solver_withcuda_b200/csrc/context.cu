@@ -26,7 +26,7 @@ void set_last_error(const std::string &msg);
 using namespace cfdb;
 
 namespace {
-std::string g_err;  // last error message (per process)
+thread_local std::string g_err;  // last error message of the calling thread
 }  // namespace
 
 void cfdb::set_last_error(const std::string &msg) { g_err = msg; }

@@ -8,6 +8,13 @@
 // control block that receives Min_dt, the completion counter of the last-block reduction and one
 // partial minimum per thread block — lives in the file-scope device array below, of fixed size,
 // which every GPU that loads the library holds until the process exits.
+//
+// The array is placed on a device when the library's device code is loaded into the caller's
+// CUDA context.  With lazy module loading (the CUDA default since 12.2) that happens during the
+// first call in a context: that call may itself need the array's 2 MiB of free device memory and
+// synchronises the device.  So a caller whose pool reserves the GPU's memory makes its first
+// call before the pool takes it, or sets CUDA_MODULE_LOADING=EAGER; and makes it before any
+// stream capture.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -22,13 +29,9 @@ constexpr int kMaxBlocks = 262144;   // partial-minimum slots: one per flux-kern
 constexpr int kCtlDoubles = cfdb::CTL_SIZE;
 constexpr int kCounterDoubles = 8;  // completion counter (unsigned) + status words (2 x int)
 constexpr int kScratchDoubles = kCtlDoubles + kCounterDoubles + kMaxBlocks;
-constexpr int kMaxDevices = 64;
 
 // Shared by every call on a device: a call overwrites what the previous one left.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
-
-// Device address of g_noalloc_scratch per device ordinal, looked up once per device.
-double *g_scratch_dev[kMaxDevices] = {nullptr};
 
 }  // namespace
 
@@ -65,16 +68,15 @@ extern "C" cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, co
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return noalloc_fail(CFD_ERR_NO_DEVICE, cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(CFD_ERR_BAD_ARG, "device ordinal out of range");
-  if (!g_scratch_dev[dev]) {
-    // One-time set-up on this device (the current one): resolve the device address of the
-    // scratch array.  The host-side name g_noalloc_scratch is not a device address.
-    double *p = nullptr;
-    e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return noalloc_fail(CFD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_dev[dev] = p;
-  }
-  double *scratch = g_scratch_dev[dev];
+  // The device address of the scratch array in the calling thread's current context (the
+  // host-side name g_noalloc_scratch is not a device address).  It is looked up on every call,
+  // not cached: after a device reset, or in a driver-API context other than the primary one, the
+  // array lives at another address, and the lookup costs little once the module is loaded.
+  // Nothing is shared between threads on the host.
+  double *scratch = nullptr;
+  e = cudaGetSymbolAddress(reinterpret_cast<void **>(&scratch), g_noalloc_scratch);
+  if (e != cudaSuccess || !scratch)
+    return noalloc_fail(CFD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   cfdb::DevMesh m{};

@@ -281,26 +281,33 @@ typedef struct {
   const int *neighbours;          /* [4][NP] neighbour or ghost id of face f of cell c at f*NP+c */
   const double *nx, *ny, *dl;     /* [4][NP] face normal and length */
   const double *area, *inv_area;  /* [NP] */
-  const int *second_neighbours;   /* [4][NP] limiter stencil N2 of src/Limiters.cpp:136-191 (2nd order) */
-  const double *d1, *d2;          /* [4][NP] limiter distances d1, d2 (2nd order) */
+  const int *second_neighbours;   /* [4][NP] second cell of the directional limiter stencil (2nd order) */
+  const double *d1, *d2;          /* [4][NP] centre distances of that stencil (2nd order) */
   const uint8_t *degenerate;      /* [NP] bit f set when |n_f| < 1e-12 */
   const double *prim;             /* [5][NT] rho, u, v, p, a */
-  const double *U;                /* [4][NT] U_Cells */
-  double *net_flux;               /* out [4][NP] Cells_Net_Flux */
-  double *dt;                     /* out [NP] Cell::del_t */
-  double *min_dt;                 /* out [1] Min_dt */
+  const double *U;                /* [4][NT] conserved state, ghost rows included */
+  double *net_flux;               /* out [4][NP] per-cell residual (sum of face fluxes) */
+  double *dt;                     /* out [NP] per-cell time step */
+  double *min_dt;                 /* out [1] minimum time step over the cells */
 } cfd_flux_arrays;
 
-/* Evaluate_Cell_Net_Flux + del_t + Min_dt on caller-owned device arrays WITHOUT allocating
- * device memory.  No counterpart in the reference: it exists for callers that cannot let this
- * library call cudaMalloc (their own pool allocator owns the device memory, or their loop may not
- * take cudaMalloc's device synchronisation).  The kernel's scratch (control block, completion
- * counter, one partial minimum per thread block) is a fixed static device array of 262,168 doubles
- * (2 MiB) per GPU, held until the process exits; at most 8,388,608 physical cells per call (larger sizes
- * are rejected with CFD_ERR_BAD_ARG).  The first call on a device resolves the array's device
- * address, so make that first call before any stream capture.  Calls share the array: calls that
- * overlap on the GPU (different streams, other threads) race.  Reference MUSCL stencil, FP64,
- * ROE or first-order LLF only.  stream: cudaStream_t (NULL = default stream). */
+/* The per-cell residual, per-cell time step and minimum time step (what cfd_evaluate_net_flux
+ * computes) on caller-owned device arrays, WITHOUT allocating device memory.  It has no
+ * counterpart in the reference.  It exists for callers that cannot let this library call
+ * cudaMalloc: their own pool allocator owns the GPU's memory, or their loop cannot take
+ * cudaMalloc's device synchronisation or its possible failure.
+ * The kernel's scratch (control block, completion counter, one partial minimum per thread block)
+ * is a fixed static device array of 262,168 doubles (2 MiB) per GPU, held until the process
+ * exits; at most 8,388,608 physical cells per call (larger sizes are rejected with
+ * CFD_ERR_BAD_ARG).  The array is placed on the device when the library's device code is loaded
+ * into the CUDA context; with lazy module loading (the CUDA default) that is the first call in a
+ * context, which then needs 2 MiB of free device memory and synchronises the device.  So make the
+ * first call on each device before your pool reserves the GPU's memory (or run with
+ * CUDA_MODULE_LOADING=EAGER), and before any stream capture.  The array's device address is
+ * looked up in the current context on every call.  Calls share the array and every call clears
+ * what must start at zero: calls that overlap on the GPU (different streams, other threads) race.
+ * Reference MUSCL stencil, FP64, ROE or first-order LLF only.
+ * stream: cudaStream_t (NULL = default stream). */
 cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_config *cfg, void *stream);
 
 /* ------------------------------------------------------------------------------------------

@@ -33,6 +33,10 @@
 #include "Gradients.h"
 #include "Weno.h"
 #include "IO_Write.h"
+#include "Viscous_Functions.h"
+
+#include <algorithm>
+#include <cmath>
 
 #include <unistd.h>
 #include <fcntl.h>
@@ -342,6 +346,35 @@ void refh_amr(double threshold, double max_fraction, double *indicator, unsigned
     indicator[c] = Gradient_Refinement_Indicator[c];
     tags[c] = Cells[c].Is_Splittable ? 1 : 0;
   }
+}
+
+// The reference's viscous residual on the current state: the set-up its Form_Cells does for a
+// viscous wall (Construct_Co_Volumes per physical cell, src/Grid_Computations.cpp:367-375), the
+// secondary neighbours of its face-gradient stencil (Identify_Neighbours_For_Second_Gradients,
+// src/Grid_Refine_Functions.cpp:107-170), then Evaluate_Viscous_Fluxes
+// (src/Grid_Refine_Functions.cpp:482-500) with Inv_Re and K1 set to the given nonzero values.
+// flux: [NP][4] Cells_Viscous_Flux.  covol[0..2]: the largest |co-volume face area|, |co-volume
+// face normal component| and |co-volume Inv_Area| over the cells.  stdout is left as it is: the
+// reference reports a degenerate co-volume there and terminates the process (exit(0) in
+// Evaluate_Cross_Product, src/Grid_Computations.cpp:834-844).
+void refh_viscous_flux(double inv_re, double k1, double *flux, double *covol) {
+  Co_Volume_Cells.clear();
+  for (int c = 0; c < No_Physical_Cells; c++) {
+    int cc = c;
+    Identify_Neighbours_For_Second_Gradients(cc);
+    Construct_Co_Volumes(cc);
+  }
+  Inv_Re = inv_re;
+  K1 = k1;
+  Evaluate_Viscous_Fluxes();
+  covol[0] = covol[1] = covol[2] = 0.0;
+  for (const Cell &C : Co_Volume_Cells) {
+    for (double a : C.Face_Areas) covol[0] = std::max(covol[0], std::fabs(a));
+    for (double n : C.Face_Normals) covol[1] = std::max(covol[1], std::fabs(n));
+    covol[2] = std::max(covol[2], std::fabs(C.Inv_Area));
+  }
+  for (int c = 0; c < No_Physical_Cells; c++)
+    for (int k = 0; k < 4; k++) flux[4 * c + k] = Cells_Viscous_Flux[c][k];
 }
 
 }  // extern "C"

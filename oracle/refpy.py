@@ -15,7 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libcfdref.so")
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
-REF_SRC = os.environ.get("CFD_REFERENCE_DIR", "/root/reference")
+# The reference checkout: CFD_REFERENCE_DIR, else a directory "reference" beside this repository.
+REF_SRC = os.environ.get("CFD_REFERENCE_DIR", os.path.abspath(os.path.join(HERE, "..", "..", "reference")))
 
 _DP = ctypes.POINTER(ctypes.c_double)
 _IP = ctypes.POINTER(ctypes.c_int)
@@ -184,22 +185,36 @@ class RefRun:
     """The reference CPU path on one mesh (process-global state: one instance at a time)."""
 
     def __init__(self, mesh, params, lib_path=REF_LIB):
-        L = reflib(lib_path)
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "mesh.vtk")
             mesh.write_vtk(path)
-            np_ = L.refh_load_vtk(path.encode())
-        if np_ != mesh.n_physical:
-            raise RuntimeError("reference reader returned %d cells, expected %d" % (np_, mesh.n_physical))
-        # Boundary lists from the mesh layer (identical to the bounding-box lists on box domains).
-        L.refh_clear_boundary_lists()
-        for kind, c, f, g in mesh.boundary:
-            L.refh_add_boundary(int(kind), int(c), int(f), int(g))
+            # Boundary lists from the mesh layer (identical to the bounding-box lists on box domains).
+            self._setup(path, mesh.boundary, params, lib_path)
+        if self.NP != mesh.n_physical:
+            raise RuntimeError("reference reader returned %d cells, expected %d" % (self.NP, mesh.n_physical))
+
+    @classmethod
+    def from_vtk(cls, path, boundary, params, lib_path=REF_LIB):
+        """The reference path on a VTK file read by its own reader.  boundary: (kind, cell, face,
+        ghost) rows replacing the reader's bounding-box lists, or None to keep them."""
+        self = cls.__new__(cls)
+        self._setup(path, boundary, params, lib_path)
+        return self
+
+    def _setup(self, path, boundary, params, lib_path):
+        L = reflib(lib_path)
+        np_ = L.refh_load_vtk(path.encode())
+        if np_ <= 0:
+            raise RuntimeError("the reference reader could not read %s" % path)
+        if boundary is not None:
+            L.refh_clear_boundary_lists()
+            for kind, c, f, g in boundary:
+                L.refh_add_boundary(int(kind), int(c), int(f), int(g))
         for k, v in params.items():
             if L.refh_set_param(k.encode(), float(v)) != 0:
                 raise KeyError(k)
         self.NT = L.refh_finalize_mesh()
-        self.NP = mesh.n_physical
+        self.NP = np_
         self.L = L
 
     def set_state(self, U):

@@ -9,7 +9,7 @@ import cfd_solver_withcuda_b200 as cb
 from cases import CASES, make_mesh
 from conftest import assert_bits_equal, load_golden
 
-REF_DIR = os.environ.get("CFD_REFERENCE_DIR", "/root/reference")
+from oracle.refpy import REF_SRC as REF_DIR  # CFD_REFERENCE_DIR, else "reference" beside the repository
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

@@ -3,7 +3,9 @@ allocate device memory (their own pool allocator owns the GPU's memory, or their
 cudaMalloc's device synchronisation).  The test owns every device array (allocated here with
 torch), calls the entry point through the C ABI twice in a row on two different states, and
 checks each result bit for bit against the existing entry point, cfd_evaluate_net_flux, of a
-context on the same mesh and state.  This file is collected last on purpose."""
+context on the same mesh and state, and that calls after the first take no device memory (free
+device memory unchanged across a call, also on another stream).  This file is collected last on
+purpose."""
 import ctypes
 
 import numpy as np
@@ -95,12 +97,29 @@ def test_noalloc_matches_context_on_two_calls():
         for name, t in keep.items():
             setattr(a, name, t.data_ptr())
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         rc = cb.lib().cfd_evaluate_net_flux_noalloc(ctypes.byref(a), ctypes.byref(cfg), None)
         assert rc == cb.CFD_OK, cb.lib().cfd_last_error()
         torch.cuda.synchronize()
+        if call == 1:
+            # The first call may load the library's device code into this context (which places
+            # the static scratch array); from then on a call takes no device memory.
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, "the second call changed free device memory"
         assert_bits_equal(keep["net_flux"].cpu().numpy().T, want["net_flux"], "net flux, call %d" % call)
         assert_bits_equal(keep["dt"].cpu().numpy(), want["dt"], "del_t, call %d" % call)
         assert_bits_equal(keep["min_dt"].cpu().numpy(), np.array([want_min_dt]), "Min_dt, call %d" % call)
+
+    # A further call on a stream of its own: same results as the second call, no device memory.
+    side = torch.cuda.Stream(device=dev)
+    want_flux = keep["net_flux"].clone()
+    keep["net_flux"].fill_(np.nan)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(dev)[0]
+    rc = cb.lib().cfd_evaluate_net_flux_noalloc(ctypes.byref(a), ctypes.byref(cfg), ctypes.c_void_p(side.cuda_stream))
+    assert rc == cb.CFD_OK, cb.lib().cfd_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(dev)[0] == free_before, "a call on another stream changed free device memory"
+    assert_bits_equal(keep["net_flux"].cpu().numpy(), want_flux.cpu().numpy(), "net flux on a second stream")
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
