@@ -55,7 +55,7 @@ class Config(ctypes.Structure):
                 ("inlet_u", ctypes.c_double), ("inlet_v", ctypes.c_double), ("inlet_p0", ctypes.c_double),
                 ("inlet_t0", ctypes.c_double), ("exit_p", ctypes.c_double), ("r_gas", ctypes.c_double),
                 ("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("weno", ctypes.c_int),
-                ("weno_characteristic", ctypes.c_int)]
+                ("weno_characteristic", ctypes.c_int), ("entropy_fix_linear", ctypes.c_double)]
 
 
 class FluxArrays(ctypes.Structure):
@@ -64,6 +64,34 @@ class FluxArrays(ctypes.Structure):
                [(n, ctypes.c_void_p) for n in ("n_faces", "neighbours", "nx", "ny", "dl", "area", "inv_area",
                                                 "second_neighbours", "d1", "d2", "degenerate", "prim", "U",
                                                 "net_flux", "dt", "min_dt")]
+
+
+class MlpSeg(ctypes.Structure):
+    """cfd_mlp_seg: one input segment of a dense block (device pointers as integers)."""
+    _fields_ = [("src", ctypes.c_void_p), ("idx", ctypes.c_void_p), ("width", ctypes.c_int), ("ld", ctypes.c_int),
+                ("silu", ctypes.c_int)]
+
+
+class MlpFwd(ctypes.Structure):
+    """cfd_mlp_fwd."""
+    _fields_ = [("rows", ctypes.c_int), ("nseg", ctypes.c_int), ("seg", MlpSeg * 3), ("out", ctypes.c_int),
+                ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p),
+                ("resid", ctypes.c_void_p), ("ld_resid", ctypes.c_int), ("z1", ctypes.c_void_p),
+                ("y", ctypes.c_void_p), ("ld_y", ctypes.c_int)]
+
+
+class MlpBwd(ctypes.Structure):
+    """cfd_mlp_bwd."""
+    _fields_ = [("rows", ctypes.c_int), ("in_width", ctypes.c_int), ("out", ctypes.c_int), ("dy", ctypes.c_void_p),
+                ("ld_dy", ctypes.c_int), ("z1", ctypes.c_void_p), ("w1", ctypes.c_void_p), ("w2", ctypes.c_void_p),
+                ("dz1", ctypes.c_void_p), ("dx", ctypes.c_void_p), ("ld_dx", ctypes.c_int)]
+
+
+class MlpWgrad(ctypes.Structure):
+    """cfd_mlp_wgrad."""
+    _fields_ = [("rows", ctypes.c_int), ("n", ctypes.c_int), ("dz", ctypes.c_void_p), ("ld_dz", ctypes.c_int),
+                ("nseg", ctypes.c_int), ("seg", MlpSeg * 3), ("workspace", ctypes.c_void_p), ("dw", ctypes.c_void_p),
+                ("db", ctypes.c_void_p), ("accumulate", ctypes.c_int)]
 
 
 class StepInfo(ctypes.Structure):
@@ -131,6 +159,14 @@ SIGNATURES = {
     "cfd_batch_destroy": (None, [_P]),
     "cfd_batch_set_boundary_values": (_I, [_P, _DP, _DP]),
     "cfd_mpnn_segment_sum": (_I, [_P, _P, _P, _I, _I, _P, _P]),
+    "cfd_mpnn_mlp_forward": (_I, [ctypes.POINTER(MlpFwd), _P]),
+    "cfd_mpnn_mlp_backward": (_I, [ctypes.POINTER(MlpBwd), _P]),
+    "cfd_mpnn_weight_grad": (_I, [ctypes.POINTER(MlpWgrad), _P]),
+    "cfd_mpnn_wgrad_blocks": (_I, []),
+    "cfd_mpnn_add": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _P]),
+    "cfd_mpnn_gather_add": (_I, [_P, _I, _P, _I, _P, _I, _I, _P]),
+    "cfd_mpnn_segment_sum_acc": (_I, [_P, _I, _P, _P, _I, _I, _P, _I, _I, _P]),
+    "cfd_mpnn_mse": (_I, [_P, _P, _I, _P, _P, _P]),
     "cfd_mpnn_adam": (_I, [_P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _I,
                            _P]),
     "cfd_batch_set_reference_residual": (_I, [_P, _DP]),

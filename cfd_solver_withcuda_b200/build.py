@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcfd_b200.so")
-SOURCES = ["kernels.cu", "context.cu", "mesh.cpp", "json_config.cpp", "noalloc.cu", "mpnn.cu", "solution_io.cpp"]
+SOURCES = ["kernels.cu", "context.cu", "mesh.cpp", "json_config.cpp", "noalloc.cu", "mpnn.cu", "mpnn_tc.cu", "solution_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

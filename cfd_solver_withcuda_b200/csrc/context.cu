@@ -557,6 +557,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if (diss == CFD_DISS_LLF && cfg->is_second_order)
     return fail(CFD_ERR_BAD_ARG, "LLF_2O reads uninitialised state in the reference (src/LLF.cpp:101); not supported");
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
+  if (!(cfg->entropy_fix_linear >= 0.0) || !std::isfinite(cfg->entropy_fix_linear))
+    return fail(CFD_ERR_BAD_ARG, "entropy_fix_linear must be a finite value >= 0");
   if (cfg->reorder < 0 || cfg->reorder > 3) return fail(CFD_ERR_BAD_ARG, "reorder must be 0, 1, 2 or 3");
   if (cfg->inlet_bc < 0 || cfg->inlet_bc > CFD_INLET_FARFIELD || cfg->exit_bc < 0 || cfg->exit_bc > CFD_EXIT_FIXED_P_REF)
     return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
@@ -976,6 +978,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.cfl = cfg->cfl;
   fp.zeta = cfg->limiter_zeta;
   fp.zeta1 = cfg->limiter_zeta1;
+  fp.eflin = cfg->entropy_fix_linear;
   BcParams &bp = ctx->bp;
   bp.inlet_bc = cfg->inlet_bc;
   bp.exit_bc = cfg->exit_bc;

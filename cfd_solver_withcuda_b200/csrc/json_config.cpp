@@ -236,13 +236,15 @@ std::string config_from_json(const std::string &text, cfd_config *cfg) {
     cfg->reconstruct_primitive = enum_from(sol->get("Reconstruction"), {"conserved", "primitive"}, cfg->reconstruct_primitive);
     as_int(sol->get("Reorder"), cfg->reorder);
     cfg->muscl = enum_from(sol->get("MUSCL"), {"reference", "gradient"}, cfg->muscl);
+    as_double(sol->get("Entropy_Fix_Linear"), cfg->entropy_fix_linear);
   }
   if (lim) {
     as_double(lim->get("Limiter_Zeta"), cfg->limiter_zeta);
     as_double(lim->get("Limiter_Zeta1"), cfg->limiter_zeta1);
   }
   if (bc) {
-    cfg->inlet_bc = enum_from(bc->get("Inlet_BC"), {"supersonic", "subsonic_reference", "total_pt"}, cfg->inlet_bc);
+    cfg->inlet_bc = enum_from(bc->get("Inlet_BC"), {"supersonic", "subsonic_reference", "total_pt", "fixed", "farfield"},
+                             cfg->inlet_bc);
     cfg->exit_bc = enum_from(bc->get("Exit_BC"), {"supersonic", "subsonic_reference", "static_p"}, cfg->exit_bc);
     int sub = 0;
     if (as_bool(bc->get("Is_Inlet_SubSonic"), sub)) cfg->inlet_bc = sub ? CFD_INLET_SUBSONIC_REF : CFD_INLET_SUPERSONIC;

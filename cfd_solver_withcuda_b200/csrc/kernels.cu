@@ -810,13 +810,14 @@ __global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, Flu
 // D-_N = 2 grad q_N . d - D+; q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+
 // (phi(a, b), r = a/b).  A ghost neighbour uses the owner's gradient.  A non-positive
 // reconstructed density or pressure falls back to the cell-centre state.  Flux: average of the two
-// face states plus Roe dissipation between them.
+// face states plus Roe dissipation between them (with the linear-wave entropy fix when
+// fp.eflin > 0).
 // Flux of one unique face from the owner's record (c0: rho, u, v, p; c1, c2: gradients) and the
 // neighbour's (n0, n1, n2), face normal (nx, ny), length dl and centre-to-centre vector (dx, dy).
 template <typename T, int DISS>
 __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, const double4 c1, const double4 c2,
                                                  const double4 n0, const double4 n1, const double4 n2, const T nx,
-                                                 const T ny, const T dl, const T dx, const T dy) {
+                                                 const T ny, const T dl, const T dx, const T dy, const T eflin) {
   const T qc[4] = {T(c0.x), T(c0.y), T(c0.z), T(c0.w)};
   const T qn[4] = {T(n0.x), T(n0.y), T(n0.z), T(n0.w)};
   const T gc[8] = {T(c1.x), T(c1.y), T(c1.z), T(c1.w), T(c2.x), T(c2.y), T(c2.z), T(c2.w)};
@@ -842,7 +843,7 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
   T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
   if (DISS == 3) {
     average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
-    roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D);
+    roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D, eflin);
   } else {
     // Conserved face states for AUSM / HLLC: E = p/(g-1) + rho |V|^2 / 2.
     const T UL[4] = {qL[0], qL[0] * qL[1], qL[0] * qL[2],
@@ -897,7 +898,7 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
     n1 = nphys ? rn[0] : c1;
     n2 = nphys ? rn[1] : c2;
   }
-  st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy);
+  st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy, T(fp.eflin));
 }
 
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
@@ -1504,7 +1505,8 @@ __global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevSt
       n1r = make_double4(srec[4 * rows + ln], srec[5 * rows + ln], srec[6 * rows + ln], srec[7 * rows + ln]);
       n2r = make_double4(srec[8 * rows + ln], srec[9 * rows + ln], srec[10 * rows + ln], srec[11 * rows + ln]);
     }
-    const double4 F = face_flux_rec<double, DISS>(glim, c0r, c1r, c2r, n0r, n1r, n2r, fe.nx, fe.ny, fe.dl, fe.dx, fe.dy);
+    const double4 F = face_flux_rec<double, DISS>(glim, c0r, c1r, c2r, n0r, n1r, n2r, fe.nx, fe.ny, fe.dl, fe.dx, fe.dy,
+                                                    fp.eflin);
     if (so < 4) {
       sF[(so * 4 + 0) * kPatchCells + lo] = F.x;
       sF[(so * 4 + 1) * kPatchCells + lo] = F.y;

@@ -137,6 +137,7 @@ struct FluxParams {
   int consistent;       // 1: limiter/LLF/exit read the stage state instead of U^n
   int precision;
   double cfl, zeta, zeta1;
+  double eflin;         // entropy fix of the linear waves in the gradient-MUSCL Roe flux (0: off)
 };
 
 struct BcParams {

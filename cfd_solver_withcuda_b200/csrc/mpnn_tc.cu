@@ -1,0 +1,598 @@
+// Dense layers of the warm-start surrogate on the tensor cores (no reference counterpart).
+//
+// Every dense block of the network is a two-layer perceptron y = W2 silu(W1 x + b1) + b2 (+ r),
+// hidden width 64, whose input row x is up to three row segments side by side, each read from
+// its own array, directly or through a row index (the per-edge gathers of the message-passing
+// layers are fused into the operand staging).  Operands are rounded to BF16 when they are staged
+// into shared memory; the products accumulate in FP32 (mma.sync m16n8k16, BF16 inputs, FP32
+// accumulators); bias, SiLU, residual and the SiLU derivative are FP32 epilogues.
+//
+//   k_mlp_fwd    y and the hidden pre-activation z1 (kept for the backward pass), one 64-row tile
+//                per loop trip, weights staged once per block.
+//   k_mlp_bwd    dz1 = (dy W2) * silu'(z1) and dx = dz1 W1 for a tile of rows.
+//   k_wgrad      dW = dz^T x and db = sum of dz over the rows: each block accumulates its tiles in
+//                registers and writes one partial; k_wgrad_reduce sums the partials in block
+//                order, so the gradients are the same on every run.
+//
+// The CPU FP64 restatement these kernels are checked against is oracle/mpnn_ref.py.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "cfd_b200.h"
+
+namespace cfdb {
+void set_last_error(const std::string &msg);
+}
+
+namespace {
+
+constexpr int TM = 64;    // rows per tile
+constexpr int HID = 64;   // hidden width
+constexpr int KMAX = 192; // widest input row
+constexpr int LDH = HID + 8;
+constexpr int LDT = TM + 8;
+
+struct SegDev {
+  const float *src;
+  const int *idx;
+  int width, ld, silu;
+};
+
+__device__ __forceinline__ float silu_f(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float dsilu_f(float z) {
+  const float s = 1.0f / (1.0f + expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+__device__ __forceinline__ uint16_t bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ uint32_t ld2(const uint16_t *p) { return *reinterpret_cast<const uint32_t *>(p); }
+
+// D += A B with A 16x16 (row-major fragment), B 16x8 (column-major fragment), BF16 in, FP32 acc.
+__device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// A fragment of rows [r, r+16), columns [k, k+16) of a row-major BF16 tile with leading dimension ld.
+__device__ __forceinline__ void frag_a(const uint16_t *s, int ld, int r, int k, int g, int t, uint32_t a[4]) {
+  a[0] = ld2(s + (r + g) * ld + k + 2 * t);
+  a[1] = ld2(s + (r + g + 8) * ld + k + 2 * t);
+  a[2] = ld2(s + (r + g) * ld + k + 2 * t + 8);
+  a[3] = ld2(s + (r + g + 8) * ld + k + 2 * t + 8);
+}
+// B fragment of columns [n, n+8), rows [k, k+16) of B, stored as B^T row-major ([n][k], ld).
+__device__ __forceinline__ void frag_b(const uint16_t *s, int ld, int n, int k, int g, int t, uint32_t b[2]) {
+  b[0] = ld2(s + (n + g) * ld + k + 2 * t);
+  b[1] = ld2(s + (n + g) * ld + k + 2 * t + 8);
+}
+
+// Value of column k of input row `row` (the segments side by side).
+__device__ __forceinline__ float seg_value(const SegDev *seg, int nseg, int row, int k) {
+  int off = 0;
+  for (int s = 0; s < nseg; s++) {
+    const int w = seg[s].width;
+    if (k < off + w) {
+      const int r = seg[s].idx ? seg[s].idx[row] : row;
+      const float v = seg[s].src[(size_t)r * seg[s].ld + (k - off)];
+      return seg[s].silu ? silu_f(v) : v;
+    }
+    off += w;
+  }
+  return 0.0f;
+}
+
+struct FwdArgs {
+  int M, K, N2, nseg;
+  SegDev seg[3];
+  const float *w1, *b1, *w2, *b2, *resid;
+  int ld_resid;
+  float *z1, *y;
+  int ld_y;
+};
+
+__global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  const int Kp = (a.K + 15) & ~15, LDX = Kp + 8, N2p = (a.N2 + 7) & ~7;
+  uint16_t *sW1 = sm;                // [HID][LDX]      W1 (B operand of GEMM 1, [n][k])
+  uint16_t *sW2 = sW1 + HID * LDX;   // [N2p][LDH]      W2 (B operand of GEMM 2)
+  uint16_t *sX = sW2 + N2p * LDH;    // [TM][LDX]       input rows
+  uint16_t *sS = sX + TM * LDX;      // [TM][LDH]       silu(z1)
+  for (int e = threadIdx.x; e < HID * Kp; e += blockDim.x) {
+    const int n = e / Kp, k = e - n * Kp;
+    sW1[n * LDX + k] = k < a.K ? bf(a.w1[n * a.K + k]) : 0;
+  }
+  for (int e = threadIdx.x; e < N2p * HID; e += blockDim.x) {
+    const int n = e / HID, k = e - n * HID;
+    sW2[n * LDH + k] = n < a.N2 ? bf(a.w2[n * HID + k]) : 0;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, wr = warp * 16;
+  const int ntiles = (a.M + TM - 1) / TM;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * TM;
+    __syncthreads();
+    for (int e = threadIdx.x; e < TM * Kp; e += blockDim.x) {
+      const int r = e / Kp, k = e - r * Kp, row = r0 + r;
+      sX[r * LDX + k] = (row < a.M && k < a.K) ? bf(seg_value(a.seg, a.nseg, row, k)) : 0;
+    }
+    __syncthreads();
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+    for (int k0 = 0; k0 < Kp; k0 += 16) {
+      uint32_t af[4];
+      frag_a(sX, LDX, wr, k0, g, t, af);
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        uint32_t bfr[2];
+        frag_b(sW1, LDX, nt * 8, k0, g, t, bfr);
+        mma16816(acc[nt], af, bfr);
+      }
+    }
+    const int ra = r0 + wr + g, rb = ra + 8;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const int col = nt * 8 + 2 * t;
+      const float b0 = a.b1[col], b1v = a.b1[col + 1];
+      const float z00 = acc[nt][0] + b0, z01 = acc[nt][1] + b1v, z10 = acc[nt][2] + b0, z11 = acc[nt][3] + b1v;
+      if (a.z1) {
+        if (ra < a.M) *reinterpret_cast<float2 *>(a.z1 + (size_t)ra * HID + col) = make_float2(z00, z01);
+        if (rb < a.M) *reinterpret_cast<float2 *>(a.z1 + (size_t)rb * HID + col) = make_float2(z10, z11);
+      }
+      sS[(wr + g) * LDH + col] = bf(silu_f(z00));
+      sS[(wr + g) * LDH + col + 1] = bf(silu_f(z01));
+      sS[(wr + g + 8) * LDH + col] = bf(silu_f(z10));
+      sS[(wr + g + 8) * LDH + col + 1] = bf(silu_f(z11));
+    }
+    __syncwarp();
+    float acc2[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) acc2[nt][0] = acc2[nt][1] = acc2[nt][2] = acc2[nt][3] = 0.0f;
+#pragma unroll
+    for (int k0 = 0; k0 < HID; k0 += 16) {
+      uint32_t af[4];
+      frag_a(sS, LDH, wr, k0, g, t, af);
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        if (nt * 8 < N2p) {
+          uint32_t bfr[2];
+          frag_b(sW2, LDH, nt * 8, k0, g, t, bfr);
+          mma16816(acc2[nt], af, bfr);
+        }
+      }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const int col = nt * 8 + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int row = h ? rb : ra;
+        if (row >= a.M) continue;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = col + q;
+          if (c >= a.N2) continue;
+          float v = acc2[nt][2 * h + q] + a.b2[c];
+          if (a.resid) v += a.resid[(size_t)row * a.ld_resid + c];
+          a.y[(size_t)row * a.ld_y + c] = v;
+        }
+      }
+    }
+  }
+}
+
+struct BwdArgs {
+  int M, K, N2;
+  const float *dy;
+  int ld_dy;
+  const float *z1, *w1, *w2;
+  float *dz1, *dx;
+  int ld_dx;
+};
+
+__global__ void __launch_bounds__(128) k_mlp_bwd(BwdArgs a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  const int Kp = (a.K + 15) & ~15, N2p = (a.N2 + 15) & ~15, LDN = N2p + 8;
+  uint16_t *sW2T = sm;                 // [HID][LDN]   W2^T: B operand of dS = dY W2
+  uint16_t *sW1T = sW2T + HID * LDN;   // [Kp][LDH]    W1^T: B operand of dX = dZ1 W1
+  uint16_t *sDY = sW1T + Kp * LDH;     // [TM][LDN]
+  uint16_t *sDZ = sDY + TM * LDN;      // [TM][LDH]
+  for (int e = threadIdx.x; e < HID * N2p; e += blockDim.x) {
+    const int j = e / N2p, o = e - j * N2p;
+    sW2T[j * LDN + o] = o < a.N2 ? bf(a.w2[o * HID + j]) : 0;
+  }
+  for (int e = threadIdx.x; e < Kp * HID; e += blockDim.x) {
+    const int c = e / HID, j = e - c * HID;
+    sW1T[c * LDH + j] = c < a.K ? bf(a.w1[j * a.K + c]) : 0;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, wr = warp * 16;
+  const int ntiles = (a.M + TM - 1) / TM;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * TM;
+    __syncthreads();
+    for (int e = threadIdx.x; e < TM * N2p; e += blockDim.x) {
+      const int r = e / N2p, o = e - r * N2p, row = r0 + r;
+      sDY[r * LDN + o] = (row < a.M && o < a.N2) ? bf(a.dy[(size_t)row * a.ld_dy + o]) : 0;
+    }
+    __syncthreads();
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+    for (int k0 = 0; k0 < N2p; k0 += 16) {
+      uint32_t af[4];
+      frag_a(sDY, LDN, wr, k0, g, t, af);
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        uint32_t bfr[2];
+        frag_b(sW2T, LDN, nt * 8, k0, g, t, bfr);
+        mma16816(acc[nt], af, bfr);
+      }
+    }
+    const int ra = r0 + wr + g, rb = ra + 8;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const int col = nt * 8 + 2 * t;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int row = h ? rb : ra;
+        float d0 = 0.0f, d1 = 0.0f;
+        if (row < a.M) {
+          const float2 z = *reinterpret_cast<const float2 *>(a.z1 + (size_t)row * HID + col);
+          d0 = acc[nt][2 * h] * dsilu_f(z.x);
+          d1 = acc[nt][2 * h + 1] * dsilu_f(z.y);
+          *reinterpret_cast<float2 *>(a.dz1 + (size_t)row * HID + col) = make_float2(d0, d1);
+        }
+        sDZ[(wr + g + 8 * h) * LDH + col] = bf(d0);
+        sDZ[(wr + g + 8 * h) * LDH + col + 1] = bf(d1);
+      }
+    }
+    __syncwarp();
+    if (!a.dx) continue;
+    for (int c0 = 0; c0 < Kp; c0 += 64) {
+      float ax[8][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) ax[nt][0] = ax[nt][1] = ax[nt][2] = ax[nt][3] = 0.0f;
+#pragma unroll
+      for (int k0 = 0; k0 < HID; k0 += 16) {
+        uint32_t af[4];
+        frag_a(sDZ, LDH, wr, k0, g, t, af);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+          if (c0 + nt * 8 < Kp) {
+            uint32_t bfr[2];
+            frag_b(sW1T, LDH, c0 + nt * 8, k0, g, t, bfr);
+            mma16816(ax[nt], af, bfr);
+          }
+        }
+      }
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        const int col = c0 + nt * 8 + 2 * t;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int row = h ? rb : ra;
+          if (row >= a.M) continue;
+          if (col < a.K) a.dx[(size_t)row * a.ld_dx + col] = ax[nt][2 * h];
+          if (col + 1 < a.K) a.dx[(size_t)row * a.ld_dx + col + 1] = ax[nt][2 * h + 1];
+        }
+      }
+    }
+  }
+}
+
+struct WgArgs {
+  int M, N, K, nseg;
+  SegDev seg[3];
+  const float *dz;
+  int ld_dz;
+  float *partial;  // [gridDim.x][N*K + N]
+};
+
+// dW[n][c] = sum over rows of dz[row][n] x[row][c] as D = A B with A = dz^T (N x TM) and
+// B = x (TM x K).  MT = number of 16-row tiles of N (1 or 4); the four warps split the N tiles
+// and the 8-column tiles of K between them.
+template <int MT>
+__global__ void __launch_bounds__(128) k_wgrad(WgArgs a) {
+  extern __shared__ __align__(16) uint16_t sm[];
+  constexpr int WPM = 4 / MT;            // warps per N tile
+  constexpr int NTW = (KMAX / 8 + WPM - 1) / WPM;  // K tiles per warp, at most
+  const int Kp = (a.K + 15) & ~15, Np = MT * 16;
+  uint16_t *sDZT = sm;                 // [Np][LDT]   dz^T
+  uint16_t *sXT = sDZT + Np * LDT;     // [Kp][LDT]   x^T
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int mrow = (warp % MT) * 16, ntile0 = warp / MT;
+  const int nkt = Kp / 8;
+  float acc[NTW][4];
+#pragma unroll
+  for (int i = 0; i < NTW; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0f;
+  float bsum = 0.0f;
+  const int ntiles = (a.M + TM - 1) / TM;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * TM;
+    __syncthreads();
+    for (int e = threadIdx.x; e < TM * Np; e += blockDim.x) {
+      const int m = e / Np, n = e - m * Np, row = r0 + m;
+      sDZT[n * LDT + m] = (row < a.M && n < a.N) ? bf(a.dz[(size_t)row * a.ld_dz + n]) : 0;
+    }
+    for (int e = threadIdx.x; e < TM * Kp; e += blockDim.x) {
+      const int m = e / Kp, c = e - m * Kp, row = r0 + m;
+      sXT[c * LDT + m] = (row < a.M && c < a.K) ? bf(seg_value(a.seg, a.nseg, row, c)) : 0;
+    }
+    if (threadIdx.x < a.N) {
+      const int rend = min(TM, a.M - r0);
+      for (int m = 0; m < rend; m++) bsum += a.dz[(size_t)(r0 + m) * a.ld_dz + threadIdx.x];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k0 = 0; k0 < TM; k0 += 16) {
+      uint32_t af[4];
+      frag_a(sDZT, LDT, mrow, k0, g, t, af);
+#pragma unroll
+      for (int i = 0; i < NTW; i++) {
+        const int kt = ntile0 + i * WPM;
+        if (kt < nkt) {
+          uint32_t bfr[2];
+          frag_b(sXT, LDT, kt * 8, k0, g, t, bfr);
+          mma16816(acc[i], af, bfr);
+        }
+      }
+    }
+  }
+  float *out = a.partial + (size_t)blockIdx.x * (a.N * a.K + a.N);
+#pragma unroll
+  for (int i = 0; i < NTW; i++) {
+    const int kt = ntile0 + i * WPM;
+    if (kt >= nkt) continue;
+    const int c = kt * 8 + 2 * t;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int n = mrow + g + 8 * h;
+      if (n >= a.N) continue;
+      if (c < a.K) out[n * a.K + c] = acc[i][2 * h];
+      if (c + 1 < a.K) out[n * a.K + c + 1] = acc[i][2 * h + 1];
+    }
+  }
+  if (threadIdx.x < a.N) out[a.N * a.K + threadIdx.x] = bsum;
+}
+
+// dw[j] (j < N*K) and db[j] (j < N) from the per-block partials, summed in block order.
+__global__ void k_wgrad_reduce(const float *__restrict__ partial, int nblk, int N, int K, float *__restrict__ dw,
+                               float *__restrict__ db, int accumulate) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = N * K + N;
+  if (j >= stride) return;
+  float s = 0.0f;
+  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * stride + j];
+  float *o = j < N * K ? dw + j : db + (j - N * K);
+  *o = accumulate ? *o + s : s;
+}
+
+// out[r][j] = a[r][j] + b[r][j] (j < width; leading dimensions given).
+__global__ void k_add(float *out, int ldo, const float *a, int lda, const float *b, int ldb, int rows, int width) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)rows * width) return;
+  const int r = (int)(e / width), j = (int)(e - (size_t)r * width);
+  out[(size_t)r * ldo + j] = a[(size_t)r * lda + j] + b[(size_t)r * ldb + j];
+}
+
+// out[r][j] += src[idx[r]][j].
+__global__ void k_gather_add(float *out, int ldo, const float *src, int lds, const int *idx, int rows, int width) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)rows * width) return;
+  const int r = (int)(e / width), j = (int)(e - (size_t)r * width);
+  out[(size_t)r * ldo + j] += src[(size_t)idx[r] * lds + j];
+}
+
+// out[r][:] (+)= sum over j in [ptr[r], ptr[r+1]) of x[idx[j]][:], in list order (warp per row).
+__global__ void k_segment_sum_acc(const float *__restrict__ x, int ldx, const int *__restrict__ ptr,
+                                  const int *__restrict__ idx, int n_rows, int width, float *__restrict__ out, int ldo,
+                                  int accumulate) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n_rows) return;
+  const int b = ptr[row], e = ptr[row + 1];
+  for (int col = lane; col < width; col += 32) {
+    float acc = 0.f;
+    for (int j = b; j < e; j++) acc += x[(size_t)idx[j] * ldx + col];
+    float *o = out + (size_t)row * ldo + col;
+    *o = accumulate ? *o + acc : acc;
+  }
+}
+
+// Mean-squared error: grad = 2 (pred - target) / n and loss = sum (pred - target)^2 / n, one block,
+// fixed-order tree.
+__global__ void __launch_bounds__(1024) k_mse(const float *pred, const float *target, int n, float *grad, float *loss) {
+  __shared__ float sh[1024];
+  float s = 0.0f;
+  const float inv = 1.0f / (float)n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float d = pred[i] - target[i];
+    grad[i] = 2.0f * d * inv;
+    s += d * d;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 512; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *loss = sh[0] * inv;
+}
+
+cfd_status status_of(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return CFD_OK;
+  cfdb::set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return CFD_ERR_CUDA;
+}
+
+cfd_status bad(const char *what) {
+  cfdb::set_last_error(what);
+  return CFD_ERR_BAD_ARG;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+bool copy_segs(int nseg, const cfd_mlp_seg *in, SegDev *out, int &K) {
+  if (nseg < 1 || nseg > 3) return false;
+  K = 0;
+  for (int s = 0; s < nseg; s++) {
+    if (!in[s].src || in[s].width < 1 || in[s].ld < in[s].width) return false;
+    out[s] = SegDev{in[s].src, in[s].idx, in[s].width, in[s].ld, in[s].silu};
+    K += in[s].width;
+  }
+  for (int s = nseg; s < 3; s++) out[s] = SegDev{nullptr, nullptr, 0, 0, 0};
+  return K <= KMAX;
+}
+
+size_t fwd_smem(int K, int N2) {
+  const int Kp = (K + 15) & ~15, LDX = Kp + 8, N2p = (N2 + 7) & ~7;
+  return sizeof(uint16_t) * ((size_t)HID * LDX + (size_t)N2p * LDH + (size_t)TM * LDX + (size_t)TM * LDH);
+}
+size_t bwd_smem(int K, int N2) {
+  const int Kp = (K + 15) & ~15, N2p = (N2 + 15) & ~15, LDN = N2p + 8;
+  return sizeof(uint16_t) * ((size_t)HID * LDN + (size_t)Kp * LDH + (size_t)TM * LDN + (size_t)TM * LDH);
+}
+size_t wg_smem(int K, int MT) {
+  const int Kp = (K + 15) & ~15;
+  return sizeof(uint16_t) * ((size_t)MT * 16 * LDT + (size_t)Kp * LDT);
+}
+
+template <typename F>
+void set_smem(F f, size_t bytes) {
+  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfd_mpnn_wgrad_blocks(void) { return CFD_MPNN_WGRAD_BLOCKS; }
+
+cfd_status cfd_mpnn_mlp_forward(const cfd_mlp_fwd *p, void *stream) {
+  if (!p || p->rows < 0 || p->out < 1 || p->out > HID || !p->w1 || !p->b1 || !p->w2 || !p->b2 || !p->y ||
+      p->ld_y < p->out || (p->resid && p->ld_resid < p->out))
+    return bad("cfd_mpnn_mlp_forward: bad argument");
+  FwdArgs a{};
+  if (!copy_segs(p->nseg, p->seg, a.seg, a.K)) return bad("cfd_mpnn_mlp_forward: bad input segments (total width <= 192)");
+  if (p->rows == 0) return CFD_OK;
+  a.M = p->rows;
+  a.N2 = p->out;
+  a.nseg = p->nseg;
+  a.w1 = p->w1;
+  a.b1 = p->b1;
+  a.w2 = p->w2;
+  a.b2 = p->b2;
+  a.resid = p->resid;
+  a.ld_resid = p->ld_resid;
+  a.z1 = p->z1;
+  a.y = p->y;
+  a.ld_y = p->ld_y;
+  const size_t sm = fwd_smem(a.K, a.N2);
+  set_smem(k_mlp_fwd, sm);
+  const int ntiles = (a.M + TM - 1) / TM;
+  const int grid = ntiles < 3 * sm_count() ? ntiles : 3 * sm_count();
+  k_mlp_fwd<<<grid, 128, sm, static_cast<cudaStream_t>(stream)>>>(a);
+  return status_of("cfd_mpnn_mlp_forward");
+}
+
+cfd_status cfd_mpnn_mlp_backward(const cfd_mlp_bwd *p, void *stream) {
+  if (!p || p->rows < 0 || p->in_width < 1 || p->in_width > KMAX || p->out < 1 || p->out > HID || !p->dy ||
+      p->ld_dy < p->out || !p->z1 || !p->w1 || !p->w2 || !p->dz1 || (p->dx && p->ld_dx < p->in_width))
+    return bad("cfd_mpnn_mlp_backward: bad argument");
+  if (p->rows == 0) return CFD_OK;
+  BwdArgs a{p->rows, p->in_width, p->out, p->dy, p->ld_dy, p->z1, p->w1, p->w2, p->dz1, p->dx, p->ld_dx};
+  const size_t sm = bwd_smem(a.K, a.N2);
+  set_smem(k_mlp_bwd, sm);
+  const int ntiles = (a.M + TM - 1) / TM;
+  const int grid = ntiles < 3 * sm_count() ? ntiles : 3 * sm_count();
+  k_mlp_bwd<<<grid, 128, sm, static_cast<cudaStream_t>(stream)>>>(a);
+  return status_of("cfd_mpnn_mlp_backward");
+}
+
+cfd_status cfd_mpnn_weight_grad(const cfd_mlp_wgrad *p, void *stream) {
+  if (!p || p->rows < 0 || !(p->n == HID || (p->n >= 1 && p->n <= 16)) || !p->dz || p->ld_dz < p->n || !p->dw ||
+      !p->db || !p->workspace)
+    return bad("cfd_mpnn_weight_grad: bad argument (n must be 64 or at most 16)");
+  WgArgs a{};
+  int K = 0;
+  if (!copy_segs(p->nseg, p->seg, a.seg, K)) return bad("cfd_mpnn_weight_grad: bad input segments (total width <= 192)");
+  a.M = p->rows;
+  a.N = p->n;
+  a.K = K;
+  a.nseg = p->nseg;
+  a.dz = p->dz;
+  a.ld_dz = p->ld_dz;
+  a.partial = p->workspace;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int ntiles = (a.M + TM - 1) / TM;
+  const int grid = ntiles < 1 ? 1 : (ntiles < CFD_MPNN_WGRAD_BLOCKS ? ntiles : CFD_MPNN_WGRAD_BLOCKS);
+  if (a.N == HID) {
+    const size_t sm = wg_smem(K, 4);
+    set_smem(k_wgrad<4>, sm);
+    k_wgrad<4><<<grid, 128, sm, s>>>(a);
+  } else {
+    const size_t sm = wg_smem(K, 1);
+    set_smem(k_wgrad<1>, sm);
+    k_wgrad<1><<<grid, 128, sm, s>>>(a);
+  }
+  cfd_status st = status_of("cfd_mpnn_weight_grad");
+  if (st != CFD_OK) return st;
+  const int total = a.N * a.K + a.N;
+  k_wgrad_reduce<<<(total + 255) / 256, 256, 0, s>>>(a.partial, grid, a.N, a.K, p->dw, p->db, p->accumulate);
+  return status_of("cfd_mpnn_weight_grad (reduce)");
+}
+
+cfd_status cfd_mpnn_add(float *out, int ldo, const float *a, int lda, const float *b, int ldb, int rows, int width,
+                        void *stream) {
+  if (rows < 0 || width < 1 || ldo < width || lda < width || ldb < width || (rows > 0 && (!out || !a || !b)))
+    return bad("cfd_mpnn_add: bad argument");
+  if (rows == 0) return CFD_OK;
+  const size_t n = (size_t)rows * width;
+  k_add<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, ldo, a, lda, b, ldb, rows,
+                                                                                    width);
+  return status_of("cfd_mpnn_add");
+}
+
+cfd_status cfd_mpnn_gather_add(float *out, int ldo, const float *src, int lds, const int *idx, int rows, int width,
+                               void *stream) {
+  if (rows < 0 || width < 1 || ldo < width || lds < width || (rows > 0 && (!out || !src || !idx)))
+    return bad("cfd_mpnn_gather_add: bad argument");
+  if (rows == 0) return CFD_OK;
+  const size_t n = (size_t)rows * width;
+  k_gather_add<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, ldo, src, lds, idx,
+                                                                                           rows, width);
+  return status_of("cfd_mpnn_gather_add");
+}
+
+cfd_status cfd_mpnn_segment_sum_acc(const float *x, int ldx, const int *ptr, const int *idx, int n_rows, int width,
+                                    float *out, int ldo, int accumulate, void *stream) {
+  if (n_rows < 0 || width < 1 || ldx < width || ldo < width || (n_rows > 0 && (!x || !ptr || !idx || !out)))
+    return bad("cfd_mpnn_segment_sum_acc: bad argument");
+  if (n_rows == 0) return CFD_OK;
+  const int rows_per_block = 256 / 32;
+  k_segment_sum_acc<<<(n_rows + rows_per_block - 1) / rows_per_block, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      x, ldx, ptr, idx, n_rows, width, out, ldo, accumulate);
+  return status_of("cfd_mpnn_segment_sum_acc");
+}
+
+cfd_status cfd_mpnn_mse(const float *pred, const float *target, int n, float *grad, float *loss, void *stream) {
+  if (n < 1 || !pred || !target || !grad || !loss) return bad("cfd_mpnn_mse: bad argument");
+  k_mse<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(pred, target, n, grad, loss);
+  return status_of("cfd_mpnn_mse");
+}
+
+}  // extern "C"

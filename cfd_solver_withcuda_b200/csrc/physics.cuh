@@ -64,11 +64,13 @@ __device__ __forceinline__ void average_flux(const T rL, const T uL, const T vL,
 }
 
 // The wave-decomposition tail shared by ROE and ROE_2O (src/Roe_Scheme.cpp:193-228, :376-423):
-// eigenvalues with Harten's fix delta = 0.1*a_Roe, right eigenvectors, D = 0.5*sum|l|a r*dl.
+// eigenvalues with Harten's fix delta = 0.1*a_Roe on the acoustic waves, right eigenvectors,
+// D = 0.5*sum|l|a r*dl.  eflin > 0 (no reference counterpart; the gradient-MUSCL form's option
+// against the carbuncle) also fixes the two linear waves, |Un| below eflin*a_Roe.
 template <typename T>
 __device__ __forceinline__ void roe_tail(const T Ru, const T Rv, const T RH, const T RVm, const T Ra, const T RoeRho,
                                          const T Un, const T Ut, const T dP, const T dRho, const T dUn, const T dUt,
-                                         const T nx, const T ny, const T dl, T D[4]) {
+                                         const T nx, const T ny, const T dl, T D[4], const T eflin = T(0.0)) {
   T R11 = T(1.0), R12 = Ru - nx * Ra, R13 = Rv - ny * Ra, R14 = RH - Ra * Un;
   T R21 = T(1.0), R22 = Ru, R23 = Rv, R24 = RVm;
   T R31 = T(0.0), R32 = -ny, R33 = nx, R34 = Ut;
@@ -82,6 +84,13 @@ __device__ __forceinline__ void roe_tail(const T Ru, const T Rv, const T RH, con
   T ef = T(0.1) * Ra;
   if (L1 < ef) L1 = T(0.5) * (L1 * L1 / ef + ef);
   if (L4 < ef) L4 = T(0.5) * (L4 * L4 / ef + ef);
+  if (eflin > T(0.0)) {
+    const T el = eflin * Ra;
+    if (L2 < el) {
+      L2 = T(0.5) * (L2 * L2 / el + el);
+      L3 = L2;
+    }
+  }
   D[0] = T(0.5) * (L1 * a1 * R11 + L2 * a2 * R21 + L3 * a3 * R31 + L4 * a4 * R41) * dl;
   D[1] = T(0.5) * (L1 * a1 * R12 + L2 * a2 * R22 + L3 * a3 * R32 + L4 * a4 * R42) * dl;
   D[2] = T(0.5) * (L1 * a1 * R13 + L2 * a2 * R23 + L3 * a3 * R33 + L4 * a4 * R43) * dl;
@@ -93,7 +102,7 @@ __device__ __forceinline__ void roe_tail(const T Ru, const T Rv, const T RH, con
 template <typename T>
 __device__ __forceinline__ void roe_1o(const T rL, const T uL, const T vL, const T pL, const T cL, const T rR,
                                        const T uR, const T vR, const T pR, const T cR, const T nx, const T ny,
-                                       const T dl, bool degenerate, T D[4]) {
+                                       const T dl, bool degenerate, T D[4], const T eflin = T(0.0)) {
   D[0] = D[1] = D[2] = D[3] = T(0.0);
   if (degenerate) return;
   if (rL <= T(0.0) || pL <= T(0.0) || cL <= T(0.0)) return;
@@ -119,7 +128,7 @@ __device__ __forceinline__ void roe_1o(const T rL, const T uL, const T vL, const
   T du = (uR - uL), dv = (vR - vL), dP = (pR - pL), dRho = (rR - rL);
   T dUn = nx * du + ny * dv;
   T dUt = -ny * du + nx * dv;
-  roe_tail<T>(Ru, Rv, RH, RVm, Ra, RoeRho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D);
+  roe_tail<T>(Ru, Rv, RH, RVm, Ra, RoeRho, Un, Ut, dP, dRho, dUn, dUt, nx, ny, dl, D, eflin);
 }
 
 // ROE_2O, src/Roe_Scheme.cpp:257-447: Roe averages of the unreconstructed cell states, wave

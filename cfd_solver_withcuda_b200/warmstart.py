@@ -10,9 +10,11 @@ cell graph (cells as nodes, faces as directed edges) maps (geometry, t, M, ratio
 
 The network: node and edge encoders, L message-passing layers (edge update from the two end
 cells and the edge, aggregation of the incoming messages of each cell in a fixed order, node
-update), a decoder; width 64, SiLU, residual updates.  Dense layers run as BF16 GEMMs with FP32
-accumulation (torch autocast, cuBLAS); the graph operations are the library's deterministic segment
-sums (cfd_mpnn_segment_sum) and the optimiser its fused Adam step (cfd_mpnn_adam).
+update), a decoder; width 64, SiLU, residual updates.  Forward, backward and optimiser are the
+library's own kernels: the dense blocks on the tensor cores with BF16 operands and FP32
+accumulation (cfd_mpnn_mlp_forward / _backward / cfd_mpnn_weight_grad), the graph operations as
+deterministic segment sums and gathers, the loss gradient and a fused Adam step.  torch only
+allocates the device buffers.
 """
 import ctypes
 import time
@@ -166,11 +168,19 @@ def primitive(U):
 
 
 # ---------------------------------------------------------------------------------------------
-# Network (torch: tensors, autocast GEMMs; graph operations and optimiser: library kernels)
+# Network: the library's kernels (csrc/mpnn_tc.cu, csrc/mpnn.cu); torch only holds device memory
 # ---------------------------------------------------------------------------------------------
 def _torch():
     import torch
     return torch
+
+
+def _ptr(t, col=0):
+    return ctypes.c_void_p(t.data_ptr() + 4 * col) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(t):
+    return ctypes.c_void_p(_torch().cuda.current_stream(t.device).cuda_stream)
 
 
 def segment_sum(x, ptr, idx, n_rows):
@@ -178,45 +188,9 @@ def segment_sum(x, ptr, idx, n_rows):
     torch = _torch()
     x = x.float().contiguous()
     out = torch.empty((n_rows, x.shape[1]), dtype=torch.float32, device=x.device)
-    st = torch.cuda.current_stream(x.device).cuda_stream
-    cb._check(cb.lib().cfd_mpnn_segment_sum(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ptr.data_ptr()),
-                                            ctypes.c_void_p(idx.data_ptr()), n_rows, x.shape[1],
-                                            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st)))
+    cb._check(cb.lib().cfd_mpnn_segment_sum(_ptr(x), _ptr(ptr), _ptr(idx), n_rows, x.shape[1], _ptr(out),
+                                            _stream(x)))
     return out
-
-
-def _functions():
-    torch = _torch()
-
-    class Gather(torch.autograd.Function):
-        """Rows h[idx]; the backward pass sums the row gradients of each source row over the CSR
-        list (ptr, order) of the rows that read it, in a fixed order."""
-
-        @staticmethod
-        def forward(ctx, h, idx, ptr, order):
-            ctx.save_for_backward(ptr, order)
-            ctx.n = h.shape[0]
-            return h.index_select(0, idx.long())
-
-        @staticmethod
-        def backward(ctx, g):
-            ptr, order = ctx.saved_tensors
-            return segment_sum(g, ptr, order, ctx.n), None, None, None
-
-    class Aggregate(torch.autograd.Function):
-        """Sum of the incoming edge messages of each cell (edges sorted by destination)."""
-
-        @staticmethod
-        def forward(ctx, m, ptr, ident, dst):
-            ctx.save_for_backward(dst)
-            return segment_sum(m, ptr, ident, ptr.shape[0] - 1)
-
-        @staticmethod
-        def backward(ctx, g):
-            (dst,) = ctx.saved_tensors
-            return g.index_select(0, dst.long()), None, None, None
-
-    return Gather, Aggregate
 
 
 class GraphBatch:
@@ -238,110 +212,243 @@ class GraphBatch:
         self.ident = t(np.arange(B * E))
 
 
-def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0):
-    """Encoders, `layers` message-passing layers and a decoder (about 187k parameters at width 64,
-    6 layers)."""
-    torch = _torch()
-    nn = torch.nn
-    torch.manual_seed(seed)
-    Gather, Aggregate = _functions()
-
-    def mlp(i, o):
-        return nn.Sequential(nn.Linear(i, width), nn.SiLU(), nn.Linear(width, o))
-
-    class MPNN(nn.Module):
-        def __init__(self):
-            super().__init__()
-            self.enc_n = mlp(node_in, width)
-            self.enc_e = mlp(edge_in, width)
-            self.edge = nn.ModuleList([mlp(3 * width, width) for _ in range(layers)])
-            self.node = nn.ModuleList([mlp(2 * width, width) for _ in range(layers)])
-            self.dec = mlp(width, out)
-
-        def forward(self, xn, xe, gb):
-            h = self.enc_n(xn).float()
-            e = self.enc_e(xe).float()
-            for fe, fn in zip(self.edge, self.node):
-                hs = Gather.apply(h, gb.src, gb.src_ptr, gb.src_order)
-                hd = Gather.apply(h, gb.dst, gb.dst_ptr, gb.ident)
-                e = e + fe(torch.cat([hs, hd, e], dim=1)).float()
-                agg = Aggregate.apply(e, gb.dst_ptr, gb.ident, gb.dst)
-                h = h + fn(torch.cat([h, agg], dim=1)).float()
-            return self.dec(h).float()
-
-    return MPNN()
+def _seg(t, idx=None, col=0, width=None, silu=0):
+    """One input segment: columns [col, col + width) of the rows of t (through idx when given)."""
+    return (t, idx, col, t.shape[1] - col if width is None else width, silu)
 
 
-class Adam:
-    """Adam on the model's FP32 parameters with the library's fused step (cfd_mpnn_adam)."""
+class Net:
+    """The message-passing surrogate: node and edge encoders, `layers` message-passing layers
+    (edge update from the two end cells and the edge, in-order aggregation of each cell's incoming
+    messages, node update; residual updates), a decoder; every block a two-layer perceptron
+    W2 silu(W1 x + b1) + b2 of hidden width 64.  Parameters live in one FP32 device buffer (master
+    copy; the kernels round operands to BF16 and accumulate in FP32); forward, backward and Adam
+    are the library's kernels; torch provides device buffers only."""
 
-    def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8):
+    HIDDEN = 64
+
+    def __init__(self, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda"):
         torch = _torch()
-        self.params = [p for p in params if p.requires_grad]
-        self.m = [torch.zeros_like(p) for p in self.params]
-        self.v = [torch.zeros_like(p) for p in self.params]
-        self.lr, self.b1, self.b2, self.eps, self.t = lr, betas[0], betas[1], eps, 0
+        W = self.HIDDEN
+        self.L, self.out, self.device = layers, out, torch.device(device)
+        self.dims = {"enc_n": (node_in, W), "enc_e": (edge_in, W), "dec": (W, out)}
+        for l in range(layers):
+            self.dims["edge%d" % l] = (3 * W, W)
+            self.dims["node%d" % l] = (2 * W, W)
+        self.names = ["enc_n", "enc_e"] + ["edge%d" % l for l in range(layers)] + \
+                     ["node%d" % l for l in range(layers)] + ["dec"]
+        sizes = [W * K + W + N * W + N for K, N in (self.dims[n] for n in self.names)]
+        self.n_params = int(sum(sizes))
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.flat = torch.zeros(self.n_params, **f32)
+        self.grad = torch.zeros(self.n_params, **f32)
+        self.m = torch.zeros(self.n_params, **f32)
+        self.v = torch.zeros(self.n_params, **f32)
+        self.p, self.g = {}, {}
+        o = 0
+        for name in self.names:
+            K, N = self.dims[name]
+            views = []
+            for buf, store in ((self.flat, self.p), (self.grad, self.g)):
+                q = o
+                w1 = buf[q:q + W * K].view(W, K); q += W * K
+                b1 = buf[q:q + W]; q += W
+                w2 = buf[q:q + N * W].view(N, W); q += N * W
+                b2 = buf[q:q + N]; q += N
+                store[name] = (w1, b1, w2, b2)
+            o = q
+        rng = np.random.default_rng(seed)
+        for name in self.names:
+            K, N = self.dims[name]
+            a, c = 1.0 / np.sqrt(K), 1.0 / np.sqrt(W)
+            vals = (rng.uniform(-a, a, (W, K)), rng.uniform(-a, a, W), rng.uniform(-c, c, (N, W)), rng.uniform(-c, c, N))
+            for dst, v in zip(self.p[name], vals):
+                dst.copy_(torch.from_numpy(v.astype(np.float32)))
+        self.workspace = torch.empty(cb.lib().cfd_mpnn_wgrad_blocks() * (W * 3 * W + W), **f32)
+        self.steps = 0
+        self._bufs = None
 
-    def step(self):
+    # -- parameters as numpy (tests, checkpoints)
+    def get_params(self):
+        return {n: tuple(t.detach().cpu().numpy().astype(np.float64) for t in self.p[n]) for n in self.names}
+
+    def set_params(self, P):
         torch = _torch()
-        self.t += 1
-        for p, m, v in zip(self.params, self.m, self.v):
-            if p.grad is None:
-                continue
-            g = p.grad.float().contiguous()
-            st = torch.cuda.current_stream(p.device).cuda_stream
-            cb._check(cb.lib().cfd_mpnn_adam(ctypes.c_void_p(p.data.data_ptr()), ctypes.c_void_p(g.data_ptr()),
-                                             ctypes.c_void_p(m.data_ptr()), ctypes.c_void_p(v.data_ptr()), p.numel(),
-                                             self.lr, self.b1, self.b2, self.eps, self.t, ctypes.c_void_p(st)))
+        for n in self.names:
+            for dst, v in zip(self.p[n], P[n]):
+                dst.copy_(torch.from_numpy(np.asarray(v, np.float32)))
 
-    def zero_grad(self):
-        for p in self.params:
-            p.grad = None
+    def get_grads(self):
+        return {n: tuple(t.detach().cpu().numpy().astype(np.float64) for t in self.g[n]) for n in self.names}
+
+    # -- buffers per (nodes, edges)
+    def _buffers(self, N, E):
+        if self._bufs is not None and self._bufs["key"] == (N, E):
+            return self._bufs
+        torch = _torch()
+        W, L = self.HIDDEN, self.L
+        f = lambda r, c: torch.empty((r, c), dtype=torch.float32, device=self.device)
+        b = {"key": (N, E), "h": [f(N, W) for _ in range(L + 1)], "e": [f(E, W) for _ in range(L + 1)],
+             "agg": [f(N, W) for _ in range(L)], "z_enc_n": f(N, W), "z_enc_e": f(E, W),
+             "z_edge": [f(E, W) for _ in range(L)], "z_node": [f(N, W) for _ in range(L)], "z_dec": f(N, W),
+             "pred": f(N, self.out), "dpred": f(N, self.out), "dh": f(N, W), "de": f(E, W),
+             "dx": f(max(N, E), 3 * W), "dz": f(max(N, E), W),
+             "loss": torch.zeros(1, dtype=torch.float32, device=self.device)}
+        self._bufs = b
+        return b
+
+    @staticmethod
+    def _segs(segs):
+        out = (cb.MlpSeg * 3)()
+        for i, (t, idx, col, width, silu) in enumerate(segs):
+            out[i].src = _ptr(t, col)
+            out[i].idx = _ptr(idx) if idx is not None else ctypes.c_void_p(0)
+            out[i].width, out[i].ld, out[i].silu = width, t.stride(0), silu
+        return out
+
+    def _mlp(self, name, segs, rows, y, z1, resid=None):
+        a = cb.MlpFwd()
+        a.rows, a.nseg, a.seg = rows, len(segs), self._segs(segs)
+        w1, b1, w2, b2 = self.p[name]
+        a.out = w2.shape[0]
+        a.w1, a.b1, a.w2, a.b2 = _ptr(w1), _ptr(b1), _ptr(w2), _ptr(b2)
+        a.resid = _ptr(resid)
+        a.ld_resid = resid.stride(0) if resid is not None else 0
+        a.z1, a.y, a.ld_y = _ptr(z1), _ptr(y), y.stride(0)
+        cb._check(cb.lib().cfd_mpnn_mlp_forward(ctypes.byref(a), _stream(y)))
+
+    def _mlp_back(self, name, dy, z1, rows, dx=None):
+        """dz1 of block `name` into the dz buffer; dx (the input gradient) when a buffer is given."""
+        b = self._bufs
+        w1, _, w2, _ = self.p[name]
+        a = cb.MlpBwd()
+        a.rows, a.in_width, a.out = rows, w1.shape[1], w2.shape[0]
+        a.dy, a.ld_dy, a.z1 = _ptr(dy), dy.stride(0), _ptr(z1)
+        a.w1, a.w2, a.dz1 = _ptr(w1), _ptr(w2), _ptr(b["dz"])
+        a.dx, a.ld_dx = _ptr(dx), dx.stride(0) if dx is not None else 0
+        cb._check(cb.lib().cfd_mpnn_mlp_backward(ctypes.byref(a), _stream(dy)))
+
+    def _wgrad(self, dz, rows, segs, dw, db):
+        a = cb.MlpWgrad()
+        a.rows, a.n, a.dz, a.ld_dz = rows, dw.shape[0], _ptr(dz), dz.stride(0)
+        a.nseg, a.seg = len(segs), self._segs(segs)
+        a.workspace, a.dw, a.db, a.accumulate = _ptr(self.workspace), _ptr(dw), _ptr(db), 0
+        cb._check(cb.lib().cfd_mpnn_weight_grad(ctypes.byref(a), _stream(dz)))
+
+    def _block_grads(self, name, dy, z1, rows, x_segs, dx=None):
+        """Parameter gradients of block `name` (and dx) from its output gradient dy."""
+        gw1, gb1, gw2, gb2 = self.g[name]
+        self._mlp_back(name, dy, z1, rows, dx)
+        self._wgrad(dy, rows, [_seg(z1, silu=1)], gw2, gb2)
+        self._wgrad(self._bufs["dz"], rows, x_segs, gw1, gb1)
+
+    def forward(self, xn, xe, gb):
+        """Prediction [nodes][out] for node features xn and edge features xe (float32 device
+        tensors) on the stacked graph gb; keeps the activations for backward()."""
+        N, E = xn.shape[0], xe.shape[0]
+        b = self._buffers(N, E)
+        h, e, agg = b["h"], b["e"], b["agg"]
+        self._mlp("enc_n", [_seg(xn)], N, h[0], b["z_enc_n"])
+        self._mlp("enc_e", [_seg(xe)], E, e[0], b["z_enc_e"])
+        lib, st = cb.lib(), _stream(xn)
+        for l in range(self.L):
+            self._mlp("edge%d" % l, [_seg(h[l], gb.src), _seg(h[l], gb.dst), _seg(e[l])], E, e[l + 1],
+                      b["z_edge"][l], resid=e[l])
+            cb._check(lib.cfd_mpnn_segment_sum_acc(_ptr(e[l + 1]), self.HIDDEN, _ptr(gb.dst_ptr), _ptr(gb.ident), N,
+                                                   self.HIDDEN, _ptr(agg[l]), self.HIDDEN, 0, st))
+            self._mlp("node%d" % l, [_seg(h[l]), _seg(agg[l])], N, h[l + 1], b["z_node"][l], resid=h[l])
+        self._mlp("dec", [_seg(h[self.L])], N, b["pred"], b["z_dec"])
+        self._graph = gb
+        self._x = (xn, xe)
+        return b["pred"]
+
+    def backward(self, dpred):
+        """Gradients of every parameter (into self.grad) from the prediction gradient dpred."""
+        b, gb, W, L = self._bufs, self._graph, self.HIDDEN, self.L
+        xn, xe = self._x
+        N, E = xn.shape[0], xe.shape[0]
+        lib, st = cb.lib(), _stream(dpred)
+        dh, de, dx = b["dh"], b["de"], b["dx"]
+        self._block_grads("dec", dpred, b["z_dec"], N, [_seg(b["h"][L])], dx=dh)
+        de.zero_()
+        for l in reversed(range(L)):
+            h, e, agg = b["h"][l], b["e"][l], b["agg"][l]
+            dxn = dx[:N, :2 * W]
+            self._block_grads("node%d" % l, dh, b["z_node"][l], N, [_seg(h), _seg(agg)], dx=dxn)
+            ldx = dx.stride(0)
+            cb._check(lib.cfd_mpnn_add(_ptr(dh), W, _ptr(dh), W, _ptr(dxn), ldx, N, W, st))
+            cb._check(lib.cfd_mpnn_gather_add(_ptr(de), W, _ptr(dxn, W), ldx, _ptr(gb.dst), E, W, st))
+            dxe = dx[:E, :3 * W]
+            self._block_grads("edge%d" % l, de, b["z_edge"][l], E, [_seg(h, gb.src), _seg(h, gb.dst), _seg(e)],
+                              dx=dxe)
+            cb._check(lib.cfd_mpnn_segment_sum_acc(_ptr(dxe), ldx, _ptr(gb.src_ptr), _ptr(gb.src_order), N, W,
+                                                   _ptr(dh), W, 1, st))
+            cb._check(lib.cfd_mpnn_segment_sum_acc(_ptr(dxe, W), ldx, _ptr(gb.dst_ptr), _ptr(gb.ident), N, W,
+                                                   _ptr(dh), W, 1, st))
+            cb._check(lib.cfd_mpnn_add(_ptr(de), W, _ptr(de), W, _ptr(dxe, 2 * W), ldx, E, W, st))
+        self._block_grads("enc_e", de, b["z_enc_e"], E, [_seg(xe)])
+        self._block_grads("enc_n", dh, b["z_enc_n"], N, [_seg(xn)])
+
+    def loss_grad(self, target):
+        """Mean-squared error of the last prediction against target (device scalar) and its
+        gradient into the dpred buffer."""
+        b = self._bufs
+        n = b["pred"].numel()
+        cb._check(cb.lib().cfd_mpnn_mse(_ptr(b["pred"]), _ptr(target), n, _ptr(b["dpred"]), _ptr(b["loss"]),
+                                        _stream(target)))
+        return b["loss"], b["dpred"]
+
+    def adam_step(self, lr=1e-3, betas=(0.9, 0.999), eps=1e-8):
+        """One Adam step over every parameter (cfd_mpnn_adam, one launch)."""
+        self.steps += 1
+        cb._check(cb.lib().cfd_mpnn_adam(_ptr(self.flat), _ptr(self.grad), _ptr(self.m), _ptr(self.v), self.n_params,
+                                         lr, betas[0], betas[1], eps, self.steps, _stream(self.flat)))
+
+
+def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda"):
+    """The surrogate (about 187k parameters at width 64, 6 layers)."""
+    assert width == Net.HIDDEN
+    return Net(layers=layers, node_in=node_in, edge_in=edge_in, out=out, seed=seed, device=device)
 
 
 def train(model, graph, node_feats, edge_feats, targets, epochs=200, batch=8, lr=1e-3, seed=0, device="cuda"):
-    """Mean-squared error on the normalised (rho, u, v, p) targets; returns the per-epoch loss."""
+    """Mean-squared error on the normalised (rho, u, v, p) targets, Adam; returns the per-epoch
+    loss."""
     torch = _torch()
-    model.to(device)
     rng = np.random.default_rng(seed)
     n = len(node_feats)
     xn = torch.from_numpy(np.stack(node_feats)).to(device)
     xe = torch.from_numpy(np.stack(edge_feats)).to(device)
     y = torch.from_numpy(np.stack(targets).astype(np.float32)).to(device)
-    opt = Adam(model.parameters(), lr=lr)
     batches = {}
     losses = []
     for ep in range(epochs):
         perm = rng.permutation(n)
-        tot = 0.0
+        tot = torch.zeros(1, dtype=torch.float64, device=device)
         for s in range(0, n, batch):
             idx = torch.from_numpy(perm[s:s + batch]).to(device)
             B = len(idx)
             if B not in batches:
                 batches[B] = GraphBatch(graph, B, device)
             gb = batches[B]
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                pred = model(xn[idx].reshape(-1, xn.shape[2]), xe[idx].reshape(-1, xe.shape[2]), gb)
-            loss = torch.mean((pred - y[idx].reshape(-1, 4)) ** 2)
-            opt.zero_grad()
-            loss.backward()
-            opt.step()
-            tot += float(loss.detach()) * B
-        losses.append(tot / n)
+            model.forward(xn[idx].reshape(-1, xn.shape[2]).contiguous(), xe[idx].reshape(-1, xe.shape[2]).contiguous(), gb)
+            loss, dpred = model.loss_grad(y[idx].reshape(-1, 4).contiguous())
+            model.backward(dpred)
+            model.adam_step(lr)
+            tot += loss.double() * B
+        losses.append(float(tot) / n)
     return losses
 
 
 def predict(model, graph, node_feats, edge_feats, batch=8, device="cuda"):
     torch = _torch()
     out = []
-    with torch.no_grad():
-        for s in range(0, len(node_feats), batch):
-            xn = torch.from_numpy(np.stack(node_feats[s:s + batch])).to(device)
-            xe = torch.from_numpy(np.stack(edge_feats[s:s + batch])).to(device)
-            gb = GraphBatch(graph, xn.shape[0], device)
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                p = model(xn.reshape(-1, xn.shape[2]), xe.reshape(-1, xe.shape[2]), gb)
-            out.extend(p.float().reshape(xn.shape[0], graph.N, 4).cpu().numpy())
+    for s in range(0, len(node_feats), batch):
+        xn = torch.from_numpy(np.stack(node_feats[s:s + batch])).to(device)
+        xe = torch.from_numpy(np.stack(edge_feats[s:s + batch])).to(device)
+        gb = GraphBatch(graph, xn.shape[0], device)
+        p = model.forward(xn.reshape(-1, xn.shape[2]).contiguous(), xe.reshape(-1, xe.shape[2]).contiguous(), gb)
+        out.extend(p.reshape(xn.shape[0], graph.N, 4).cpu().numpy())
     return out
 
 
@@ -383,7 +490,7 @@ def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-4, max_steps=150
 
     # 2. Surrogate training.
     model = build_model()
-    out["parameters"] = int(sum(p.numel() for p in model.parameters()))
+    out["parameters"] = model.n_params
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     losses = train(model, graph, [f[0] for f in feats[tr]], [f[1] for f in feats[tr]], norm, epochs=epochs,

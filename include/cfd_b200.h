@@ -143,13 +143,19 @@ typedef struct {
   int weno;                  /* Is_WENO: the reference's WENO path (Evaluate_Cell_Net_Flux_WENO,
                                 src/WENO2D.cpp:395-456; quad cells; replaces the MUSCL forms) */
   int weno_characteristic;   /* Is_Char: WENO on characteristic variables (src/WENO2D.cpp:228-236) */
+  double entropy_fix_linear; /* Harten's entropy fix on the linear (entropy and shear) waves of the
+                                Roe flux in the gradient-MUSCL form: |Un| below delta = value *
+                                a_Roe becomes (Un^2/delta + delta)/2.  0 (default): only the
+                                acoustic waves are fixed, with delta = 0.1 * a_Roe, as in the
+                                reference's ROE.  No reference counterpart; it suppresses the
+                                carbuncle of grid-aligned strong shocks (0.2 - 0.4 typical). */
 } cfd_config;
 
 /* Defaults of json_Files/Solver_Config.json with Dissipation_Type = ROE. */
 void cfd_config_default(cfd_config *cfg);
 /* Parses a Solver_Config JSON file (the reference schema; // comments allowed) into cfg.
  * Unknown keys are ignored; additive keys: Limiter_Type, Flux_Scheme, Integrator, Precision,
- * Inlet_BC, Exit_BC, Reorder. */
+ * Inlet_BC, Exit_BC, Reorder, MUSCL, Reconstruction, Entropy_Fix_Linear. */
 cfd_status cfd_config_read_json(const char *path, cfd_config *cfg);
 
 /* ------------------------------------------------------------------------------------------
@@ -354,6 +360,76 @@ cfd_status cfd_mpnn_segment_sum(const float *x, const int *ptr, const int *idx, 
                                 void *stream);
 cfd_status cfd_mpnn_adam(float *param, const float *grad, float *m, float *v, int n, float lr, float beta1,
                          float beta2, float eps, int step, void *stream);
+
+/* Dense blocks on the tensor cores: y = W2 silu(W1 x + b1) + b2 (+ r), hidden width 64, BF16
+ * operands (rounded when staged), FP32 accumulation and epilogues.  The input row x is up to three
+ * segments side by side (total width <= 192); segment s supplies columns of row
+ * (idx ? idx[row] : row) of src (leading dimension ld), through silu() when silu = 1. */
+typedef struct {
+  const float *src;
+  const int *idx; /* row map of the segment, or NULL */
+  int width, ld;
+  int silu;       /* 1: values pass through silu(z) = z / (1 + exp(-z)) when loaded */
+} cfd_mlp_seg;
+
+typedef struct {
+  int rows;
+  int nseg;
+  cfd_mlp_seg seg[3];
+  int out;                 /* output width, 1..64 */
+  const float *w1, *b1;    /* [64][in_width], [64] */
+  const float *w2, *b2;    /* [out][64], [out] */
+  const float *resid;      /* optional residual added to y, [rows][ld_resid] */
+  int ld_resid;
+  float *z1;               /* out (optional): hidden pre-activation [rows][64] */
+  float *y;                /* out [rows][ld_y] */
+  int ld_y;
+} cfd_mlp_fwd;
+cfd_status cfd_mpnn_mlp_forward(const cfd_mlp_fwd *a, void *stream);
+
+/* Backward data path of one dense block: dz1 = (dy W2) * silu'(z1) and dx = dz1 W1. */
+typedef struct {
+  int rows, in_width, out;
+  const float *dy;         /* [rows][ld_dy] */
+  int ld_dy;
+  const float *z1;         /* [rows][64] from the forward pass */
+  const float *w1, *w2;
+  float *dz1;              /* out [rows][64] */
+  float *dx;               /* out (optional) [rows][ld_dx] */
+  int ld_dx;
+} cfd_mlp_bwd;
+cfd_status cfd_mpnn_mlp_backward(const cfd_mlp_bwd *a, void *stream);
+
+/* Weight gradient of one linear layer: dw = dz^T x ([n][in_width]) and db = column sums of dz, with
+ * x given as segments as above (n = 64, or n <= 16).  Each of at most CFD_MPNN_WGRAD_BLOCKS thread
+ * blocks accumulates its rows into one partial in `workspace` (CFD_MPNN_WGRAD_BLOCKS * (n *
+ * in_width + n) floats); the partials are summed in block order, so results repeat bit for bit.
+ * accumulate = 1 adds to dw and db instead of overwriting them. */
+#define CFD_MPNN_WGRAD_BLOCKS 296
+typedef struct {
+  int rows, n;
+  const float *dz;
+  int ld_dz;
+  int nseg;
+  cfd_mlp_seg seg[3];
+  float *workspace;
+  float *dw, *db;
+  int accumulate;
+} cfd_mlp_wgrad;
+cfd_status cfd_mpnn_weight_grad(const cfd_mlp_wgrad *a, void *stream);
+int cfd_mpnn_wgrad_blocks(void);
+
+/* Helpers of the training step (float32, device pointers, leading dimensions in elements):
+ * out = a + b on a [rows][width] window; out[r] += src[idx[r]]; out[r] (+)= sum over the CSR list
+ * of row r of x[idx[j]] in list order; the mean-squared error of n values with its gradient
+ * 2 (pred - target) / n (loss to a device scalar, fixed-order sum). */
+cfd_status cfd_mpnn_add(float *out, int ldo, const float *a, int lda, const float *b, int ldb, int rows, int width,
+                        void *stream);
+cfd_status cfd_mpnn_gather_add(float *out, int ldo, const float *src, int lds, const int *idx, int rows, int width,
+                               void *stream);
+cfd_status cfd_mpnn_segment_sum_acc(const float *x, int ldx, const int *ptr, const int *idx, int n_rows, int width,
+                                    float *out, int ldo, int accumulate, void *stream);
+cfd_status cfd_mpnn_mse(const float *pred, const float *target, int n, float *grad, float *loss, void *stream);
 
 /* Accumulated device time of one kernel family ("flux", "stage", "bc", and for the face-based
  * forms "gradients", "faces", "gather_stage", "patch") over the launches made while option "profile" was

@@ -203,6 +203,13 @@ void orc_apply_bc(orc_state *s) {
       if (s->c.inlet_bc == 4) {
         farfield_state(ucur(s, c), s->nrm[8 * c + 2 * f], s->nrm[8 * c + 2 * f + 1], s->c.inlet_rho, s->c.inlet_u,
                        s->c.inlet_v, s->c.inlet_p, G);
+      } else if (s->c.inlet_bc == 3) {
+        /* Fully prescribed inflow (rho, u, v, p) (no reference counterpart). */
+        const double r = s->c.inlet_rho, ui = s->c.inlet_u, vi = s->c.inlet_v;
+        G[0] = r;
+        G[1] = r * ui;
+        G[2] = r * vi;
+        G[3] = s->c.inlet_p / GM1 + 0.5 * r * (ui * ui + vi * vi);
       } else if (s->c.inlet_bc == 0) {
         double vmag = (u * u + v * v) * 0.5;
         G[0] = s->c.inlet_rho;

@@ -21,6 +21,7 @@ typedef struct {
       reconstruct_primitive, muscl, precision, inlet_bc, exit_bc;
   double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas, inlet_u, inlet_v;
   int weno, weno_char;
+  double ef_linear; /* entropy fix of the linear waves in the gradient-MUSCL Roe flux (0: off) */
 } orc_config;
 
 typedef struct orc_state orc_state;

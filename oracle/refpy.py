@@ -297,7 +297,7 @@ class _OrcConfig(ctypes.Structure):
                                             "muscl", "precision", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
                                                "exit_p", "r_gas", "inlet_u", "inlet_v"]] + \
-               [(n, ctypes.c_int) for n in ["weno", "weno_char"]]
+               [(n, ctypes.c_int) for n in ["weno", "weno_char"]] + [("ef_linear", ctypes.c_double)]
 
 
 _orc = None
@@ -362,6 +362,7 @@ class OracleRun:
         c.inlet_v = params.get("inlet_v", 0.0)
         c.weno = params.get("weno", 0)
         c.weno_char = params.get("weno_characteristic", 0)
+        c.ef_linear = params.get("entropy_fix_linear", 0.0)
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,

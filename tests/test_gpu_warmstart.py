@@ -1,5 +1,6 @@
-"""Warm-start surrogate: its library kernels (deterministic segment sums, fused Adam), the
-gradients of the graph operations, the batch machinery it relies on (per-member boundary values,
+"""Warm-start surrogate: its library kernels (dense blocks on the tensor cores, deterministic
+segment sums, fused Adam) checked against the CPU FP64 restatement oracle/mpnn_ref.py (single
+blocks and whole-network gradients), the batch machinery it relies on (per-member boundary values,
 shared residual normalisers) and a small end-to-end run."""
 import numpy as np
 import pytest
@@ -34,55 +35,128 @@ def test_segment_sum_matches_direct_sums_and_is_deterministic():
 
 
 def test_adam_step_matches_formula():
+    import ctypes
     import torch
     rng = np.random.default_rng(2)
     p0 = rng.normal(size=500).astype(np.float32)
     grads = [rng.normal(size=500).astype(np.float32) for _ in range(3)]
-    p = torch.nn.Parameter(torch.from_numpy(p0.copy()).cuda())
-    opt = ws.Adam([p], lr=1e-2)
+    p = torch.from_numpy(p0.copy()).cuda()
+    mt, vt = torch.zeros_like(p), torch.zeros_like(p)
     m = np.zeros(500)
     v = np.zeros(500)
     q = p0.astype(np.float64)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
     for t, g in enumerate(grads, start=1):
-        p.grad = torch.from_numpy(g).cuda()
-        opt.step()
+        gt = torch.from_numpy(g).cuda()
+        cb._check(cb.lib().cfd_mpnn_adam(vp(p), vp(gt), vp(mt), vp(vt), 500, 1e-2, 0.9, 0.999, 1e-8, t, None))
         m = 0.9 * m + 0.1 * g
         v = 0.999 * v + 0.001 * g.astype(np.float64) ** 2
         q -= 1e-2 * (m / (1 - 0.9 ** t)) / (np.sqrt(v / (1 - 0.999 ** t)) + 1e-8)
-    np.testing.assert_allclose(p.detach().cpu().numpy(), q, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(p.cpu().numpy(), q, rtol=1e-5, atol=1e-6)
 
 
-def test_graph_operations_gradients_match_torch_reference():
-    """Gather and Aggregate (custom backward through the segment sums) against torch's own
-    index_select / index_add on the same data."""
+def _graph_batch(nx, ny, B):
+    g = ws.MeshGraph(ws.make_mesh(nx, ny, 0.08))
+    gb = ws.GraphBatch(g, B, "cuda")
+    host = {k: getattr(gb, k).cpu().numpy().astype(np.int64) for k in ("src", "dst", "dst_ptr")}
+    return g, gb, host
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-30))
+
+
+def test_dense_block_kernels_match_cpu_restatement():
+    """One dense block with gathered input segments: forward (y, z1), backward data (dz1, dx) and
+    weight gradients (dW1, db1, dW2, db2) against the CPU FP64 restatement with the kernels' BF16
+    operand rounding (tight: only the FP32 accumulation differs) and without it (loose)."""
     import torch
-    m = ws.make_mesh(12, 6, 0.1)
-    g = ws.MeshGraph(m)
-    gb = ws.GraphBatch(g, 2, "cuda")
-    Gather, Aggregate = ws._functions()
-    rng = np.random.default_rng(3)
-    h0 = torch.from_numpy(rng.normal(size=(2 * g.N, 8)).astype(np.float32)).cuda()
-    w = torch.from_numpy(rng.normal(size=(2 * g.E, 8)).astype(np.float32)).cuda()
+    from oracle import mpnn_ref as R
+    rng = np.random.default_rng(11)
+    rows, n_src = 1000, 300
+    h = rng.normal(size=(n_src, 64))
+    e = rng.normal(size=(rows, 64))
+    src = rng.integers(0, n_src, rows)
+    dst = rng.integers(0, n_src, rows)
+    net = ws.Net(layers=1)
+    P = R.init_params(9, 5, 4, 1, seed=5)
+    net.set_params(P)
+    p = P["edge0"]
+    x = np.concatenate([h[src], h[dst], e], axis=1)
+    T = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dt)
+    th, te, ts, td = T(h), T(e), T(src, torch.int32), T(dst, torch.int32)
+    y = torch.empty((rows, 64), device="cuda")
+    z1 = torch.empty((rows, 64), device="cuda")
+    net._mlp("edge0", [ws._seg(th, ts), ws._seg(th, td), ws._seg(te)], rows, y, z1, resid=te)
+    q = R.bf16
+    yq, zq = R.mlp_forward(x, p, q)
+    y64, z64 = R.mlp_forward(x, p, lambda a: a)
+    assert _rel(z1.cpu().numpy(), zq) < 1e-5 and _rel(y.cpu().numpy(), yq + e) < 1e-5
+    assert _rel(y.cpu().numpy(), y64 + e) < 1e-2
+    dy = rng.normal(size=(rows, 64))
+    net._bufs = {"dz": torch.empty((rows, 64), device="cuda")}
+    dx = torch.empty((rows, 192), device="cuda")
+    net._block_grads("edge0", T(dy), z1, rows, [ws._seg(th, ts), ws._seg(th, td), ws._seg(te)], dx=dx)
+    dxq, gq = R.mlp_backward(x, z1.cpu().numpy().astype(np.float64), dy, p, q)
+    assert _rel(dx.cpu().numpy(), dxq) < 1e-4
+    got = [t.cpu().numpy() for t in net.g["edge0"]]
+    for a, b in zip(got, gq):
+        assert _rel(a, b) < 1e-4
+    _, g64 = R.mlp_backward(x, z64, dy, p, lambda a: a)
+    for a, b in zip(got, g64):
+        assert _rel(a, b) < 3e-2
 
-    def ours(h):
-        hs = Gather.apply(h, gb.src, gb.src_ptr, gb.src_order)
-        hd = Gather.apply(h, gb.dst, gb.dst_ptr, gb.ident)
-        agg = Aggregate.apply(hs * w + hd, gb.dst_ptr, gb.ident, gb.dst)
-        return (agg ** 2).sum()
 
-    def ref(h):
-        hs = h.index_select(0, gb.src.long())
-        hd = h.index_select(0, gb.dst.long())
-        agg = torch.zeros_like(h).index_add_(0, gb.dst.long(), hs * w + hd)
-        return (agg ** 2).sum()
+def test_network_gradients_match_cpu_fp64_restatement():
+    """The whole network (2 message-passing layers on two stacked mesh graphs): loss and every
+    parameter gradient of the library's kernels against the CPU restatement, with BF16 operand
+    rounding emulated (tight) and in exact FP64 (loose: BF16 operands)."""
+    import torch
+    from oracle import mpnn_ref as R
+    layers = 2
+    g, gb, hg = _graph_batch(12, 6, 2)
+    rng = np.random.default_rng(4)
+    xn = rng.normal(size=(2 * g.N, 9))
+    xe = rng.normal(size=(2 * g.E, 5))
+    target = rng.normal(size=(2 * g.N, 4))
+    P = R.init_params(9, 5, 4, layers, seed=9)
+    net = ws.Net(layers=layers)
+    net.set_params(P)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    pred = net.forward(T(xn), T(xe), gb)
+    loss, dpred = net.loss_grad(T(target))
+    net.backward(dpred)
+    G = net.get_grads()
+    Lq, predq, Gq = R.loss_and_grad(P, xn, xe, hg["src"], hg["dst"], hg["dst_ptr"], target, layers, use_bf16=True)
+    L64, pred64, G64 = R.loss_and_grad(P, xn, xe, hg["src"], hg["dst"], hg["dst_ptr"], target, layers)
+    assert _rel(pred.cpu().numpy(), predq) < 1e-4
+    assert abs(float(loss) - Lq) <= 1e-4 * Lq
+    assert _rel(pred.cpu().numpy(), pred64) < 2e-2
+    for name in net.names:
+        for part in range(4):
+            a, bq, b64 = G[name][part], Gq[name][part], G64[name][part]
+            assert _rel(a, bq) < 2e-3, (name, part, _rel(a, bq))
+            assert _rel(a, b64) < 5e-2, (name, part, _rel(a, b64))
+    # Repeatable to the bit.
+    net.forward(T(xn), T(xe), gb)
+    net.loss_grad(T(target))
+    net.backward(net._bufs["dpred"])
+    G2 = net.get_grads()
+    for name in net.names:
+        for a, b in zip(G[name], G2[name]):
+            assert np.array_equal(a, b)
 
-    a = h0.clone().requires_grad_(True)
-    b = h0.clone().requires_grad_(True)
-    la, lb = ours(a), ref(b)
-    la.backward()
-    lb.backward()
-    np.testing.assert_allclose(float(la.detach()), float(lb.detach()), rtol=1e-5)
-    np.testing.assert_allclose(a.grad.cpu().numpy(), b.grad.cpu().numpy(), rtol=1e-4, atol=1e-4)
+
+def test_training_with_library_kernels_reduces_the_loss():
+    P = ws.draw_parameters(6, 3)
+    meshes = [ws.make_mesh(12, 6, t) for t, _, _ in P]
+    g = ws.MeshGraph(meshes[0])
+    feats = [g.features(m, p) for m, p in zip(meshes, P)]
+    rng = np.random.default_rng(0)
+    targets = [np.tanh(f[0][:, :4] + 0.1 * rng.normal(size=(g.N, 4))).astype(np.float32) for f in feats]
+    net = ws.build_model()
+    losses = ws.train(net, g, [f[0] for f in feats], [f[1] for f in feats], targets, epochs=30, batch=3)
+    assert losses[-1] < 0.3 * losses[0], losses
 
 
 def test_restart_from_converged_states_meets_the_shared_tolerance_at_once():
