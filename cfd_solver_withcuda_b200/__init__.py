@@ -158,6 +158,7 @@ SIGNATURES = {
                            ctypes.POINTER(_I)]),
     "cfd_batch_destroy": (None, [_P]),
     "cfd_batch_set_boundary_values": (_I, [_P, _DP, _DP]),
+    "cfd_set_delu": (_I, [_P, _DP]),
     "cfd_mpnn_segment_sum": (_I, [_P, _P, _P, _I, _I, _P, _P]),
     "cfd_mpnn_mlp_forward": (_I, [ctypes.POINTER(MlpFwd), _P]),
     "cfd_mpnn_mlp_backward": (_I, [ctypes.POINTER(MlpBwd), _P]),

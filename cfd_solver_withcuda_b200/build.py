@@ -57,7 +57,31 @@ def build(force=False, verbose=False):
     link = ["-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map"), "-Xlinker", "--exclude-libs,ALL"]
     subprocess.check_call([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + link + ["-lcudart"])
     os.replace(tmp, LIB)
+    build_pybind()
     return LIB
+
+
+def pybind_path():
+    import sysconfig
+    return os.path.join(HERE, "CFD_Solver" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_pybind():
+    """The Python module CFD_Solver (pybind/cfd_solver_module.cpp: the reference wrapper's
+    interface over the C ABI), host code only, linked against libcfd_b200.so beside it."""
+    import sysconfig
+    try:
+        import pybind11
+    except ImportError:  # the module is optional; the ctypes binding covers the same calls
+        return None
+    out = pybind_path()
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I" + pybind11.get_include(),
+           "-I" + sysconfig.get_paths()["include"], "-I" + os.path.join(ROOT, "include"),
+           os.path.join(HERE, "pybind", "cfd_solver_module.cpp"), "-o", out + ".tmp", "-L" + HERE, "-lcfd_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    subprocess.check_call(cmd)
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":

@@ -1178,6 +1178,20 @@ cfd_status cfd_estimate_error(cfd_ctx *ctx, double error[4]) {
   return s;
 }
 
+// Set_DelU (src/Basic_Functions.cpp:9-18): the caller's increments [NP][4] in reference order
+// replace the device's dU, so that the next cfd_update applies U += dU.
+cfd_status cfd_set_delu(cfd_ctx *ctx, const double *dU) {
+  if (!ctx || !dU) return fail(CFD_ERR_BAD_ARG, "null argument");
+  const int NP = ctx->NP;
+  std::vector<double> h(4 * (size_t)NP);
+  for (int i = 0; i < NP; i++) {
+    const int r = ctx->perm[i];
+    for (int k = 0; k < 4; k++) h[k * (size_t)NP + i] = dU[4 * (size_t)r + k];
+  }
+  CUDA_TRY(cudaMemcpyAsync(ctx->ds.dU, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  return sync_status(ctx, nullptr);
+}
+
 cfd_status cfd_update(cfd_ctx *ctx) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
   const int direct = ctx->cfg.integrator == CFD_INT_RK3_GPU_REF || ctx->cfg.integrator == CFD_INT_RK4_GPU_REF;

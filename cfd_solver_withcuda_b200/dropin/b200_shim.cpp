@@ -3,20 +3,33 @@
 // Link this file in place of the reference's src/Numerical_Method.cpp, src/Net_Flux.cpp and
 // src/Error_Estimate_Update.cpp, and link libcfd_b200.so: the reference's own driver then runs
 // its residual/update path on the GPU.  It implements the same entry points with the same
-// signatures over the reference's globals (include/Globals.h:332-416), keeps every
-// post-condition of the reference (e.g. after Runge_Kutta_Method: Cells_DelU = dU,
-// Primitive_Cells = stage-2 primitives, U_Cells unchanged, Min_dt set) by copying the device
-// state back into the globals after each call, and, like the reference, exits on errors.
-// Compiled against the reference's headers; it is not part of libcfd_b200.so.
+// signatures over the reference's globals (include/Globals.h:332-416) and, like the reference,
+// exits on errors.  Compiled against the reference's headers; it is not part of libcfd_b200.so.
+//
+// Post-conditions (e.g. after Runge_Kutta_Method: Cells_DelU = dU, Primitive_Cells = stage-2
+// primitives, U_Cells unchanged, Min_dt set) are met by copying the device state back into the
+// globals.  By default that happens after every entry point, so every global is what the
+// reference would hold.  A driver whose loop reads only Min_dt and Error between its output steps
+// can make the copies lazy: b200_shim_set_sync_every(k) (or CFD_B200_SYNC_EVERY=k in the
+// environment) copies the state back at every k-th Update() only (k = 0: never by itself), and
+// b200_shim_sync() copies it at once, e.g. before Write_Solution.  Min_dt and Error are always
+// set after each call.
 #include "definitions.h"
 #include "Globals.h"
+#include "Flux.h"
 #include "Primitive_Computational.h"
 #include "cfd_b200.h"
+
+#include <algorithm>
+#include <cstdlib>
 
 V_D Error(4, 0.0);  // src/Error_Estimate_Update.cpp:7
 
 namespace {
 cfd_ctx *g_ctx = nullptr;
+int g_sync_every = -1;   // -1: not yet read from the environment; 1: eager; k > 1: every k-th Update(); 0: on request
+long long g_updates = 0;
+bool g_dirty = false;    // the device holds state the globals do not
 std::vector<int> g_nf, g_nbr, g_bnd;
 std::vector<double> g_nrm, g_len, g_ccd, g_cvec, g_area, g_inva;
 
@@ -89,6 +102,10 @@ void b200_init() {
 }
 
 void ensure() {
+  if (g_sync_every < 0) {
+    const char *e = std::getenv("CFD_B200_SYNC_EVERY");
+    g_sync_every = e ? std::max(0, std::atoi(e)) : 1;
+  }
   if (!g_ctx) b200_init();
 }
 
@@ -109,21 +126,44 @@ void sync_globals() {
     }
   }
   b200_check(cfd_get_min_dt(g_ctx, &Min_dt));
+  g_dirty = false;
+}
+
+// After an entry point that changed the device state: Min_dt at once, the rest by the sync rule.
+void changed(bool is_update) {
+  b200_check(cfd_get_min_dt(g_ctx, &Min_dt));
+  g_dirty = true;
+  if (is_update) g_updates++;
+  if (g_sync_every == 1 || (is_update && g_sync_every > 1 && g_updates % g_sync_every == 0)) sync_globals();
 }
 }  // namespace
+
+// Copies the device state into the reference's globals now (a no-op when they are current).
+extern "C" void b200_shim_sync() {
+  if (g_ctx && g_dirty) sync_globals();
+}
+
+// k = 1 (default): copy after every entry point; k > 1: at every k-th Update(); k = 0: only on
+// b200_shim_sync().
+extern "C" void b200_shim_set_sync_every(int k) {
+  b200_shim_sync();
+  g_sync_every = k < 0 ? 0 : k;
+}
 
 // Releases the device context (the next entry point re-reads mesh, configuration and state from
 // the globals); for drivers that load a new mesh into the same process.
 extern "C" void b200_shim_reset() {
   if (g_ctx) cfd_destroy(g_ctx);
   g_ctx = nullptr;
+  g_dirty = false;
+  g_updates = 0;
 }
 
 // src/Net_Flux.cpp:46,97 — both orders: the context was configured from Is_Second_Order.
 void Evaluate_Cell_Net_Flux_1O() {
   ensure();
   b200_check(cfd_evaluate_net_flux(g_ctx));
-  sync_globals();
+  changed(false);
 }
 void Evaluate_Cell_Net_Flux_2O() { Evaluate_Cell_Net_Flux_1O(); }
 
@@ -134,6 +174,7 @@ double get_Min_dt() {
   return Min_dt;
 }
 double get_Max_dt() {
+  b200_shim_sync();
   double m = 0.0;
   for (int c = 0; c < No_Physical_Cells; c++) m = std::max(m, Cells[c].del_t);
   Max_dt = m;
@@ -151,13 +192,13 @@ void Explicit_Method() {
     exit(EXIT_FAILURE);
   }
   b200_check(s);
-  sync_globals();
+  changed(false);
 }
 void Runge_Kutta_Method() {
   ensure();
   b200_check(cfd_apply_boundary_conditions(g_ctx));
   b200_check(cfd_runge_kutta_method(g_ctx));
-  sync_globals();
+  changed(false);
 }
 void Implicit_Method() { fprintf(stderr, "Implicit_Method is not part of the B200 path.\n"); }
 
@@ -171,7 +212,29 @@ void Estimate_Error() {
 void Update() {
   ensure();
   b200_check(cfd_update(g_ctx));
-  sync_globals();
+  changed(true);
+}
+
+// src/Net_Flux.cpp:7-43: adds the average flux minus the given dissipation of every face of one
+// cell to Cells_Net_Flux.  The dissipation is a host function by its signature (ROE, LLF, ... of
+// the reference), so this helper runs on the host over the globals, brought up to date first; the
+// solver's own net-flux entry points above do not use it.
+void Calculate_Flux_For_All_Faces(int &Current_Cell_No, void (*Dissipation_Function)(const int &, int &, const int &)) {
+  b200_shim_sync();
+  const Cell &C = Cells[Current_Cell_No];
+  const int n_faces = C.numFaces > 0 ? C.numFaces : static_cast<int>(C.Face_Areas.size());
+  const int n_nbr = static_cast<int>(C.Neighbours.size());
+  for (int face = 0; face < n_faces && face < n_nbr; face++) {
+    int nb = C.Neighbours[face];
+    if (nb < 0) continue;
+    const bool on_boundary = Current_Cell_No < static_cast<int>(Cells_Face_Boundary_Type.size()) &&
+                             face < static_cast<int>(Cells_Face_Boundary_Type[Current_Cell_No].size()) &&
+                             Cells_Face_Boundary_Type[Current_Cell_No][face];
+    Calculate_Face_Average_Flux(Current_Cell_No, nb, face, on_boundary);
+    Dissipation_Function(Current_Cell_No, nb, face);
+    for (int v = 0; v < NUM_FLUX_COMPONENTS; v++)
+      Cells_Net_Flux[Current_Cell_No][v] += Average_Convective_Flux[v] - Dissipative_Flux[v];
+  }
 }
 
 // Per-cell primitive refreshes of src/Error_Estimate_Update.cpp:46-77, still used by other

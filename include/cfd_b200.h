@@ -220,6 +220,9 @@ cfd_status cfd_explicit_method(cfd_ctx *ctx);           /* Explicit_Method, src/
 cfd_status cfd_runge_kutta_method(cfd_ctx *ctx);        /* Runge_Kutta_Method, src/Numerical_Method.cpp:342 */
 cfd_status cfd_estimate_error(cfd_ctx *ctx, double error[4]); /* Estimate_Error, src/Error_Estimate_Update.cpp:10 */
 cfd_status cfd_update(cfd_ctx *ctx);                    /* Update(), src/Error_Estimate_Update.cpp:31 */
+/* Set_DelU, src/Basic_Functions.cpp:9-18: dU [NP][4] (reference order) becomes the increment the
+ * next cfd_update adds to U (the reference, SSP-RK3 and RK4 integrators). */
+cfd_status cfd_set_delu(cfd_ctx *ctx, const double *dU);
 cfd_status cfd_get_min_dt(cfd_ctx *ctx, double *min_dt); /* get_Min_dt, src/Numerical_Method.cpp:322 */
 
 /* Downloads (reference cell order).  Any pointer may be NULL.

@@ -84,17 +84,20 @@ def classify_boundary(geo, n_physical):
     return rows
 
 
-def reference_half_cylinder(ntheta, nr, r_body, r_outer, ratio, params, mach=3.0, rho=1.0, p=1.0 / GAMMA):
-    """The reference's CPU solver (oracle/_ref) set up on the O-grid with the given Solver_Config
+def reference_half_cylinder(ntheta, nr, r_body, r_outer, ratio, params, mach=3.0, rho=1.0, p=1.0 / GAMMA,
+                            lib_path=None):
+    """The reference's CPU solver (oracle/_ref/libcfdref.so, or the library at lib_path, e.g. the
+    reference linked with the B200 drop-in) set up on the O-grid with the given Solver_Config
     parameters, at a uniform freestream state (rho, u = mach * a, v = 0, p) on every physical and
     ghost row.  Returns the refpy.RefRun."""
+    lib = lib_path or refpy.REF_LIB
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "ogrid.vtk")
         write_half_cylinder_vtk(path, ntheta, nr, r_body, r_outer, ratio)
-        probe = refpy.RefRun.from_vtk(path, None, {})
+        probe = refpy.RefRun.from_vtk(path, None, {}, lib_path=refpy.REF_LIB)
         geo = probe.geometry()
         rows = classify_boundary(geo, probe.NP)
-        run = refpy.RefRun.from_vtk(path, rows, params)
+        run = refpy.RefRun.from_vtk(path, rows, params, lib_path=lib)
     u = mach * math.sqrt(GAMMA * p / rho)
     U = np.zeros((run.NT, 4))
     U[:, 0] = rho

@@ -48,6 +48,8 @@ void Ausm_Flux(const int &Cell_No);     // src/Ausm_Flux.cpp:5 (no header declar
 
 // Present only when the B200 drop-in shim is linked in (oracle/_ref/libcfdref_dropin.so).
 extern "C" void b200_shim_reset() __attribute__((weak));
+extern "C" void b200_shim_sync() __attribute__((weak));
+extern "C" void b200_shim_set_sync_every(int) __attribute__((weak));
 
 namespace {
 int g_saved_stdout = -1;
@@ -281,6 +283,18 @@ void refh_net_flux() {
   quiet_end();
 }
 double refh_get_min_dt() { return get_Min_dt(); }
+// Net flux of every physical cell from zero through Calculate_Flux_For_All_Faces
+// (src/Net_Flux.cpp:7-43) with the reference's ROE / ROE_2O as the dissipation callback.
+void refh_net_flux_by_faces(double *out) {
+  quiet_begin();
+  for (int c = 0; c < No_Physical_Cells; c++) {
+    for (int k = 0; k < 4; k++) Cells_Net_Flux[c][k] = 0.0;
+    int cc = c;
+    Calculate_Flux_For_All_Faces(cc, Is_Second_Order ? ROE_2O : ROE);
+    for (int k = 0; k < 4; k++) out[4 * c + k] = Cells_Net_Flux[c][k];
+  }
+  quiet_end();
+}
 void refh_explicit() { quiet_begin(); Explicit_Method(); quiet_end(); }
 void refh_rk3() { quiet_begin(); Runge_Kutta_Method(); quiet_end(); }
 void refh_estimate_error() { Estimate_Error(); }
@@ -322,8 +336,19 @@ int refh_iterate(int n, double t_end) {
     done++;
     if (t_end > 0.0 && Total_Time >= t_end) break;
   }
+  // With the B200 drop-in linked and lazy copies chosen, the globals the getters read are brought
+  // up to date once here.
+  if (b200_shim_sync) b200_shim_sync();
   quiet_end();
   return done;
+}
+
+// With the B200 drop-in linked: copy the device state into the globals after every entry point
+// (k = 1, the default) or at every k-th Update() only.  Returns 0, or -1 without the drop-in.
+int refh_set_shim_sync(int k) {
+  if (!b200_shim_set_sync_every) return -1;
+  b200_shim_set_sync_every(k);
+  return 0;
 }
 
 // Green-Gauss gradient of primitive slot `var` (src/Grid_Refine_Functions.cpp:221-246).
