@@ -15,6 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcfd_b200.so")
 
 CFD_OK = 0
+CFD_ERR_TIMEOUT = 5
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NONPHYSICAL", 4: "DT_NONPOSITIVE", 5: "TIMEOUT",
                 6: "DIVERGED", 7: "MESH", 8: "IO", 9: "NO_DEVICE"}
 
@@ -55,7 +56,8 @@ class Config(ctypes.Structure):
                 ("inlet_u", ctypes.c_double), ("inlet_v", ctypes.c_double), ("inlet_p0", ctypes.c_double),
                 ("inlet_t0", ctypes.c_double), ("exit_p", ctypes.c_double), ("r_gas", ctypes.c_double),
                 ("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("weno", ctypes.c_int),
-                ("weno_characteristic", ctypes.c_int), ("entropy_fix_linear", ctypes.c_double)]
+                ("weno_characteristic", ctypes.c_int), ("entropy_fix_linear", ctypes.c_double),
+                ("shock_fix", ctypes.c_double)]
 
 
 class FluxArrays(ctypes.Structure):
@@ -159,6 +161,7 @@ SIGNATURES = {
     "cfd_batch_destroy": (None, [_P]),
     "cfd_batch_set_boundary_values": (_I, [_P, _DP, _DP]),
     "cfd_set_delu": (_I, [_P, _DP]),
+    "cfd_batch_set_option": (_I, [_P, ctypes.c_char_p, _D]),
     "cfd_mpnn_segment_sum": (_I, [_P, _P, _P, _I, _I, _P, _P]),
     "cfd_mpnn_mlp_forward": (_I, [ctypes.POINTER(MlpFwd), _P]),
     "cfd_mpnn_mlp_backward": (_I, [ctypes.POINTER(MlpBwd), _P]),
@@ -365,6 +368,10 @@ class Solver:
     def Update(self):
         _check(lib().cfd_update(self._h))
 
+    def Set_DelU(self, dU):
+        dU = np.ascontiguousarray(dU, np.float64)
+        _check(lib().cfd_set_delu(self._h, dU.ctypes.data_as(_DP)))
+
     def get_Min_dt(self):
         v = ctypes.c_double()
         _check(lib().cfd_get_min_dt(self._h, ctypes.byref(v)))
@@ -504,6 +511,9 @@ class Batch:
             out.append(U[r:r + n])
             r += n
         return out
+
+    def set_option(self, name, value):
+        _check(lib().cfd_batch_set_option(self._h, name.encode(), float(value)))
 
     def run(self, max_steps, tol, check_every=50):
         n = len(self.meshes)

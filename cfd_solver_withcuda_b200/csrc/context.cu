@@ -207,6 +207,17 @@ struct cfd_ctx {
   double *pbuf[2] = {nullptr, nullptr};  // stage primitives of the patch form ([5][NT] each)
   cudaGraphExec_t graph = nullptr;
   int graph_launches = 0;
+  // Persistent batched form (option "persistent"): one cooperative launch per RK stage, one
+  // CUDA graph per stage; persist_grid = co-resident blocks used; persist_test_arrivals = barrier
+  // arrivals that never come (option "barrier_timeout_test", a test of the timeout path).
+  bool persistent = false;
+  int persist_grid = 0;
+  int partial_blocks = 0;  // blocks the reduction buffers (st.partial) are sized for
+  unsigned int persist_test_arrivals = 0;
+  bool stage_graphs_ok = true;
+  cudaGraphExec_t stage_graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  int stage_graph_launches[4] = {0, 0, 0, 0};
+  int n_stage_graphs = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
   int *d_perm = nullptr;    // device copy of perm
   // Per-kernel timing (option "profile"): event pairs recorded around each launch on the
@@ -243,7 +254,8 @@ cfd_status ctx_upload(cfd_ctx *ctx, T **dst, const std::vector<T> &v) {
 
 int dev_of(const cfd_ctx *ctx, int ref) { return ref < ctx->NP ? ctx->inv[ref] : ref; }
 
-enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_PATCH = 6, TK_N = 7 };
+enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_PATCH = 6, TK_PERSIST = 7,
+       TK_N = 8 };
 
 struct TimedScope {
   cfd_ctx *ctx;
@@ -286,9 +298,21 @@ int stage_lts(const StagePlan &p, const cfd_config &c, int k) {
   return (k == 0 && c.local_time_stepping) ? 1 : 0;
 }
 
-// Launch sequence of one pseudo-step (loop body of src/Solver.cpp:94-125): per stage the boundary
-// conditions, the residual (face-based forms: gradients, face fluxes, gather) and the update.
-int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
+void drop_graphs(cfd_ctx *ctx) {
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  ctx->graph = nullptr;
+  for (int k = 0; k < 4; k++) {
+    if (ctx->stage_graph[k]) cudaGraphExecDestroy(ctx->stage_graph[k]);
+    ctx->stage_graph[k] = nullptr;
+  }
+  ctx->n_stage_graphs = 0;
+}
+
+// Launch sequence of stage k of one pseudo-step (loop body of src/Solver.cpp:94-125): the
+// boundary conditions, the residual (face-based forms: gradients, face fluxes, gather) and the
+// update.  ghosts_written carries "the previous stage's owner threads wrote this stage's ghosts"
+// from stage to stage (false before stage 0).
+int enqueue_stage(cfd_ctx *ctx, int k, bool fuse_final, bool &ghosts_written) {
   const cfd_config &c = ctx->cfg;
   cudaStream_t s = ctx->stream;
   DevMesh &m = ctx->dm;
@@ -296,65 +320,80 @@ int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
   int n = 0;
   const StagePlan p = stage_plan(c, ctx->fp.consistent);
   const bool faces = ctx->dm.NF > 0;
-  bool ghosts_written = false;  // the previous stage's owner threads wrote this stage's ghosts
   // Patch form: one kernel per stage.  Stage k reads the primitives of buffer in(k) and writes
   // out(k): in(0) = st.prim, out(k) = pbuf[k % 2] for the other stages and st.prim for the last,
   // in(k + 1) = out(k), so every stage writes a buffer that no block of it reads.
   const bool patch = faces && ctx->patch_stage && m.npatch > 0 && !m.cblk && !m.fblk && fuse_final &&
                      ctx->fp.precision == CFD_PREC_FP64 && !ctx->fp.weno && p.kind0 != 0 && p.lts_mode == 1 &&
                      c.local_time_stepping;
-  for (int k = 0; k < p.n; k++) {
-    const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
-    const int lts = stage_lts(p, c, k);
-    const int fin = (k == p.n - 1) ? fuse_final : 0;
-    // Fused face-based stages take the first stage's boundary conditions into the gradient pass
-    // (each cell applies its own entries before its gradient) when no ghost is shared.
-    const bool fused_faces = faces && ctx->fuse_gather && (lts == 1 || lts == 2);
-    const bool bc_in_grad = fused_faces && !patch && k == 0 && ctx->ghost_private;
-    if (!ghosts_written && !bc_in_grad) {
-      TimedScope ts(ctx, TK_BC);
-      n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
-    }
-    ghosts_written = false;
-    if (patch) {
-      TimedScope ts(ctx, TK_PATCH);
+  const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
+  const int lts = stage_lts(p, c, k);
+  const int fin = (k == p.n - 1) ? fuse_final : 0;
+  // Fused face-based stages take the first stage's boundary conditions into the gradient pass
+  // (each cell applies its own entries before its gradient) when no ghost is shared.
+  const bool fused_faces = faces && ctx->fuse_gather && (lts == 1 || lts == 2);
+  const bool bc_in_grad = fused_faces && !patch && k == 0 && ctx->ghost_private;
+  if (!ghosts_written && !bc_in_grad) {
+    TimedScope ts(ctx, TK_BC);
+    n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
+  }
+  ghosts_written = false;
+  if (patch) {
+    TimedScope ts(ctx, TK_PATCH);
+    const bool bc_next = k < p.n - 1;
+    const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+    DevState sk = st;
+    sk.prim = bc_next ? ctx->pbuf[k % 2] : st.prim;
+    const double *pin = k == 0 ? st.prim : ctx->pbuf[(k - 1) % 2];
+    n += launch_patch_stage(s, m, sk, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags, pin);
+    ghosts_written = bc_next;
+    return n;
+  }
+  if (faces) {
+    // Fused form (per-cell dt): del_t comes from the gradient pass, the stage kernel writes
+    // the next stage's ghost states from the owner cells, and the last stage forms the step's
+    // Min_dt from the per-cell dt frozen at the first stage.
+    const bool fused = ctx->fuse_gather && (lts == 1 || lts == 2);
+    // del_t is formed where a stage uses it (lts 1, or the first stage, which freezes it) and
+    // at the last stage, whose value is the Cells[].del_t a download returns.
+    const bool with_dt = fused && (lts == 1 || k == 0 || k == p.n - 1);
+    if (fused && ctx->persistent && ctx->persist_grid > 0) {
+      TimedScope ts(ctx, TK_PERSIST);
       const bool bc_next = k < p.n - 1;
       const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
-      DevState sk = st;
-      sk.prim = bc_next ? ctx->pbuf[k % 2] : st.prim;
-      const double *pin = k == 0 ? st.prim : ctx->pbuf[(k - 1) % 2];
-      n += launch_patch_stage(s, m, sk, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags, pin);
+      n += launch_persistent_stage(s, m, st, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags, with_dt ? 1 : 0,
+                                   bc_in_grad ? 1 : 0, ctx->persist_grid, ctx->persist_test_arrivals);
       ghosts_written = bc_next;
-      continue;
+      return n;
     }
-    if (faces) {
-      // Fused form (per-cell dt): del_t comes from the gradient pass, the stage kernel writes
-      // the next stage's ghost states from the owner cells, and the last stage forms the step's
-      // Min_dt from the per-cell dt frozen at the first stage.
-      const bool fused = ctx->fuse_gather && (lts == 1 || lts == 2);
-      {
-        TimedScope ts(ctx, TK_GRAD);
-        // del_t is formed where a stage uses it (lts 1, or the first stage, which freezes it) and
-        // at the last stage, whose value is the Cells[].del_t a download returns.
-        const bool with_dt = fused && (lts == 1 || k == 0 || k == p.n - 1);
-        n += launch_muscl_gradients(s, m, st, ctx->fp, with_dt ? 1 : 0, bc_in_grad ? &ctx->bp : nullptr);
-      }
-      { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
-      if (fused) {
-        TimedScope ts(ctx, TK_GATHER_STAGE);
-        const bool bc_next = k < p.n - 1;
-        const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
-        n += launch_gather_stage(s, m, st, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags);
-        ghosts_written = bc_next;
-      } else {
-        { TimedScope ts(ctx, TK_FLUX); n += launch_gather(s, m, st, ctx->fp); }
-        { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
-      }
-      continue;
+    {
+      TimedScope ts(ctx, TK_GRAD);
+      n += launch_muscl_gradients(s, m, st, ctx->fp, with_dt ? 1 : 0, bc_in_grad ? &ctx->bp : nullptr);
     }
-    { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
-    { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
+    { TimedScope ts(ctx, TK_FACES); n += launch_faces(s, m, st, ctx->fp); }
+    if (fused) {
+      TimedScope ts(ctx, TK_GATHER_STAGE);
+      const bool bc_next = k < p.n - 1;
+      const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+      n += launch_gather_stage(s, m, st, ctx->fp, ctx->bp, kind, lts, fin, ctx->keep_delu, flags);
+      ghosts_written = bc_next;
+    } else {
+      { TimedScope ts(ctx, TK_FLUX); n += launch_gather(s, m, st, ctx->fp); }
+      { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
+    }
+    return n;
   }
+  { TimedScope ts(ctx, TK_FLUX); n += launch_flux(s, m, st, ctx->fp, k > 0); }
+  { TimedScope ts(ctx, TK_STAGE); n += launch_stage(s, m, st, kind, lts, fin, ctx->keep_delu); }
+  return n;
+}
+
+// Launch sequence of one pseudo-step: its stages in order.
+int enqueue_step(cfd_ctx *ctx, bool fuse_final) {
+  const StagePlan p = stage_plan(ctx->cfg, ctx->fp.consistent);
+  bool ghosts_written = false;
+  int n = 0;
+  for (int k = 0; k < p.n; k++) n += enqueue_stage(ctx, k, fuse_final, ghosts_written);
   return n;
 }
 
@@ -507,7 +546,7 @@ cfd_status cfd_config_read_json(const char *path, cfd_config *cfg) {
 // ----------------------------------------- context ----------------------------------------
 void cfd_destroy(cfd_ctx *ctx) {
   if (!ctx) return;
-  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  drop_graphs(ctx);
   for (auto &t : ctx->timed) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -559,6 +598,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   if (cfg->limiter < 0 || cfg->limiter > 4) return fail(CFD_ERR_BAD_ARG, "bad limiter");
   if (!(cfg->entropy_fix_linear >= 0.0) || !std::isfinite(cfg->entropy_fix_linear))
     return fail(CFD_ERR_BAD_ARG, "entropy_fix_linear must be a finite value >= 0");
+  if (!(cfg->shock_fix >= 0.0) || !std::isfinite(cfg->shock_fix))
+    return fail(CFD_ERR_BAD_ARG, "shock_fix must be a finite value >= 0");
   if (cfg->reorder < 0 || cfg->reorder > 3) return fail(CFD_ERR_BAD_ARG, "reorder must be 0, 1, 2 or 3");
   if (cfg->inlet_bc < 0 || cfg->inlet_bc > CFD_INLET_FARFIELD || cfg->exit_bc < 0 || cfg->exit_bc > CFD_EXIT_FIXED_P_REF)
     return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
@@ -886,6 +927,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   DevState &st = ctx->ds;
   const size_t dsz = sizeof(double);
   const int nblk = std::max(flux_block_count(NP), m.npatch);
+  ctx->partial_blocks = nblk;
   if ((s = ctx_alloc(ctx, (void **)&st.U, 4 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.S, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.prim, 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
@@ -979,6 +1021,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   fp.zeta = cfg->limiter_zeta;
   fp.zeta1 = cfg->limiter_zeta1;
   fp.eflin = cfg->entropy_fix_linear;
+  fp.shock_fix = cfg->shock_fix;
   BcParams &bp = ctx->bp;
   bp.inlet_bc = cfg->inlet_bc;
   bp.exit_bc = cfg->exit_bc;
@@ -997,6 +1040,27 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   if (!ctx || !name) return fail(CFD_ERR_BAD_ARG, "null argument");
   std::string n(name);
+  if (n == "persistent") {
+    // Persistent batched form: one cooperative launch per RK stage over the work lists, at most
+    // the co-resident grid and the reduction buffers' block count.
+    drop_graphs(ctx);
+    ctx->persistent = false;
+    ctx->persist_grid = 0;
+    if (value != 0.0) {
+      const int g = persistent_grid(ctx->fp);
+      if (g <= 0) return fail(CFD_ERR_BAD_ARG, "cooperative launches are not available on this device");
+      ctx->persistent = true;
+      ctx->persist_grid = std::min(g, ctx->partial_blocks);
+    }
+    return CFD_OK;
+  }
+  if (n == "barrier_timeout_test") {
+    // Test of the bounded barrier: every barrier of the persistent form waits for `value` more
+    // arrivals than the grid has, so each wait runs out and the run reports CFD_ERR_TIMEOUT.
+    drop_graphs(ctx);
+    ctx->persist_test_arrivals = value > 0.0 ? static_cast<unsigned int>(value) : 0u;
+    return CFD_OK;
+  }
   if (n == "keep_delu") ctx->keep_delu = value != 0.0;
   else if (n == "use_graph") ctx->use_graph = value != 0.0;
   else if (n == "flux_lanes") {
@@ -1014,10 +1078,7 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "patch_stage") ctx->patch_stage = value != 0.0;
   else if (n == "l2_persist") ctx->dm.l2_bytes = value != 0.0 ? ctx->l2_window : 0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  drop_graphs(ctx);
   return CFD_OK;
 }
 
@@ -1070,7 +1131,47 @@ cfd_status cfd_download_U(cfd_ctx *ctx, double *U) {
   return CFD_OK;
 }
 
+// Persistent form: one CUDA graph per RK stage (each holds the stage's boundary-condition launch,
+// if any, and its cooperative launch), replayed stage after stage.  A capture the driver rejects
+// leaves the form on plain launches.
+static cfd_status enqueue_steps_persistent(cfd_ctx *ctx, int n_steps) {
+  const StagePlan p = stage_plan(ctx->cfg, ctx->fp.consistent);
+  if (ctx->use_graph && !ctx->profile && ctx->stage_graphs_ok && ctx->n_stage_graphs == 0) {
+    bool gw = false;
+    for (int k = 0; k < p.n && ctx->stage_graphs_ok; k++) {
+      cudaGraph_t g;
+      CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      ctx->stage_graph_launches[k] = enqueue_stage(ctx, k, true, gw);
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (e == cudaSuccess) {
+        e = cudaGraphInstantiate(&ctx->stage_graph[k], g, 0);
+        cudaGraphDestroy(g);
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->stage_graphs_ok = false;
+      }
+    }
+    if (ctx->stage_graphs_ok) ctx->n_stage_graphs = p.n;
+    else drop_graphs(ctx);
+  }
+  for (int i = 0; i < n_steps; i++) {
+    if (ctx->n_stage_graphs == p.n) {
+      for (int k = 0; k < p.n; k++) {
+        CUDA_TRY(cudaGraphLaunch(ctx->stage_graph[k], ctx->stream));
+        ctx->launches += ctx->stage_graph_launches[k];
+      }
+    } else {
+      ctx->launches += enqueue_step(ctx, true);
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  ctx->prim_from_S = false;
+  return CFD_OK;
+}
+
 static cfd_status enqueue_steps(cfd_ctx *ctx, int n_steps) {
+  if (ctx->persistent && ctx->persist_grid > 0 && ctx->dm.NF > 0) return enqueue_steps_persistent(ctx, n_steps);
   if (ctx->use_graph && !ctx->profile && n_steps > 1) {
     if (!ctx->graph) {
       cudaGraph_t g;
@@ -1447,10 +1548,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     ctx->fp.lanes = cd.lanes;
     ctx->dm.pdl = cd.pdl;
     ctx->patch_stage = cd.patch;
-    if (ctx->graph) {
-      cudaGraphExecDestroy(ctx->graph);
-      ctx->graph = nullptr;
-    }
+    drop_graphs(ctx);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_TEND, 0.0);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_DONE, 0.0);
     if ((status = enqueue_steps(ctx, 2)) != CFD_OK) break;
@@ -1470,10 +1568,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   cudaFree(snap);
   ctx->profile = prof;
   ctx->use_graph = graph_on;
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  drop_graphs(ctx);
   if (status != CFD_OK) return status;
   const Cand *best = &cands[0];
   for (const Cand &cd : cands)
@@ -1559,7 +1654,8 @@ cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, l
   if (!ctx || !kernel || !total_ms || !launches) return fail(CFD_ERR_BAD_ARG, "null argument");
   std::string k(kernel);
   int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : k == "gradients" ? TK_GRAD
-           : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : k == "patch" ? TK_PATCH : -1;
+           : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : k == "patch" ? TK_PATCH
+           : k == "persistent" ? TK_PERSIST : -1;
   if (kind < 0) return fail(CFD_ERR_BAD_ARG, "unknown kernel " + k);
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   for (auto &t : ctx->timed) {
@@ -1624,10 +1720,7 @@ static cfd_status batch_tables(cfd_batch *b) {
   ctx->dm.n_bblk = static_cast<int>(t[2].size());
   ctx->dm.rblk = p[3];
   ctx->dm.n_rblk = static_cast<int>(t[3].size());
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  drop_graphs(ctx);
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return CFD_OK;
 }
@@ -1788,10 +1881,7 @@ cfd_status cfd_batch_set_boundary_values(cfd_batch *b, const double *inlet, cons
     CUDA_TRY(cudaMemcpy(b->d_bexit, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
     ctx->dm.bexit = b->d_bexit;
   }
-  if (ctx->graph) {
-    cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-  }
+  drop_graphs(ctx);
   return CFD_OK;
 }
 
@@ -1835,6 +1925,11 @@ cfd_status cfd_batch_residuals(cfd_batch *b, double *res) {
   if (s != CFD_OK) return s;
   for (int i = 0; i < b->n; i++) res[i] = r[i];
   return CFD_OK;
+}
+
+cfd_status cfd_batch_set_option(cfd_batch *b, const char *name, double value) {
+  if (!b) return fail(CFD_ERR_BAD_ARG, "null batch");
+  return cfd_set_option(b->ctx, name, value);
 }
 
 cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,

@@ -237,6 +237,7 @@ std::string config_from_json(const std::string &text, cfd_config *cfg) {
     as_int(sol->get("Reorder"), cfg->reorder);
     cfg->muscl = enum_from(sol->get("MUSCL"), {"reference", "gradient"}, cfg->muscl);
     as_double(sol->get("Entropy_Fix_Linear"), cfg->entropy_fix_linear);
+    as_double(sol->get("Shock_Fix"), cfg->shock_fix);
   }
   if (lim) {
     as_double(lim->get("Limiter_Zeta"), cfg->limiter_zeta);

@@ -817,7 +817,8 @@ __global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, Flu
 template <typename T, int DISS>
 __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, const double4 c1, const double4 c2,
                                                  const double4 n0, const double4 n1, const double4 n2, const T nx,
-                                                 const T ny, const T dl, const T dx, const T dy, const T eflin) {
+                                                 const T ny, const T dl, const T dx, const T dy, const T eflin,
+                                                 const T shock_fix = T(0.0)) {
   const T qc[4] = {T(c0.x), T(c0.y), T(c0.z), T(c0.w)};
   const T qn[4] = {T(n0.x), T(n0.y), T(n0.z), T(n0.w)};
   const T gc[8] = {T(c1.x), T(c1.y), T(c1.z), T(c1.w), T(c2.x), T(c2.y), T(c2.z), T(c2.w)};
@@ -843,7 +844,27 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
   T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
   if (DISS == 3) {
     average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
-    roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D, eflin);
+    // Shock sensor of the hybrid: |grad p|^2 |d|^2 > (shock_fix p)^2 in either cell.
+    bool rusanov = false;
+    if (shock_fix > T(0.0)) {
+      const T d2 = dx * dx + dy * dy;
+      const T gpc = gc[6] * gc[6] + gc[7] * gc[7], gpn = gn[6] * gn[6] + gn[7] * gn[7];
+      const T tc = shock_fix * qc[3], tn = shock_fix * qn[3];
+      rusanov = gpc * d2 > tc * tc || gpn * d2 > tn * tn;
+    }
+    if (rusanov) {
+      const T vnL = qL[1] * nx + qL[2] * ny, vnR = qR[1] * nx + qR[2] * ny;
+      const T sL = fabs(vnL) + aL, sR = fabs(vnR) + aR;
+      const T sm = sL > sR ? sL : sR;
+      const T UL[4] = {qL[0], qL[0] * qL[1], qL[0] * qL[2],
+                       qL[3] / T(kGM1) + T(0.5) * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2])};
+      const T UR[4] = {qR[0], qR[0] * qR[1], qR[0] * qR[2],
+                       qR[3] / T(kGM1) + T(0.5) * qR[0] * (qR[1] * qR[1] + qR[2] * qR[2])};
+#pragma unroll
+      for (int k = 0; k < 4; k++) D[k] = T(0.5) * sm * (UR[k] - UL[k]) * dl;
+    } else {
+      roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D, eflin);
+    }
   } else {
     // Conserved face states for AUSM / HLLC: E = p/(g-1) + rho |V|^2 / 2.
     const T UL[4] = {qL[0], qL[0] * qL[1], qL[0] * qL[2],
@@ -898,14 +919,23 @@ __global__ void __launch_bounds__(MINB >= 6 ? 128 : 256, MINB) k_faces(DevMesh m
     n1 = nphys ? rn[0] : c1;
     n2 = nphys ? rn[1] : c2;
   }
-  st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy, T(fp.eflin));
+  st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy, T(fp.eflin),
+                                     T(fp.shock_fix));
 }
 
 // Sum of the face fluxes of cell c in face order (+F on the owner side, -F on the neighbour
 // side) and the del_t denominator.  The cell's four face-table slots come in one 16-byte load
 // without waiting for the face count (an unused slot holds face 0), so the flux loads of every
 // face are in flight together; only the sums are predicated on the count.
-template <bool DEN = true>
+// CG: the face fluxes were written earlier in the same launch by other thread blocks (the
+// persistent stage kernel), so they are loaded from L2 (ld.global.cg), not through L1.
+__device__ __forceinline__ double4 ldcg4(const double4 *p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+template <bool DEN = true, bool CG = false>
 __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &st, int c, double R[4], double &den) {
   const int NP = m.NP, NT = m.NT;
   const double uc = DEN ? st.prim[NT + c] : 0.0, vc = DEN ? st.prim[2 * NT + c] : 0.0,
@@ -917,7 +947,7 @@ __device__ __forceinline__ void gather_faces(const DevMesh &m, const DevState &s
 #pragma unroll
   for (int f = 0; f < 4; f++) {
     const int id = e[f] < 0 ? -e[f] - 1 : e[f];
-    F[f] = st.F[id];
+    F[f] = CG ? ldcg4(st.F + id) : st.F[id];
   }
   R[0] = R[1] = R[2] = R[3] = 0.0;
   den = 0.0;
@@ -1424,6 +1454,143 @@ __global__ void __launch_bounds__(kBlock, 4) k_muscl_gradients(DevMesh m, DevSta
   (void)NT;
 }
 
+// ---- Persistent form of one stage for batched solves (no reference counterpart) ----
+// One cooperative launch per RK stage does the work of k_muscl_gradients, k_faces and
+// k_gather_stage: its resident thread blocks walk the (instance, block) work lists of the active
+// instances (record rows, faces, cells), phase after phase, with a grid barrier between the
+// phases.  Values written in the same launch by other blocks (records, ghost rows, del_t, face
+// fluxes) are read from L2.  Every per-cell and per-face operation is the one the three kernels
+// do, so the state is bit-identical to theirs; the error norms of the last stage are reduced over
+// the persistent blocks (a different summation order than the three-kernel grid).
+//
+// The barrier waits are bounded: a block that waits longer than kBarrierCycles (about half a
+// second) records CFD_ERR_TIMEOUT in the status word and goes on; once the status is set no block
+// waits again, so the launch always ends and the host reads the error.  test_arrivals adds
+// arrivals that never come (a test of the timeout path; 0 in every run).
+constexpr long long kBarrierCycles = 1ll << 30;
+constexpr int kPersistBlock = 128;
+
+__device__ __forceinline__ void grid_barrier(unsigned int *count, unsigned int *gen, int *status,
+                                             unsigned int test_arrivals) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *vgen = gen;
+    volatile int *vstatus = status;
+    const unsigned int g = *vgen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(count, 1u) + 1u;
+    if (arrived == gridDim.x + test_arrivals) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == g) {
+        if (*vstatus != 0) break;
+        if (clock64() - t0 > kBarrierCycles) {
+          atomicCAS(status, 0, 5 /* CFD_ERR_TIMEOUT */);
+          break;
+        }
+        __nanosleep(128);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <typename T, int DISS>
+__global__ void __launch_bounds__(kPersistBlock, 4) k_persistent_stage(DevMesh m, DevState st, FluxParams fp,
+                                                                       BcParams bp, int kind, int lts, int fuse_final,
+                                                                       int keep_delu, int flags, int with_dt,
+                                                                       int with_bc, unsigned int test_arrivals) {
+  const int NP = m.NP;
+  if (step_done(st.ctl)) return;  // every block sees the same flag (written by an earlier launch)
+  unsigned int *bar_count = st.counter + 4, *bar_gen = st.counter + 5;
+  // Phase 1: gradient records (and del_t), the first stage's boundary conditions.
+  // Without work lists (a single solve) the phases walk all rows, faces and cells in chunks.
+  const int nr = m.rblk ? m.n_rblk : (NP + kWorkItemBlock - 1) / kWorkItemBlock;
+  const int nfb = m.fblk ? m.n_fblk : (m.NF + kWorkFaceBlock - 1) / kWorkFaceBlock;
+  const int ncb = m.cblk ? m.n_cblk : (NP + kWorkCellBlock - 1) / kWorkCellBlock;
+  for (int w = blockIdx.x; w < nr; w += gridDim.x) {
+    const int2 b = m.rblk ? m.rblk[w] : make_int2(w * kWorkItemBlock, min((w + 1) * kWorkItemBlock, NP));
+    for (int c = b.x + threadIdx.x; c < b.y; c += blockDim.x) {
+      if (c >= NP) continue;
+      if (with_bc) {
+        const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+        for (int i = b0; i < b1; i++) bc_entry(m, st, bp, m.bidx[i], 0, 0);
+      }
+      const double4 v = st.q4[c];
+      const double qc[4] = {v.x, v.y, v.z, v.w};
+      double g[8], den;
+      if (with_dt) cell_gradients<true, true>(m, st.prim, st.q4, c, qc, g, den);
+      else cell_gradients<false, true>(m, st.prim, st.q4, c, qc, g, den);
+      if (st.recf) {
+        float4 *r = st.recf + 2 * (size_t)c;
+        r[0] = make_float4(float(g[0]), float(g[1]), float(g[2]), float(g[3]));
+        r[1] = make_float4(float(g[4]), float(g[5]), float(g[6]), float(g[7]));
+      } else {
+        double4 *r = reinterpret_cast<double4 *>(st.rec + 8 * (size_t)c);
+        r[0] = make_double4(g[0], g[1], g[2], g[3]);
+        r[1] = make_double4(g[4], g[5], g[6], g[7]);
+      }
+      if (with_dt) st.dtc[c] = cell_dt(m, fp, c, den);
+    }
+  }
+  grid_barrier(bar_count, bar_gen, st.status, test_arrivals);
+  // Phase 2: face fluxes.
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+  for (int w = blockIdx.x; w < nfb; w += gridDim.x) {
+    const int2 b = m.fblk ? m.fblk[w] : make_int2(w * kWorkFaceBlock, min((w + 1) * kWorkFaceBlock, m.NF));
+    for (int i = b.x + threadIdx.x; i < b.y; i += blockDim.x) {
+      const int2 on = m.fon[i];
+      const int c = on.x, N = on.y;
+      const double4 gq = m.fg4[i];
+      const T nx = T(gq.x), ny = T(gq.y), dl = T(gq.z), dx = T(gq.w), dy = T(m.fdy[i]);
+      const double4 c0 = ldcg4(st.q4 + c), n0 = ldcg4(st.q4 + N);
+      const bool nphys = N < NP;
+      double4 c1, c2, n1, n2;
+      if (sizeof(T) == sizeof(float)) {
+        const float4 a = __ldcg(st.recf + 2 * (size_t)c), bb = __ldcg(st.recf + 2 * (size_t)c + 1);
+        c1 = make_double4(a.x, a.y, a.z, a.w);
+        c2 = make_double4(bb.x, bb.y, bb.z, bb.w);
+        if (nphys) {
+          const float4 p = __ldcg(st.recf + 2 * (size_t)N), q = __ldcg(st.recf + 2 * (size_t)N + 1);
+          n1 = make_double4(p.x, p.y, p.z, p.w);
+          n2 = make_double4(q.x, q.y, q.z, q.w);
+        } else {
+          n1 = c1;
+          n2 = c2;
+        }
+      } else {
+        const double4 *rc = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)c);
+        const double4 *rn = reinterpret_cast<const double4 *>(st.rec + 8 * (size_t)N);
+        c1 = ldcg4(rc);
+        c2 = ldcg4(rc + 1);
+        n1 = nphys ? ldcg4(rn) : c1;
+        n2 = nphys ? ldcg4(rn + 1) : c2;
+      }
+      st.F[i] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, nx, ny, dl, dx, dy, T(fp.eflin),
+                                     T(fp.shock_fix));
+    }
+  }
+  grid_barrier(bar_count, bar_gen, st.status, test_arrivals);
+  // Phase 3: gather of each cell's face fluxes in face order and the stage update.
+  double dtu = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int w = blockIdx.x; w < ncb; w += gridDim.x) {
+    const int2 b = m.cblk ? m.cblk[w] : make_int2(w * kWorkCellBlock, min((w + 1) * kWorkCellBlock, NP));
+    for (int c = b.x + threadIdx.x; c < b.y; c += blockDim.x) {
+      double R[4], den = 0.0;
+      gather_faces<false, true>(m, st, c, R, den);
+      const double dtc = (lts == 1 || first_kind(kind)) ? __ldcg(st.dtc + c) : 0.0;
+      const double dt = stage_cell(m, st, bp, c, R, dtc, kind, lts, fuse_final, keep_delu, flags, e);
+      dtu = dt < dtu ? dt : dtu;
+    }
+  }
+  if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
+}
+
 // Patch form of one stage of the face-based per-cell-dt forms: one thread block per patch of up
 // to kPatchCells cells does the work of k_muscl_gradients, k_faces and k_gather_stage for its
 // cells, with the records and face fluxes in shared memory instead of HBM.
@@ -1506,7 +1673,7 @@ __global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevSt
       n2r = make_double4(srec[8 * rows + ln], srec[9 * rows + ln], srec[10 * rows + ln], srec[11 * rows + ln]);
     }
     const double4 F = face_flux_rec<double, DISS>(glim, c0r, c1r, c2r, n0r, n1r, n2r, fe.nx, fe.ny, fe.dl, fe.dx, fe.dy,
-                                                    fp.eflin);
+                                                    fp.eflin, fp.shock_fix);
     if (so < 4) {
       sF[(so * 4 + 0) * kPatchCells + lo] = F.x;
       sF[(so * 4 + 1) * kPatchCells + lo] = F.y;
@@ -1923,6 +2090,50 @@ int launch_update(cudaStream_t s, const DevMesh &m, DevState &st, int from_S) {
 
 int launch_gradient(cudaStream_t s, const DevMesh &m, DevState &st, int var, double *grad) {
   k_gradient<<<nblk(m.NP, kBlock), kBlock, 0, s>>>(m, st, var, grad);
+  return 1;
+}
+
+template <typename T, int DISS>
+void persistent_kernel_ptr(void (**k)(DevMesh, DevState, FluxParams, BcParams, int, int, int, int, int, int, int,
+                                      unsigned int)) {
+  *k = k_persistent_stage<T, DISS>;
+}
+
+// Largest co-resident grid of the persistent stage kernel on this device (0: not available).
+int persistent_grid(const FluxParams &fp) {
+  void (*k)(DevMesh, DevState, FluxParams, BcParams, int, int, int, int, int, int, int, unsigned int) = nullptr;
+  const bool f32 = fp.precision == 1;
+  switch (fp.dissipation) {
+    case 6: f32 ? persistent_kernel_ptr<float, 6>(&k) : persistent_kernel_ptr<double, 6>(&k); break;
+    case 7: f32 ? persistent_kernel_ptr<float, 7>(&k) : persistent_kernel_ptr<double, 7>(&k); break;
+    case 8: f32 ? persistent_kernel_ptr<float, 8>(&k) : persistent_kernel_ptr<double, 8>(&k); break;
+    default: f32 ? persistent_kernel_ptr<float, 3>(&k) : persistent_kernel_ptr<double, 3>(&k); break;
+  }
+  int dev = 0, sms = 0, per_sm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kPersistBlock, 0) != cudaSuccess) return 0;
+  return sms * per_sm;
+}
+
+int launch_persistent_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp,
+                            const BcParams &bp, int kind, int lts, int fuse_final, int keep_delu, int flags,
+                            int with_dt, int with_bc, int grid, unsigned int test_arrivals) {
+  void (*k)(DevMesh, DevState, FluxParams, BcParams, int, int, int, int, int, int, int, unsigned int) = nullptr;
+  const bool f32 = fp.precision == 1;
+  switch (fp.dissipation) {
+    case 6: f32 ? persistent_kernel_ptr<float, 6>(&k) : persistent_kernel_ptr<double, 6>(&k); break;
+    case 7: f32 ? persistent_kernel_ptr<float, 7>(&k) : persistent_kernel_ptr<double, 7>(&k); break;
+    case 8: f32 ? persistent_kernel_ptr<float, 8>(&k) : persistent_kernel_ptr<double, 8>(&k); break;
+    default: f32 ? persistent_kernel_ptr<float, 3>(&k) : persistent_kernel_ptr<double, 3>(&k); break;
+  }
+  DevMesh mm = m;
+  DevState ss = st;
+  FluxParams ff = fp;
+  BcParams bb = bp;
+  void *args[] = {&mm, &ss, &ff, &bb, &kind, &lts, &fuse_final, &keep_delu, &flags, &with_dt, &with_bc, &test_arrivals};
+  cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kPersistBlock), args, 0, s);
   return 1;
 }
 

@@ -138,6 +138,7 @@ struct FluxParams {
   int precision;
   double cfl, zeta, zeta1;
   double eflin;         // entropy fix of the linear waves in the gradient-MUSCL Roe flux (0: off)
+  double shock_fix;     // Rusanov dissipation on faces with |grad p| |d| > shock_fix * p (0: off)
 };
 
 struct BcParams {
@@ -156,6 +157,14 @@ int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int l
 // Face-based forms with a per-cell stage dt (lts 1 or 2): gradients, face fluxes and the fused
 // gather + stage update.
 int launch_faces(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
+// Persistent form of one face-based stage (batched solves): gradients, faces and gather + update
+// in one cooperative launch of `grid` blocks over the work lists, bounded grid barriers between
+// the phases (CFD_ERR_TIMEOUT in the status word when a wait runs out).  persistent_grid: the
+// largest co-resident grid (0 when cooperative launches are not available).
+int persistent_grid(const FluxParams &fp);
+int launch_persistent_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp,
+                            const BcParams &bp, int kind, int lts, int fuse_final, int keep_delu, int flags,
+                            int with_dt, int with_bc, int grid, unsigned int test_arrivals);
 int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 // Fused gather + stage update of the per-cell-dt forms; del_t comes from the gradient pass
 // (launch_muscl_gradients with with_dt).  flags: bit 1 the owner thread writes its ghosts for the

@@ -1,8 +1,8 @@
 // Drop-in translation unit for the reference solver (rameshkolluru43/CFD_Solver_withCUDA).
 //
-// Link this file in place of the reference's src/Numerical_Method.cpp, src/Net_Flux.cpp and
-// src/Error_Estimate_Update.cpp, and link libcfd_b200.so: the reference's own driver then runs
-// its residual/update path on the GPU.  It implements the same entry points with the same
+// Link this file in place of the reference's src/Numerical_Method.cpp, src/Net_Flux.cpp,
+// src/Error_Estimate_Update.cpp and src/Boundary_Conditions.cpp, and link libcfd_b200.so: the
+// reference's own driver then runs its boundary-condition, residual and update path on the GPU.  It implements the same entry points with the same
 // signatures over the reference's globals (include/Globals.h:332-416) and, like the reference,
 // exits on errors.  Compiled against the reference's headers; it is not part of libcfd_b200.so.
 //
@@ -159,6 +159,13 @@ extern "C" void b200_shim_reset() {
   g_updates = 0;
 }
 
+// src/Boundary_Conditions.cpp:12-61: the ghost rows of every boundary entry, on the device.
+void Apply_Boundary_Conditions() {
+  ensure();
+  b200_check(cfd_apply_boundary_conditions(g_ctx));
+  changed(false);
+}
+
 // src/Net_Flux.cpp:46,97 — both orders: the context was configured from Is_Second_Order.
 void Evaluate_Cell_Net_Flux_1O() {
   ensure();
@@ -181,8 +188,9 @@ double get_Max_dt() {
   return Max_dt;
 }
 
-// src/Numerical_Method.cpp:26 / :342.  The driver applies the boundary conditions on the host
-// just before; they are applied again on the device (same values) before the flux evaluation.
+// src/Numerical_Method.cpp:26 / :342.  The boundary conditions are applied on the device first,
+// as the driver's Apply_Boundary_Conditions just did (same values), so that a driver that changed
+// nothing in between and one that calls the method alone get the same result.
 void Explicit_Method() {
   ensure();
   b200_check(cfd_apply_boundary_conditions(g_ctx));

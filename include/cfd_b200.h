@@ -149,6 +149,11 @@ typedef struct {
                                 acoustic waves are fixed, with delta = 0.1 * a_Roe, as in the
                                 reference's ROE.  No reference counterpart; it suppresses the
                                 carbuncle of grid-aligned strong shocks (0.2 - 0.4 typical). */
+  double shock_fix;          /* Shock-stable hybrid of the gradient-MUSCL Roe flux: on a face where
+                                either cell's pressure gradient marks a shock, |grad p| |d| >
+                                value * p (d: centre-to-centre vector), the Roe dissipation is
+                                replaced by the Rusanov dissipation 1/2 max(|Vn| + a) (U_R - U_L) dl.
+                                0 (default): Roe everywhere.  No reference counterpart. */
 } cfd_config;
 
 /* Defaults of json_Files/Solver_Config.json with Dissipation_Type = ROE. */
@@ -205,8 +210,15 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * in L2 as persisting lines between the kernels of a stage, when they fit in the device's largest
  * persisting set-aside; default 1.  Creating such a context
  * raises the device's persisting-L2 set-aside, cudaLimitPersistingL2CacheSize, to hold them, up to
- * the device maximum; it is never lowered and lasts as long as the process's CUDA context).
- * None of the options changes a result bit. */
+ * the device maximum; it is never lowered and lasts as long as the process's CUDA context),
+ * "persistent" (face-based forms with a per-cell dt: each RK stage as one persistent cooperative
+ * kernel over the cells, faces and cells again, with bounded grid barriers between the phases and
+ * one CUDA graph per RK stage; default 0; the batched solves' form, see cfd_batch_set_option),
+ * "barrier_timeout_test" (a test of the bounded barriers: every barrier of the persistent form
+ * waits for `value` more blocks than it has, so each wait runs out and the step reports
+ * CFD_ERR_TIMEOUT; default 0).
+ * None of the options changes a state bit (the persistent form sums the error norms in another
+ * order). */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
 /* Times every combination of the options above that applies to this configuration over `steps`
  * pseudo-steps of the context's own mesh and state, keeps the fastest and restores the state
@@ -351,6 +363,11 @@ cfd_status cfd_batch_download_state(cfd_batch *b, double *U);
  * actually advanced.  Any output pointer may be NULL. */
 cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_every, int *steps_to_tol,
                          double *time_to_tol, double *res_ratio, long long *cell_updates, int *steps_done);
+/* Run-time options of the batch's solver context (cfd_set_option), e.g. "persistent" = 1: each RK
+ * stage of every instance runs as one persistent cooperative kernel over the (instance, block)
+ * work lists, bounded grid barriers between its phases, one CUDA graph per RK stage (results
+ * bit-identical to the three-kernel form; CFD_ERR_TIMEOUT when a barrier wait runs out). */
+cfd_status cfd_batch_set_option(cfd_batch *b, const char *name, double value);
 void cfd_batch_destroy(cfd_batch *b);
 
 /* ------------------------------------------------------------------------------------------

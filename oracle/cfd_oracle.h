@@ -22,6 +22,7 @@ typedef struct {
   double cfl, zeta, zeta1, inlet_rho, inlet_p, inlet_p0, inlet_t0, exit_p, r_gas, inlet_u, inlet_v;
   int weno, weno_char;
   double ef_linear; /* entropy fix of the linear waves in the gradient-MUSCL Roe flux (0: off) */
+  double shock_fix; /* Rusanov dissipation on faces with |grad p| |d| > shock_fix * p (0: off) */
 } orc_config;
 
 typedef struct orc_state orc_state;

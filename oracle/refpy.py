@@ -297,7 +297,8 @@ class _OrcConfig(ctypes.Structure):
                                             "muscl", "precision", "inlet_bc", "exit_bc"]] + \
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
                                                "exit_p", "r_gas", "inlet_u", "inlet_v"]] + \
-               [(n, ctypes.c_int) for n in ["weno", "weno_char"]] + [("ef_linear", ctypes.c_double)]
+               [(n, ctypes.c_int) for n in ["weno", "weno_char"]] + [("ef_linear", ctypes.c_double),
+                                                                            ("shock_fix", ctypes.c_double)]
 
 
 _orc = None
@@ -363,6 +364,7 @@ class OracleRun:
         c.weno = params.get("weno", 0)
         c.weno_char = params.get("weno_characteristic", 0)
         c.ef_linear = params.get("entropy_fix_linear", 0.0)
+        c.shock_fix = params.get("shock_fix", 0.0)
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,

@@ -117,6 +117,12 @@ ADDITIVE = {
                                                  integrator=cb.INT_SSPRK3, local_time_stepping=1,
                                                  entropy_fix_linear=0.3, inlet_bc=cb.INLET_FIXED,
                                                  inlet_u="free stream", inlet_v=0.0),
+    "grad_muscl_vanleer_shock_fix_fixed_inlet": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANLEER,
+                                                     integrator=cb.INT_SSPRK3, local_time_stepping=1,
+                                                     entropy_fix_linear=0.4, shock_fix=0.2, inlet_bc=cb.INLET_FIXED,
+                                                     inlet_u="free stream", inlet_v=0.0),
+    "grad_muscl_minmod_shock_fix_fp32": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_MINMOD, precision=cb.PREC_FP32_FLUX,
+                                             integrator=cb.INT_SSPRK3, local_time_stepping=1, shock_fix=0.1),
     "grad_muscl_vanalbada_eflin_fp32": dict(muscl=cb.MUSCL_GRADIENT, limiter=cb.LIM_VANALBADA,
                                             precision=cb.PREC_FP32_FLUX, integrator=cb.INT_SSPRK3,
                                             local_time_stepping=1, entropy_fix_linear=0.4),
