@@ -1687,6 +1687,7 @@ struct cfd_batch {
   double4 *d_bstate = nullptr;
   double *d_bexit = nullptr;
   std::vector<double> r0_fixed;  // per-instance residual normalisers (empty: first-step residual)
+  double diverge = 0.0;          // > 0: an instance whose residual ratio exceeds it stops (steps_to_tol -2)
 };
 
 static cfd_status batch_tables(cfd_batch *b) {
@@ -1928,7 +1929,12 @@ cfd_status cfd_batch_residuals(cfd_batch *b, double *res) {
 }
 
 cfd_status cfd_batch_set_option(cfd_batch *b, const char *name, double value) {
-  if (!b) return fail(CFD_ERR_BAD_ARG, "null batch");
+  if (!b || !name) return fail(CFD_ERR_BAD_ARG, "null argument");
+  if (std::string(name) == "divergence_ratio") {
+    if (!(value >= 0.0)) return fail(CFD_ERR_BAD_ARG, "divergence_ratio must be >= 0");
+    b->diverge = value;
+    return CFD_OK;
+  }
   return cfd_set_option(b->ctx, name, value);
 }
 
@@ -1976,6 +1982,10 @@ cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_ever
         b->active[i] = 0;
         sto[i] = steps;
         tto[i] = t;
+        changed = true;
+      } else if (b->diverge > 0.0 && ratio[i] > b->diverge) {
+        b->active[i] = 0;  // residual growth: the instance stops, the caller falls back
+        sto[i] = -2;
         changed = true;
       }
     }

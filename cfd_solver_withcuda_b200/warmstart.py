@@ -76,11 +76,18 @@ def member_batch(meshes, params, precision=cb.PREC_FP64):
     return b
 
 
-def solve(meshes, params, states, tol, max_steps, check_every=200, r0=None, precision=cb.PREC_FP64):
+def solve(meshes, params, states, tol, max_steps, check_every=200, r0=None, precision=cb.PREC_FP64,
+          persistent=False, diverge=0.0):
     """Batched steady solves of the members from `states`, each until ||R_rho|| has dropped to
     tol * r0 (r0: given normalisers, else each member's first-step residual); returns (run
-    result, final states, wall seconds)."""
+    result, final states, wall seconds).  persistent: the batch runs each RK stage as one
+    persistent kernel (one CUDA graph per stage); diverge > 0: a member whose residual ratio grows
+    past it stops (steps_to_tol -2)."""
     b = member_batch(meshes, params, precision)
+    if persistent:
+        b.set_option("persistent", 1)
+    if diverge > 0.0:
+        b.set_option("divergence_ratio", diverge)
     b.upload_state(states)
     if r0 is not None:
         b.set_reference_residual(r0)
@@ -90,6 +97,51 @@ def solve(meshes, params, states, tol, max_steps, check_every=200, r0=None, prec
     out = b.download_state()
     b.close()
     return res, out, wall
+
+
+def solve_plain(meshes, params, states, tol, max_steps, check_every, r0):
+    """The plain path: each member alone through the single-solve API, FP64, one after another,
+    from its state until ||R_rho|| <= tol * r0[i] (checked every check_every pseudo-steps) or
+    max_steps; returns (steps per member, -1 if not reached; final states; wall seconds)."""
+    steps, out = [], []
+    t0 = time.perf_counter()
+    for m, (_, M, ratio), U, r in zip(meshes, params, states, r0):
+        p0, T0, pe = boundary_values(M, ratio)
+        s = cb.Solver(m, solver_config(inlet_p0=p0, inlet_t0=T0, exit_p=pe))
+        s.set_option("keep_delu", 0)
+        s.upload_state(U)
+        done, k = 0, -1
+        while done < max_steps:
+            info = s.step(min(check_every, max_steps - done))
+            done += min(check_every, max_steps - done)
+            if info.res_l2[0] <= tol * r:
+                k = done
+                break
+        steps.append(k)
+        out.append(s.download_U())
+        s.close()
+    return np.array(steps), out, time.perf_counter() - t0
+
+
+def solve_chosen(meshes, params, states, tol, max_steps, check_every, r0, switch_tol, diverge=0.0):
+    """The chosen path: every member in one persistent batch; the FP32-flux form until
+    ||R_rho|| <= switch_tol * r0 (its rounding floor lies near 1e-6 of the start), then the FP64
+    form from that state to tol * r0.  Returns (steps per member over both phases, -1 if not
+    reached, -2 if the residual grew past `diverge`; final states; wall seconds of both phases and
+    the hand-over)."""
+    switch_tol = max(switch_tol, tol)
+    t0 = time.perf_counter()
+    res1, U1, _ = solve(meshes, params, states, switch_tol, max_steps, check_every, r0=r0,
+                        precision=cb.PREC_FP32_FLUX, persistent=True, diverge=diverge)
+    k1 = res1["steps_to_tol"]
+    grown = k1 == -2
+    res2, U2, _ = solve(meshes, params, U1, tol, max_steps, check_every, r0=r0, precision=cb.PREC_FP64,
+                        persistent=True, diverge=diverge)
+    wall = time.perf_counter() - t0
+    k2 = res2["steps_to_tol"]
+    first = np.where(k1 > 0, k1, res1["steps"])
+    steps = np.where(grown | (k2 == -2), -2, np.where(k2 > 0, first + k2, -1))
+    return steps, U2, wall
 
 
 def first_residuals(meshes, params, states):
@@ -463,9 +515,20 @@ def _with_ghosts(mesh, U_phys):
     return full
 
 
-def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-4, max_steps=150000, check_every=500, epochs=200,
-                   batch=8, lr=1e-3, seed=2024, device="cuda", log=None):
-    """The whole warm-start study; returns a dict of measured figures."""
+def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-8, max_steps=400000, check_every=500, epochs=200,
+                   batch=8, lr=1e-3, seed=2024, device="cuda", log=None, switch_tol=1e-5, n_plain=8, diverge=10.0):
+    """The whole warm-start study; returns a dict of measured figures.
+
+    1. Training members solved from the freestream start by the FP64 batched solver.
+    2. The surrogate trained on their (rho, u, v, p) (library kernels, Adam).
+    3. Held-out members: the plain path (FP64 single solves from the freestream, one after
+       another; timed on the first n_plain members, the wall time per member scaled to all) and
+       the chosen path (prediction, then the persistent batch in FP32-flux to switch_tol and FP64
+       to tol), both to the same absolute target tol * r0 (r0: each member's first residual from
+       the freestream).  Fallback, live: a prediction with a non-positive density or pressure
+       starts from the freestream; a member whose residual grows past `diverge` x r0, or that
+       misses the target, is solved again from the freestream (the time counts).
+    4. The same batched form from the freestream start, for the gain of the prediction alone."""
     torch = _torch()
     say = log or (lambda *a: None)
     P = draw_parameters(n_train + n_test, seed)
@@ -475,11 +538,10 @@ def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-4, max_steps=150
     fs_states = [freestream_state(m, M) for m, (_, M, _) in zip(meshes, P)]
     tr, te = slice(0, n_train), slice(n_train, n_train + n_test)
     out = {"mesh": "%dx%d" % (nx, ny), "cells": graph.N, "train": n_train, "test": n_test, "tol": tol,
-           "max_steps": max_steps, "epochs": epochs, "seed": seed}
+           "switch_tol": switch_tol, "max_steps": max_steps, "epochs": epochs, "seed": seed, "n_plain": n_plain}
 
-    # 1. Training members solved from the freestream start (the plain FP64 solver).
-    t0 = time.perf_counter()
-    res_tr, U_tr, wall_tr = solve(meshes[tr], P[tr], fs_states[tr], tol, max_steps, check_every)
+    # 1. Training members solved from the freestream start (the plain FP64 solver, batched).
+    res_tr, U_tr, wall_tr = solve(meshes[tr], P[tr], fs_states[tr], tol, max_steps, check_every, persistent=True)
     out["train_solve_s"] = wall_tr
     out["train_converged"] = int((res_tr["steps_to_tol"] > 0).sum())
     say("train solves", wall_tr, out["train_converged"])
@@ -500,39 +562,71 @@ def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-4, max_steps=150
     out["loss_first"], out["loss_last"] = losses[0], losses[-1]
     say("training", out["train_s"], losses[0], losses[-1])
 
-    # 3. Held-out members from the freestream start: reference solutions and normalisers.
+    # 3a. Normalisers: each held-out member's first residual from the freestream.
     r0 = first_residuals(meshes[te], P[te], fs_states[te])
-    res_fs, U_fs, wall_fs = solve(meshes[te], P[te], fs_states[te], tol, max_steps, check_every, r0=r0)
 
-    # 4. Predicted starts (denormalised; non-physical predictions fall back to freestream).
+    # 3b. The plain path on the first n_plain members.
+    npl = max(1, min(n_plain, n_test))
+    k_pl, U_pl, wall_pl = solve_plain(meshes[te][:npl], P[te][:npl], fs_states[te][:npl], tol, max_steps,
+                                      check_every, r0[:npl])
+    out["plain_converged"] = int((k_pl > 0).sum())
+    out["plain_steps_median"] = float(np.median(k_pl[k_pl > 0])) if (k_pl > 0).any() else None
+    out["plain_wall_per_member_s"] = wall_pl / npl
+    out["plain_wall_s"] = wall_pl / npl * n_test
+    say("plain", out["plain_wall_s"], k_pl)
+
+    # 3c. The chosen path: prediction, fallback of non-physical predictions, persistent batch.
+    torch.cuda.synchronize()
     t2 = time.perf_counter()
     pred = predict(model, graph, [f[0] for f in feats[te]], [f[1] for f in feats[te]], batch=batch, device=device)
-    out["predict_s"] = time.perf_counter() - t2
     starts, fallback = [], np.zeros(n_test, bool)
-    pred_err = []
     for i, (m, q) in enumerate(zip(meshes[te], pred)):
         q = q * sd + mu
-        ref = primitive(U_fs[i][:graph.N])
-        pred_err.append(np.linalg.norm(q - ref) / np.linalg.norm(ref))
         if not (np.all(q[:, 0] > 0) and np.all(q[:, 3] > 0)):
             fallback[i] = True
             starts.append(fs_states[n_train + i])
             continue
         starts.append(_with_ghosts(m, cb.conserved_from_primitive(q[:, 0], q[:, 1], q[:, 2], q[:, 3])))
-    res_ws, U_ws, wall_ws = solve(meshes[te], P[te], starts, tol, max_steps, check_every, r0=r0)
-    k_fs, k_ws = res_fs["steps_to_tol"], res_ws["steps_to_tol"]
-    fallback |= (k_ws < 0) & (k_fs > 0)
-    ok = (k_fs > 0) & ~fallback
-    out.update({
-        "freestream_converged": int((k_fs > 0).sum()), "warm_converged": int((k_ws > 0).sum()),
-        "fallback_rate": float(fallback.mean()),
-        "steps_freestream_median": float(np.median(k_fs[k_fs > 0])) if (k_fs > 0).any() else None,
-        "steps_warm_median": float(np.median(k_ws[ok])) if ok.any() else None,
-        "steps_ratio_median": float(np.median(k_ws[ok] / k_fs[ok])) if ok.any() else None,
-        "wall_freestream_s": wall_fs, "wall_warm_s": wall_ws + out["predict_s"],
-        "prediction_rel_l2_median": float(np.median(pred_err)),
-        "final_state_rel_l2_max": float(max(np.linalg.norm(U_ws[i][:graph.N] - U_fs[i][:graph.N]) /
-                                            np.linalg.norm(U_fs[i][:graph.N]) for i in range(n_test))),
-    })
+    out["predict_s"] = time.perf_counter() - t2
+    k_ch, U_ch, wall_ch = solve_chosen(meshes[te], P[te], starts, tol, max_steps, check_every, r0, switch_tol,
+                                       diverge)
+    redo = np.where(k_ch < 0)[0]
+    wall_fb = 0.0
+    if redo.size:
+        # Live fallback: members whose residual grew or that missed the target, from the freestream.
+        test_meshes = meshes[te]
+        k_fb, U_fb, wall_fb = solve_chosen([test_meshes[i] for i in redo], P[te][redo],
+                                           [fs_states[n_train + i] for i in redo], tol, max_steps, check_every,
+                                           r0[redo], switch_tol)
+        for j, i in enumerate(redo):
+            k_ch[i] = k_fb[j]
+            U_ch[i] = U_fb[j]
+        fallback[redo] = True
+    out["chosen_wall_s"] = out["predict_s"] + wall_ch + wall_fb
+    out["chosen_converged"] = int((k_ch > 0).sum())
+    out["chosen_steps_median"] = float(np.median(k_ch[k_ch > 0])) if (k_ch > 0).any() else None
+    out["fallback_rate"] = float(fallback.mean())
+    out["speedup_chosen_vs_plain"] = out["plain_wall_s"] / out["chosen_wall_s"]
+    say("chosen", out["chosen_wall_s"], k_ch)
+
+    # 4. The batched form from the freestream (same phases): the prediction's own gain.
+    k_fs, U_fs, wall_fs = solve_chosen(meshes[te], P[te], fs_states[te], tol, max_steps, check_every, r0,
+                                       switch_tol)
+    ok = (k_fs > 0) & (k_ch > 0) & ~fallback
+    out["batched_freestream_wall_s"] = wall_fs
+    out["batched_freestream_steps_median"] = float(np.median(k_fs[k_fs > 0])) if (k_fs > 0).any() else None
+    out["steps_ratio_median"] = float(np.median(k_ch[ok] / k_fs[ok])) if ok.any() else None
+    out["speedup_prediction_in_batch"] = wall_fs / (out["predict_s"] + wall_ch)
+
+    # Accuracy: prediction error and the final states of the chosen path against the plain FP64
+    # solutions (the members the plain path ran) and against the batched FP64-from-freestream ones.
+    pred_err = [np.linalg.norm(q * sd + mu - primitive(U_fs[i][:graph.N])) / np.linalg.norm(primitive(U_fs[i][:graph.N]))
+                for i, q in enumerate(pred)]
+    out["prediction_rel_l2_median"] = float(np.median(pred_err))
+    out["final_state_rel_l2_vs_plain_max"] = float(max(
+        np.linalg.norm(U_ch[i][:graph.N] - U_pl[i][:graph.N]) / np.linalg.norm(U_pl[i][:graph.N]) for i in range(npl)))
+    out["final_state_rel_l2_vs_batched_freestream_max"] = float(max(
+        np.linalg.norm(U_ch[i][:graph.N] - U_fs[i][:graph.N]) / np.linalg.norm(U_fs[i][:graph.N])
+        for i in range(n_test)))
     say("warm start", out)
     return out

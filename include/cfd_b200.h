@@ -366,7 +366,9 @@ cfd_status cfd_batch_run(cfd_batch *b, int max_steps, double tol, int check_ever
 /* Run-time options of the batch's solver context (cfd_set_option), e.g. "persistent" = 1: each RK
  * stage of every instance runs as one persistent cooperative kernel over the (instance, block)
  * work lists, bounded grid barriers between its phases, one CUDA graph per RK stage (results
- * bit-identical to the three-kernel form; CFD_ERR_TIMEOUT when a barrier wait runs out). */
+ * bit-identical to the three-kernel form; CFD_ERR_TIMEOUT when a barrier wait runs out).
+ * "divergence_ratio" = x > 0: in cfd_batch_run an instance whose residual ratio exceeds x at a
+ * check stops updating and gets steps_to_tol = -2 (residual growth; 0 = never). */
 cfd_status cfd_batch_set_option(cfd_batch *b, const char *name, double value);
 void cfd_batch_destroy(cfd_batch *b);
 

@@ -190,9 +190,26 @@ def test_per_member_boundary_values_equal_single_solves():
 
 
 def test_warm_start_experiment_small():
-    out = ws.run_experiment(nx=16, ny=8, n_train=8, n_test=3, tol=1e-2, max_steps=20000, check_every=100, epochs=5,
-                            batch=4)
+    out = ws.run_experiment(nx=16, ny=8, n_train=8, n_test=3, tol=1e-3, max_steps=20000, check_every=100, epochs=5,
+                            batch=4, switch_tol=1e-2, n_plain=2)
     assert out["parameters"] > 150000
-    assert out["train_converged"] == 8 and out["freestream_converged"] == 3
+    assert out["train_converged"] == 8 and out["plain_converged"] == 2 and out["chosen_converged"] == 3
     assert 0.0 <= out["fallback_rate"] <= 1.0
     assert np.isfinite(out["loss_last"]) and np.isfinite(out["prediction_rel_l2_median"])
+    assert out["speedup_chosen_vs_plain"] > 0.0
+    # Both paths reach the same absolute residual target; their steady states agree closely.
+    assert out["final_state_rel_l2_vs_plain_max"] < 1e-2
+
+
+def test_divergence_guard_stops_a_growing_member():
+    """A member whose residual ratio exceeds the batch's divergence_ratio stops with steps_to_tol
+    -2: a member started from a state far from its steady state, guarded with a ratio below its
+    early residual growth."""
+    P = ws.draw_parameters(2, 13)
+    meshes = [ws.make_mesh(16, 8, t) for t, _, _ in P]
+    fs = [ws.freestream_state(m, M) for m, (_, M, _) in zip(meshes, P)]
+    r0 = ws.first_residuals(meshes, P, fs)
+    # Normalisers a thousand times smaller than the freestream's first residual: every ratio is
+    # far above the guard at the first check.
+    res, _, _ = ws.solve(meshes, P, fs, tol=1e-12, max_steps=400, check_every=100, r0=r0 * 1e-3, diverge=10.0)
+    assert np.all(res["steps_to_tol"] == -2), res
