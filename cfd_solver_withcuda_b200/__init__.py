@@ -79,7 +79,7 @@ class MlpFwd(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_int), ("nseg", ctypes.c_int), ("seg", MlpSeg * 3), ("out", ctypes.c_int),
                 ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p),
                 ("resid", ctypes.c_void_p), ("ld_resid", ctypes.c_int), ("z1", ctypes.c_void_p),
-                ("y", ctypes.c_void_p), ("ld_y", ctypes.c_int)]
+                ("y", ctypes.c_void_p), ("ld_y", ctypes.c_int), ("engine", ctypes.c_int)]
 
 
 class MlpBwd(ctypes.Structure):
@@ -167,6 +167,7 @@ SIGNATURES = {
     "cfd_mpnn_mlp_backward": (_I, [ctypes.POINTER(MlpBwd), _P]),
     "cfd_mpnn_weight_grad": (_I, [ctypes.POINTER(MlpWgrad), _P]),
     "cfd_mpnn_wgrad_blocks": (_I, []),
+    "cfd_mpnn_status": (_I, [ctypes.POINTER(ctypes.c_int), _I]),
     "cfd_mpnn_add": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _P]),
     "cfd_mpnn_gather_add": (_I, [_P, _I, _P, _I, _P, _I, _I, _P]),
     "cfd_mpnn_segment_sum_acc": (_I, [_P, _I, _P, _P, _I, _I, _P, _I, _I, _P]),

@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(kFluxBlock) k_weno(DevMesh m, DevState st, Flu
 // scheme is conservative to the last bit.  MUSCL on (rho, u, v, p): with d = x_N - x_c and
 // D+ = q_N - q_c, the upwind differences are D-_c = 2 grad q_c . d - D+ and
 // D-_N = 2 grad q_N . d - D+; q_L = q_c + 0.5 phi(D-_c, D+) D+, q_R = q_N - 0.5 phi(D-_N, D+) D+
-// (phi(a, b), r = a/b).  A ghost neighbour uses the owner's gradient.  A non-positive
+// (phi(a, b), r = a/b; the product phi D+ evaluated as muscl_slope).  A ghost neighbour uses the owner's gradient.  A non-positive
 // reconstructed density or pressure falls back to the cell-centre state.  Flux: average of the two
 // face states plus Roe dissipation between them (with the linear-wave entropy fix when
 // fp.eflin > 0).
@@ -829,8 +829,8 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
     const T dp = qn[k] - qc[k];
     const T dmc = T(2.0) * (gc[2 * k] * dx + gc[2 * k + 1] * dy) - dp;
     const T dmn = T(2.0) * (gn[2 * k] * dx + gn[2 * k + 1] * dy) - dp;
-    qL[k] = qc[k] + T(0.5) * phi_ab<T>(glim, dmc, dp) * dp;
-    qR[k] = qn[k] - T(0.5) * phi_ab<T>(glim, dmn, dp) * dp;
+    qL[k] = qc[k] + T(0.5) * muscl_slope<T>(glim, dmc, dp);
+    qR[k] = qn[k] - T(0.5) * muscl_slope<T>(glim, dmn, dp);
   }
   if (!(qL[0] > T(0.0)) || !(qL[3] > T(0.0))) {
 #pragma unroll

@@ -185,6 +185,201 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a) {
   }
 }
 
+// ---- The forward block on the 5th-generation tensor cores (tcgen05) ----
+// One CTA of 128 threads per 128-row tile (persistent over tiles): the input rows and the
+// weights are staged in shared memory as BF16 in the K-major, no-swizzle canonical layout of the
+// tcgen05 matrix descriptors (8-row x 16-byte core matrices, consecutive rows 16 bytes apart,
+// row groups SBO = 128 bytes apart, 8-column chunks LBO = rows x 16 bytes apart); one elected
+// thread issues the M = 128 MMAs (kind::f16, BF16 operands, FP32 accumulators in tensor memory)
+// and commits them to an mbarrier; each warp reads its 32 rows of the accumulator with
+// tcgen05.ld, applies bias and SiLU in FP32, writes the hidden layer back to shared memory as the
+// A operand of the second MMA, and so on.  The results equal the mma.sync kernel's up to the FP32
+// summation order.  Every mbarrier wait is bounded; a wait that runs out records an error in
+// g_tc_status (read by cfd_mpnn_status), and the CTA releases its tensor memory and returns.
+constexpr int TM_TC = 128;
+constexpr long long kTcSpin = 1ll << 22;
+__device__ int g_tc_status = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// Byte offset of element (row, k) of a rows x K tile in the canonical K-major layout.
+__device__ __forceinline__ uint32_t canon_off(int row, int k, int rows) {
+  return (uint32_t)((((k >> 3) * (rows >> 3) + (row >> 3)) << 7) + ((row & 7) << 4) + ((k & 7) << 1));
+}
+// Shared-memory matrix descriptor: start address, LBO and SBO in 16-byte units, version 1,
+// no swizzle.
+__device__ __forceinline__ uint64_t make_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t make_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kTcSpin; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    __nanosleep(64);
+  }
+  return false;
+}
+// 16 consecutive FP32 accumulator columns of this thread's row.
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__global__ void __launch_bounds__(128) k_mlp_fwd_tc(FwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t smb[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  const int Kp = (a.K + 15) & ~15, N2p = a.N2 <= 16 ? 16 : 64;
+  uint8_t *sX = smb;                                  // [128 x Kp]  input rows
+  uint8_t *sW1 = sX + (size_t)TM_TC * Kp * 2;         // [64 x Kp]   W1
+  uint8_t *sS = sW1 + (size_t)HID * Kp * 2;           // [128 x 64]  silu(z1)
+  uint8_t *sW2 = sS + (size_t)TM_TC * HID * 2;        // [N2p x 64]  W2
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < HID * Kp; e += blockDim.x) {
+    const int n = e / Kp, k = e - n * Kp;
+    *reinterpret_cast<uint16_t *>(sW1 + canon_off(n, k, HID)) = k < a.K ? bf(a.w1[n * a.K + k]) : 0;
+  }
+  for (int e = tid; e < N2p * HID; e += blockDim.x) {
+    const int n = e / HID, k = e - n * HID;
+    *reinterpret_cast<uint16_t *>(sW2 + canon_off(n, k, N2p)) = n < a.N2 ? bf(a.w2[n * HID + k]) : 0;
+  }
+  const uint32_t bar_a = smem_u32(&bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+    abort_sh = 0;
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t d1 = tmem, d2 = tmem + 64;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+  const uint32_t idesc1 = make_idesc(TM_TC, HID), idesc2 = make_idesc(TM_TC, N2p);
+  uint32_t parity = 0;
+  const int ntiles = (a.M + TM_TC - 1) / TM_TC;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * TM_TC;
+    for (int e = tid; e < TM_TC * Kp; e += blockDim.x) {
+      const int r = e / Kp, k = e - r * Kp, row = r0 + r;
+      *reinterpret_cast<uint16_t *>(sX + canon_off(r, k, TM_TC)) =
+          (row < a.M && k < a.K) ? bf(seg_value(a.seg, a.nseg, row, k)) : 0;
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t xa = smem_u32(sX), wa = smem_u32(sW1);
+      for (int k0 = 0; k0 < Kp; k0 += 16) {
+        const uint64_t da = make_sdesc(xa + (uint32_t)((k0 >> 3) * (TM_TC >> 3) * 128), TM_TC * 16, 128);
+        const uint64_t db = make_sdesc(wa + (uint32_t)((k0 >> 3) * (HID >> 3) * 128), HID * 16, 128);
+        tc_mma(d1, da, db, idesc1, k0 > 0 ? 1u : 0u);
+      }
+      tc_commit(bar_a);
+    }
+    if (!mbar_wait(bar_a, parity)) {
+      if (tid == 0) atomicExch(&g_tc_status, 5 /* CFD_ERR_TIMEOUT */);
+      abort_sh = 1;
+    }
+    parity ^= 1u;
+    __syncthreads();
+    if (abort_sh) break;
+    tc_fence_after();
+    const int r = 32 * warp + (tid & 31), row = r0 + r;
+#pragma unroll
+    for (int c0 = 0; c0 < HID; c0 += 16) {
+      float v[16];
+      tmem_ld16(d1 + lane_base + c0, v);
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const float z = v[j] + a.b1[c0 + j];
+        if (a.z1 && row < a.M) a.z1[(size_t)row * HID + c0 + j] = z;
+        *reinterpret_cast<uint16_t *>(sS + canon_off(r, c0 + j, TM_TC)) = bf(silu_f(z));
+      }
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t sa = smem_u32(sS), wa = smem_u32(sW2);
+      for (int k0 = 0; k0 < HID; k0 += 16) {
+        const uint64_t da = make_sdesc(sa + (uint32_t)((k0 >> 3) * (TM_TC >> 3) * 128), TM_TC * 16, 128);
+        const uint64_t db = make_sdesc(wa + (uint32_t)((k0 >> 3) * (N2p >> 3) * 128), N2p * 16, 128);
+        tc_mma(d2, da, db, idesc2, k0 > 0 ? 1u : 0u);
+      }
+      tc_commit(bar_a);
+    }
+    if (!mbar_wait(bar_a, parity)) {
+      if (tid == 0) atomicExch(&g_tc_status, 5);
+      abort_sh = 1;
+    }
+    parity ^= 1u;
+    __syncthreads();
+    if (abort_sh) break;
+    tc_fence_after();
+    for (int c0 = 0; c0 < N2p; c0 += 16) {
+      float v[16];
+      tmem_ld16(d2 + lane_base + c0, v);
+      if (row < a.M) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int c = c0 + j;
+          if (c >= a.N2) continue;
+          float y = v[j] + a.b2[c];
+          if (a.resid) y += a.resid[(size_t)row * a.ld_resid + c];
+          a.y[(size_t)row * a.ld_y + c] = y;
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  // After a timed-out wait the MMAs may still be in flight: wait for them (bounded) before the
+  // tensor memory is released.
+  if (abort_sh) mbar_wait(bar_a, parity);
+  tc_fence_after();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+}
+
 struct BwdArgs {
   int M, K, N2;
   const float *dy;
@@ -462,6 +657,10 @@ size_t fwd_smem(int K, int N2) {
   const int Kp = (K + 15) & ~15, LDX = Kp + 8, N2p = (N2 + 7) & ~7;
   return sizeof(uint16_t) * ((size_t)HID * LDX + (size_t)N2p * LDH + (size_t)TM * LDX + (size_t)TM * LDH);
 }
+size_t tc_smem(int K, int N2) {
+  const int Kp = (K + 15) & ~15, N2p = N2 <= 16 ? 16 : 64;
+  return 2 * ((size_t)TM_TC * Kp + (size_t)HID * Kp + (size_t)TM_TC * HID + (size_t)N2p * HID);
+}
 size_t bwd_smem(int K, int N2) {
   const int Kp = (K + 15) & ~15, N2p = (N2 + 15) & ~15, LDN = N2p + 8;
   return sizeof(uint16_t) * ((size_t)HID * LDN + (size_t)Kp * LDH + (size_t)TM * LDN + (size_t)TM * LDH);
@@ -482,6 +681,20 @@ extern "C" {
 
 int cfd_mpnn_wgrad_blocks(void) { return CFD_MPNN_WGRAD_BLOCKS; }
 
+cfd_status cfd_mpnn_status(int *status, int reset) {
+  if (!status) return bad("cfd_mpnn_status: null argument");
+  cudaError_t e = cudaMemcpyFromSymbol(status, g_tc_status, sizeof(int));
+  if (e == cudaSuccess && reset) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(int));
+  }
+  if (e != cudaSuccess) {
+    cfdb::set_last_error(std::string("cfd_mpnn_status: ") + cudaGetErrorString(e));
+    return CFD_ERR_CUDA;
+  }
+  return CFD_OK;
+}
+
 cfd_status cfd_mpnn_mlp_forward(const cfd_mlp_fwd *p, void *stream) {
   if (!p || p->rows < 0 || p->out < 1 || p->out > HID || !p->w1 || !p->b1 || !p->w2 || !p->b2 || !p->y ||
       p->ld_y < p->out || (p->resid && p->ld_resid < p->out))
@@ -501,6 +714,16 @@ cfd_status cfd_mpnn_mlp_forward(const cfd_mlp_fwd *p, void *stream) {
   a.z1 = p->z1;
   a.y = p->y;
   a.ld_y = p->ld_y;
+  if (p->engine == 1) {
+    // tcgen05 form: the tiles plus 48 KB, and at least 80 KB, of shared memory per CTA, so that at
+    // most two CTAs (2 x 128 tensor-memory columns of the SM's 512) share an SM.
+    const size_t need = tc_smem(a.K, a.N2) + 48 * 1024, sm = need > 80 * 1024 ? need : 80 * 1024;
+    set_smem(k_mlp_fwd_tc, sm);
+    const int ntiles = (a.M + TM_TC - 1) / TM_TC;
+    const int grid = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();
+    k_mlp_fwd_tc<<<grid, 128, sm, static_cast<cudaStream_t>(stream)>>>(a);
+    return status_of("cfd_mpnn_mlp_forward (tcgen05)");
+  }
   const size_t sm = fwd_smem(a.K, a.N2);
   set_smem(k_mlp_fwd, sm);
   const int ntiles = (a.M + TM - 1) / TM;

@@ -215,6 +215,33 @@ __device__ __forceinline__ T phi_ab(int kind, T a, T b) {
   }
 }
 
+// The limited slope phi(a / b) * b of the gradient-MUSCL reconstruction (no reference
+// counterpart), algebraically the phi forms above times b but with at most one division:
+//   minmod  |a| < |b| ? a : b;   Van Leer 2ab / (a + b);
+//   superbee sign(b) max(min(2|a|, |b|), min(|a|, 2|b|));   Van Albada b (a^2 + ab) / (a^2 + b^2);
+// 0 when |b| < 1e-12 or ab <= 0 (r <= 0).  The face kernel evaluates eight of these per face, and
+// FP64 division chains bound it.
+template <typename T>
+__device__ __forceinline__ T muscl_slope(int kind, T a, T b) {
+  if (fabs(b) < T(1e-12)) return T(0.0);
+  const T ab = a * b;
+  if (ab <= T(0.0)) return T(0.0);
+  switch (kind) {
+    case LIM_MINMOD: return fabs(a) < fabs(b) ? a : b;
+    case LIM_VANLEER: return T(2.0) * ab / (a + b);
+    case LIM_SUPERBEE: {
+      const T aa = fabs(a), bb = fabs(b);
+      const T m = fmax(fmin(T(2.0) * aa, bb), fmin(aa, T(2.0) * bb));
+      return b > T(0.0) ? m : -m;
+    }
+    case LIM_VANALBADA: {
+      const T a2 = a * a;
+      return b * (a2 + ab) / (a2 + b * b);
+    }
+    default: return T(0.0);
+  }
+}
+
 // Limited slope of one variable on the reference's directional stencil (src/Limiters.cpp:109-134):
 //   S1 = zeta*(q_c - q_N1)/d1 (across the face), S2 = zeta1*(q_N1 - q_N2)/d2 (beyond N1)
 // Reference minmod (src/Limiters.cpp:58-63): 0.5*(sgn S1 + sgn S2)*min(|S1|,|S2|).

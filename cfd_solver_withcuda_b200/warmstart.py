@@ -279,9 +279,10 @@ class Net:
 
     HIDDEN = 64
 
-    def __init__(self, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda"):
+    def __init__(self, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=0):
         torch = _torch()
         W = self.HIDDEN
+        self.engine = engine  # forward blocks: 0 mma.sync, 1 tcgen05 (tensor memory accumulators)
         self.L, self.out, self.device = layers, out, torch.device(device)
         self.dims = {"enc_n": (node_in, W), "enc_e": (edge_in, W), "dec": (W, out)}
         for l in range(layers):
@@ -367,6 +368,7 @@ class Net:
         a.resid = _ptr(resid)
         a.ld_resid = resid.stride(0) if resid is not None else 0
         a.z1, a.y, a.ld_y = _ptr(z1), _ptr(y), y.stride(0)
+        a.engine = self.engine
         cb._check(cb.lib().cfd_mpnn_mlp_forward(ctypes.byref(a), _stream(y)))
 
     def _mlp_back(self, name, dy, z1, rows, dx=None):
@@ -457,10 +459,10 @@ class Net:
                                          lr, betas[0], betas[1], eps, self.steps, _stream(self.flat)))
 
 
-def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda"):
+def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=0):
     """The surrogate (about 187k parameters at width 64, 6 layers)."""
     assert width == Net.HIDDEN
-    return Net(layers=layers, node_in=node_in, edge_in=edge_in, out=out, seed=seed, device=device)
+    return Net(layers=layers, node_in=node_in, edge_in=edge_in, out=out, seed=seed, device=device, engine=engine)
 
 
 def train(model, graph, node_feats, edge_feats, targets, epochs=200, batch=8, lr=1e-3, seed=0, device="cuda"):

@@ -406,8 +406,14 @@ typedef struct {
   float *z1;               /* out (optional): hidden pre-activation [rows][64] */
   float *y;                /* out [rows][ld_y] */
   int ld_y;
+  int engine;              /* 0: mma.sync m16n8k16 (64-row tiles); 1: tcgen05.mma with the accumulators in
+                              tensor memory (128-row tiles, operands in shared memory by matrix
+                              descriptors); the two agree up to the FP32 summation order */
 } cfd_mlp_fwd;
 cfd_status cfd_mpnn_mlp_forward(const cfd_mlp_fwd *a, void *stream);
+/* Status word of the tcgen05 kernels (0, or CFD_ERR_TIMEOUT when a bounded wait ran out); reset = 1
+ * clears it.  Synchronises with the device. */
+cfd_status cfd_mpnn_status(int *status, int reset);
 
 /* Backward data path of one dense block: dz1 = (dy W2) * silu'(z1) and dx = dz1 W1. */
 typedef struct {
