@@ -307,6 +307,8 @@ def run_ramps(args, rank, world):
                                 local_time_stepping=1, cfl=0.8, limiter=lim, muscl=1, integrator=2, inlet_bc=3,
                                 reorder=0, precision=prec)
         b = cb.Batch(meshes, cfg, inflow=inflow)
+        if args.persistent:
+            b.set_option("persistent", 1)  # one persistent kernel per RK stage, a CUDA graph per stage
         b.upload_state(states)
         if world > 1:
             dist.barrier()
@@ -319,12 +321,20 @@ def run_ramps(args, rank, world):
         tt = r["time_to_tol"]
         conv = tt[tt >= 0]
         rr = r["res_ratio"]
+        # Over all instances: an instance that did not reach the tolerance counts at the run's end.
+        tt_all = np.where(tt >= 0, tt, el)
+        st = r["steps_to_tol"]
+        st_all = np.where(st > 0, st, r["steps"])
         results[name] = {"value": cu / el, "seconds": el, "cell_updates": cu, "steps": r["steps"],
                          "limiter": "van_leer" if lim == 2 else "minmod",
                          "converged": int(conv.size), "instances": len(mine),
                          "res_ratio_p50": float(np.percentile(rr, 50)), "res_ratio_max": float(rr.max()),
                          "time_to_tol_p50": float(np.percentile(conv, 50)) if conv.size else None,
                          "time_to_tol_p99": float(np.percentile(conv, 99)) if conv.size else None,
+                         "time_to_tol_p50_all": float(np.percentile(tt_all, 50)),
+                         "time_to_tol_p99_all": float(np.percentile(tt_all, 99)),
+                         "steps_to_tol_p50_all": float(np.percentile(st_all, 50)),
+                         "steps_to_tol_p99_all": float(np.percentile(st_all, 99)),
                          "steps_to_tol_p50": float(np.percentile(r["steps_to_tol"][r["steps_to_tol"] > 0], 50))
                          if conv.size else None}
         b.close()
@@ -334,6 +344,7 @@ def run_ramps(args, rank, world):
                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64", "data": "synthetic (seeded ramp generator, freestream start)",
                "config": {"workload": "batched_ramps_15deg", "instances": args.instances, "seed": args.seed,
+                          "persistent": bool(args.persistent),
                           "tol": args.tol, "max_steps": args.max_steps, "vl_steps": args.vl_steps,
                           "check_every": args.check_every,
                           "total_cells": int(sum(nx * ny for nx, ny, _ in specs)),
@@ -470,6 +481,57 @@ def run_warmstart(args, rank, world):
     print(json.dumps(out))
 
 
+def run_convergence(args, rank, world):
+    """--workload convergence: residual histories of the half-cylinder case (the configured
+    form and the variants of the convergence study) on the full O-grid, or a smaller one with the
+    same radial stretching per cell row (--conv-mesh NTxNR): L2 density residual relative to its
+    first value every --check-every steps up to --max-steps."""
+    import torch
+    import cfd_solver_withcuda_b200 as cb
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    nt, nr = (int(x) for x in args.conv_mesh.split("x"))
+    m = cb.Mesh.half_cylinder(nt, nr, R_BODY, R_OUTER, RATIO ** (NR / nr))
+    NP = m.n_physical
+    rho, p = 1.0, 1.0 / GAMMA
+    u = MACH * np.sqrt(GAMMA * p / rho)
+    U = cb.conserved_from_primitive(np.full(NP, rho), np.full(NP, u), np.zeros(NP), np.full(NP, p))
+    U0 = np.zeros((m.n_total, 4))
+    U0[:NP] = U
+    U0[m.boundary[:, 3]] = U[m.boundary[:, 1]]
+    variants = {
+        "configured_van_leer": {},
+        "reference_inlet_van_leer": {"inlet_bc": 0},
+        "van_albada_entropy_fix": {"limiter": 4, "entropy_fix_linear": 0.4},
+        "minmod_entropy_fix": {"limiter": 1, "entropy_fix_linear": 0.4},
+        "minmod_entropy_fix_shock_fix": {"limiter": 1, "entropy_fix_linear": 0.4, "shock_fix": 0.15},
+    }
+    _, _, kw = workload_state(cb)
+    out = {"metric": "L2 density residual / first value", "unit": "ratio", "higher_is_better": False,
+           "config": {"workload": "half_cylinder_convergence_%dx%d" % (nt, nr), "max_steps": args.max_steps,
+                      "check_every": args.check_every}, "histories": {}}
+    for name, over in variants.items():
+        k = dict(kw)
+        k.update(over)
+        s = cb.Solver(m, cb.default_config(device=local, **k))
+        s.set_option("keep_delu", 0)
+        s.upload_state(U0)
+        r0 = s.step(1).res_l2[0]
+        hist, done = [], 1
+        while done < args.max_steps:
+            n = min(args.check_every, args.max_steps - done)
+            hist.append(s.step(n).res_l2[0] / r0)
+            done += n
+            if hist[-1] <= args.tol:
+                break
+        out["histories"][name] = {"steps": done, "ratio": [float("%.3g" % h) for h in hist],
+                                  "min_ratio": float(min(hist)), "reached_tol": bool(hist[-1] <= args.tol)}
+        s.close()
+    print(json.dumps(out))
+
+
 def _reference_replica(steps, ready, go, out):
     """One single-threaded reference solve of the workload (a spawned process): set-up and one
     untimed step, then `steps` timed pseudo-steps once every replica is ready."""
@@ -571,7 +633,8 @@ def main():
     ap.add_argument("--no-steady", action="store_true", help="skip the time-to-steady leg of the default workload")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--e2e-contexts", type=int, default=3, help="contexts the end-to-end jobs rotate over")
-    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart"])
+    ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart", "convergence"])
+    ap.add_argument("--conv-mesh", default="1024x512", help="--workload convergence: O-grid cells NTxNR")
     ap.add_argument("--ws-nx", type=int, default=64)
     ap.add_argument("--ws-ny", type=int, default=32)
     ap.add_argument("--ws-train", type=int, default=192)
@@ -584,6 +647,7 @@ def main():
     ap.add_argument("--steady-nx", type=int, default=120)
     ap.add_argument("--steady-ny", type=int, default=40)
     ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--persistent", type=int, default=1, help="--workload ramps: 1 = the persistent batched form")
     ap.add_argument("--vl-steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--launch-options", default="auto",
@@ -606,6 +670,8 @@ def main():
         return run_bump(args, rank, world)
     if args.workload == "warmstart":
         return run_warmstart(args, rank, world)
+    if args.workload == "convergence":
+        return run_convergence(args, rank, world)
 
     import torch
     import torch.distributed as dist
