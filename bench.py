@@ -816,11 +816,14 @@ def main():
         f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
         f.set_option("keep_delu", 0)
         f.upload_state(U0)
+        tune_form = f.autotune(steps=10) if name.startswith("reference") else ""
         f.step_async(3)
         f.sync()
         n_timed = min(nform, 50) if name.startswith("reference_roe2") else nform
         fms, _ = timed_steps(f, stream, n_timed, torch)
         forms[name] = {"value": NP * n_timed / (fms * 1e-3), "ms_per_step": fms / n_timed, "steps": n_timed}
+        if tune_form:
+            forms[name]["launch_options"] = [l.split(":")[0] for l in tune_form.splitlines() if "(chosen)" in l]
         f.close()
     # FP32-flux error: both precisions from the same freestream start, same number of steps.
     finals = {}

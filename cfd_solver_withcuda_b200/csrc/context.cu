@@ -1063,7 +1063,11 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   }
   if (n == "keep_delu") ctx->keep_delu = value != 0.0;
   else if (n == "use_graph") ctx->use_graph = value != 0.0;
-  else if (n == "flux_lanes") {
+  else if (n == "flux_minb") {
+    if (value != 1.0 && value != 6.0 && value != 8.0) return fail(CFD_ERR_BAD_ARG, "flux_minb must be 1, 6 or 8");
+    ctx->fp.flux_minb = static_cast<int>(value);
+    drop_graphs(ctx);
+  } else if (n == "flux_lanes") {
     if (value != 1.0 && value != 4.0) return fail(CFD_ERR_BAD_ARG, "flux_lanes must be 1 or 4");
     ctx->fp.lanes = static_cast<int>(value);
   }
@@ -1521,18 +1525,23 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     }
   };
   struct Cand {
-    int faces_shape, fuse, lanes, pdl, patch;
+    int faces_shape, fuse, lanes, pdl, patch, minb;
     double ms;
   };
   std::vector<Cand> cands;
   if (ctx->dm.NF > 0) {
     for (int f = 0; f < 5; f++)
       for (int g = 0; g < 2; g++)
-        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, 0.0});
+        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, 0.0});
     if (ctx->dm.npatch > 0)
-      for (int p = 0; p < 2; p++) cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, 0.0});
+      for (int p = 0; p < 2; p++) cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, ctx->fp.flux_minb, 0.0});
   } else {
-    for (int l : {1, 4}) cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, l, ctx->dm.pdl, 0, 0.0});
+    const bool roe2 = ctx->fp.dissipation == 3 && ctx->fp.second_order && !ctx->fp.weno;
+    for (int mb : {1, 6, 8}) {
+      if (mb != 1 && !roe2) continue;
+      cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 1, ctx->dm.pdl, 0, mb, 0.0});
+    }
+    cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 4, ctx->dm.pdl, 0, 1, 0.0});
   }
   const int prof = ctx->profile, graph_on = ctx->use_graph;
   ctx->profile = 0;
@@ -1548,6 +1557,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     ctx->fp.lanes = cd.lanes;
     ctx->dm.pdl = cd.pdl;
     ctx->patch_stage = cd.patch;
+    ctx->fp.flux_minb = cd.minb;
     drop_graphs(ctx);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_TEND, 0.0);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_DONE, 0.0);
@@ -1578,12 +1588,14 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   ctx->fp.lanes = best->lanes;
   ctx->dm.pdl = best->pdl;
   ctx->patch_stage = best->patch;
+  ctx->fp.flux_minb = best->minb;
   if (report && report_len > 0) {
     std::string r;
     char line[160];
     for (const Cand &cd : cands) {
-      snprintf(line, sizeof(line), "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d patch_stage=%d: %.4f ms/step%s\n",
-               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.patch, cd.ms, &cd == best ? " (chosen)" : "");
+      snprintf(line, sizeof(line),
+               "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d patch_stage=%d flux_minb=%d: %.4f ms/step%s\n",
+               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.patch, cd.minb, cd.ms, &cd == best ? " (chosen)" : "");
       r += line;
     }
     snprintf(report, report_len, "%s", r.c_str());

@@ -581,8 +581,11 @@ __device__ __forceinline__ void min_dt_epilogue(DevState &st, double dt, double 
 
 // Evaluate_Cell_Net_Flux_1O/2O (src/Net_Flux.cpp:46-129) + Evaluate_Time_Step (src/Time_Step.cpp:293-359)
 // fused, one thread per cell: faces in order, Net += avg - diss; then del_t; block min + Min_dt.
-template <int DISS, int ORDER>
-__global__ void __launch_bounds__(kFluxBlock) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
+// MINB: minimum resident blocks per SM the register allocation is made for (1: unconstrained;
+// the second-order Roe form is also built for 6 and 8, which cap its 110 registers at 80 and 64 for
+// more resident warps; the autotuner picks, the results are the same bits).
+template <int DISS, int ORDER, int MINB = 1>
+__global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
   __shared__ double sh[32];
   const int NP = m.NP, NT = m.NT;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -842,11 +845,13 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
   }
   const T aL = sqrt(T(kGamma) * qL[3] / qL[0]), aR = sqrt(T(kGamma) * qR[3] / qR[0]);
   T A[4], D[4] = {T(0.0), T(0.0), T(0.0), T(0.0)};
-  if (DISS == 3) {
+  // DISS 3: Roe; DISS 103: Roe with the options of the form (linear-wave entropy fix, shock-stable
+  // hybrid), a separate instance so that the plain form keeps its register footprint.
+  if (DISS == 3 || DISS == 103) {
     average_flux<T>(qL[0], qL[1], qL[2], qL[3], qR[0], qR[1], qR[2], qR[3], nx, ny, dl, A);
     // Shock sensor of the hybrid: |grad p|^2 |d|^2 > (shock_fix p)^2 in either cell.
     bool rusanov = false;
-    if (shock_fix > T(0.0)) {
+    if (DISS == 103 && shock_fix > T(0.0)) {
       const T d2 = dx * dx + dy * dy;
       const T gpc = gc[6] * gc[6] + gc[7] * gc[7], gpn = gn[6] * gn[6] + gn[7] * gn[7];
       const T tc = shock_fix * qc[3], tn = shock_fix * qn[3];
@@ -863,7 +868,8 @@ __device__ __forceinline__ double4 face_flux_rec(int glim, const double4 c0, con
 #pragma unroll
       for (int k = 0; k < 4; k++) D[k] = T(0.5) * sm * (UR[k] - UL[k]) * dl;
     } else {
-      roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D, eflin);
+      roe_1o<T>(qL[0], qL[1], qL[2], qL[3], aL, qR[0], qR[1], qR[2], qR[3], aR, nx, ny, dl, false, D,
+                DISS == 103 ? eflin : T(0.0));
     }
   } else {
     // Conserved face states for AUSM / HLLC: E = p/(g-1) + rho |V|^2 / 2.
@@ -1948,6 +1954,8 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
     if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 6) k_flux<6, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 7) k_flux<7, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3 && fp.flux_minb == 6) k_flux<3, 2, 6><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3 && fp.flux_minb == 8) k_flux<3, 2, 8><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   } else {
@@ -1973,9 +1981,15 @@ int launch_gather(cudaStream_t s, const DevMesh &m, DevState &st, const FluxPara
   return 1;
 }
 
+// Flux scheme of the face kernels: 3 (Roe) becomes 103 when the Roe options are on.
+__host__ __forceinline__ int face_scheme(const FluxParams &fp) {
+  return fp.dissipation == 3 && (fp.eflin > 0.0 || fp.shock_fix > 0.0) ? 103 : fp.dissipation;
+}
+
 template <typename T, int MINB>
 void launch_faces_b(cudaStream_t s, int g, int b, const DevMesh &m, DevState &st, const FluxParams &fp) {
-  if (fp.dissipation == 6) launch_k(m, k_faces<T, 6, MINB>, g, b, s, m, st, fp);
+  if (face_scheme(fp) == 103) launch_k(m, k_faces<T, 103, MINB>, g, b, s, m, st, fp);
+  else if (fp.dissipation == 6) launch_k(m, k_faces<T, 6, MINB>, g, b, s, m, st, fp);
   else if (fp.dissipation == 7) launch_k(m, k_faces<T, 7, MINB>, g, b, s, m, st, fp);
   else if (fp.dissipation == 8) launch_k(m, k_faces<T, 8, MINB>, g, b, s, m, st, fp);
   else launch_k(m, k_faces<T, 3, MINB>, g, b, s, m, st, fp);
@@ -2037,7 +2051,8 @@ int patch_prepare(const DevMesh &m) {
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
   if (bytes + 4096 > (size_t)optin) return 0;
   const int n = static_cast<int>(bytes);
-  if (cudaFuncSetAttribute(k_patch_stage<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
+  if (cudaFuncSetAttribute(k_patch_stage<103>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
+      cudaFuncSetAttribute(k_patch_stage<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
       cudaFuncSetAttribute(k_patch_stage<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
       cudaFuncSetAttribute(k_patch_stage<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess ||
       cudaFuncSetAttribute(k_patch_stage<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) != cudaSuccess)
@@ -2049,7 +2064,10 @@ int launch_patch_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Flu
                        int kind, int lts, int fuse_final, int keep_delu, int flags, const double *prim_in) {
   const size_t sm = patch_smem_bytes(m);
   const int g = m.npatch;
-  if (fp.dissipation == 6)
+  if (face_scheme(fp) == 103)
+    launch_ks(m, k_patch_stage<103>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
+              prim_in);
+  else if (fp.dissipation == 6)
     launch_ks(m, k_patch_stage<6>, g, kPatchCells, sm, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags,
               prim_in);
   else if (fp.dissipation == 7)
@@ -2103,7 +2121,8 @@ void persistent_kernel_ptr(void (**k)(DevMesh, DevState, FluxParams, BcParams, i
 int persistent_grid(const FluxParams &fp) {
   void (*k)(DevMesh, DevState, FluxParams, BcParams, int, int, int, int, int, int, int, unsigned int) = nullptr;
   const bool f32 = fp.precision == 1;
-  switch (fp.dissipation) {
+  switch (face_scheme(fp)) {
+    case 103: f32 ? persistent_kernel_ptr<float, 103>(&k) : persistent_kernel_ptr<double, 103>(&k); break;
     case 6: f32 ? persistent_kernel_ptr<float, 6>(&k) : persistent_kernel_ptr<double, 6>(&k); break;
     case 7: f32 ? persistent_kernel_ptr<float, 7>(&k) : persistent_kernel_ptr<double, 7>(&k); break;
     case 8: f32 ? persistent_kernel_ptr<float, 8>(&k) : persistent_kernel_ptr<double, 8>(&k); break;
@@ -2122,7 +2141,8 @@ int launch_persistent_stage(cudaStream_t s, const DevMesh &m, DevState &st, cons
                             int with_dt, int with_bc, int grid, unsigned int test_arrivals) {
   void (*k)(DevMesh, DevState, FluxParams, BcParams, int, int, int, int, int, int, int, unsigned int) = nullptr;
   const bool f32 = fp.precision == 1;
-  switch (fp.dissipation) {
+  switch (face_scheme(fp)) {
+    case 103: f32 ? persistent_kernel_ptr<float, 103>(&k) : persistent_kernel_ptr<double, 103>(&k); break;
     case 6: f32 ? persistent_kernel_ptr<float, 6>(&k) : persistent_kernel_ptr<double, 6>(&k); break;
     case 7: f32 ? persistent_kernel_ptr<float, 7>(&k) : persistent_kernel_ptr<double, 7>(&k); break;
     case 8: f32 ? persistent_kernel_ptr<float, 8>(&k) : persistent_kernel_ptr<double, 8>(&k); break;

@@ -202,6 +202,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
  * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0-4, default 3),
  * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1),
+ * "flux_minb" (the one-lane second-order Roe kernel register-capped for 1, 6 or 8 resident blocks per
+ * SM, default 1),
  * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0),
  * "patch_stage" (with reorder 3, the face-based forms with a per-cell dt frozen per step run each
  * stage as one kernel: a thread block per 128-cell patch computes the records, face fluxes, gather

@@ -2,7 +2,8 @@
 memory; cfd_mpnn_mlp_forward with engine = 1) against the mma.sync kernel (engine = 0) and the CPU
 restatement with BF16 operands (oracle/mpnn_ref.py), for every block shape of the network: input
 widths 9, 5, 192, 128 and 64 (gathered and plain segments), outputs 64 and 4, row counts that are
-and are not multiples of the 128-row tile."""
+and are not multiples of the 128-row tile, and more tiles than thread blocks (each block then runs
+several tiles, alternating the phases of its mbarrier)."""
 import ctypes
 
 import numpy as np
@@ -19,7 +20,8 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("block,rows", [("enc_n", 1000), ("enc_e", 4096), ("edge0", 1000), ("edge0", 256),
-                                        ("node0", 777), ("dec", 1000)])
+                                        ("node0", 777), ("dec", 1000), ("edge0", 128 * 700 + 5),
+                                        ("dec", 128 * 900)])
 def test_tcgen05_forward_matches_mma_sync_and_restatement(block, rows):
     import torch
     from oracle import mpnn_ref as R
