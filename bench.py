@@ -55,7 +55,7 @@ def workload_state(cb):
     full[m.boundary[:, 3]] = U[m.boundary[:, 1]]
     kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
               limiter=2, muscl=1, integrator=2, inlet_rho=rho, inlet_p=p, inlet_bc=3, inlet_u=u, inlet_v=0.0,
-              reorder=3)
+              reorder=4)
     return m, full, kw
 
 
@@ -184,6 +184,19 @@ def gradient_bytes_per_cell():
     the sound speed 8, the area 8 and del_t written 8 (244 B).  Neighbour rows are re-reads, and
     the first stage's ghost rows (< 0.1 %) are left out."""
     return (244 + 220 + 244) / 3.0
+
+
+def tile_bytes_per_cell():
+    """Algorithmic DRAM bytes per cell of the tile stage k_tile_stage, averaged over the three
+    TVD-RK3 stages with frozen local dt (halo rows, halo faces and the neighbour tiles' re-reads come
+    from L2 and are not algorithmic).  Every stage reads the cell's (rho, u, v, p) row 32, its slot
+    code 1, 1/area 8, its two structured faces (W and S: normal, length, centre vector 40 and the
+    owner flag 1 each) 82, U^n 32 and the boundary-entry offsets 4, and writes the next stage's row
+    32, the primitive planes 40 and R 32 (263 B); stage 1 adds the sound speed and area 16, del_t and
+    the frozen dt written 16 and the stage state written 32 (327 B); stage 2 the stage state and
+    frozen dt read 40 and the stage state written 32 (335 B); stage 3 the stage state and frozen dt
+    read 40, the sound speed and area 16, del_t written 8 and U written 32 (359 B)."""
+    return (327 + 335 + 359) / 3.0
 
 
 def patch_bytes_per_cell():
@@ -737,6 +750,7 @@ def main():
     bc_ms, bc_n = s.kernel_time("bc")
     gs_ms, gs_n = s.kernel_time("gather_stage")
     pa_ms, pa_n = s.kernel_time("patch")
+    ti_ms, ti_n = s.kernel_time("tile")
     peaks, peak_kind = measured_peaks()
     NF = s.n_faces
 
@@ -766,6 +780,12 @@ def main():
     # Per-kernel rooflines of the chosen launch options; the one with the largest device time per
     # pseudo-step is the line's `roofline`, the others are listed beside it.
     rl = {}
+    if ti_n:
+        rl["k_tile_stage"] = (ti_ms, roofline(
+            "k_tile_stage<double, Roe> (gradients, face fluxes, gather and RK stage update of one 32 x 8 tile "
+            "per block, states of the tile and two rings in shared memory)", ti_ms, ti_n, tile_bytes_per_cell() * NP,
+            "k_tile_stage_traffic.json",
+            fp64_pipe_active_pct=profile_figure("k_tile_stage_traffic.json", "fp64_pipe_active_pct")))
     if pa_n:
         rl["k_patch_stage"] = (pa_ms, roofline(
             "k_patch_stage<Roe> (records, face fluxes, gather and RK stage update of one 128-cell patch per "

@@ -118,6 +118,8 @@ SIGNATURES = {
     "cfd_mesh_write_vtk": (_I, [_P, ctypes.c_char_p]),
     "cfd_mesh_describe": (_I, [_P, ctypes.POINTER(MeshDesc)]),
     "cfd_mesh_centers": (_I, [_P, _DP]),
+    "cfd_mesh_block_order": (_I, [ctypes.POINTER(MeshDesc), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                  ctypes.POINTER(_I)]),
     "cfd_mesh_points": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_DP)]),
     "cfd_mesh_destroy": (None, [_P]),
     "cfd_config_default": (None, [ctypes.POINTER(Config)]),
@@ -265,6 +267,16 @@ class Mesh:
 
     def write_vtk(self, path):
         _check(lib().cfd_mesh_write_vtk(self._h, path.encode()))
+
+    def block_order(self):
+        """(ni, nj, lh, cells) of the structured-block numbering (reorder 4): cells[j * ni + i] is
+        the mesh cell at (i, j).  Raises CfdError (CFD_ERR_MESH) when the mesh is not a single
+        structured block of quads."""
+        ni, nj, lh = _I(), _I(), _I()
+        cells = np.zeros(self.n_physical, np.int32)
+        _check(lib().cfd_mesh_block_order(ctypes.byref(self.desc), ctypes.byref(ni), ctypes.byref(nj), ctypes.byref(lh),
+                                          cells.ctypes.data_as(ctypes.POINTER(_I))))
+        return ni.value, nj.value, lh.value, cells
 
     def points(self):
         n = ctypes.c_int()

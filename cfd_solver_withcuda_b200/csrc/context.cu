@@ -170,6 +170,130 @@ void rcb_patches(int NP, const int *nf, const int *nbr, const double *cvec, int 
   }
 }
 
+// Structured-block numbering (reorder 4): recognises a mesh that is one block of ni x nj quads
+// (every cell a quad, one corner cell with ghosts on two adjacent faces, straight lines of faces
+// from it) and numbers its cells c = j * ni + i.  Walking from a cell c through face slot s to its
+// neighbour n continues straight through the slot opposite the one of n that faces c (slot + 2:
+// the four faces of a quad are stored in order around it).  The i direction is the one whose
+// length is a multiple of the tile width if only one is, else the longer one.  Per cell the slot
+// of +i (E) and +j (N); lh = 1 when the slot after E is S (clockwise slot order in (i, j)).
+struct BlockOrder {
+  int ni = 0, nj = 0, lh = 0;
+  std::vector<int> cell;     // [nj * ni] reference cell of (i, j)
+  std::vector<int> sE, sN;   // per reference cell: slot of its +i and +j faces
+};
+
+bool structured_block(int NP, const int *nf, const int *nbr, BlockOrder &b, std::string &why) {
+  auto phys = [&](int n) { return n >= 0 && n < NP; };
+  auto back = [&](int n, int c) {
+    for (int k = 0; k < 4; k++)
+      if (nbr[4 * n + k] == c) return k;
+    return -1;
+  };
+  for (int c = 0; c < NP; c++)
+    if (nf[c] != 4) {
+      why = "cell " + std::to_string(c) + " is not a quad";
+      return false;
+    }
+  int c0 = -1, fa = -1, fb = -1;
+  for (int c = 0; c < NP && c0 < 0; c++)
+    for (int f = 0; f < 4; f++)
+      if (!phys(nbr[4 * c + f]) && !phys(nbr[4 * c + ((f + 1) & 3)]) && phys(nbr[4 * c + ((f + 2) & 3)]) &&
+          phys(nbr[4 * c + ((f + 3) & 3)])) {
+        c0 = c;
+        fa = (f + 2) & 3;
+        fb = (f + 3) & 3;
+        break;
+      }
+  if (c0 < 0) {
+    why = "no corner cell (a cell with ghosts on two adjacent faces)";
+    return false;
+  }
+  auto walk = [&](int c, int s) {
+    int len = 1;
+    while (len <= NP) {
+      const int n = nbr[4 * c + s];
+      if (!phys(n)) return len;
+      const int g = back(n, c);
+      if (g < 0) return -1;
+      s = (g + 2) & 3;
+      c = n;
+      len++;
+    }
+    return -1;
+  };
+  const int la = walk(c0, fa), lb = walk(c0, fb);
+  if (la < 2 || lb < 2) {
+    why = "the block is thinner than two cells";
+    return false;
+  }
+  const bool a32 = la % 32 == 0, b32 = lb % 32 == 0;
+  const bool a_is_i = (a32 != b32) ? a32 : la >= lb;
+  b.ni = a_is_i ? la : lb;
+  b.nj = a_is_i ? lb : la;
+  const int si = a_is_i ? fa : fb, sj = a_is_i ? fb : fa;
+  if ((long long)b.ni * b.nj != NP) {
+    why = "the lines from the corner cell span " + std::to_string(b.ni) + " x " + std::to_string(b.nj) + " cells, not " +
+          std::to_string(NP);
+    return false;
+  }
+  const int h = (si - sj) & 3;  // slot(E) - slot(N)
+  b.lh = h == 1;
+  b.cell.assign((size_t)NP, -1);
+  b.sE.assign(NP, -1);
+  b.sN.assign(NP, -1);
+  int rowc = c0, rows = sj;
+  for (int j = 0; j < b.nj; j++) {
+    if (j > 0) {
+      const int n = nbr[4 * rowc + rows];
+      const int g = phys(n) ? back(n, rowc) : -1;
+      if (g < 0) {
+        why = "column walk leaves the block at row " + std::to_string(j);
+        return false;
+      }
+      rows = (g + 2) & 3;
+      rowc = n;
+    }
+    int c = rowc, se = (rows + h) & 3;
+    for (int i = 0; i < b.ni; i++) {
+      if (i > 0) {
+        const int n = nbr[4 * c + se];
+        const int g = phys(n) ? back(n, c) : -1;
+        if (g < 0) {
+          why = "row walk leaves the block at (" + std::to_string(i) + ", " + std::to_string(j) + ")";
+          return false;
+        }
+        se = (g + 2) & 3;
+        c = n;
+      }
+      if (b.sE[c] >= 0) {
+        why = "cell " + std::to_string(c) + " is reached twice";
+        return false;
+      }
+      b.cell[(size_t)j * b.ni + i] = c;
+      b.sE[c] = se;
+      b.sN[c] = (se - h) & 3;
+    }
+  }
+  // Every neighbour relation must be the block's: (i +- 1, j), (i, j +- 1), or a ghost on the rim.
+  for (int j = 0; j < b.nj; j++)
+    for (int i = 0; i < b.ni; i++) {
+      const int c = b.cell[(size_t)j * b.ni + i];
+      const int want[4] = {i + 1 < b.ni ? b.cell[(size_t)j * b.ni + i + 1] : -1,
+                           j + 1 < b.nj ? b.cell[(size_t)(j + 1) * b.ni + i] : -1,
+                           i > 0 ? b.cell[(size_t)j * b.ni + i - 1] : -1, j > 0 ? b.cell[(size_t)(j - 1) * b.ni + i] : -1};
+      const int slot[4] = {b.sE[c], b.sN[c], (b.sE[c] + 2) & 3, (b.sN[c] + 2) & 3};
+      for (int q = 0; q < 4; q++) {
+        const int n = nbr[4 * c + slot[q]];
+        if (want[q] >= 0 ? n != want[q] : phys(n)) {
+          why = "cell (" + std::to_string(i) + ", " + std::to_string(j) + ") does not neighbour the block's cells";
+          return false;
+        }
+      }
+    }
+  return true;
+}
+
 template <typename T>
 cfd_status dev_upload(T **dst, const std::vector<T> &v) {
   CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), std::max<size_t>(1, v.size()) * sizeof(T)));
@@ -220,6 +344,13 @@ struct cfd_ctx {
   int n_stage_graphs = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
   int *d_perm = nullptr;    // device copy of perm
+  // Tile form (reorder 4 on a structured block, option "tile_stage"): the block tables and the two
+  // further (rho, u, v, p) row buffers the stages of a step rotate through (st.q4 -> qbuf[0] ->
+  // qbuf[1] -> st.q4).
+  TileMesh tm{};
+  bool tile_ok = false;
+  int tile_stage = 0;
+  double4 *qbuf[2] = {nullptr, nullptr};
   // Per-kernel timing (option "profile"): event pairs recorded around each launch on the
   // context's stream, resolved lazily by cfd_kernel_time.
   int profile = 0;
@@ -228,8 +359,8 @@ struct cfd_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Timed> timed;
-  double kind_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  long long kind_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double kind_ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  long long kind_n[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   double *d_stage = nullptr;  // [NT*4] reference-order AoS staging rows
   void *d_amr = nullptr;      // AMR indicator, tags and selection scratch (allocated on first use)
   int2 *d_tables = nullptr;   // work lists of batched solves (cells, faces, entries, records)
@@ -255,7 +386,7 @@ cfd_status ctx_upload(cfd_ctx *ctx, T **dst, const std::vector<T> &v) {
 int dev_of(const cfd_ctx *ctx, int ref) { return ref < ctx->NP ? ctx->inv[ref] : ref; }
 
 enum { TK_FLUX = 0, TK_STAGE = 1, TK_BC = 2, TK_GRAD = 3, TK_FACES = 4, TK_GATHER_STAGE = 5, TK_PATCH = 6, TK_PERSIST = 7,
-       TK_N = 8 };
+       TK_TILE = 8, TK_N = 9 };
 
 struct TimedScope {
   cfd_ctx *ctx;
@@ -326,18 +457,36 @@ int enqueue_stage(cfd_ctx *ctx, int k, bool fuse_final, bool &ghosts_written) {
   const bool patch = faces && ctx->patch_stage && m.npatch > 0 && !m.cblk && !m.fblk && fuse_final &&
                      ctx->fp.precision == CFD_PREC_FP64 && !ctx->fp.weno && p.kind0 != 0 && p.lts_mode == 1 &&
                      c.local_time_stepping;
+  // Tile form: one kernel per stage on a structured block; the three stages rotate the
+  // (rho, u, v, p) rows through st.q4 -> qbuf[0] -> qbuf[1] -> st.q4 (each stage writes a buffer
+  // that no block of it reads), and the step's boundary conditions come from launch_bc.
+  const bool tile = faces && ctx->tile_ok && ctx->tile_stage && !m.cblk && !m.fblk && fuse_final && !ctx->fp.weno &&
+                    p.n == 3 && p.kind0 != 0 && p.lts_mode == 1 && c.local_time_stepping;
   const int kind = p.kind0 == 0 ? 0 : p.kind0 + k;
   const int lts = stage_lts(p, c, k);
   const int fin = (k == p.n - 1) ? fuse_final : 0;
   // Fused face-based stages take the first stage's boundary conditions into the gradient pass
   // (each cell applies its own entries before its gradient) when no ghost is shared.
   const bool fused_faces = faces && ctx->fuse_gather && (lts == 1 || lts == 2);
-  const bool bc_in_grad = fused_faces && !patch && k == 0 && ctx->ghost_private;
+  const bool bc_in_grad = fused_faces && !patch && !tile && k == 0 && ctx->ghost_private;
   if (!ghosts_written && !bc_in_grad) {
     TimedScope ts(ctx, TK_BC);
     n += launch_bc(s, m, st, ctx->bp, k > 0 && p.src_S, k > 0);
   }
   ghosts_written = false;
+  if (tile) {
+    TimedScope ts(ctx, TK_TILE);
+    const bool bc_next = k < p.n - 1;
+    const int flags = (bc_next ? 2 : 0) | (p.src_S ? 4 : 0);
+    double4 *bufs[3] = {st.q4, ctx->qbuf[0], ctx->qbuf[1]};
+    DevState sk = st;
+    sk.q4 = bufs[(k + 1) % 3];
+    const bool with_dt = k == 0 || k == p.n - 1;
+    n += launch_tile_stage(s, m, sk, ctx->fp, ctx->bp, ctx->tm, bufs[k], kind, lts, fin, ctx->keep_delu, flags,
+                           with_dt ? 1 : 0);
+    ghosts_written = bc_next;
+    return n;
+  }
   if (patch) {
     TimedScope ts(ctx, TK_PATCH);
     const bool bc_next = k < p.n - 1;
@@ -444,6 +593,20 @@ static cfd_status finish_mesh(cfd_mesh *h, const std::string &gen_err, cfd_mesh 
     return fail(CFD_ERR_MESH, e);
   }
   *out = h;
+  return CFD_OK;
+}
+
+cfd_status cfd_mesh_block_order(const cfd_mesh_desc *d, int *ni, int *nj, int *lh, int *cells) {
+  if (!d || !ni || !nj || !lh || !d->n_faces || !d->neighbours || d->n_physical <= 0)
+    return fail(CFD_ERR_BAD_ARG, "bad argument");
+  BlockOrder b;
+  std::string why;
+  if (!structured_block(d->n_physical, d->n_faces, d->neighbours, b, why))
+    return fail(CFD_ERR_MESH, "not a single structured block of quads: " + why);
+  *ni = b.ni;
+  *nj = b.nj;
+  *lh = b.lh;
+  if (cells) std::copy(b.cell.begin(), b.cell.end(), cells);
   return CFD_OK;
 }
 
@@ -600,7 +763,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     return fail(CFD_ERR_BAD_ARG, "entropy_fix_linear must be a finite value >= 0");
   if (!(cfg->shock_fix >= 0.0) || !std::isfinite(cfg->shock_fix))
     return fail(CFD_ERR_BAD_ARG, "shock_fix must be a finite value >= 0");
-  if (cfg->reorder < 0 || cfg->reorder > 3) return fail(CFD_ERR_BAD_ARG, "reorder must be 0, 1, 2 or 3");
+  if (cfg->reorder < 0 || cfg->reorder > 4) return fail(CFD_ERR_BAD_ARG, "reorder must be 0, 1, 2, 3 or 4");
   if (cfg->inlet_bc < 0 || cfg->inlet_bc > CFD_INLET_FARFIELD || cfg->exit_bc < 0 || cfg->exit_bc > CFD_EXIT_FIXED_P_REF)
     return fail(CFD_ERR_BAD_ARG, "bad boundary-condition kind");
   if (cfg->precision != CFD_PREC_FP64 && !(cfg->precision == CFD_PREC_FP32_FLUX && cfg->muscl && cfg->is_second_order))
@@ -632,7 +795,13 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     return bail(fail(CFD_ERR_CUDA, "pinned allocation failed"));
 
   // Renumbering (reverse Cuthill-McKee over physical cells; ghosts keep their ids).
-  if (cfg->reorder == 3 && d->center_vectors)
+  BlockOrder blk;
+  if (cfg->reorder == 4) {
+    std::string why;
+    if (!structured_block(NP, d->n_faces, d->neighbours, blk, why))
+      return bail(fail(CFD_ERR_MESH, "reorder 4 needs a single structured block of quads: " + why));
+    ctx->perm = blk.cell;
+  } else if (cfg->reorder == 3 && d->center_vectors)
     rcb_patches(NP, d->n_faces, d->neighbours, d->center_vectors, kPatchCells, ctx->perm, ctx->patch_starts);
   else if (cfg->reorder == 2) ctx->perm = patch_from_arrays(NP, d->n_faces, d->neighbours, 128);
   else if (cfg->reorder) ctx->perm = rcm_from_arrays(NP, d->n_faces, d->neighbours);
@@ -752,6 +921,79 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
         cface[(size_t)f * NP + i] = e >= 0 ? pos[e] : -(pos[-e - 1] + 1);
       }
     }
+  }
+  // Tile tables (reorder 4, face-based forms): per cell its slot rotation and the faces it owns,
+  // the two structured face families with their unique-face values, and the ghost rows beside the
+  // block's rim.  The form is offered only when every slot normal and length of a cell equals its
+  // face's owner-side values (negated normal on the non-owner side) bit for bit, which is what the
+  // kernel relies on when it forms the gradients from the face values.
+  std::vector<int> tgW, tgE, tgS, tgN;
+  std::vector<unsigned char> tcode, two, tso;
+  std::vector<double4> tfw, tfs;
+  std::vector<double> twdy, tsdy;
+  bool tile_tables = false;
+  if (cfg->reorder == 4 && !fo.empty()) {
+    const int ni = blk.ni, nj = blk.nj;
+    bool ok = true;
+    tcode.assign(NP, 0);
+    tfw.assign((size_t)(ni + 1) * nj, make_double4(0, 0, 0, 0));
+    twdy.assign((size_t)(ni + 1) * nj, 0.0);
+    two.assign((size_t)(ni + 1) * nj, 0);
+    tfs.assign((size_t)ni * (nj + 1), make_double4(0, 0, 0, 0));
+    tsdy.assign((size_t)ni * (nj + 1), 0.0);
+    tso.assign((size_t)ni * (nj + 1), 0);
+    tgW.assign(nj, 0);
+    tgE.assign(nj, 0);
+    tgS.assign(ni, 0);
+    tgN.assign(ni, 0);
+    // Face of slot s of device cell i: its id, whether the cell owns it, and the exactness check.
+    auto face_of = [&](int i, int s, int &id) {
+      const int e = cface[(size_t)s * NP + i];
+      id = e >= 0 ? e : -e - 1;
+      const size_t idx = (size_t)s * NP + i;
+      const bool own = e >= 0;
+      if (!(nx[idx] == (own ? fnx[id] : -fnx[id]) && ny[idx] == (own ? fny[id] : -fny[id]) && dl[idx] == fdl[id]))
+        ok = false;
+      return own;
+    };
+    for (int j = 0; j < nj && ok; j++)
+      for (int i = 0; i < ni && ok; i++) {
+        const int c = j * ni + i, r = ctx->perm[c];
+        const int sE = blk.sE[r], sN = blk.sN[r], sW = (sE + 2) & 3, sS = (sN + 2) & 3;
+        // Position p (E, N, W, S; E, S, W, N when lh) is slot (sE + p) & 3.
+        unsigned char code = static_cast<unsigned char>((4 - sE) & 3);
+        for (int p = 0; p < 4; p++) {
+          int id;
+          if (face_of(c, (sE + p) & 3, id)) code |= static_cast<unsigned char>(1u << (2 + p));
+        }
+        tcode[c] = code;
+        int id;
+        const size_t wi = (size_t)j * (ni + 1) + i;
+        two[wi] = face_of(c, sW, id) ? 1 : 0;
+        tfw[wi] = make_double4(fnx[id], fny[id], fdl[id], fdx[id]);
+        twdy[wi] = fdy[id];
+        if (i == ni - 1) {
+          if (!face_of(c, sE, id)) ok = false;  // a boundary face belongs to its cell
+          tfw[wi + 1] = make_double4(fnx[id], fny[id], fdl[id], fdx[id]);
+          twdy[wi + 1] = fdy[id];
+          two[wi + 1] = 0;
+        }
+        const size_t si = (size_t)j * ni + i;
+        tso[si] = face_of(c, sS, id) ? 1 : 0;
+        tfs[si] = make_double4(fnx[id], fny[id], fdl[id], fdx[id]);
+        tsdy[si] = fdy[id];
+        if (j == nj - 1) {
+          if (!face_of(c, sN, id)) ok = false;
+          tfs[si + ni] = make_double4(fnx[id], fny[id], fdl[id], fdx[id]);
+          tsdy[si + ni] = fdy[id];
+          tso[si + ni] = 0;
+        }
+        if (i == 0) tgW[j] = nbr[(size_t)sW * NP + c];
+        if (i == ni - 1) tgE[j] = nbr[(size_t)sE * NP + c];
+        if (j == 0) tgS[i] = nbr[(size_t)sS * NP + c];
+        if (j == nj - 1) tgN[i] = nbr[(size_t)sN * NP + c];
+      }
+    tile_tables = ok;
   }
   // Patch tables of the one-kernel stage form (reorder 3): per patch its halo cells and the faces
   // touching its cells, each with the shared-memory rows of its two cells and the face slots they
@@ -911,6 +1153,26 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
   }
 
   m.wave_blocks = gather_stage_wave_blocks();
+  if (tile_tables && tile_prepare()) {
+    TileMesh &tm = ctx->tm;
+    tm.ni = blk.ni;
+    tm.nj = blk.nj;
+    tm.lh = blk.lh;
+    tm.tiles_i = (blk.ni + kTileCellsX - 1) / kTileCellsX;
+    tm.tiles_j = (blk.nj + kTileCellsY - 1) / kTileCellsY;
+    if ((s = ctx_upload(ctx, const_cast<int **>(&tm.gW), tgW)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&tm.gE), tgE)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&tm.gS), tgS)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<int **>(&tm.gN), tgN)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<unsigned char **>(&tm.code), tcode)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double4 **>(&tm.fw), tfw)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&tm.fwdy), twdy)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<unsigned char **>(&tm.fwo), two)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double4 **>(&tm.fs), tfs)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&tm.fsdy), tsdy)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<unsigned char **>(&tm.fso), tso)) != CFD_OK) return bail(s);
+    ctx->tile_ok = true;
+  }
   if (!patches.empty()) {
     m.npatch = static_cast<int>(patches.size());
     m.patch_rows = patch_rows;
@@ -926,7 +1188,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
 
   DevState &st = ctx->ds;
   const size_t dsz = sizeof(double);
-  const int nblk = std::max(flux_block_count(NP), m.npatch);
+  const int nblk = std::max(std::max(flux_block_count(NP), m.npatch), ctx->tile_ok ? ctx->tm.tiles_i * ctx->tm.tiles_j : 0);
   ctx->partial_blocks = nblk;
   if ((s = ctx_alloc(ctx, (void **)&st.U, 4 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
   if ((s = ctx_alloc(ctx, (void **)&st.S, 4 * (size_t)NP * dsz)) != CFD_OK) return bail(s);
@@ -978,6 +1240,12 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     }
     cudaGetLastError();
   }
+  for (int q = 0; q < 2 && ctx->tile_ok; q++) {
+    if ((s = ctx_alloc(ctx, (void **)&ctx->qbuf[q], (size_t)NT * sizeof(double4))) != CFD_OK) return bail(s);
+    if (cudaMemset(ctx->qbuf[q], 0, (size_t)NT * sizeof(double4)) != cudaSuccess)
+      return bail(fail(CFD_ERR_CUDA, "memset failed"));
+  }
+  ctx->tile_stage = ctx->tile_ok ? 1 : 0;
   for (int q = 0; q < 2 && m.npatch > 0; q++) {
     if ((s = ctx_alloc(ctx, (void **)&ctx->pbuf[q], 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
     if (cudaMemset(ctx->pbuf[q], 0, 5 * (size_t)NT * dsz) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
@@ -1080,6 +1348,11 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "profile") ctx->profile = value != 0.0;
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
   else if (n == "patch_stage") ctx->patch_stage = value != 0.0;
+  else if (n == "tile_stage") {
+    if (value != 0.0 && !ctx->tile_ok)
+      return fail(CFD_ERR_BAD_ARG, "the tile form needs reorder 4 on a structured block with the gradient-MUSCL scheme");
+    ctx->tile_stage = value != 0.0;
+  }
   else if (n == "l2_persist") ctx->dm.l2_bytes = value != 0.0 ? ctx->l2_window : 0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   drop_graphs(ctx);
@@ -1525,23 +1798,27 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     }
   };
   struct Cand {
-    int faces_shape, fuse, lanes, pdl, patch, minb;
+    int faces_shape, fuse, lanes, pdl, patch, minb, tile;
     double ms;
   };
   std::vector<Cand> cands;
   if (ctx->dm.NF > 0) {
     for (int f = 0; f < 5; f++)
       for (int g = 0; g < 2; g++)
-        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, 0.0});
+        for (int p = 0; p < 2; p++) cands.push_back({f, g, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, 0, 0.0});
     if (ctx->dm.npatch > 0)
-      for (int p = 0; p < 2; p++) cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, ctx->fp.flux_minb, 0.0});
+      for (int p = 0; p < 2; p++)
+        cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, ctx->fp.flux_minb, 0, 0.0});
+    if (ctx->tile_ok)
+      for (int p = 0; p < 2; p++)
+        cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, 1, 0.0});
   } else {
     const bool roe2 = ctx->fp.dissipation == 3 && ctx->fp.second_order && !ctx->fp.weno;
     for (int mb : {1, 6, 8}) {
       if (mb != 1 && !roe2) continue;
-      cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 1, ctx->dm.pdl, 0, mb, 0.0});
+      cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 1, ctx->dm.pdl, 0, mb, 0, 0.0});
     }
-    cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 4, ctx->dm.pdl, 0, 1, 0.0});
+    cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 4, ctx->dm.pdl, 0, 1, 0, 0.0});
   }
   const int prof = ctx->profile, graph_on = ctx->use_graph;
   ctx->profile = 0;
@@ -1558,6 +1835,7 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
     ctx->dm.pdl = cd.pdl;
     ctx->patch_stage = cd.patch;
     ctx->fp.flux_minb = cd.minb;
+    ctx->tile_stage = cd.tile;
     drop_graphs(ctx);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_TEND, 0.0);
     ctx->launches += launch_set_ctl(ctx->stream, st, CTL_DONE, 0.0);
@@ -1589,13 +1867,15 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
   ctx->dm.pdl = best->pdl;
   ctx->patch_stage = best->patch;
   ctx->fp.flux_minb = best->minb;
+  ctx->tile_stage = best->tile;
   if (report && report_len > 0) {
     std::string r;
     char line[160];
     for (const Cand &cd : cands) {
       snprintf(line, sizeof(line),
-               "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d patch_stage=%d flux_minb=%d: %.4f ms/step%s\n",
-               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.patch, cd.minb, cd.ms, &cd == best ? " (chosen)" : "");
+               "faces_shape=%d fuse_gather=%d flux_lanes=%d pdl=%d patch_stage=%d flux_minb=%d tile_stage=%d: %.4f "
+               "ms/step%s\n",
+               cd.faces_shape, cd.fuse, cd.lanes, cd.pdl, cd.patch, cd.minb, cd.tile, cd.ms, &cd == best ? " (chosen)" : "");
       r += line;
     }
     snprintf(report, report_len, "%s", r.c_str());
@@ -1667,7 +1947,8 @@ cfd_status cfd_kernel_time(cfd_ctx *ctx, const char *kernel, double *total_ms, l
   std::string k(kernel);
   int kind = k == "flux" ? TK_FLUX : k == "stage" ? TK_STAGE : k == "bc" ? TK_BC : k == "gradients" ? TK_GRAD
            : k == "faces" ? TK_FACES : k == "gather_stage" ? TK_GATHER_STAGE : k == "patch" ? TK_PATCH
-           : k == "persistent" ? TK_PERSIST : -1;
+           : k == "persistent" ? TK_PERSIST
+           : k == "tile" ? TK_TILE : -1;
   if (kind < 0) return fail(CFD_ERR_BAD_ARG, "unknown kernel " + k);
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   for (auto &t : ctx->timed) {

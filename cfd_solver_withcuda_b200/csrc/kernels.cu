@@ -1722,6 +1722,284 @@ __global__ void __launch_bounds__(kPatchCells, 5) k_patch_stage(DevMesh m, DevSt
   if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
 
+// ---- Tile form of one stage on a structured block (no reference counterpart) ----
+// One thread block per tile of kTileX x kTileY cells does the work of k_muscl_gradients, k_faces
+// and k_gather_stage for its cells with everything between them in shared memory:
+//   0. the (rho, u, v, p) rows of the tile and of two rings of cells around it (ghost rows
+//      beside the block's boundary) from q_in, one coalesced pass per row of the region;
+//   1. gradients of the tile's cells and of the halo cells along its four sides (the cells across
+//      its boundary faces), del_t of its own cells;
+//   2. the flux of every W and S face of its cells, each from its owner's side (a face on the
+//      tile boundary is evaluated by both tiles from the same inputs, so both get the same bits);
+//   3. per own cell the four fluxes summed in slot order and the stage update (stage_cell), which
+//      writes the stage's rows and the next stage's ghost rows to st.q4 (not q_in: other tiles
+//      are still reading their halo rows from it).
+// Every operation on a value is the one the three-kernel form does, in the same order: the
+// gradient terms and the face fluxes are formed per position around the cell and summed in the
+// cell's slot order; a slot normal is the owner-side normal negated exactly on the non-owner side
+// (checked on the host before the form is offered).
+constexpr int kTileX = kTileCellsX;
+constexpr int kTileY = kTileCellsY;
+constexpr int kTileQW = kTileX + 4, kTileQH = kTileY + 4;  // state region: tile + 2 rings
+constexpr int kTileRW = kTileX + 2, kTileRH = kTileY + 2;  // gradient region: tile + 1 ring
+constexpr int kTileNW = (kTileX + 1) * kTileY;              // W faces of the tile
+constexpr int kTileNS = kTileX * (kTileY + 1);              // S faces of the tile
+
+template <typename T>
+struct TileRecT {
+  typedef double4 type;
+};
+template <>
+struct TileRecT<float> {
+  typedef float4 type;
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t tile_smem_bytes() {
+  return sizeof(double4) * (size_t)(kTileQW * kTileQH + kTileNW + kTileNS) +
+         2 * sizeof(typename TileRecT<T>::type) * (size_t)(kTileRW * kTileRH);
+}
+
+// acc[k] += t[(R + f) & 3][k] for f = 0..3: position terms summed in the cell's slot order.
+template <int R, int K>
+__device__ __forceinline__ void rot_sum(const double (&t)[4][K], double (&acc)[K]) {
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] += t[(R + f) & 3][k];
+  }
+}
+template <int K>
+__device__ __forceinline__ void slot_order_sum(int r, const double (&t)[4][K], double (&acc)[K]) {
+  switch (r) {
+    case 0: rot_sum<0, K>(t, acc); break;
+    case 1: rot_sum<1, K>(t, acc); break;
+    case 2: rot_sum<2, K>(t, acc); break;
+    default: rot_sum<3, K>(t, acc); break;
+  }
+}
+
+// Shared-memory offsets of the four neighbours and the face-table indices of the four faces of
+// cell (i, j) at positions E, N, W, S (N and S exchanged when lh).
+struct TilePos {
+  int dq[4];
+  int face[4];  // W-family index (positions 0, 2) or S-family index (1, 3)
+};
+__device__ __forceinline__ TilePos tile_pos(const TileMesh &tm, int i, int j) {
+  TilePos t;
+  const int wi = j * (tm.ni + 1) + i, si = j * tm.ni + i;
+  t.dq[0] = 1;
+  t.dq[2] = -1;
+  t.face[0] = wi + 1;
+  t.face[2] = wi;
+  const int up = tm.lh ? 3 : 1, dn = tm.lh ? 1 : 3;
+  t.dq[up] = kTileQW;
+  t.dq[dn] = -kTileQW;
+  t.face[up] = si + tm.ni;
+  t.face[dn] = si;
+  return t;
+}
+
+// Gradients of physical cell c = (i, j), row qi of the state region, as cell_gradients<DT> forms
+// them; with DT also the del_t denominator.
+__device__ __forceinline__ void tile_gradients(const DevMesh &m, const DevState &st, const TileMesh &tm,
+                                               const double4 *sq, int qi, int c, int i, int j, bool dt, double g[8],
+                                               double &den) {
+  const unsigned code = tm.code[c];
+  const double ia = m.inv_area[c];
+  const double ac = dt ? st.prim[4 * m.NT + c] : 0.0;
+  const TilePos tp = tile_pos(tm, i, j);
+  const double4 qv = sq[qi];
+  const double qc[4] = {qv.x, qv.y, qv.z, qv.w};
+  double t[4][9];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const double4 fg = (p & 1) ? tm.fs[tp.face[p]] : tm.fw[tp.face[p]];
+    const double4 qn = sq[qi + tp.dq[p]];
+    const bool own = (code >> (2 + p)) & 1u;
+    const double nxf = own ? fg.x : -fg.x, nyf = own ? fg.y : -fg.y, dlf = fg.z;
+    const double wx = nxf * dlf, wy = nyf * dlf;
+    const double qnv[4] = {qn.x, qn.y, qn.z, qn.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double qf = 0.5 * (qc[k] + qnv[k]);
+      t[p][2 * k] = qf * wx;
+      t[p][2 * k + 1] = qf * wy;
+    }
+    const double vnf = qc[1] * nxf + qc[2] * nyf;
+    t[p][8] = (fabs(vnf) + ac) * dlf;
+  }
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  slot_order_sum<9>(code & 3u, t, acc);
+#pragma unroll
+  for (int k = 0; k < 8; k++) g[k] = acc[k] * ia;
+  den = acc[8];
+}
+
+template <typename T, int DISS>
+__global__ void __launch_bounds__(kTileX * kTileY, 2)
+    k_tile_stage(DevMesh m, DevState st, FluxParams fp, BcParams bp, TileMesh tm, const double4 *__restrict__ q_in,
+                 int kind, int lts, int fuse_final, int keep_delu, int flags, int with_dt) {
+  typedef typename TileRecT<T>::type RecV;
+  pdl_enter();
+  if (step_done(st.ctl)) return;
+  extern __shared__ double4 tsm[];
+  double4 *sq = tsm;                                           // [QH][QW]
+  double4 *sF = sq + kTileQW * kTileQH;                        // W faces [TY][TX + 1], then S faces [TY + 1][TX]
+  RecV *srec = reinterpret_cast<RecV *>(sF + kTileNW + kTileNS);  // [RH][RW] x 2
+  const int ni = tm.ni, nj = tm.nj, tid = threadIdx.x;
+  const int i0 = (blockIdx.x % tm.tiles_i) * kTileX, j0 = (blockIdx.x / tm.tiles_i) * kTileY;
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+
+  // 0. States of the region (corners of the outer rings beyond the block are never read).
+  for (int t = tid; t < kTileQW * kTileQH; t += blockDim.x) {
+    const int jj = t / kTileQW, ii = t - jj * kTileQW;
+    const int i = i0 + ii - 2, j = j0 + jj - 2;
+    const bool in_i = i >= 0 && i < ni, in_j = j >= 0 && j < nj;
+    int r = -1;
+    if (in_i && in_j) r = j * ni + i;
+    else if (in_j && i == -1) r = tm.gW[j];
+    else if (in_j && i == ni) r = tm.gE[j];
+    else if (in_i && j == -1) r = tm.gS[i];
+    else if (in_i && j == nj) r = tm.gN[i];
+    sq[t] = r >= 0 ? q_in[r] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  __syncthreads();
+
+  // 1. Gradients: own cells (thread tid has cell tid), then the halo strips W, E, S, N.
+  double dtc = 0.0;
+  constexpr int NG = kTileX * kTileY + 2 * kTileY + 2 * kTileX;
+  for (int t = tid; t < NG; t += blockDim.x) {
+    int gi, gj;
+    if (t < kTileX * kTileY) {
+      gi = t % kTileX;
+      gj = t / kTileX;
+    } else {
+      const int u = t - kTileX * kTileY;
+      if (u < kTileY) {
+        gi = -1;
+        gj = u;
+      } else if (u < 2 * kTileY) {
+        gi = kTileX;
+        gj = u - kTileY;
+      } else if (u < 2 * kTileY + kTileX) {
+        gi = u - 2 * kTileY;
+        gj = -1;
+      } else {
+        gi = u - 2 * kTileY - kTileX;
+        gj = kTileY;
+      }
+    }
+    const int i = i0 + gi, j = j0 + gj;
+    if (i < 0 || i >= ni || j < 0 || j >= nj) continue;
+    const int c = j * ni + i;
+    const bool own = t < kTileX * kTileY;
+    double g[8], den;
+    tile_gradients(m, st, tm, sq, (gj + 2) * kTileQW + gi + 2, c, i, j, own && with_dt, g, den);
+    RecV *r = srec + 2 * ((gj + 1) * kTileRW + gi + 1);
+    if (sizeof(T) == sizeof(float)) {
+      r[0] = RecV{T(float(g[0])), T(float(g[1])), T(float(g[2])), T(float(g[3]))};
+      r[1] = RecV{T(float(g[4])), T(float(g[5])), T(float(g[6])), T(float(g[7]))};
+    } else {
+      r[0] = RecV{T(g[0]), T(g[1]), T(g[2]), T(g[3])};
+      r[1] = RecV{T(g[4]), T(g[5]), T(g[6]), T(g[7])};
+    }
+    if (own && with_dt) {
+      dtc = cell_dt(m, fp, c, den);
+      st.dtc[c] = dtc;
+    }
+  }
+  __syncthreads();
+
+  // 2. Face fluxes: W faces (i0..i0+TX, rows of the tile), then S faces (columns, j0..j0+TY).
+  for (int t = tid; t < kTileNW + kTileNS; t += blockDim.x) {
+    int fi, fj, lx, ly, hx, hy, gidx;
+    bool lo_phys, hi_phys, ohigh;
+    double4 gq;
+    double gdy;
+    if (t < kTileNW) {
+      fj = t / (kTileX + 1);
+      fi = t - fj * (kTileX + 1);
+      const int i = i0 + fi, j = j0 + fj;
+      if (i > ni || j >= nj) continue;
+      gidx = j * (ni + 1) + i;
+      lx = fi - 1;
+      ly = fj;
+      hx = fi;
+      hy = fj;
+      lo_phys = i > 0;
+      hi_phys = i < ni;
+      gq = tm.fw[gidx];
+      gdy = tm.fwdy[gidx];
+      ohigh = tm.fwo[gidx] != 0;
+    } else {
+      const int u = t - kTileNW;
+      fj = u / kTileX;
+      fi = u - fj * kTileX;
+      const int i = i0 + fi, j = j0 + fj;
+      if (i >= ni || j > nj) continue;
+      gidx = j * ni + i;
+      lx = fi;
+      ly = fj - 1;
+      hx = fi;
+      hy = fj;
+      lo_phys = j > 0;
+      hi_phys = j < nj;
+      gq = tm.fs[gidx];
+      gdy = tm.fsdy[gidx];
+      ohigh = tm.fso[gidx] != 0;
+    }
+    const int ox = ohigh ? hx : lx, oy = ohigh ? hy : ly, nx_ = ohigh ? lx : hx, ny_ = ohigh ? ly : hy;
+    const bool nphys = ohigh ? lo_phys : hi_phys;
+    const double4 c0 = sq[(oy + 2) * kTileQW + ox + 2], n0 = sq[(ny_ + 2) * kTileQW + nx_ + 2];
+    const RecV *ro = srec + 2 * ((oy + 1) * kTileRW + ox + 1);
+    const RecV *rn = nphys ? srec + 2 * ((ny_ + 1) * kTileRW + nx_ + 1) : ro;
+    const RecV a = ro[0], b = ro[1], p = rn[0], q = rn[1];
+    const double4 c1 = make_double4(a.x, a.y, a.z, a.w), c2 = make_double4(b.x, b.y, b.z, b.w);
+    const double4 n1 = make_double4(p.x, p.y, p.z, p.w), n2 = make_double4(q.x, q.y, q.z, q.w);
+    sF[t] = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, T(gq.x), T(gq.y), T(gq.z), T(gq.w), T(gdy),
+                                   T(fp.eflin), T(fp.shock_fix));
+  }
+  __syncthreads();
+
+  // 3. Gather in slot order and stage update of the own cells.
+  double dtu = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  {
+    const int tx = tid % kTileX, ty = tid / kTileX;
+    const int i = i0 + tx, j = j0 + ty;
+    if (i < ni && j < nj) {
+      const int c = j * ni + i;
+      const unsigned code = tm.code[c];
+      const int wE = ty * (kTileX + 1) + tx + 1, wW = wE - 1;
+      const int sS = kTileNW + ty * kTileX + tx, sN = sS + kTileX;
+      const int pf[4] = {wE, tm.lh ? sS : sN, wW, tm.lh ? sN : sS};
+      double t[4][4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const double4 F = sF[pf[p]];
+        const bool own = (code >> (2 + p)) & 1u;
+        t[p][0] = own ? F.x : -F.x;
+        t[p][1] = own ? F.y : -F.y;
+        t[p][2] = own ? F.z : -F.z;
+        t[p][3] = own ? F.w : -F.w;
+      }
+      double R[4] = {0.0, 0.0, 0.0, 0.0};
+      slot_order_sum<4>(code & 3u, t, R);
+      // Ghost rows move to the output buffer with their owner (boundary kinds that leave a ghost
+      // unchanged, and the final stage, keep its current state); non-final stages overwrite them.
+      const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+      for (int q = b0; q < b1; q++) {
+        const int g = m.bnd[m.bidx[q]].w;
+        st.q4[g] = q_in[g];
+      }
+      const double dts = (lts == 1 || first_kind(kind)) ? dtc : 0.0;
+      dtu = stage_cell(m, st, bp, c, R, dts, kind, lts, fuse_final, keep_delu, flags, e);
+    }
+  }
+  if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
+}
+
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.NP) return;
@@ -2037,6 +2315,56 @@ int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Fl
              flags);
   else
     launch_k(m, k_gather_stage<false>, g, kFluxBlock, s, m, st, fp, bp, kind, lts, fuse_final, keep_delu, flags);
+  return 1;
+}
+
+template <typename T>
+int tile_prepare_t() {
+  const int n = static_cast<int>(tile_smem_bytes<T>());
+  return cudaFuncSetAttribute(k_tile_stage<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_stage<T, 103>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_stage<T, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_stage<T, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_stage<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, n) == cudaSuccess;
+}
+
+int tile_prepare() {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  if (tile_smem_bytes<double>() > (size_t)optin) return 0;
+  const int ok = tile_prepare_t<double>() && tile_prepare_t<float>();
+  cudaGetLastError();
+  return ok;
+}
+
+template <typename T>
+void launch_tile_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                   const TileMesh &tm, const double4 *q_in, int kind, int lts, int fin, int keep_delu, int flags,
+                   int with_dt) {
+  const unsigned g = static_cast<unsigned>(tm.tiles_i) * static_cast<unsigned>(tm.tiles_j);
+  const unsigned b = kTileX * kTileY;
+  const size_t sm = tile_smem_bytes<T>();
+  const int sch = face_scheme(fp);
+  if (sch == 103)
+    launch_ks(m, k_tile_stage<T, 103>, g, b, sm, s, m, st, fp, bp, tm, q_in, kind, lts, fin, keep_delu, flags, with_dt);
+  else if (sch == 6)
+    launch_ks(m, k_tile_stage<T, 6>, g, b, sm, s, m, st, fp, bp, tm, q_in, kind, lts, fin, keep_delu, flags, with_dt);
+  else if (sch == 7)
+    launch_ks(m, k_tile_stage<T, 7>, g, b, sm, s, m, st, fp, bp, tm, q_in, kind, lts, fin, keep_delu, flags, with_dt);
+  else if (sch == 8)
+    launch_ks(m, k_tile_stage<T, 8>, g, b, sm, s, m, st, fp, bp, tm, q_in, kind, lts, fin, keep_delu, flags, with_dt);
+  else
+    launch_ks(m, k_tile_stage<T, 3>, g, b, sm, s, m, st, fp, bp, tm, q_in, kind, lts, fin, keep_delu, flags, with_dt);
+}
+
+int launch_tile_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                      const TileMesh &tm, const double4 *q_in, int kind, int lts, int fuse_final, int keep_delu,
+                      int flags, int with_dt) {
+  if (fp.precision == 1)
+    launch_tile_t<float>(s, m, st, fp, bp, tm, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt);
+  else
+    launch_tile_t<double>(s, m, st, fp, bp, tm, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt);
   return 1;
 }
 

@@ -147,6 +147,27 @@ struct BcParams {
   double inlet_rho, inlet_p, inlet_u, inlet_v, inlet_p0, inlet_t0, exit_p, r_gas;
 };
 
+// Structured-block tables of the tile form (a single block of ni x nj quads numbered
+// c = j * ni + i in device order).  The unique faces come in two structured families:
+// W(i, j) between cells (i - 1, j) and (i, j), i = 0..ni, and S(i, j) between (i, j - 1) and
+// (i, j), j = 0..nj; each keeps the values of its unique face (owner-side normal, length and
+// centre-to-centre vector) and a flag, 1 when its owner is the cell on the high side (i, j).
+// Around each cell the positions p = 0..3 run E, N, W, S (E, S, W, N when lh = 1); the cell's
+// face slot f is position (f + r) & 3.  Per cell one byte: r in bits 0-1, and bit 2 + p set
+// when the cell owns the face at position p.
+constexpr int kTileCellsX = 32, kTileCellsY = 8;  // cells of one tile (one thread block)
+struct TileMesh {
+  int ni, nj, tiles_i, tiles_j, lh;
+  const int *gW, *gE, *gS, *gN;  // ghost rows beside the block's boundary cells: [nj], [nj], [ni], [ni]
+  const unsigned char *code;     // [NP]
+  const double4 *fw;             // [nj][ni + 1] nx, ny, dl, dx of the W faces
+  const double *fwdy;            // [nj][ni + 1] dy
+  const unsigned char *fwo;      // [nj][ni + 1] owner on the high side
+  const double4 *fs;             // [nj + 1][ni] the same for the S faces
+  const double *fsdy;
+  const unsigned char *fso;
+};
+
 // Kernel launchers (stream-ordered, no host synchronisation).  Each returns the number of
 // kernels launched.
 int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st);
@@ -178,6 +199,17 @@ int launch_gather_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Fl
 // flags as launch_gather_stage; ghost rows are carried to st.prim at every stage.
 int launch_patch_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
                        int kind, int lts, int fuse_final, int keep_delu, int flags, const double *prim_in);
+// Tile form of one stage on a structured block (per-cell dt, three-stage integrators): one thread
+// block per tile of 32 x 8 cells reads the (rho, u, v, p) rows `q_in` of its cells and two rings
+// around them into shared memory, forms the gradients of its cells and of the halo cells beside
+// its sides, the fluxes of every face of its cells and the gather + stage update, and writes the
+// stage's rows (and the next stage's ghost rows) to st.q4, which must be a different buffer.
+// Same flags as launch_gather_stage; with_dt as launch_muscl_gradients.
+int launch_tile_stage(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                      const TileMesh &tm, const double4 *q_in, int kind, int lts, int fuse_final, int keep_delu,
+                      int flags, int with_dt);
+// Opt-in to the tile kernels' dynamic shared memory (0 if the device cannot give it).
+int tile_prepare();
 // Dynamic shared memory of the patch kernel for m.patch_rows, and the opt-in to it (0 if the
 // device cannot give it).
 size_t patch_smem_bytes(const DevMesh &m);

@@ -82,6 +82,12 @@ cfd_status cfd_mesh_write_vtk(const cfd_mesh *m, const char *path);
 cfd_status cfd_mesh_describe(const cfd_mesh *m, cfd_mesh_desc *out);
 /* Cell centres of physical and ghost cells, [(NP+NG)*3] (Cell::Cell_Center). */
 cfd_status cfd_mesh_centers(const cfd_mesh *m, double *out);
+/* The structured-block numbering of reorder 4 (host only, no device needed): when the mesh is a
+ * single block of ni x nj quads, *ni, *nj, *lh (1 when the face slots run clockwise in the block's
+ * (i, j) axes) and, if cells is not NULL, cells[j * ni + i] = the mesh cell at (i, j) (n_physical
+ * entries).  The i axis is the one whose length is a multiple of 32 if only one is, else the longer.
+ * CFD_ERR_MESH (with the reason in cfd_last_error) for any other mesh. */
+cfd_status cfd_mesh_block_order(const cfd_mesh_desc *d, int *ni, int *nj, int *lh, int *cells);
 /* Points and cell node lists as given ([npts*3], [ncells*4] -1 padded). */
 cfd_status cfd_mesh_points(const cfd_mesh *m, int *n_points, const double **points);
 void cfd_mesh_destroy(cfd_mesh *m);
@@ -130,7 +136,11 @@ typedef struct {
                                 2 patches of 128 cells grown breadth-first in RCM seed order,
                                 3 patches of 128 cells by recursive coordinate bisection (needs
                                 centre vectors; face-based per-cell-dt forms then run each
-                                stage as one kernel per patch, option "patch_stage") */
+                                stage as one kernel per patch, option "patch_stage"),
+                                4 a single structured block of ni x nj quads numbered j*ni+i
+                                (CFD_ERR_MESH otherwise; see cfd_mesh_block_order); the
+                                gradient-MUSCL forms with a per-cell dt and three stages then run
+                                each stage as one kernel per 32 x 8 tile, option "tile_stage") */
   double cfl;                /* CFL */
   double limiter_zeta;       /* Limiter_Zeta */
   double limiter_zeta1;      /* Limiter_Zeta1 */
@@ -218,7 +228,13 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * one CUDA graph per RK stage; default 0; the batched solves' form, see cfd_batch_set_option),
  * "barrier_timeout_test" (a test of the bounded barriers: every barrier of the persistent form
  * waits for `value` more blocks than it has, so each wait runs out and the step reports
- * CFD_ERR_TIMEOUT; default 0).
+ * CFD_ERR_TIMEOUT; default 0),
+ * "tile_stage" (with reorder 4 on a structured block, the gradient-MUSCL forms with a per-cell dt
+ * frozen per step and three stages (CFD_INT_SSPRK3, CFD_INT_RK3_GPU_REF with local time stepping)
+ * run each stage as one kernel: a thread block per tile of 32 x 8 cells stages the (rho, u, v, p)
+ * rows of the tile and two rings around it in shared memory and forms the gradients, face fluxes,
+ * gather and update of its cells there; default 1 where available, else 0 and setting it is
+ * CFD_ERR_BAD_ARG).
  * None of the options changes a state bit (the persistent form sums the error norms in another
  * order). */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);
