@@ -836,7 +836,7 @@ def main():
         f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
         f.set_option("keep_delu", 0)
         f.upload_state(U0)
-        tune_form = f.autotune(steps=10) if name.startswith("reference") else ""
+        tune_form = f.autotune(steps=10)
         f.step_async(3)
         f.sync()
         n_timed = min(nform, 50) if name.startswith("reference_roe2") else nform

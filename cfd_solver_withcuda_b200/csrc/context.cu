@@ -38,6 +38,34 @@ cfd_status fail(cfd_status s, const std::string &msg) {
   return s;
 }
 
+// Tiled tensor map of a 3-D array of doubles (d0 contiguous doubles per element, then d1, then
+// d2; rows packed) with box extents box[3], zeros for out-of-range elements.  The encoder is the
+// driver's cuTensorMapEncodeTiled, fetched through the runtime (no link to the driver library).
+// False when the driver does not offer it or refuses the map.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+bool encode_tensor_3d(CUtensorMap *map, const void *base, int d0, int d1, int d2, const int box[3]) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f) {
+      cudaGetLastError();
+      return false;
+    }
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+  const cuuint64_t strides[2] = {(cuuint64_t)d0 * 8, (cuuint64_t)d0 * 8 * d1};
+  const cuuint32_t bx[3] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2]};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dims, strides, bx, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 #define CUDA_TRY(expr)                                                                              \
   do {                                                                                              \
     cudaError_t _e = (expr);                                                                        \
@@ -349,8 +377,15 @@ struct cfd_ctx {
   // qbuf[1] -> st.q4).
   TileMesh tm{};
   bool tile_ok = false;
+  // 0 off, 1 the tile kernel, 2 its TMA form (stage inputs prefetched), 3 TMA form with 3 blocks
+  // per SM, 4 TMA form with 288 threads
   int tile_stage = 0;
   double4 *qbuf[2] = {nullptr, nullptr};
+  // TMA form: tensor maps of the three row buffers (st.q4, qbuf[0], qbuf[1]) and of the two
+  // face-record tensors; tile_tma_ok when all of them were encoded.
+  bool tile_tma_ok = false;
+  CUtensorMap tmap_q[3];
+  CUtensorMap tmap_gw, tmap_gs;
   // Per-kernel timing (option "profile"): event pairs recorded around each launch on the
   // context's stream, resolved lazily by cfd_kernel_time.
   int profile = 0;
@@ -482,8 +517,17 @@ int enqueue_stage(cfd_ctx *ctx, int k, bool fuse_final, bool &ghosts_written) {
     DevState sk = st;
     sk.q4 = bufs[(k + 1) % 3];
     const bool with_dt = k == 0 || k == p.n - 1;
-    n += launch_tile_stage(s, m, sk, ctx->fp, ctx->bp, ctx->tm, bufs[k], kind, lts, fin, ctx->keep_delu, flags,
-                           with_dt ? 1 : 0);
+    if (ctx->tile_stage >= 2 && ctx->tile_tma_ok) {
+      TileMaps maps;
+      maps.q = ctx->tmap_q[k];
+      maps.gw = ctx->tmap_gw;
+      maps.gs = ctx->tmap_gs;
+      n += launch_tile_tma(s, m, sk, ctx->fp, ctx->bp, ctx->tm, maps, bufs[k], kind, lts, fin, ctx->keep_delu, flags,
+                           with_dt ? 1 : 0, ctx->tile_stage - 2);
+    } else {
+      n += launch_tile_stage(s, m, sk, ctx->fp, ctx->bp, ctx->tm, bufs[k], kind, lts, fin, ctx->keep_delu, flags,
+                             with_dt ? 1 : 0);
+    }
     ghosts_written = bc_next;
     return n;
   }
@@ -1171,6 +1215,18 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if ((s = ctx_upload(ctx, const_cast<double4 **>(&tm.fs), tfs)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<double **>(&tm.fsdy), tsdy)) != CFD_OK) return bail(s);
     if ((s = ctx_upload(ctx, const_cast<unsigned char **>(&tm.fso), tso)) != CFD_OK) return bail(s);
+    // 48-byte face records of the TMA form: nx, ny, dl, dx, dy, owner on the high side.
+    std::vector<double> gw6(tfw.size() * 6), gs6(tfs.size() * 6);
+    for (size_t f = 0; f < tfw.size(); f++) {
+      const double r[6] = {tfw[f].x, tfw[f].y, tfw[f].z, tfw[f].w, twdy[f], two[f] ? 1.0 : 0.0};
+      std::copy(r, r + 6, gw6.begin() + 6 * f);
+    }
+    for (size_t f = 0; f < tfs.size(); f++) {
+      const double r[6] = {tfs[f].x, tfs[f].y, tfs[f].z, tfs[f].w, tsdy[f], tso[f] ? 1.0 : 0.0};
+      std::copy(r, r + 6, gs6.begin() + 6 * f);
+    }
+    if ((s = ctx_upload(ctx, const_cast<double **>(&tm.gw6), gw6)) != CFD_OK) return bail(s);
+    if ((s = ctx_upload(ctx, const_cast<double **>(&tm.gs6), gs6)) != CFD_OK) return bail(s);
     ctx->tile_ok = true;
   }
   if (!patches.empty()) {
@@ -1246,6 +1302,19 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       return bail(fail(CFD_ERR_CUDA, "memset failed"));
   }
   ctx->tile_stage = ctx->tile_ok ? 1 : 0;
+  if (ctx->tile_ok && tile_tma_prepare()) {
+    double4 *bufs[3] = {ctx->ds.q4, ctx->qbuf[0], ctx->qbuf[1]};
+    int bq[3], bw[3], bs[3];
+    tile_tma_boxes(bq, bw, bs);
+    const TileMesh &tm = ctx->tm;
+    bool ok = true;
+    for (int q = 0; q < 3; q++)
+      ok = ok && encode_tensor_3d(&ctx->tmap_q[q], bufs[q], 4, tm.ni, tm.nj, bq);
+    ok = ok && encode_tensor_3d(&ctx->tmap_gw, tm.gw6, 6, tm.ni + 1, tm.nj, bw);
+    ok = ok && encode_tensor_3d(&ctx->tmap_gs, tm.gs6, 6, tm.ni, tm.nj + 1, bs);
+    ctx->tile_tma_ok = ok;
+    if (ok) ctx->tile_stage = 2;
+  }
   for (int q = 0; q < 2 && m.npatch > 0; q++) {
     if ((s = ctx_alloc(ctx, (void **)&ctx->pbuf[q], 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);
     if (cudaMemset(ctx->pbuf[q], 0, 5 * (size_t)NT * dsz) != cudaSuccess) return bail(fail(CFD_ERR_CUDA, "memset failed"));
@@ -1349,11 +1418,16 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
   else if (n == "fuse_gather") ctx->fuse_gather = value != 0.0;
   else if (n == "patch_stage") ctx->patch_stage = value != 0.0;
   else if (n == "tile_stage") {
+    if (value != 0.0 && value != 1.0 && value != 2.0 && value != 3.0 && value != 4.0)
+      return fail(CFD_ERR_BAD_ARG, "tile_stage must be 0, 1, 2, 3 or 4");
     if (value != 0.0 && !ctx->tile_ok)
       return fail(CFD_ERR_BAD_ARG, "the tile form needs reorder 4 on a structured block with the gradient-MUSCL scheme");
-    ctx->tile_stage = value != 0.0;
+    if (value >= 2.0 && !ctx->tile_tma_ok)
+      return fail(CFD_ERR_BAD_ARG, "the TMA tile form is not available on this device");
+    ctx->tile_stage = static_cast<int>(value);
   }
   else if (n == "l2_persist") ctx->dm.l2_bytes = value != 0.0 ? ctx->l2_window : 0;
+  else if (n == "tile_prefetch") ctx->tm.prefetch_ahead = value != 0.0;
   else return fail(CFD_ERR_BAD_ARG, "unknown option " + n);
   drop_graphs(ctx);
   return CFD_OK;
@@ -1810,8 +1884,9 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
       for (int p = 0; p < 2; p++)
         cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 1, ctx->fp.flux_minb, 0, 0.0});
     if (ctx->tile_ok)
-      for (int p = 0; p < 2; p++)
-        cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, 1, 0.0});
+      for (int t = 1; t <= (ctx->tile_tma_ok ? 4 : 1); t++)
+        for (int p = 0; p < 2; p++)
+          cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, t, 0.0});
   } else {
     const bool roe2 = ctx->fp.dissipation == 3 && ctx->fp.second_order && !ctx->fp.weno;
     for (int mb : {1, 6, 8}) {

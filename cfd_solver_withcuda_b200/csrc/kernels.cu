@@ -555,9 +555,12 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
 
 // del_t = CFL * Area / sum (|V.n| + a) dl, 0 when the sum is not a positive finite number
 // (Inviscid_Time_Step, src/Time_Step.cpp:337-358).
-__device__ __forceinline__ double cell_dt(const DevMesh &m, const FluxParams &fp, int c, double den) {
+__device__ __forceinline__ double cell_dt_a(const FluxParams &fp, double area, double den) {
   if (den <= 0.0 || !isfinite(den)) return 0.0;
-  return fp.cfl * m.area[c] / den;
+  return fp.cfl * area / den;
+}
+__device__ __forceinline__ double cell_dt(const DevMesh &m, const FluxParams &fp, int c, double den) {
+  return cell_dt_a(fp, m.area[c], den);
 }
 
 // Block min of del_t to `partial`; the last block writes Min_dt (get_Min_dt,
@@ -1220,14 +1223,14 @@ __global__ void __launch_bounds__(kBlock) k_stage(DevMesh m, DevState st, int ki
 // updates the cell, and with flags bit 1 writes the next stage's ghost states from the owner
 // thread (every ghost depends only on its owner cell's new state: Apply_Boundary_Conditions of the
 // next stage).  Returns the dt used.
-__device__ __forceinline__ double stage_cell(const DevMesh &m, DevState &st, const BcParams &bp, int c,
-                                             const double R[4], double dtc, int kind, int lts, int fuse_final,
-                                             int keep_delu, int flags, double e[8]) {
+// stage_cell_in: the same with the stage inputs and the frozen dt already loaded (the TMA tile
+// form prefetches them into shared memory).
+__device__ __forceinline__ double stage_cell_in(const DevMesh &m, DevState &st, const BcParams &bp, int c,
+                                                const double R[4], double dtc, double dt_frozen, const StageIn &in,
+                                                int kind, int lts, int fuse_final, int keep_delu, int flags,
+                                                double e[8]) {
   const int NP = m.NP;
   const bool first = first_kind(kind);
-  StageIn in;
-  load_stage_in(m, st, c, kind, in);
-  const double dt_frozen = (lts != 1 && !first) ? st.dtk[c] : 0.0;
 #pragma unroll
   for (int k = 0; k < 4; k++) st.R[k * NP + c] = R[k];
   double dt;
@@ -1243,14 +1246,22 @@ __device__ __forceinline__ double stage_cell(const DevMesh &m, DevState &st, con
   }
   return dt;
 }
+__device__ __forceinline__ double stage_cell(const DevMesh &m, DevState &st, const BcParams &bp, int c,
+                                             const double R[4], double dtc, int kind, int lts, int fuse_final,
+                                             int keep_delu, int flags, double e[8]) {
+  StageIn in;
+  load_stage_in(m, st, c, kind, in);
+  const double dt_frozen = (lts != 1 && !first_kind(kind)) ? st.dtk[c] : 0.0;
+  return stage_cell_in(m, st, bp, c, R, dtc, dt_frozen, in, kind, lts, fuse_final, keep_delu, flags, e);
+}
 
 // Last stage of the fused forms: Estimate_Error's terms, the residual squares and the step's dt
 // (the minimum of the per-cell dt frozen at the first stage, i.e. that stage's Min_dt), reduced
 // over the grid, then the Total_Time epilogue of the loop body.  Called by every thread.
-__device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[8], double dtu) {
-  __shared__ double sh[32];
-  __shared__ double sh8[8 * 32];
-  __shared__ double red[9];
+// stage_final_reduce_sm: the same with its scratch (32 + 8 * 32 + 9 doubles) in caller-provided
+// shared memory.
+__device__ __forceinline__ void stage_final_reduce_sm(DevState &st, const double e[8], double dtu, double *scratch) {
+  double *sh = scratch, *sh8 = scratch + 32, *red = scratch + 32 + 8 * 32;
   const double sq = block_sums8(e, sh8);
   if (threadIdx.x < 8) st.partial[(1 + threadIdx.x) * gridDim.x + blockIdx.x] = sq;
   const double bm = block_min(dtu, sh);
@@ -1265,6 +1276,10 @@ __device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[
     double te = st.ctl[CTL_TEND];
     if (te > 0.0 && t >= te) st.ctl[CTL_DONE] = 1.0;
   }
+}
+__device__ __forceinline__ void stage_final_reduce(DevState &st, const double e[8], double dtu) {
+  __shared__ double scratch[32 + 8 * 32 + 9];
+  stage_final_reduce_sm(st, e, dtu, scratch);
 }
 
 // Face-based forms with a per-cell time step (lts 1 or 2): the gather of k_gather and the stage
@@ -2000,6 +2015,434 @@ __global__ void __launch_bounds__(kTileX * kTileY, 2)
   if (fuse_final && final_kind(kind)) stage_final_reduce(st, e, dtu);
 }
 
+// ---- TMA form of the tile stage (no reference counterpart) ----
+// The work of k_tile_stage, tile by tile and operation by operation the same (so the same bits),
+// with every global load moved to the start of the block and made asynchronous:
+//   * one thread issues three cp.async.bulk.tensor loads on one mbarrier: the (rho, u, v, p) rows
+//     of the tile and two rings (box 36 x 12 of 32-byte rows; rows beyond the block arrive as
+//     zeros), and the 48-byte face records of the W faces (35 x 10) and S faces (34 x 11) that the
+//     tile's cells and its one-ring halo cells touch;
+//   * every thread issues cp.async copies of its own cell's stage inputs (U^n, the stage state,
+//     the frozen dt, sound speed and area for del_t) and of the 1/area of the gradient region,
+//     and plain loads of the region's slot codes and of the ghost rows beside the block's rim
+//     (which the bulk load fills with zeros; they are written after it lands).
+// The gradient, face and update phases then read shared memory only.  A face's flux is written
+// over the first 32 bytes of its own record (read only by the thread that computes it).
+// The mbarrier wait is bounded (kTmaWaitCycles, about half a second): a block whose wait runs out
+// records CFD_ERR_TIMEOUT in the status word and ends.
+constexpr int kTmaGW = kTileX + 3, kTmaGH = kTileY + 2;  // W-face records: i0-1 .. i0+TX+1, j0-1 .. j0+TY
+constexpr int kTmaSW = kTileX + 2, kTmaSH = kTileY + 3;  // S-face records: i0-1 .. i0+TX, j0-1 .. j0+TY+1
+constexpr int kTmaRecD = 6;                              // doubles per face record
+constexpr int kTmaSin = 11;  // stage inputs per own cell: U^n [4], stage state [4], frozen dt, a, area
+// PRE (true): the stage inputs are prefetched into shared memory at block start (96 KB per block,
+// 2 blocks per SM); false: they are loaded where they are used, which leaves room for 3 blocks per
+// SM (74 KB each, registers capped at 85).
+constexpr unsigned kTmaQBytes = kTileQW * kTileQH * 32u;
+constexpr unsigned kTmaGWBytes = kTmaGW * kTmaGH * kTmaRecD * 8u;
+constexpr unsigned kTmaGSBytes = kTmaSW * kTmaSH * kTmaRecD * 8u;
+constexpr long long kTmaWaitCycles = 1ll << 30;
+// Threads of the wide variant: 9 warps for the 256 cells of a tile, so the 552 face fluxes take
+// two rounds instead of three (the ninth warp has no own cell; it loads and computes gradients and
+// faces).  112 registers x 288 threads still leaves two blocks per SM.
+constexpr int kTileThreadsWide = 288;
+
+__host__ __device__ constexpr unsigned tma_round128(unsigned x) { return (x + 127u) & ~127u; }
+
+template <typename T, bool PRE>
+struct TileTmaLayout {
+  static constexpr unsigned q = 0;
+  static constexpr unsigned gw = tma_round128(kTmaQBytes);
+  static constexpr unsigned gs = gw + tma_round128(kTmaGWBytes);
+  static constexpr unsigned rec = gs + tma_round128(kTmaGSBytes);
+  static constexpr unsigned sin =
+      rec + tma_round128(2u * (unsigned)sizeof(typename TileRecT<T>::type) * kTileRW * kTileRH);
+  static constexpr unsigned ia = sin + (PRE ? kTmaSin * kTileX * kTileY * 8u : 0u);
+  static constexpr unsigned code = ia + kTileRW * kTileRH * 8u;
+  static constexpr unsigned bar = (code + kTileRW * kTileRH + 7u) & ~7u;
+  static constexpr unsigned bytes = bar + 8u + 128u;  // + slack to align the base to 128 bytes
+};
+
+__device__ __forceinline__ uint32_t sm_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sm_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+// L2 prefetch of the bytes [p, p + n) (widened to 16-byte bounds, as the bulk prefetch needs).
+__device__ __forceinline__ void l2_prefetch_range(const void *p, size_t n) {
+  if (n == 0) return;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~static_cast<uintptr_t>(15);
+  const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + n + 15) & ~static_cast<uintptr_t>(15);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<unsigned>(e - a)) : "memory");
+}
+__device__ __forceinline__ bool tma_bar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kTmaWaitCycles) return false;
+  }
+}
+
+// Gradients of cell (gi, gj) of the tile's gradient region (row ri = (gj + 1) * kTileRW + gi + 1)
+// as tile_gradients forms them, the face values read from the shared records.
+__device__ __forceinline__ void tile_gradients_sm(const TileMesh &tm, const double4 *sq, const double *sgw,
+                                                  const double *sgs, int qi, int gi, int gj, unsigned code, double ia,
+                                                  double ac, double g[8], double &den) {
+  const double *fp4[4];
+  const int up = tm.lh ? 3 : 1, dn = tm.lh ? 1 : 3;
+  fp4[0] = sgw + kTmaRecD * ((gj + 1) * kTmaGW + gi + 2);
+  fp4[2] = sgw + kTmaRecD * ((gj + 1) * kTmaGW + gi + 1);
+  fp4[up] = sgs + kTmaRecD * ((gj + 2) * kTmaSW + gi + 1);
+  fp4[dn] = sgs + kTmaRecD * ((gj + 1) * kTmaSW + gi + 1);
+  int dq[4];
+  dq[0] = 1;
+  dq[2] = -1;
+  dq[up] = kTileQW;
+  dq[dn] = -kTileQW;
+  const double4 qv = sq[qi];
+  const double qc[4] = {qv.x, qv.y, qv.z, qv.w};
+  double t[4][9];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const double2 nxy = *reinterpret_cast<const double2 *>(fp4[p]);
+    const double dlf = fp4[p][2];
+    const double4 qn = sq[qi + dq[p]];
+    const bool own = (code >> (2 + p)) & 1u;
+    const double nxf = own ? nxy.x : -nxy.x, nyf = own ? nxy.y : -nxy.y;
+    const double wx = nxf * dlf, wy = nyf * dlf;
+    const double qnv[4] = {qn.x, qn.y, qn.z, qn.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double qf = 0.5 * (qc[k] + qnv[k]);
+      t[p][2 * k] = qf * wx;
+      t[p][2 * k + 1] = qf * wy;
+    }
+    const double vnf = qc[1] * nxf + qc[2] * nyf;
+    t[p][8] = (fabs(vnf) + ac) * dlf;
+  }
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  slot_order_sum<9>(code & 3u, t, acc);
+#pragma unroll
+  for (int k = 0; k < 8; k++) g[k] = acc[k] * ia;
+  den = acc[8];
+}
+
+template <typename T, int DISS, bool PRE, int NTHR>
+__global__ void __launch_bounds__(NTHR, PRE ? 2 : 3)
+    k_tile_tma(DevMesh m, DevState st, FluxParams fp, BcParams bp, TileMesh tm, const __grid_constant__ TileMaps maps,
+               const double4 *__restrict__ q_in, int kind, int lts, int fuse_final, int keep_delu, int flags,
+               int with_dt, int ahead) {
+  typedef typename TileRecT<T>::type RecV;
+  typedef TileTmaLayout<T, PRE> L;
+  pdl_enter();
+  if (step_done(st.ctl)) return;
+  extern __shared__ unsigned char tma_smem_raw[];
+  unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tma_smem_raw) + 127) &
+                                                          ~static_cast<uintptr_t>(127));
+  double4 *sq = reinterpret_cast<double4 *>(base + L::q);          // [QH][QW]
+  double *sgw = reinterpret_cast<double *>(base + L::gw);          // [GH][GW][6]
+  double *sgs = reinterpret_cast<double *>(base + L::gs);          // [SH][SW][6]
+  RecV *srec = reinterpret_cast<RecV *>(base + L::rec);            // [RH][RW] x 2
+  double *sin = reinterpret_cast<double *>(base + L::sin);         // [kTmaSin][TX * TY]
+  double *sia = reinterpret_cast<double *>(base + L::ia);          // [RH][RW]
+  unsigned char *scode = base + L::code;                           // [RH][RW]
+  const uint32_t bar = sm_u32(base + L::bar);
+  const int NP = m.NP, NT = m.NT, ni = tm.ni, nj = tm.nj, tid = threadIdx.x;
+  constexpr int NC = kTileX * kTileY;
+  static_assert(NTHR >= NC && NTHR % 32 == 0, "one thread per own cell, whole warps");
+  static_assert(2 * NTHR >= kTileQW * kTileQH && 2 * NTHR >= kTileRW * kTileRH, "two region rows per thread");
+  const int i0 = (blockIdx.x % tm.tiles_i) * kTileX, j0 = (blockIdx.x / tm.tiles_i) * kTileY;
+  const int glim = fp.limiter == LIM_REF_MINMOD ? LIM_MINMOD : fp.limiter;
+  const bool first = first_kind(kind);
+  const bool use_s = kind == 2 || kind == 3 || kind == 22 || kind == 23;
+
+  // 0. Loads.  The mbarrier is initialised, made visible to the async proxy and to the block,
+  // then thread 0 posts the byte count and issues the three tensor loads.
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(kTmaQBytes + kTmaGWBytes + kTmaGSBytes)
+                 : "memory");
+    tma_load_3d(sm_u32(sgw), &maps.gw, 0, i0 - 1, j0 - 1, bar);
+    tma_load_3d(sm_u32(sgs), &maps.gs, 0, i0 - 1, j0 - 1, bar);
+    tma_load_3d(sm_u32(sq), &maps.q, 0, i0 - 2, j0 - 2, bar);
+  }
+  // Stage inputs of the own cell (thread tid has cell tid of the tile).
+  const int tx = tid % kTileX, ty = tid / kTileX;
+  const int ci = i0 + tx, cj = j0 + ty;
+  const bool own_ok = tid < NC && ci < ni && cj < nj;
+  const int c = cj * ni + ci;
+  if (PRE && own_ok) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) cp_async8(sin + k * NC + tid, st.U + (size_t)k * NT + c);
+    if (use_s) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) cp_async8(sin + (4 + k) * NC + tid, st.S + (size_t)k * NP + c);
+    }
+    if (lts != 1 && !first) cp_async8(sin + 8 * NC + tid, st.dtk + c);
+    if (with_dt) {
+      cp_async8(sin + 9 * NC + tid, st.prim + 4 * (size_t)NT + c);
+      cp_async8(sin + 10 * NC + tid, m.area + c);
+    }
+  }
+  // 1/area and slot codes of the gradient region (tile + one ring, cells inside the block).
+  constexpr int NR = kTileRW * kTileRH;
+  unsigned char code_r[2] = {0, 0};
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int r = tid + h * NTHR;
+    if (r < NR) {
+      const int gi = r % kTileRW - 1, gj = r / kTileRW - 1;
+      const int i = i0 + gi, j = j0 + gj;
+      if (i >= 0 && i < ni && j >= 0 && j < nj) {
+        cp_async8(sia + r, m.inv_area + (j * ni + i));
+        code_r[h] = tm.code[j * ni + i];
+      }
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  // Ghost rows beside the block's rim in the state region (the tensor load leaves zeros there).
+  constexpr int NQ = kTileQW * kTileQH;
+  double4 gq[2];
+  int gpos[2] = {-1, -1};
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int t = tid + h * NTHR;
+    if (t < NQ) {
+      const int jj = t / kTileQW, ii = t - jj * kTileQW;
+      const int i = i0 + ii - 2, j = j0 + jj - 2;
+      const bool in_i = i >= 0 && i < ni, in_j = j >= 0 && j < nj;
+      int r = -1;
+      if (in_j && i == -1) r = tm.gW[j];
+      else if (in_j && i == ni) r = tm.gE[j];
+      else if (in_i && j == -1) r = tm.gS[i];
+      else if (in_i && j == nj) r = tm.gN[i];
+      if (r >= 0) {
+        gq[h] = q_in[r];
+        gpos[h] = t;
+      }
+    }
+  }
+  const bool landed = tma_bar_wait(bar, 0);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if (__syncthreads_or(!landed)) {
+    if (tid == 0) atomicCAS(st.status, 0, 5 /* CFD_ERR_TIMEOUT */);
+    return;
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    if (gpos[h] >= 0) sq[gpos[h]] = gq[h];
+    const int r = tid + h * NTHR;
+    if (r < NR) scode[r] = code_r[h];
+  }
+  __syncthreads();
+
+  // L2 prefetch of the inputs of tile blockIdx.x + ahead (the tile that starts on this SM's slot in
+  // the next wave, ahead = resident blocks of the grid), while this tile computes: its three tensor
+  // boxes, and the rows of its stage inputs, 1/area and slot codes.  Hints only; the data are final.
+  if (ahead > 0 && blockIdx.x + ahead < gridDim.x) {
+    const int nbk = blockIdx.x + ahead;
+    const int pi0 = (nbk % tm.tiles_i) * kTileX, pj0 = (nbk / tm.tiles_i) * kTileY;
+    if (tid == 0) {
+      tma_prefetch_3d(&maps.gw, 0, pi0 - 1, pj0 - 1);
+      tma_prefetch_3d(&maps.gs, 0, pi0 - 1, pj0 - 1);
+      tma_prefetch_3d(&maps.q, 0, pi0 - 2, pj0 - 2);
+    } else if (tid >= 32 && tid < 32 + kTileRH) {
+      // rows of the gradient region (1/area, slot codes) and of the own cells (stage inputs)
+      const int gj = tid - 32 - 1, j = pj0 + gj;
+      if (j >= 0 && j < nj) {
+        const int ia0 = max(pi0 - 1, 0), ia1 = min(pi0 + kTileX + 1, ni);
+        const size_t r0 = (size_t)j * ni;
+        l2_prefetch_range(m.inv_area + r0 + ia0, (size_t)(ia1 - ia0) * 8);
+        l2_prefetch_range(tm.code + r0 + ia0, (size_t)(ia1 - ia0));
+        if (PRE && gj >= 0 && gj < kTileY) {
+          const int o1 = min(pi0 + kTileX, ni);
+          const size_t nb8 = (size_t)(o1 - pi0) * 8;
+#pragma unroll
+          for (int k = 0; k < 4; k++) l2_prefetch_range(st.U + (size_t)k * NT + r0 + pi0, nb8);
+          if (use_s) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) l2_prefetch_range(st.S + (size_t)k * NP + r0 + pi0, nb8);
+          }
+          if (lts != 1 && !first) l2_prefetch_range(st.dtk + r0 + pi0, nb8);
+          if (with_dt) {
+            l2_prefetch_range(st.prim + 4 * (size_t)NT + r0 + pi0, nb8);
+            l2_prefetch_range(m.area + r0 + pi0, nb8);
+          }
+        }
+      }
+    }
+  }
+
+  // 1. Gradients: own cells (thread tid has cell tid), then the halo strips W, E, S, N.
+  double dtc = 0.0;
+  constexpr int NG = kTileX * kTileY + 2 * kTileY + 2 * kTileX;
+  for (int t = tid; t < NG; t += blockDim.x) {
+    int gi, gj;
+    if (t < kTileX * kTileY) {
+      gi = t % kTileX;
+      gj = t / kTileX;
+    } else {
+      const int u = t - kTileX * kTileY;
+      if (u < kTileY) {
+        gi = -1;
+        gj = u;
+      } else if (u < 2 * kTileY) {
+        gi = kTileX;
+        gj = u - kTileY;
+      } else if (u < 2 * kTileY + kTileX) {
+        gi = u - 2 * kTileY;
+        gj = -1;
+      } else {
+        gi = u - 2 * kTileY - kTileX;
+        gj = kTileY;
+      }
+    }
+    const int i = i0 + gi, j = j0 + gj;
+    if (i < 0 || i >= ni || j < 0 || j >= nj) continue;
+    const bool own = t < kTileX * kTileY;
+    const bool dt = own && with_dt;
+    const int ri = (gj + 1) * kTileRW + gi + 1;
+    double g[8], den;
+    const double ac = dt ? (PRE ? sin[9 * NC + t] : st.prim[4 * (size_t)NT + c]) : 0.0;
+    tile_gradients_sm(tm, sq, sgw, sgs, (gj + 2) * kTileQW + gi + 2, gi, gj, scode[ri], sia[ri], ac, g, den);
+    RecV *r = srec + 2 * ri;
+    if (sizeof(T) == sizeof(float)) {
+      r[0] = RecV{T(float(g[0])), T(float(g[1])), T(float(g[2])), T(float(g[3]))};
+      r[1] = RecV{T(float(g[4])), T(float(g[5])), T(float(g[6])), T(float(g[7]))};
+    } else {
+      r[0] = RecV{T(g[0]), T(g[1]), T(g[2]), T(g[3])};
+      r[1] = RecV{T(g[4]), T(g[5]), T(g[6]), T(g[7])};
+    }
+    if (dt) {
+      dtc = cell_dt_a(fp, PRE ? sin[10 * NC + t] : m.area[c], den);
+      st.dtc[c] = dtc;
+    }
+  }
+  __syncthreads();
+
+  // 2. Face fluxes: W faces (i0..i0+TX, rows of the tile), then S faces (columns, j0..j0+TY);
+  // each flux over the first four doubles of its own record.
+  for (int t = tid; t < kTileNW + kTileNS; t += blockDim.x) {
+    int lx, ly, hx, hy;
+    bool lo_phys, hi_phys;
+    double *rec;
+    if (t < kTileNW) {
+      const int fj = t / (kTileX + 1), fi = t - fj * (kTileX + 1);
+      const int i = i0 + fi, j = j0 + fj;
+      if (i > ni || j >= nj) continue;
+      rec = sgw + kTmaRecD * ((fj + 1) * kTmaGW + fi + 1);
+      lx = fi - 1;
+      ly = fj;
+      hx = fi;
+      hy = fj;
+      lo_phys = i > 0;
+      hi_phys = i < ni;
+    } else {
+      const int u = t - kTileNW;
+      const int fj = u / kTileX, fi = u - fj * kTileX;
+      const int i = i0 + fi, j = j0 + fj;
+      if (i >= ni || j > nj) continue;
+      rec = sgs + kTmaRecD * ((fj + 1) * kTmaSW + fi + 1);
+      lx = fi;
+      ly = fj - 1;
+      hx = fi;
+      hy = fj;
+      lo_phys = j > 0;
+      hi_phys = j < nj;
+    }
+    const double2 g01 = *reinterpret_cast<const double2 *>(rec);
+    const double2 g23 = *reinterpret_cast<const double2 *>(rec + 2);
+    const double2 g45 = *reinterpret_cast<const double2 *>(rec + 4);
+    const bool ohigh = g45.y != 0.0;
+    const int ox = ohigh ? hx : lx, oy = ohigh ? hy : ly, nx_ = ohigh ? lx : hx, ny_ = ohigh ? ly : hy;
+    const bool nphys = ohigh ? lo_phys : hi_phys;
+    const double4 c0 = sq[(oy + 2) * kTileQW + ox + 2], n0 = sq[(ny_ + 2) * kTileQW + nx_ + 2];
+    const RecV *ro = srec + 2 * ((oy + 1) * kTileRW + ox + 1);
+    const RecV *rn = nphys ? srec + 2 * ((ny_ + 1) * kTileRW + nx_ + 1) : ro;
+    const RecV a = ro[0], b = ro[1], p = rn[0], q = rn[1];
+    const double4 c1 = make_double4(a.x, a.y, a.z, a.w), c2 = make_double4(b.x, b.y, b.z, b.w);
+    const double4 n1 = make_double4(p.x, p.y, p.z, p.w), n2 = make_double4(q.x, q.y, q.z, q.w);
+    const double4 F = face_flux_rec<T, DISS>(glim, c0, c1, c2, n0, n1, n2, T(g01.x), T(g01.y), T(g23.x), T(g23.y),
+                                             T(g45.x), T(fp.eflin), T(fp.shock_fix));
+    *reinterpret_cast<double2 *>(rec) = make_double2(F.x, F.y);
+    *reinterpret_cast<double2 *>(rec + 2) = make_double2(F.z, F.w);
+  }
+  __syncthreads();
+
+  // 3. Gather in slot order and stage update of the own cells.
+  double dtu = 1e308 * 10.0;
+  double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (own_ok) {
+    const unsigned code = scode[(ty + 1) * kTileRW + tx + 1];
+    const double *fE = sgw + kTmaRecD * ((ty + 1) * kTmaGW + tx + 2);
+    const double *fW = sgw + kTmaRecD * ((ty + 1) * kTmaGW + tx + 1);
+    const double *fN = sgs + kTmaRecD * ((ty + 2) * kTmaSW + tx + 1);
+    const double *fS = sgs + kTmaRecD * ((ty + 1) * kTmaSW + tx + 1);
+    const double *pf[4] = {fE, tm.lh ? fS : fN, fW, tm.lh ? fN : fS};
+    double t[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const double2 a = *reinterpret_cast<const double2 *>(pf[p]);
+      const double2 b = *reinterpret_cast<const double2 *>(pf[p] + 2);
+      const bool own = (code >> (2 + p)) & 1u;
+      t[p][0] = own ? a.x : -a.x;
+      t[p][1] = own ? a.y : -a.y;
+      t[p][2] = own ? b.x : -b.x;
+      t[p][3] = own ? b.y : -b.y;
+    }
+    double R[4] = {0.0, 0.0, 0.0, 0.0};
+    slot_order_sum<4>(code & 3u, t, R);
+    // Ghost rows move to the output buffer with their owner (as in k_tile_stage).
+    const int b0 = m.bptr[c], b1 = m.bptr[c + 1];
+    for (int q = b0; q < b1; q++) {
+      const int g = m.bnd[m.bidx[q]].w;
+      st.q4[g] = q_in[g];
+    }
+    const double dts = (lts == 1 || first) ? dtc : 0.0;
+    if (PRE) {
+      StageIn in;
+      in.invA = sia[(ty + 1) * kTileRW + tx + 1];
+#pragma unroll
+      for (int k = 0; k < 4; k++) in.Un[k] = sin[k * NC + tid];
+      if (use_s) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) in.Sk[k] = sin[(4 + k) * NC + tid];
+      }
+      const double dt_frozen = (lts != 1 && !first) ? sin[8 * NC + tid] : 0.0;
+      dtu = stage_cell_in(m, st, bp, c, R, dts, dt_frozen, in, kind, lts, fuse_final, keep_delu, flags, e);
+    } else {
+      dtu = stage_cell(m, st, bp, c, R, dts, kind, lts, fuse_final, keep_delu, flags, e);
+    }
+  }
+  // The state region is no longer read: its first 2.4 KB hold the reduction scratch.
+  if (fuse_final && final_kind(kind)) stage_final_reduce_sm(st, e, dtu, reinterpret_cast<double *>(sq));
+}
+
 __global__ void k_gradient(DevMesh m, DevState st, int var, double *grad) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.NP) return;
@@ -2365,6 +2808,104 @@ int launch_tile_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Flux
     launch_tile_t<float>(s, m, st, fp, bp, tm, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt);
   else
     launch_tile_t<double>(s, m, st, fp, bp, tm, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt);
+  return 1;
+}
+
+template <typename T, bool PRE, int NTHR>
+int tile_tma_prepare_t() {
+  const int n = static_cast<int>(TileTmaLayout<T, PRE>::bytes);
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  return cudaFuncSetAttribute(k_tile_tma<T, 3, PRE, NTHR>, a, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_tma<T, 103, PRE, NTHR>, a, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_tma<T, 6, PRE, NTHR>, a, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_tma<T, 7, PRE, NTHR>, a, n) == cudaSuccess &&
+         cudaFuncSetAttribute(k_tile_tma<T, 8, PRE, NTHR>, a, n) == cudaSuccess;
+}
+
+int tile_tma_prepare() {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  if (TileTmaLayout<double, true>::bytes > (unsigned)optin) return 0;
+  const int ok = tile_tma_prepare_t<double, true, kTileThreadsWide>() &&
+                 tile_tma_prepare_t<float, true, kTileThreadsWide>() &&
+                 tile_tma_prepare_t<double, true, kTileX * kTileY>() &&
+                 tile_tma_prepare_t<float, true, kTileX * kTileY>() &&
+                 tile_tma_prepare_t<double, false, kTileX * kTileY>() &&
+                 tile_tma_prepare_t<float, false, kTileX * kTileY>();
+  cudaGetLastError();
+  return ok;
+}
+
+void tile_tma_boxes(int q[3], int gw[3], int gs[3]) {
+  q[0] = 4;
+  q[1] = kTileQW;
+  q[2] = kTileQH;
+  gw[0] = kTmaRecD;
+  gw[1] = kTmaGW;
+  gw[2] = kTmaGH;
+  gs[0] = kTmaRecD;
+  gs[1] = kTmaSW;
+  gs[2] = kTmaSH;
+}
+
+template <typename T, bool PRE, int NTHR>
+void launch_tile_tma_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                       const TileMesh &tm, const TileMaps &maps, const double4 *q_in, int kind, int lts, int fin,
+                       int keep_delu, int flags, int with_dt) {
+  const unsigned g = static_cast<unsigned>(tm.tiles_i) * static_cast<unsigned>(tm.tiles_j);
+  const size_t sm = TileTmaLayout<T, PRE>::bytes;
+  const int sch = face_scheme(fp);
+  int ahead = 0;
+  if (tm.prefetch_ahead) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_tma<T, 3, PRE, NTHR>, NTHR, sm) == cudaSuccess)
+      ahead = sms * per_sm;
+    cudaGetLastError();
+  }
+  if (sch == 103)
+    launch_ks(m, k_tile_tma<T, 103, PRE, NTHR>, g, NTHR, sm, s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin,
+              keep_delu, flags, with_dt, ahead);
+  else if (sch == 6)
+    launch_ks(m, k_tile_tma<T, 6, PRE, NTHR>, g, NTHR, sm, s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu,
+              flags, with_dt, ahead);
+  else if (sch == 7)
+    launch_ks(m, k_tile_tma<T, 7, PRE, NTHR>, g, NTHR, sm, s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu,
+              flags, with_dt, ahead);
+  else if (sch == 8)
+    launch_ks(m, k_tile_tma<T, 8, PRE, NTHR>, g, NTHR, sm, s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu,
+              flags, with_dt, ahead);
+  else
+    launch_ks(m, k_tile_tma<T, 3, PRE, NTHR>, g, NTHR, sm, s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu,
+              flags, with_dt, ahead);
+}
+
+template <typename T>
+void launch_tile_tma_v(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                       const TileMesh &tm, const TileMaps &maps, const double4 *q_in, int kind, int lts, int fin,
+                       int keep_delu, int flags, int with_dt, int variant) {
+  if (variant == 1)
+    launch_tile_tma_t<T, false, kTileX * kTileY>(s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu, flags,
+                                                 with_dt);
+  else if (variant == 2)
+    launch_tile_tma_t<T, true, kTileThreadsWide>(s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu, flags,
+                                                 with_dt);
+  else
+    launch_tile_tma_t<T, true, kTileX * kTileY>(s, m, st, fp, bp, tm, maps, q_in, kind, lts, fin, keep_delu, flags,
+                                                with_dt);
+}
+
+int launch_tile_tma(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                    const TileMesh &tm, const TileMaps &maps, const double4 *q_in, int kind, int lts, int fuse_final,
+                    int keep_delu, int flags, int with_dt, int variant) {
+  if (fp.precision == 1)
+    launch_tile_tma_v<float>(s, m, st, fp, bp, tm, maps, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt,
+                             variant);
+  else
+    launch_tile_tma_v<double>(s, m, st, fp, bp, tm, maps, q_in, kind, lts, fuse_final, keep_delu, flags, with_dt,
+                              variant);
   return 1;
 }
 

@@ -12,6 +12,7 @@
 //   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU); face-based forms: the primitives again as
 //   q4[NT] (rho, u, v, p), gradients rec[NP][8] and face fluxes F[NF]
 #pragma once
+#include <cuda.h>  // CUtensorMap (the tensor maps of the TMA tile form; no driver library is linked)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -166,6 +167,21 @@ struct TileMesh {
   const double4 *fs;             // [nj + 1][ni] the same for the S faces
   const double *fsdy;
   const unsigned char *fso;
+  // The same face values as 48-byte records (nx, ny, dl, dx, dy, 1.0 when the owner is on the high
+  // side else 0.0), [nj][ni + 1] and [nj + 1][ni]: the tensors the TMA tile form loads.
+  const double *gw6, *gs6;
+  // TMA form: 1 = each block prefetches into L2 the inputs of the tile one wave ahead (option
+  // "tile_prefetch", off by default: on B200 the prefetches slowed the face phase more than they
+  // shortened the loads).
+  int prefetch_ahead;
+};
+
+// Tensor maps of the TMA tile form: the (rho, u, v, p) rows of the block as a 3-D tensor
+// (4 doubles, ni, nj) with a box of the tile and two rings, and the two face-record tensors
+// (6 doubles, ni + 1, nj) and (6 doubles, ni, nj + 1) with boxes of the faces the tile and its
+// one-ring halo touch.  Passed by value as a __grid_constant__ kernel parameter.
+struct TileMaps {
+  CUtensorMap q, gw, gs;
 };
 
 // Kernel launchers (stream-ordered, no host synchronisation).  Each returns the number of
@@ -210,6 +226,20 @@ int launch_tile_stage(cudaStream_t s, const DevMesh &m, DevState &st, const Flux
                       int flags, int with_dt);
 // Opt-in to the tile kernels' dynamic shared memory (0 if the device cannot give it).
 int tile_prepare();
+// TMA form of the tile stage (same arguments and results as launch_tile_stage, bit for bit): the
+// state rows of the tile and its two rings and the face records of the tile and its halo arrive
+// by three cp.async.bulk.tensor loads on one mbarrier, the stage inputs of the tile's cells by
+// cp.async, all issued at block start, so the gradient, face and update phases read only shared
+// memory.  maps.q must describe q_in.  variant 0: the stage inputs too are prefetched into
+// shared memory (256 threads, 2 blocks per SM); 1: they are loaded where used (3 blocks per SM);
+// 2: as 0 with 288 threads (two rounds of face fluxes instead of three).  tile_tma_prepare: the
+// shared-memory opt-in (0: not available).  tile_tma_boxes: the box extents the host encodes the
+// maps with.
+int launch_tile_tma(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, const BcParams &bp,
+                    const TileMesh &tm, const TileMaps &maps, const double4 *q_in, int kind, int lts, int fuse_final,
+                    int keep_delu, int flags, int with_dt, int variant);
+int tile_tma_prepare();
+void tile_tma_boxes(int q[3], int gw[3], int gs[3]);
 // Dynamic shared memory of the patch kernel for m.patch_rows, and the opt-in to it (0 if the
 // device cannot give it).
 size_t patch_smem_bytes(const DevMesh &m);

@@ -233,8 +233,14 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * frozen per step and three stages (CFD_INT_SSPRK3, CFD_INT_RK3_GPU_REF with local time stepping)
  * run each stage as one kernel: a thread block per tile of 32 x 8 cells stages the (rho, u, v, p)
  * rows of the tile and two rings around it in shared memory and forms the gradients, face fluxes,
- * gather and update of its cells there; default 1 where available, else 0 and setting it is
- * CFD_ERR_BAD_ARG).
+ * gather and update of its cells there.  1: each phase loads what it reads; 2: the TMA form, in
+ * which the tile's state rows and face records arrive by tensor bulk copies (cp.async.bulk.tensor)
+ * and its cells' stage inputs by cp.async, all issued at block start; 3: the TMA form with the
+ * stage inputs loaded where used (three blocks per SM); 4: form 2 with 288 threads per block.
+ * Default 2 where the device offers the tensor copies, else 1 where the form applies, else 0 and
+ * setting it is CFD_ERR_BAD_ARG),
+ * "tile_prefetch" (tile forms 2-4: each block also prefetches into L2 the inputs of the tile that
+ * starts one wave later; default 0).
  * None of the options changes a state bit (the persistent form sums the error norms in another
  * order). */
 cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value);

@@ -1,6 +1,8 @@
 """The tile form (reorder = 4 on a structured block: one thread block per 32 x 8 tile does the
 gradients, face fluxes, gather and stage update of its cells with the states of two rings around it
-in shared memory) against the C restatement and against the three-kernel form, bit for bit."""
+in shared memory) against the C restatement and against the three-kernel form, bit for bit, in both
+of its variants: tile_stage 1 (loads inside the phases) and 2 (the TMA form: tensor loads of the
+state rows and face records, cp.async of the stage inputs, all issued at block start)."""
 import numpy as np
 import pytest
 
@@ -54,15 +56,17 @@ def tile_launches(s, steps):
     return s.kernel_time("tile")[1]
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("base", sorted(BASES))
 @pytest.mark.parametrize("form", sorted(TILE_FORMS))
-def test_tile_form_matches_oracle(form, base, oracle_lib):
+def test_tile_form_matches_oracle(form, base, variant, oracle_lib):
     case = BASES[base]
     over = TILE_FORMS[form]
     m = make_mesh(case)
     U0 = initial_state(case, m)
     steps = 24
     s = cb.Solver(m, solver_config(case, reorder=4, **over))
+    s.set_option("tile_stage", variant)
     s.upload_state(U0)
     assert tile_launches(s, 4) == 4 * 3
     s.step(steps - 4)
@@ -81,7 +85,7 @@ def test_tile_form_equals_three_kernel_form(form):
     m = make_mesh(case)
     U0 = initial_state(case, m)
     outs = []
-    for tile, graph in ((1, 1), (0, 1), (1, 0)):
+    for tile, graph in ((1, 1), (0, 1), (1, 0), (2, 1), (2, 0), (3, 1), (4, 1), (4, 0)):
         s = cb.Solver(m, solver_config(case, reorder=4, **TILE_FORMS[form]))
         s.set_option("tile_stage", tile)
         s.set_option("use_graph", graph)
@@ -93,7 +97,8 @@ def test_tile_form_equals_three_kernel_form(form):
         np.testing.assert_allclose(err, outs[0][1], rtol=1e-12, atol=0)
 
 
-def test_tile_form_entry_points_interleave(oracle_lib):
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+def test_tile_form_entry_points_interleave(variant, oracle_lib):
     """Entry points called between tile steps (an upload, the reference's one-call stages) see and
     leave a consistent state: the tile form starts every step from the current rows."""
     case = BASES["cyl"]
@@ -101,6 +106,7 @@ def test_tile_form_entry_points_interleave(oracle_lib):
     m = make_mesh(case)
     U0 = initial_state(case, m)
     s = cb.Solver(m, solver_config(case, reorder=4, **over))
+    s.set_option("tile_stage", variant)
     o = oracle_lib.OracleRun(m, **oracle_params(case, **over))
     s.upload_state(U0)
     o.set_state(U0)
@@ -125,6 +131,34 @@ def test_tile_option_needs_block():
     case = BASES["cyl"]
     m = make_mesh(case)
     s = cb.Solver(m, solver_config(case, reorder=1, **TILE_FORMS["roe_vanleer_ssp"]))
-    with pytest.raises(cb.CfdError):
-        s.set_option("tile_stage", 1)
+    for v in (1, 2, 3, 4):
+        with pytest.raises(cb.CfdError):
+            s.set_option("tile_stage", v)
     s.set_option("tile_stage", 0)
+    t = cb.Solver(m, solver_config(case, reorder=4, **TILE_FORMS["roe_vanleer_ssp"]))
+    with pytest.raises(cb.CfdError):
+        t.set_option("tile_stage", 5)
+
+
+def test_tile_tma_form_on_the_benchmark_block(oracle_lib):
+    """The TMA form on a 256 x 96 O-grid (8 x 12 tiles, every tile interior or on one rim) with the
+    benchmark's scheme, 30 steps, bit for bit against the C restatement."""
+    m = cb.Mesh.half_cylinder(256, 96, 1.0, 4.0, 1.005)
+    NP = m.n_physical
+    rho, p = 1.0, 1.0 / 1.4
+    u = 3.0 * np.sqrt(1.4 * p / rho)
+    U = cb.conserved_from_primitive(np.full(NP, rho), np.full(NP, u), np.zeros(NP), np.full(NP, p))
+    U0 = np.zeros((m.n_total, 4))
+    U0[:NP] = U
+    U0[m.boundary[:, 3]] = U[m.boundary[:, 1]]
+    kw = dict(dissipation_type=3, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8, limiter=2,
+              muscl=1, integrator=2, inlet_rho=rho, inlet_p=p, inlet_bc=3, inlet_u=u, inlet_v=0.0)
+    s = cb.Solver(m, cb.default_config(device=0, reorder=4, **kw))
+    s.set_option("tile_stage", 2)
+    s.upload_state(U0)
+    assert tile_launches(s, 3) == 9
+    s.step(27)
+    o = oracle_lib.OracleRun(m, **kw)
+    o.set_state(U0)
+    o.iterate(30)
+    check_state(s.download(), o.state(), "tma")
