@@ -322,6 +322,7 @@ def run_ramps(args, rank, world):
         b = cb.Batch(meshes, cfg, inflow=inflow)
         if args.persistent:
             b.set_option("persistent", 1)  # one persistent kernel per RK stage, a CUDA graph per stage
+            b.set_option("persist_minb", args.persist_minb)
         b.upload_state(states)
         if world > 1:
             dist.barrier()
@@ -661,6 +662,9 @@ def main():
     ap.add_argument("--steady-ny", type=int, default=40)
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--persistent", type=int, default=1, help="--workload ramps: 1 = the persistent batched form")
+    ap.add_argument("--persist-minb", type=int, default=0, choices=[0, 4, 6, 8],
+                    help="--workload ramps: resident blocks per SM the persistent kernel is built for "
+                         "(0: the library's default for each precision)")
     ap.add_argument("--vl-steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--launch-options", default="auto",

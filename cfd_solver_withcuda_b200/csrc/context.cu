@@ -1391,6 +1391,20 @@ cfd_status cfd_set_option(cfd_ctx *ctx, const char *name, double value) {
     }
     return CFD_OK;
   }
+  if (n == "persist_minb") {
+    // Register budget of the persistent stage kernel (4, 6 or 8 resident blocks per SM); the
+    // co-resident grid follows.
+    if (value != 0.0 && value != 4.0 && value != 6.0 && value != 8.0)
+      return fail(CFD_ERR_BAD_ARG, "persist_minb must be 0, 4, 6 or 8");
+    drop_graphs(ctx);
+    ctx->fp.persist_minb = static_cast<int>(value);
+    if (ctx->persistent) {
+      const int g = persistent_grid(ctx->fp);
+      if (g <= 0) return fail(CFD_ERR_BAD_ARG, "cooperative launches are not available on this device");
+      ctx->persist_grid = std::min(g, ctx->partial_blocks);
+    }
+    return CFD_OK;
+  }
   if (n == "barrier_timeout_test") {
     // Test of the bounded barrier: every barrier of the persistent form waits for `value` more
     // arrivals than the grid has, so each wait runs out and the run reports CFD_ERR_TIMEOUT.

@@ -226,6 +226,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "persistent" (face-based forms with a per-cell dt: each RK stage as one persistent cooperative
  * kernel over the cells, faces and cells again, with bounded grid barriers between the phases and
  * one CUDA graph per RK stage; default 0; the batched solves' form, see cfd_batch_set_option),
+ * "persist_minb" (the persistent kernel's register budget: built for 4, 6 or 8 resident blocks per
+ * SM; default 0: 6 in FP64 and 8 in the FP32-flux form, the faster of each on B200),
  * "barrier_timeout_test" (a test of the bounded barriers: every barrier of the persistent form
  * waits for `value` more blocks than it has, so each wait runs out and the step reports
  * CFD_ERR_TIMEOUT; default 0),

@@ -69,11 +69,13 @@ def test_batch_converged_instances_freeze():
     assert res["cell_updates"] == sum(int(k) * c[0].n_physical for c, k in zip(cases, sto))
 
 
+@pytest.mark.parametrize("minb", [0, 4, 6, 8])
 @pytest.mark.parametrize("precision", [cb.PREC_FP64, cb.PREC_FP32_FLUX])
-def test_persistent_batch_equals_three_kernel_batch(precision):
+def test_persistent_batch_equals_three_kernel_batch(precision, minb):
     """The persistent form (one cooperative launch per RK stage over the (instance, block) work
     lists, one CUDA graph per stage) gives every instance the bits of the three-kernel form, also
-    when instances freeze at the tolerance in the middle of the run."""
+    when instances freeze at the tolerance in the middle of the run, for every register budget of
+    the persistent kernel."""
     specs = [(24, 12, 1.5), (64, 32, 2.2), (16, 8, 3.0), (40, 24, 2.6), (12, 6, 2.0)]
     cases = [ramp_case(*sp) for sp in specs]
     out = []
@@ -81,6 +83,7 @@ def test_persistent_batch_equals_three_kernel_batch(precision):
         b = cb.Batch([c[0] for c in cases], config(precision=precision, limiter=cb.LIM_MINMOD),
                      inflow=[c[2] for c in cases])
         b.set_option("persistent", persistent)
+        b.set_option("persist_minb", minb)
         b.upload_state([c[1] for c in cases])
         res = b.run(max_steps=1500, tol=1e-4, check_every=50)
         out.append((res, b.download_state()))
