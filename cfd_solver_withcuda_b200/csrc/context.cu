@@ -1301,7 +1301,7 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     if (cudaMemset(ctx->qbuf[q], 0, (size_t)NT * sizeof(double4)) != cudaSuccess)
       return bail(fail(CFD_ERR_CUDA, "memset failed"));
   }
-  ctx->tile_stage = ctx->tile_ok ? 1 : 0;
+  ctx->tile_stage = 0;
   if (ctx->tile_ok && tile_tma_prepare()) {
     double4 *bufs[3] = {ctx->ds.q4, ctx->qbuf[0], ctx->qbuf[1]};
     int bq[3], bw[3], bs[3];
@@ -1313,7 +1313,6 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
     ok = ok && encode_tensor_3d(&ctx->tmap_gw, tm.gw6, 6, tm.ni + 1, tm.nj, bw);
     ok = ok && encode_tensor_3d(&ctx->tmap_gs, tm.gs6, 6, tm.ni, tm.nj + 1, bs);
     ctx->tile_tma_ok = ok;
-    if (ok) ctx->tile_stage = 2;
   }
   for (int q = 0; q < 2 && m.npatch > 0; q++) {
     if ((s = ctx_alloc(ctx, (void **)&ctx->pbuf[q], 5 * (size_t)NT * dsz)) != CFD_OK) return bail(s);

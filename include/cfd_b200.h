@@ -239,8 +239,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * which the tile's state rows and face records arrive by tensor bulk copies (cp.async.bulk.tensor)
  * and its cells' stage inputs by cp.async, all issued at block start; 3: the TMA form with the
  * stage inputs loaded where used (three blocks per SM); 4: form 2 with 288 threads per block.
- * Default 2 where the device offers the tensor copies, else 1 where the form applies, else 0 and
- * setting it is CFD_ERR_BAD_ARG),
+ * Default 0 (on B200 the three kernels are faster), tried by cfd_autotune; where the form does not
+ * apply (or, for 2-4, the device offers no tensor copies) setting it is CFD_ERR_BAD_ARG),
  * "tile_prefetch" (tile forms 2-4: each block also prefetches into L2 the inputs of the tile that
  * starts one wave later; default 0).
  * None of the options changes a state bit (the persistent form sums the error norms in another
