@@ -2254,7 +2254,10 @@ __global__ void __launch_bounds__(NTHR, PRE ? 2 : 3)
   const bool landed = tma_bar_wait(bar, 0);
   asm volatile("cp.async.wait_all;" ::: "memory");
   if (__syncthreads_or(!landed)) {
+    // Record the timeout, then give the copies in flight one more bounded wait before the block
+    // (and its shared memory) goes away.
     if (tid == 0) atomicCAS(st.status, 0, 5 /* CFD_ERR_TIMEOUT */);
+    tma_bar_wait(bar, 0);
     return;
   }
 #pragma unroll
