@@ -955,7 +955,13 @@ def main():
                "config": {"workload": WORKLOAD, "cells": NP, "ghost_cells": m.n_ghost, "global_cells": world * NP,
                           "parallelism": "replicas (one independent solve per GPU)" if world > 1 else "single GPU",
                           "l2": "working set %.0f MB > 126 MB L2 (no flush needed)" % (s.device_bytes / 1e6),
-                          "cuda_graph": True, "launch_options": tuned[0] if tuned else None},
+                          "cuda_graph": True, "launch_options": tuned[0] if tuned else None,
+                          "parity": "bit-identical to the C restatement of the gradient-MUSCL form (parity "
+                                    "unpinned against the reference, which has no such scheme; its shared pieces "
+                                    "-- Roe average and dissipation, EOS, limiter functions, BCs -- are pinned to "
+                                    "the reference, and a linear field gives the exact face flux); the reference's "
+                                    "own scheme is forms.reference_roe2_minmod_rk3, bit-identical to the "
+                                    "reference"},
                "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                        "mode": "independent one-step solves, %d contexts on %d streams (a solve's copies "
