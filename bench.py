@@ -651,8 +651,8 @@ def main():
     ap.add_argument("--conv-mesh", default="1024x512", help="--workload convergence: O-grid cells NTxNR")
     ap.add_argument("--ws-nx", type=int, default=64)
     ap.add_argument("--ws-ny", type=int, default=32)
-    ap.add_argument("--ws-train", type=int, default=192)
-    ap.add_argument("--ws-test", type=int, default=64)
+    ap.add_argument("--ws-train", type=int, default=2000)
+    ap.add_argument("--ws-test", type=int, default=256)
     ap.add_argument("--ws-tol", type=float, default=1e-8)
     ap.add_argument("--ws-plain", type=int, default=8, help="held-out members the plain path is timed on")
     ap.add_argument("--ws-epochs", type=int, default=200)
