@@ -521,7 +521,13 @@ def run_convergence(args, rank, world):
         "van_albada_entropy_fix": {"limiter": 4, "entropy_fix_linear": 0.4},
         "minmod_entropy_fix": {"limiter": 1, "entropy_fix_linear": 0.4},
         "minmod_entropy_fix_shock_fix": {"limiter": 1, "entropy_fix_linear": 0.4, "shock_fix": 0.15},
+        "minmod_rusanov": {"limiter": 1, "shock_fix": 1e-12},
+        "van_leer_rusanov": {"limiter": 2, "shock_fix": 1e-12},
+        "van_albada_rusanov": {"limiter": 4, "shock_fix": 1e-12},
+        "minmod_entropy_fix_shock_fix_0.05": {"limiter": 1, "entropy_fix_linear": 0.4, "shock_fix": 0.05},
     }
+    if args.conv_variants:
+        variants = {k: v for k, v in variants.items() if k in args.conv_variants.split(",")}
     _, _, kw = workload_state(cb)
     out = {"metric": "L2 density residual / first value", "unit": "ratio", "higher_is_better": False,
            "config": {"workload": "half_cylinder_convergence_%dx%d" % (nt, nr), "max_steps": args.max_steps,
@@ -649,6 +655,8 @@ def main():
     ap.add_argument("--e2e-contexts", type=int, default=3, help="contexts the end-to-end jobs rotate over")
     ap.add_argument("--workload", default="halfcyl", choices=["halfcyl", "ramps", "bump", "warmstart", "convergence"])
     ap.add_argument("--conv-mesh", default="1024x512", help="--workload convergence: O-grid cells NTxNR")
+    ap.add_argument("--conv-variants", default="", help="--workload convergence: comma-separated subset of the "
+                    "variants (default: all)")
     ap.add_argument("--ws-nx", type=int, default=64)
     ap.add_argument("--ws-ny", type=int, default=32)
     ap.add_argument("--ws-train", type=int, default=2000)
