@@ -2267,6 +2267,8 @@ __global__ void __launch_bounds__(NTHR, PRE ? 2 : 3)
     if (r < NR) scode[r] = code_r[h];
   }
   __syncthreads();
+  // Every thread has passed its wait: the mbarrier is retired.
+  if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
 
   // L2 prefetch of the inputs of tile blockIdx.x + ahead (the tile that starts on this SM's slot in
   // the next wave, ahead = resident blocks of the grid), while this tile computes: its three tensor
