@@ -486,7 +486,7 @@ def run_warmstart(args, rank, world):
         return
     r = ws.run_experiment(nx=args.ws_nx, ny=args.ws_ny, n_train=args.ws_train, n_test=args.ws_test,
                           tol=args.ws_tol, max_steps=args.max_steps, check_every=args.check_every,
-                          epochs=args.ws_epochs, seed=args.seed, n_plain=args.ws_plain)
+                          epochs=args.ws_epochs, seed=args.seed, n_plain=args.ws_plain, engine=args.ws_engine)
     out = {"metric": "wall-time speed-up to L2 density residual %g, chosen (warm start + batch + FP32 flux) vs "
                      "plain FP64" % args.ws_tol,
            "value": r["speedup_chosen_vs_plain"], "unit": "x", "n_gpus": world, "higher_is_better": True,
@@ -664,6 +664,8 @@ def main():
     ap.add_argument("--ws-tol", type=float, default=1e-8)
     ap.add_argument("--ws-plain", type=int, default=8, help="held-out members the plain path is timed on")
     ap.add_argument("--ws-epochs", type=int, default=200)
+    ap.add_argument("--ws-engine", type=int, default=0, choices=[0, 1],
+                    help="--workload warmstart: dense blocks on mma.sync (0) or tcgen05 (1)")
     ap.add_argument("--bump-nx", type=int, default=2520)
     ap.add_argument("--bump-ny", type=int, default=840)
     ap.add_argument("--steady-max-steps", type=int, default=200000,

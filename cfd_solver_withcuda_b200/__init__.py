@@ -86,7 +86,7 @@ class MlpBwd(ctypes.Structure):
     """cfd_mlp_bwd."""
     _fields_ = [("rows", ctypes.c_int), ("in_width", ctypes.c_int), ("out", ctypes.c_int), ("dy", ctypes.c_void_p),
                 ("ld_dy", ctypes.c_int), ("z1", ctypes.c_void_p), ("w1", ctypes.c_void_p), ("w2", ctypes.c_void_p),
-                ("dz1", ctypes.c_void_p), ("dx", ctypes.c_void_p), ("ld_dx", ctypes.c_int)]
+                ("dz1", ctypes.c_void_p), ("dx", ctypes.c_void_p), ("ld_dx", ctypes.c_int), ("engine", ctypes.c_int)]
 
 
 class MlpWgrad(ctypes.Structure):

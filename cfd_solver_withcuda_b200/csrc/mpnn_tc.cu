@@ -9,7 +9,8 @@
 //
 //   k_mlp_fwd    y and the hidden pre-activation z1 (kept for the backward pass), one 64-row tile
 //                per loop trip, weights staged once per block.
-//   k_mlp_bwd    dz1 = (dy W2) * silu'(z1) and dx = dz1 W1 for a tile of rows.
+//   k_mlp_bwd    dz1 = (dy W2) * silu'(z1) and dx = dz1 W1 for a tile of rows (k_mlp_bwd_tc: the
+//                same on tcgen05).
 //   k_wgrad      dW = dz^T x and db = sum of dz over the rows: each block accumulates its tiles in
 //                registers and writes one partial; k_wgrad_reduce sums the partials in block
 //                order, so the gradients are the same on every run.
@@ -479,6 +480,139 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(BwdArgs a) {
   }
 }
 
+// The backward data path on the tensor cores: dS = dY W2 (M = 128 rows, N = 64, K = the block's
+// output width rounded up to 16), dz1 = dS * silu'(z1), dX = dz1 W1 (N = the input width rounded up
+// to 16, K = 64), the same two-MMA chain as the forward with the transposed weights as the B
+// operands: W2^T as (n = 64, k = out) and W1^T as (n = in, k = 64), all BF16 in the canonical
+// K-major layout, FP32 accumulators in 64 + in columns of tensor memory.  BF16 rounding of dY, the
+// weights and dz1 as in k_mlp_bwd, so the results agree up to the FP32 summation order.
+__global__ void __launch_bounds__(128) k_mlp_bwd_tc(BwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t smb[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  const int Kp = (a.K + 15) & ~15, N2p = (a.N2 + 15) & ~15;
+  uint8_t *sDY = smb;                                 // [128 x N2p]  dY rows
+  uint8_t *sW2T = sDY + (size_t)TM_TC * N2p * 2;      // [64 x N2p]   W2^T
+  uint8_t *sDZ = sW2T + (size_t)HID * N2p * 2;        // [128 x 64]   dz1
+  uint8_t *sW1T = sDZ + (size_t)TM_TC * HID * 2;      // [Kp x 64]    W1^T
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < HID * N2p; e += blockDim.x) {
+    const int n = e / N2p, k = e - n * N2p;  // B(n, k) = W2[k][n]
+    *reinterpret_cast<uint16_t *>(sW2T + canon_off(n, k, HID)) = k < a.N2 ? bf(a.w2[k * HID + n]) : 0;
+  }
+  for (int e = tid; e < Kp * HID; e += blockDim.x) {
+    const int n = e / HID, k = e - n * HID;  // B(n, k) = W1[k][n]
+    *reinterpret_cast<uint16_t *>(sW1T + canon_off(n, k, Kp)) = n < a.K ? bf(a.w1[k * a.K + n]) : 0;
+  }
+  const uint32_t bar_a = smem_u32(&bar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(256));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+    abort_sh = 0;
+  }
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t d1 = tmem, d2 = tmem + 64;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+  const uint32_t idesc1 = make_idesc(TM_TC, HID), idesc2 = make_idesc(TM_TC, Kp);
+  uint32_t parity = 0;
+  const int ntiles = (a.M + TM_TC - 1) / TM_TC;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = tile * TM_TC;
+    for (int e = tid; e < TM_TC * N2p; e += blockDim.x) {
+      const int r = e / N2p, k = e - r * N2p, row = r0 + r;
+      *reinterpret_cast<uint16_t *>(sDY + canon_off(r, k, TM_TC)) =
+          (row < a.M && k < a.N2) ? bf(a.dy[(size_t)row * a.ld_dy + k]) : 0;
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t ya = smem_u32(sDY), wa = smem_u32(sW2T);
+      for (int k0 = 0; k0 < N2p; k0 += 16) {
+        const uint64_t da = make_sdesc(ya + (uint32_t)((k0 >> 3) * (TM_TC >> 3) * 128), TM_TC * 16, 128);
+        const uint64_t db = make_sdesc(wa + (uint32_t)((k0 >> 3) * (HID >> 3) * 128), HID * 16, 128);
+        tc_mma(d1, da, db, idesc1, k0 > 0 ? 1u : 0u);
+      }
+      tc_commit(bar_a);
+    }
+    if (!mbar_wait(bar_a, parity)) {
+      if (tid == 0) atomicExch(&g_tc_status, 5 /* CFD_ERR_TIMEOUT */);
+      abort_sh = 1;
+    }
+    parity ^= 1u;
+    __syncthreads();
+    if (abort_sh) break;
+    tc_fence_after();
+    const int r = 32 * warp + (tid & 31), row = r0 + r;
+#pragma unroll
+    for (int c0 = 0; c0 < HID; c0 += 16) {
+      float v[16];
+      tmem_ld16(d1 + lane_base + c0, v);
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        float d = 0.0f;
+        if (row < a.M) {
+          d = v[j] * dsilu_f(a.z1[(size_t)row * HID + c0 + j]);
+          a.dz1[(size_t)row * HID + c0 + j] = d;
+        }
+        *reinterpret_cast<uint16_t *>(sDZ + canon_off(r, c0 + j, TM_TC)) = bf(d);
+      }
+    }
+    if (a.dx) {
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t za = smem_u32(sDZ), wa = smem_u32(sW1T);
+        for (int k0 = 0; k0 < HID; k0 += 16) {
+          const uint64_t da = make_sdesc(za + (uint32_t)((k0 >> 3) * (TM_TC >> 3) * 128), TM_TC * 16, 128);
+          const uint64_t db = make_sdesc(wa + (uint32_t)((k0 >> 3) * (Kp >> 3) * 128), Kp * 16, 128);
+          tc_mma(d2, da, db, idesc2, k0 > 0 ? 1u : 0u);
+        }
+        tc_commit(bar_a);
+      }
+      if (!mbar_wait(bar_a, parity)) {
+        if (tid == 0) atomicExch(&g_tc_status, 5);
+        abort_sh = 1;
+      }
+      parity ^= 1u;
+      __syncthreads();
+      if (abort_sh) break;
+      tc_fence_after();
+      for (int c0 = 0; c0 < Kp; c0 += 16) {
+        float v[16];
+        tmem_ld16(d2 + lane_base + c0, v);
+        if (row < a.M) {
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            const int c = c0 + j;
+            if (c < a.K) a.dx[(size_t)row * a.ld_dx + c] = v[j];
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  // After a timed-out wait the MMAs may still be in flight: wait for them (bounded) before the
+  // tensor memory is released.
+  if (abort_sh) mbar_wait(bar_a, parity);
+  tc_fence_after();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+}
+
 struct WgArgs {
   int M, N, K, nseg;
   SegDev seg[3];
@@ -661,6 +795,10 @@ size_t tc_smem(int K, int N2) {
   const int Kp = (K + 15) & ~15, N2p = N2 <= 16 ? 16 : 64;
   return 2 * ((size_t)TM_TC * Kp + (size_t)HID * Kp + (size_t)TM_TC * HID + (size_t)N2p * HID);
 }
+size_t bwd_tc_smem(int K, int N2) {
+  const int Kp = (K + 15) & ~15, N2p = (N2 + 15) & ~15;
+  return 2 * ((size_t)TM_TC * N2p + (size_t)HID * N2p + (size_t)TM_TC * HID + (size_t)Kp * HID);
+}
 size_t bwd_smem(int K, int N2) {
   const int Kp = (K + 15) & ~15, N2p = (N2 + 15) & ~15, LDN = N2p + 8;
   return sizeof(uint16_t) * ((size_t)HID * LDN + (size_t)Kp * LDH + (size_t)TM * LDN + (size_t)TM * LDH);
@@ -738,6 +876,16 @@ cfd_status cfd_mpnn_mlp_backward(const cfd_mlp_bwd *p, void *stream) {
     return bad("cfd_mpnn_mlp_backward: bad argument");
   if (p->rows == 0) return CFD_OK;
   BwdArgs a{p->rows, p->in_width, p->out, p->dy, p->ld_dy, p->z1, p->w1, p->w2, p->dz1, p->dx, p->ld_dx};
+  if (p->engine == 1) {
+    // tcgen05 form: one CTA per SM (at least 120 KB of shared memory each), each holding 256 of
+    // the SM's 512 tensor-memory columns.
+    const size_t need = bwd_tc_smem(a.K, a.N2) + 16 * 1024, sm = need > 120 * 1024 ? need : 120 * 1024;
+    set_smem(k_mlp_bwd_tc, sm);
+    const int ntiles = (a.M + TM_TC - 1) / TM_TC;
+    const int grid = ntiles < sm_count() ? ntiles : sm_count();
+    k_mlp_bwd_tc<<<grid, 128, sm, static_cast<cudaStream_t>(stream)>>>(a);
+    return status_of("cfd_mpnn_mlp_backward (tcgen05)");
+  }
   const size_t sm = bwd_smem(a.K, a.N2);
   set_smem(k_mlp_bwd, sm);
   const int ntiles = (a.M + TM - 1) / TM;

@@ -279,10 +279,14 @@ class Net:
 
     HIDDEN = 64
 
-    def __init__(self, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=1):
+    def __init__(self, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=0, bwd_engine=None):
         torch = _torch()
         W = self.HIDDEN
-        self.engine = engine  # forward blocks: 1 tcgen05 (tensor-memory accumulators), 0 mma.sync
+        # Dense blocks: engine 0 mma.sync m16n8k16, 1 tcgen05.mma with tensor-memory accumulators
+        # (forward; the backward data path follows unless bwd_engine is given).  At this network's
+        # sizes (K <= 192, N <= 64) both are bound by operand staging, and 0 trains faster on B200.
+        self.engine = engine
+        self.bwd_engine = engine if bwd_engine is None else bwd_engine
         self.L, self.out, self.device = layers, out, torch.device(device)
         self.dims = {"enc_n": (node_in, W), "enc_e": (edge_in, W), "dec": (W, out)}
         for l in range(layers):
@@ -380,6 +384,7 @@ class Net:
         a.dy, a.ld_dy, a.z1 = _ptr(dy), dy.stride(0), _ptr(z1)
         a.w1, a.w2, a.dz1 = _ptr(w1), _ptr(w2), _ptr(b["dz"])
         a.dx, a.ld_dx = _ptr(dx), dx.stride(0) if dx is not None else 0
+        a.engine = self.bwd_engine
         cb._check(cb.lib().cfd_mpnn_mlp_backward(ctypes.byref(a), _stream(dy)))
 
     def _wgrad(self, dz, rows, segs, dw, db):
@@ -459,7 +464,7 @@ class Net:
                                          lr, betas[0], betas[1], eps, self.steps, _stream(self.flat)))
 
 
-def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=1):
+def build_model(width=64, layers=6, node_in=9, edge_in=5, out=4, seed=0, device="cuda", engine=0):
     """The surrogate (about 187k parameters at width 64, 6 layers)."""
     assert width == Net.HIDDEN
     return Net(layers=layers, node_in=node_in, edge_in=edge_in, out=out, seed=seed, device=device, engine=engine)
@@ -518,7 +523,8 @@ def _with_ghosts(mesh, U_phys):
 
 
 def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-8, max_steps=400000, check_every=500, epochs=200,
-                   batch=8, lr=1e-3, seed=2024, device="cuda", log=None, switch_tol=1e-5, n_plain=8, diverge=10.0):
+                   batch=8, lr=1e-3, seed=2024, device="cuda", log=None, switch_tol=1e-5, n_plain=8, diverge=10.0,
+                   engine=0):
     """The whole warm-start study; returns a dict of measured figures.
 
     1. Training members solved from the freestream start by the FP64 batched solver.
@@ -553,8 +559,9 @@ def run_experiment(nx=64, ny=32, n_train=192, n_test=64, tol=1e-8, max_steps=400
     norm = [((t - mu) / sd).astype(np.float32) for t in targets]
 
     # 2. Surrogate training.
-    model = build_model()
+    model = build_model(engine=engine)
     out["parameters"] = model.n_params
+    out["engine"] = "tcgen05" if engine == 1 else "mma.sync"
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     losses = train(model, graph, [f[0] for f in feats[tr]], [f[1] for f in feats[tr]], norm, epochs=epochs,

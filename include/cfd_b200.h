@@ -451,6 +451,7 @@ typedef struct {
   float *dz1;              /* out [rows][64] */
   float *dx;               /* out (optional) [rows][ld_dx] */
   int ld_dx;
+  int engine;              /* 0: mma.sync; 1: tcgen05.mma with tensor-memory accumulators */
 } cfd_mlp_bwd;
 cfd_status cfd_mpnn_mlp_backward(const cfd_mlp_bwd *a, void *stream);
 

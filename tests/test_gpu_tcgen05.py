@@ -85,3 +85,42 @@ def test_tcgen05_network_trains_like_mma_sync():
     net = ws.build_model(engine=1)
     losses = ws.train(net, g, [f[0] for f in feats], [f[1] for f in feats], targets, epochs=20, batch=2)
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+@pytest.mark.parametrize("K,N2,rows", [(9, 64, 1000), (5, 64, 4096), (192, 64, 1000), (192, 64, 128 * 300 + 7),
+                                       (128, 64, 777), (64, 4, 1000), (64, 4, 128 * 200)])
+def test_tcgen05_backward_matches_mma_sync_and_restatement(K, N2, rows):
+    """The backward data path (dz1 = (dy W2) * silu'(z1), dx = dz1 W1) on tcgen05 (engine 1)
+    against the mma.sync kernel (engine 0) and the CPU restatement with BF16 operands, for every
+    block shape of the network, with and without dx."""
+    import torch
+    from oracle import mpnn_ref as R
+    rng = np.random.default_rng(K * 1000 + N2 + rows)
+    W1, W2 = rng.normal(size=(64, K)) / np.sqrt(K), rng.normal(size=(N2, 64)) / 8.0
+    dy, z1 = rng.normal(size=(rows, N2)), rng.normal(size=(rows, 64))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    tw1, tw2, tdy, tz1 = T(W1), T(W2), T(dy), T(z1)
+    outs = []
+    for engine in (0, 1):
+        for with_dx in (True, False):
+            dz1 = torch.full((rows, 64), np.nan, device="cuda")
+            dx = torch.full((rows, K), np.nan, device="cuda") if with_dx else None
+            a = cb.MlpBwd()
+            a.rows, a.in_width, a.out = rows, K, N2
+            a.dy, a.ld_dy, a.z1 = tdy.data_ptr(), N2, tz1.data_ptr()
+            a.w1, a.w2, a.dz1 = tw1.data_ptr(), tw2.data_ptr(), dz1.data_ptr()
+            a.dx, a.ld_dx = (dx.data_ptr(), K) if with_dx else (None, 0)
+            a.engine = engine
+            cb._check(cb.lib().cfd_mpnn_mlp_backward(ctypes.byref(a), None))
+            torch.cuda.synchronize()
+            outs.append((dz1.cpu().numpy(), dx.cpu().numpy() if with_dx else None))
+    st = ctypes.c_int(-1)
+    cb._check(cb.lib().cfd_mpnn_status(ctypes.byref(st), 1))
+    assert st.value == 0
+    dz_ref = (R.bf16(dy.astype(np.float32)) @ R.bf16(W2.astype(np.float32))) * R.dsilu(z1.astype(np.float32))
+    dx_ref = R.bf16(dz_ref) @ R.bf16(W1.astype(np.float32))
+    (dz0, dx0), (dz0b, _), (dz1_, dx1), (dz1b, _) = outs
+    assert np.all(np.isfinite(dz1_)) and np.all(np.isfinite(dx1))
+    assert np.array_equal(dz1_, dz1b) and np.array_equal(dz0, dz0b)
+    assert _rel(dz1_, dz0) < 1e-5 and _rel(dx1, dx0) < 1e-4
+    assert _rel(dz1_, dz_ref) < 1e-5 and _rel(dx1, dx_ref) < 1e-4
