@@ -45,18 +45,19 @@ cfd_status fail(cfd_status s, const std::string &msg) {
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-bool encode_tensor_3d(CUtensorMap *map, const void *base, int d0, int d1, int d2, const int box[3]) {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !f) {
-      cudaGetLastError();
-      return false;
-    }
-    fn = reinterpret_cast<EncodeTiledFn>(f);
+EncodeTiledFn lookup_encode_tiled() {
+  void *f = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !f) {
+    cudaGetLastError();
+    return nullptr;
   }
+  return reinterpret_cast<EncodeTiledFn>(f);
+}
+bool encode_tensor_3d(CUtensorMap *map, const void *base, int d0, int d1, int d2, const int box[3]) {
+  static const EncodeTiledFn fn = lookup_encode_tiled();  // looked up once (thread-safe initialisation)
+  if (!fn) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
   const cuuint64_t strides[2] = {(cuuint64_t)d0 * 8, (cuuint64_t)d0 * 8 * d1};
   const cuuint32_t bx[3] = {(cuuint32_t)box[0], (cuuint32_t)box[1], (cuuint32_t)box[2]};
