@@ -43,6 +43,23 @@ def test_cuda_matches_reference_fixture(name, reorder):
         assert_bits_equal(tags, g["amr_tags"], "AMR tags")
 
 
+@pytest.mark.parametrize("opts", [dict(flux_lanes=4), dict(flux_minb=6), dict(flux_minb=8)])
+@pytest.mark.parametrize("name", sorted(n for n in CASES if not CASES[n].get("weno")))
+def test_per_cell_flux_variants_match_reference_fixture(name, opts):
+    """The per-cell flux kernel's launch variants (four lanes per cell, the register-capped
+    second-order Roe builds) against the reference's own outputs, bit for bit."""
+    case = CASES[name]
+    g = load_golden(name)
+    m = make_mesh(case)
+    s = cb.Solver(m, solver_config(case))
+    for k, v in opts.items():
+        s.set_option(k, v)
+    s.upload_state(g["U0"])
+    info = s.step(case["steps"], case.get("t_end", 0.0))
+    check_state(s.download(), g, "%s %s" % (name, opts))
+    assert_bits_equal(np.array([info.min_dt]), g["min_dt"], "Min_dt")
+
+
 @pytest.mark.parametrize("name", ["sod_roe2_rk3", "cyl_roe2_lts", "bump_roe2_rk3", "sod_llf1_rk3"])
 def test_entry_points_one_by_one(name, oracle_lib):
     """Apply_Boundary_Conditions / Evaluate_Cell_Net_Flux / Runge_Kutta_Method | Explicit_Method /
