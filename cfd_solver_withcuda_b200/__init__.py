@@ -15,7 +15,15 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libcfd_b200.so")
 
 CFD_OK = 0
+CFD_ERR_BAD_ARG = 1
+CFD_ERR_CUDA = 2
+CFD_ERR_NONPHYSICAL = 3
+CFD_ERR_DT_NONPOSITIVE = 4
 CFD_ERR_TIMEOUT = 5
+CFD_ERR_DIVERGED = 6
+CFD_ERR_MESH = 7
+CFD_ERR_IO = 8
+CFD_ERR_NO_DEVICE = 9
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NONPHYSICAL", 4: "DT_NONPOSITIVE", 5: "TIMEOUT",
                 6: "DIVERGED", 7: "MESH", 8: "IO", 9: "NO_DEVICE"}
 
