@@ -28,7 +28,7 @@ STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "NONPHYSICAL", 4: "DT_NONPO
                 6: "DIVERGED", 7: "MESH", 8: "IO", 9: "NO_DEVICE"}
 
 BC_INLET, BC_EXIT, BC_WALL, BC_SYMMETRY = 0, 1, 2, 3
-DISS_LLF, DISS_ROE, DISS_AUSM, DISS_HLLC, DISS_AUSM_GPU = 1, 3, 6, 7, 8
+DISS_LLF, DISS_MOVERS, DISS_ROE, DISS_RICCA, DISS_MOVERS_NWSC, DISS_AUSM, DISS_HLLC, DISS_AUSM_GPU = 1, 2, 3, 4, 5, 6, 7, 8
 LIM_REF_MINMOD, LIM_MINMOD, LIM_VANLEER, LIM_SUPERBEE, LIM_VANALBADA = 0, 1, 2, 3, 4
 INT_REFERENCE, INT_RK4, INT_SSPRK3, INT_RK3_GPU_REF, INT_RK4_GPU_REF = 0, 1, 2, 3, 4
 INLET_SUPERSONIC, INLET_SUBSONIC_REF, INLET_TOTAL_PT, INLET_FIXED, INLET_FARFIELD = 0, 1, 2, 3, 4
@@ -65,7 +65,8 @@ class Config(ctypes.Structure):
                 ("inlet_t0", ctypes.c_double), ("exit_p", ctypes.c_double), ("r_gas", ctypes.c_double),
                 ("device", ctypes.c_int), ("stream", ctypes.c_void_p), ("weno", ctypes.c_int),
                 ("weno_characteristic", ctypes.c_int), ("entropy_fix_linear", ctypes.c_double),
-                ("shock_fix", ctypes.c_double)]
+                ("shock_fix", ctypes.c_double), ("movers_single_alpha", ctypes.c_int),
+                ("movers_entropy_fix", ctypes.c_int)]
 
 
 class FluxArrays(ctypes.Structure):

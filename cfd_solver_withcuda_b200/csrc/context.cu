@@ -789,9 +789,14 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
       return fail(CFD_ERR_MESH, "invalid boundary entry " + std::to_string(e));
   }
   const int diss = cfg->dissipation_type;
-  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && diss != CFD_DISS_AUSM && diss != CFD_DISS_HLLC &&
-      diss != CFD_DISS_AUSM_GPU)
+  if (diss < CFD_DISS_LLF || diss > CFD_DISS_AUSM_GPU)
     return fail(CFD_ERR_BAD_ARG, "dissipation type " + std::to_string(diss) + " is not available in this build");
+  const bool movers_family = diss == CFD_DISS_MOVERS || diss == CFD_DISS_RICCA || diss == CFD_DISS_MOVERS_NWSC;
+  if (movers_family && cfg->is_second_order && cfg->muscl)
+    return fail(CFD_ERR_BAD_ARG, "MOVERS, RICCA and MOVERS_NWSC are available in the reference's per-cell form "
+                                 "only (muscl = 0)");
+  if (movers_family && cfg->is_second_order && cfg->reconstruct_primitive)
+    return fail(CFD_ERR_BAD_ARG, "RICCA_2O and MOVERS_NWSC_2O limit the conserved variables (reconstruct_primitive = 0)");
   if (diss == CFD_DISS_AUSM_GPU && !(cfg->is_second_order && cfg->muscl))
     return fail(CFD_ERR_BAD_ARG, "the reference GPU AUSM face flux is available in the gradient-MUSCL form only");
   if (cfg->integrator < CFD_INT_REFERENCE || cfg->integrator > CFD_INT_RK4_GPU_REF)
@@ -1337,6 +1342,8 @@ cfd_status cfd_create(const cfd_mesh_desc *d, const cfd_config *cfg, cfd_ctx **o
 
   FluxParams &fp = ctx->fp;
   fp.dissipation = diss;
+  fp.movers_single = cfg->movers_single_alpha ? 1 : 0;
+  fp.movers_efix = cfg->movers_entropy_fix ? 1 : 0;
   fp.second_order = cfg->is_second_order;
   fp.limiter = cfg->limiter;
   fp.recon_prim = cfg->reconstruct_primitive;

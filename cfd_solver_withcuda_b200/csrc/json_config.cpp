@@ -222,10 +222,13 @@ std::string config_from_json(const std::string &text, cfd_config *cfg) {
     as_bool(sol->get("Local_Time_Stepping"), cfg->local_time_stepping);
     as_bool(sol->get("Is_WENO"), cfg->weno);
     as_bool(sol->get("Is_Char"), cfg->weno_characteristic);
+    as_bool(sol->get("Is_MOVERS_1"), cfg->movers_single_alpha);
+    as_bool(sol->get("Enable_Entropy_Fix"), cfg->movers_entropy_fix);
     const JVal *fs = sol->get("Flux_Scheme");
     if (fs && fs->kind == JVal::STR) {
-      int k = enum_from(fs, {"llf", "roe", "ausm", "hllc", "ausm_gpu"}, -1);
-      const int map[5] = {CFD_DISS_LLF, CFD_DISS_ROE, CFD_DISS_AUSM, CFD_DISS_HLLC, CFD_DISS_AUSM_GPU};
+      int k = enum_from(fs, {"llf", "roe", "ausm", "hllc", "ausm_gpu", "movers", "ricca", "movers_nwsc"}, -1);
+      const int map[8] = {CFD_DISS_LLF,      CFD_DISS_ROE,    CFD_DISS_AUSM,  CFD_DISS_HLLC,
+                          CFD_DISS_AUSM_GPU, CFD_DISS_MOVERS, CFD_DISS_RICCA, CFD_DISS_MOVERS_NWSC};
       if (k >= 0) cfg->dissipation_type = map[k];
     }
     cfg->limiter = enum_from(sol->get("Limiter_Type"), {"minmod_reference", "minmod", "vanleer", "superbee", "vanalbada"},

@@ -465,7 +465,7 @@ __device__ __forceinline__ void load_cell(const DevMesh &m, const DevState &st, 
   q.vc = prim[2 * NT + c];
   q.pc = prim[3 * NT + c];
   q.ac = prim[4 * NT + c];
-  if (DISS == 1 || DISS == 6 || DISS == 7 || ORDER == 2) {
+  if (DISS == 1 || DISS == 2 || DISS == 5 || DISS == 6 || DISS == 7 || ORDER == 2) {
 #pragma unroll
     for (int k = 0; k < 4; k++) q.Uc[k] = us.get(k, c);
   }
@@ -525,6 +525,34 @@ __device__ __forceinline__ void face_contrib(const DevMesh &m, const DevState &s
               (qL[3] / kGM1 + 0.5 * qL[0] * (qL[1] * qL[1] + qL[2] * qL[2]));
     }
     roe_2o<double>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, nx, ny, dl, dU, D);
+  } else if (DISS == 2 || DISS == 4 || DISS == 5) {
+    // MOVERS, RICCA, MOVERS_NWSC and their second-order forms (src/MOVERS.cpp, src/RICCA.cpp,
+    // src/MOVERS_NWSC.cpp); RICCA_2O and MOVERS_NWSC_2O take the limited conserved jump of
+    // Second_Order_Limiter (src/Limiters.cpp:97-200), MOVERS_2O does not call it.
+    double UR[4], dU2[4] = {0.0, 0.0, 0.0, 0.0};
+    if (DISS != 4 || ORDER == 2) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) UR[k] = us.get(k, N);
+    }
+    if (ORDER == 2 && DISS != 2) {
+      const int n2 = m.n2[idx];
+      const double d1 = m.d1l[idx], d2 = m.d2l[idx];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const double q2 = us.get(k, n2);
+        const double phi = limited_slope<double>(fp.limiter, q.Uc[k], UR[k], q2, d1, d2, fp.zeta, fp.zeta1);
+        const double VR = UR[k] + 0.5 * phi * d1;
+        const double VL = q.Uc[k] - 0.5 * phi * d1;
+        dU2[k] = VR - VL;
+      }
+    }
+    if (DISS == 2)
+      movers_diss<double, ORDER>(rc, uc, vc, pc, ac, rn, un, vn, pn, an, q.Uc, UR, nx, ny, dl, fp.movers_single,
+                                 fp.movers_efix, D);
+    else if (DISS == 4)
+      ricca_diss<double, ORDER>(rc, uc, vc, pc, rn, un, vn, pn, nx, ny, dl, dU2, D);
+    else
+      nwsc_diss<double, ORDER>(rc, uc, vc, pc, rn, un, vn, pn, q.Uc, UR, nx, ny, dl, dU2, D);
   } else if (DISS == 6 || DISS == 7) {
     // Reference forms of AUSM (src/Ausm_Flux.cpp:26-34, from U_Cells) and HLLC
     // (CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu:98-100): faces whose neighbour is a ghost are
@@ -2682,6 +2710,12 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
   if (fp.lanes == 1) {
     const int g = nblk(m.NP, kFluxBlock);
     if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 2 && !fp.second_order) k_flux<2, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 2) k_flux<2, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 4 && !fp.second_order) k_flux<4, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 4) k_flux<4, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 5 && !fp.second_order) k_flux<5, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 5) k_flux<5, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 6) k_flux<6, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 7) k_flux<7, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3 && fp.flux_minb == 6) k_flux<3, 2, 6><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
@@ -2691,6 +2725,12 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
   } else {
     const int g = nblk(4 * m.NP, kFlux4Block);
     if (fp.dissipation == 3 && !fp.second_order) k_flux4<3, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 2 && !fp.second_order) k_flux4<2, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 2) k_flux4<2, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 4 && !fp.second_order) k_flux4<4, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 4) k_flux4<4, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 5 && !fp.second_order) k_flux4<5, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 5) k_flux4<5, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 6) k_flux4<6, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 7) k_flux4<7, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 3) k_flux4<3, 2><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);

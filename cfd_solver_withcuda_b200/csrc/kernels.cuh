@@ -126,7 +126,9 @@ enum CtrlIdx : int {
 };
 
 struct FluxParams {
-  int dissipation;      // 1 LLF, 3 ROE, 6 AUSM, 7 HLLC
+  int dissipation;      // 1 LLF, 2 MOVERS, 3 ROE, 4 RICCA, 5 MOVERS_NWSC, 6 AUSM, 7 HLLC
+  int movers_single;    // MOVERS: the energy component's alpha for all four (the reference's Is_MOVERS_1)
+  int movers_efix;      // MOVERS: entropy fix of alpha (the reference's Enable_Entropy_Fix)
   int second_order;
   int limiter;
   int recon_prim;

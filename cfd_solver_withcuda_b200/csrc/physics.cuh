@@ -193,6 +193,178 @@ __device__ __forceinline__ int sign_ref(T a) {
   return (a > T(0.0)) - (a < T(0.0));
 }
 
+// Minimum(a,b,c), src/Utility_Files.cpp:15-23.
+template <typename T>
+__device__ __forceinline__ T min3_ref(T a, T b, T c) {
+  if ((a <= b) && (a <= c)) return a;
+  if ((b <= a) && (b <= c)) return b;
+  return c;
+}
+
+// Jump of the interface flux F(q_R).n dl - F(q_L).n dl of the MOVERS family
+// (src/MOVERS.cpp:114-117, src/RICCA.cpp:103-108, src/MOVERS_NWSC.cpp:80-83), in the reference's
+// association order.  `plus_pl` is the sign the reference gives the left pressure term of the two
+// momentum components: + in MOVERS, MOVERS_2O, RICCA, RICCA_2O and MOVERS_NWSC, - in
+// MOVERS_NWSC_2O (src/MOVERS_NWSC.cpp:183-184).
+template <typename T>
+__device__ __forceinline__ void movers_flux_jump(const T rL, const T uL, const T vL, const T pL, const T rR,
+                                                 const T uR, const T vR, const T pR, const T nx, const T ny,
+                                                 const T dl, const T VnL, const T VnR, bool plus_pl, T dF[4]) {
+  const T VmL = T(0.5) * (uL * uL + vL * vL);
+  const T VmR = T(0.5) * (uR * uR + vR * vR);
+  dF[0] = (rR * VnR - rL * VnL) * dl;
+  if (plus_pl) {
+    dF[1] = (rR * uR * VnR + pR * nx - rL * uL * VnL + pL * nx) * dl;
+    dF[2] = (rR * vR * VnR + pR * ny - rL * vL * VnL + pL * ny) * dl;
+  } else {
+    dF[1] = (rR * uR * VnR + pR * nx - rL * uL * VnL - pL * nx) * dl;
+    dF[2] = (rR * vR * VnR + pR * ny - rL * vL * VnL - pL * ny) * dl;
+  }
+  dF[3] = ((((pR / T(kGM1)) + rR * VmR) + pR) * VnR - (((pL / T(kGM1)) + rL * VmL) + pL) * VnL) * dl;
+}
+
+// Conserved jump rebuilt from the two cells' primitives (src/MOVERS.cpp:208-211, src/RICCA.cpp:96-100).
+template <typename T>
+__device__ __forceinline__ void prim_jump(const T rL, const T uL, const T vL, const T pL, const T rR, const T uR,
+                                          const T vR, const T pR, T dU[4]) {
+  dU[0] = rR - rL;
+  dU[1] = rR * uR - rL * uL;
+  dU[2] = rR * vR - rL * vL;
+  dU[3] = ((pR / T(kGM1)) + T(0.5) * rR * (uR * uR + vR * vR)) - ((pL / T(kGM1)) + T(0.5) * rL * (uL * uL + vL * vL));
+}
+
+// Condition_For_MOVERS, src/MOVERS.cpp:19-43 (epsilon 1e-10).
+template <typename T>
+__device__ __forceinline__ T movers_alpha(const T dU, const T dF, const T Lmax, const T Lmin) {
+  const T eps = T(1e-10);
+  if (fabs(dF) < eps && fabs(dU) > eps) return T(0.0);
+  if (fabs(dF) < eps && fabs(dU) < eps) return Lmin;
+  if (fabs(dF) > eps && fabs(dU) > eps) {
+    T A = fabs(dF / dU);
+    if (A >= Lmax) A = T(sign_ref<T>(A)) * Lmax;
+    else if (A <= Lmin) A = T(sign_ref<T>(A)) * Lmin;
+    return A;
+  }
+  return Lmin;
+}
+
+// Entropy_Fix, src/MOVERS.cpp:7-17 (delta = 1.0 * L_Max).
+template <typename T>
+__device__ __forceinline__ T movers_entropy_fix(const T A, const T Lmax) {
+  const T delta = T(1.0) * Lmax;
+  if (fabs(A) < delta) return (A * A + delta * delta) / (T(2.0) * delta);
+  return Lmax;
+}
+
+// MOVERS (src/MOVERS.cpp:45-167) and MOVERS_2O (:169-276): wave speeds |V.n -+ a| dl of both
+// cells bound alpha = |dF/dU| between max-of-max and max-of-min; `single` (Is_MOVERS_1) uses the
+// energy component's alpha for all four; `efix` (Enable_Entropy_Fix) smooths alpha below L_Max
+// (all four components at first order, the energy one at second order).  At second order the
+// reference keeps the unreconstructed primitive jump and zero sound speeds (its MOVERS_2O never
+// sets C_L, C_R).  D = 0.5 alpha dU.
+template <typename T, int ORDER>
+__device__ __forceinline__ void movers_diss(const T rL, const T uL, const T vL, const T pL, const T cL0, const T rR,
+                                            const T uR, const T vR, const T pR, const T cR0, const T UL[4],
+                                            const T UR[4], const T nx, const T ny, const T dl, bool single, bool efix,
+                                            T D[4]) {
+  T dU[4];
+  if (ORDER == 1) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) dU[k] = UR[k] - UL[k];
+  } else {
+    prim_jump<T>(rL, uL, vL, pL, rR, uR, vR, pR, dU);
+  }
+  const T cL = ORDER == 1 ? cL0 : T(0.0), cR = ORDER == 1 ? cR0 : T(0.0);
+  const T VnL = (uL * nx + vL * ny);
+  const T VnR = (uR * nx + vR * ny);
+  T dF[4];
+  movers_flux_jump<T>(rL, uL, vL, pL, rR, uR, vR, pR, nx, ny, dl, VnL, VnR, true, dF);
+  const T S0 = fabs(VnL - cL) * dl, S1 = fabs(VnL + cL) * dl, S2 = fabs(VnL) * dl;
+  const T S3 = fabs(VnR - cR) * dl, S4 = fabs(VnR + cR) * dl, S5 = fabs(VnR) * dl;
+  const T Lmax = max2_ref<T>(max3_ref<T>(S0, S1, S2), max3_ref<T>(S3, S4, S5));
+  const T Lmin = max2_ref<T>(min3_ref<T>(S0, S1, S2), min3_ref<T>(S3, S4, S5));
+  T A[4];
+  A[3] = movers_alpha<T>(dU[3], dF[3], Lmax, Lmin);
+  A[0] = A[1] = A[2] = A[3];
+  if (!single) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) A[k] = movers_alpha<T>(dU[k], dF[k], Lmax, Lmin);
+  }
+  if (efix) {
+    if (ORDER == 1) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) A[k] = movers_entropy_fix<T>(A[k], Lmax);
+    }
+    A[3] = movers_entropy_fix<T>(A[3], Lmax);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) D[k] = T(0.5) * A[k] * dU[k];
+}
+
+// RICCA (src/RICCA.cpp:61-116) and RICCA_2O (:129-199) with Condition_For_RICCA (:31-48):
+// alpha = max|V.n| + sign(dP) sqrt(gamma p_I / rho_I), or the mean |V.n| where both jumps are
+// below 1e-8; dP = |p_L - p_R| is zeroed below 1e-8 (the reference zeroes its variable in
+// place, so it stays zero for the later components).  dU is the primitive-rebuilt jump at first
+// order and the limited conserved jump `dU2` (Second_Order_Limiter) at second order.
+// D = 0.5 alpha dl dU.
+template <typename T, int ORDER>
+__device__ __forceinline__ void ricca_diss(const T rL, const T uL, const T vL, const T pL, const T rR, const T uR,
+                                           const T vR, const T pR, const T nx, const T ny, const T dl, const T dU2[4],
+                                           T D[4]) {
+  const T VnL = uL * nx + vL * ny;
+  const T VnR = uR * nx + vR * ny;
+  T dU[4];
+  if (ORDER == 1) prim_jump<T>(rL, uL, vL, pL, rR, uR, vR, pR, dU);
+  else {
+#pragma unroll
+    for (int k = 0; k < 4; k++) dU[k] = dU2[k];
+  }
+  T dF[4];
+  movers_flux_jump<T>(rL, uL, vL, pL, rR, uR, vR, pR, nx, ny, dl, VnL, VnR, true, dF);
+  T dP = fabs(pL - pR);
+  const T PI = T(0.5) * (pL + pR);
+  const T RI = T(0.5) * (rL + rR);
+  if (dP < T(1e-8)) dP = T(0.0);
+  const T aL = fabs(VnL), aR = fabs(VnR);
+  const T Mx = (aL < aR) ? aR : aL;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    T A;
+    if (fabs(dF[k]) < T(1e-8) && fabs(dU[k]) < T(1e-8)) A = T(0.5) * (aL + aR);
+    else A = Mx + T(1.0) * T(sign_ref<T>(dP)) * sqrt(T(kGamma) * PI / RI);
+    D[k] = T(0.5) * A * dl * dU[k];
+  }
+}
+
+// MOVERS_NWSC (src/MOVERS_NWSC.cpp:23-107) and MOVERS_NWSC_2O (:109-202) with
+// Condition_For_MOVERS_NWSC (:6-21): alpha_k = sign(dU_k) |dF_k| (0 across a discontinuity),
+// pressure sensor 0.21 |dp / (2 p_I)|, D = 0.5 (sensor alpha + 0.5(|V_R.n dl| + |V_L.n dl|) dU).
+// dU: conserved jump U_R - U_L at first order, the limited jump `dU2` at second order.
+template <typename T, int ORDER>
+__device__ __forceinline__ void nwsc_diss(const T rL, const T uL, const T vL, const T pL, const T rR, const T uR,
+                                          const T vR, const T pR, const T UL[4], const T UR[4], const T nx, const T ny,
+                                          const T dl, const T dU2[4], T D[4]) {
+  const T VnL = (uL * nx + vL * ny);
+  const T VnR = (uR * nx + vR * ny);
+  T dU[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) dU[k] = ORDER == 1 ? UR[k] - UL[k] : dU2[k];
+  T dF[4];
+  movers_flux_jump<T>(rL, uL, vL, pL, rR, uR, vR, pR, nx, ny, dl, VnL, VnR, ORDER == 1, dF);
+  T A[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (fabs(dF[k]) <= T(1e-8) && fabs(dU[k]) >= T(1e-8)) A[k] = T(0.0);
+    else A[k] = T(sign_ref<T>(dU[k])) * fabs(dF[k]);
+  }
+  const T dP = pR - pL;
+  const T PI = T(0.5) * (pR + pL);
+  const T AP = T(0.5) * (fabs(VnR * dl) + fabs(VnL * dl));
+  const T Sensor = T(0.21) * fabs(dP / (T(2.0) * PI));
+#pragma unroll
+  for (int k = 0; k < 4; k++) D[k] = T(0.5) * (Sensor * A[k] + AP * dU[k]);
+}
+
 // Limiter functions phi(a, b), r = a / b, as the reference's GPU limiter family defines them
 // (CUDA_KERNELS/Limiter_Cuda_Kernels.cu:89-154): phi = 0 when |b| < 1e-12 or r <= 0, else
 //   minmod min(r, 1); Van Leer 2r/(1+r); superbee max(min(2r,1), min(r,2)); Van Albada (r^2+r)/(r^2+1).

@@ -82,6 +82,8 @@ void b200_init() {
   cfd_config cfg;
   cfd_config_default(&cfg);
   cfg.dissipation_type = Dissipation_Type;
+  cfg.movers_single_alpha = Is_MOVERS_1 ? 1 : 0;
+  cfg.movers_entropy_fix = Enable_Entropy_Fix ? 1 : 0;
   cfg.is_second_order = Is_Second_Order ? 1 : 0;
   cfg.time_accurate = Time_Accurate ? 1 : 0;
   cfg.local_time_stepping = Local_Time_Stepping ? 1 : 0;

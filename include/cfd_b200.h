@@ -96,9 +96,14 @@ void cfd_mesh_destroy(cfd_mesh *m);
  * Solver configuration: the reference's Solver_Config keys (json_Files/Solver_Config.json:1-38,
  * read at src/Configuration_Read.cpp:23-87) plus additive keys.
  * ------------------------------------------------------------------------------------------ */
-/* Flux schemes.  CFD_DISS_AUSM_GPU: the face flux of the reference's GPU kernel ausm_flux_kernel
- * (CUDA_KERNELS/Flux_Calculations_Cuda_Kernels.cu:37-113); gradient-MUSCL (face-based) form only. */
-enum { CFD_DISS_LLF = 1, CFD_DISS_ROE = 3, CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7, CFD_DISS_AUSM_GPU = 8 };
+/* Flux schemes.  The reference's Dissipation_Type switch (src/Net_Flux.cpp:74-91,109-126):
+ * 1 LLF, 2 MOVERS / MOVERS_2O (src/MOVERS.cpp:45,169), 3 ROE / ROE_2O, 4 RICCA / RICCA_2O
+ * (src/RICCA.cpp:61,129), 5 MOVERS_NWSC / MOVERS_NWSC_2O (src/MOVERS_NWSC.cpp:23,109); 2, 4 and 5
+ * in the reference's per-cell form only (muscl = CFD_MUSCL_REFERENCE, FP64).  Additive: 6 AUSM,
+ * 7 HLLC, and CFD_DISS_AUSM_GPU, the face flux of the reference's GPU kernel ausm_flux_kernel
+ * (CUDA_KERNELS/Flux_Calculations_Cuda_Kernels.cu:37-113), gradient-MUSCL (face-based) form only. */
+enum { CFD_DISS_LLF = 1, CFD_DISS_MOVERS = 2, CFD_DISS_ROE = 3, CFD_DISS_RICCA = 4, CFD_DISS_MOVERS_NWSC = 5,
+       CFD_DISS_AUSM = 6, CFD_DISS_HLLC = 7, CFD_DISS_AUSM_GPU = 8 };
 enum { CFD_LIM_REF_MINMOD = 0, CFD_LIM_MINMOD = 1, CFD_LIM_VANLEER = 2, CFD_LIM_SUPERBEE = 3, CFD_LIM_VANALBADA = 4 };
 /* Integrators.  CFD_INT_RK3_GPU_REF / CFD_INT_RK4_GPU_REF: the stage updates of the reference's
  * GPU kernels tvd_rk3_kernel and rk4_complete_kernel (CUDA_KERNELS/Time_Integration_Cuda_Kernels.cu
@@ -117,7 +122,8 @@ enum { CFD_PREC_FP64 = 0, CFD_PREC_FP32_FLUX = 1 };
 enum { CFD_MUSCL_REFERENCE = 0, CFD_MUSCL_GRADIENT = 1 };
 
 typedef struct {
-  int dissipation_type;      /* Dissipation_Type: 1 LLF, 3 ROE; additive 6 AUSM, 7 HLLC */
+  int dissipation_type;      /* Dissipation_Type: CFD_DISS_* (1 LLF, 2 MOVERS, 3 ROE, 4 RICCA,
+                                5 MOVERS_NWSC; additive 6 AUSM, 7 HLLC, 8 GPU AUSM) */
   int is_second_order;       /* Is_Second_Order */
   int time_accurate;         /* Time_Accurate: 1 -> Runge_Kutta_Method, 0 -> Explicit_Method */
   int local_time_stepping;   /* Local_Time_Stepping */
@@ -164,11 +170,17 @@ typedef struct {
                                 value * p (d: centre-to-centre vector), the Roe dissipation is
                                 replaced by the Rusanov dissipation 1/2 max(|Vn| + a) (U_R - U_L) dl.
                                 0 (default): Roe everywhere.  No reference counterpart. */
+  int movers_single_alpha;   /* Is_MOVERS_1: MOVERS uses the energy component's wave-speed
+                                coefficient for all four components (src/MOVERS.cpp:142-152) */
+  int movers_entropy_fix;    /* Enable_Entropy_Fix: MOVERS' entropy fix of the coefficients
+                                (src/MOVERS.cpp:7-17,153-160) */
 } cfd_config;
 
 /* Defaults of json_Files/Solver_Config.json with Dissipation_Type = ROE. */
 void cfd_config_default(cfd_config *cfg);
 /* Parses a Solver_Config JSON file (the reference schema; // comments allowed) into cfg.
+ * Is_MOVERS_1 and Enable_Entropy_Fix are read as the reference reads them
+ * (src/Configuration_Read.cpp:72-73).
  * Unknown keys are ignored; additive keys: Limiter_Type, Flux_Scheme, Integrator, Precision,
  * Inlet_BC, Exit_BC, Reorder, MUSCL, Reconstruction, Entropy_Fix_Linear. */
 cfd_status cfd_config_read_json(const char *path, cfd_config *cfg);

@@ -470,6 +470,146 @@ static void llf_1o(orc_state *s, const double *Ur, int c, int N, int f, double *
   for (int k = 0; k < 4; k++) D[k] = 0.5 * mev * (Ur[4 * (size_t)N + k] - Ur[4 * (size_t)c + k]);
 }
 
+static double min3(double a, double b, double c) {
+  if ((a <= b) && (a <= c)) return a;
+  if ((b <= a) && (b <= c)) return b;
+  return c;
+}
+
+/* Interface flux jump of the MOVERS family, src/MOVERS.cpp:114-117 (plus_pl = 1: the reference's
+ * "+ P_L * nx" / "+ P_L * ny" momentum terms of MOVERS, MOVERS_2O, RICCA, RICCA_2O, MOVERS_NWSC;
+ * 0: the "- P_L" terms of MOVERS_NWSC_2O, src/MOVERS_NWSC.cpp:183-184). */
+static void flux_jump(const double *L, const double *R, double nx, double ny, double dl, int plus_pl, double *dF) {
+  double Rho_L = L[0], P_L = L[4], u_L = L[1], v_L = L[2];
+  double Rho_R = R[0], P_R = R[4], u_R = R[1], v_R = R[2];
+  double Vdotn_L = (u_L * nx + v_L * ny), Vdotn_R = (u_R * nx + v_R * ny);
+  double Vmag_L = 0.5 * (u_L * u_L + v_L * v_L), Vmag_R = 0.5 * (u_R * u_R + v_R * v_R);
+  dF[0] = (Rho_R * Vdotn_R - Rho_L * Vdotn_L) * dl;
+  if (plus_pl) {
+    dF[1] = (Rho_R * u_R * Vdotn_R + P_R * nx - Rho_L * u_L * Vdotn_L + P_L * nx) * dl;
+    dF[2] = (Rho_R * v_R * Vdotn_R + P_R * ny - Rho_L * v_L * Vdotn_L + P_L * ny) * dl;
+  } else {
+    dF[1] = (Rho_R * u_R * Vdotn_R + P_R * nx - Rho_L * u_L * Vdotn_L - P_L * nx) * dl;
+    dF[2] = (Rho_R * v_R * Vdotn_R + P_R * ny - Rho_L * v_L * Vdotn_L - P_L * ny) * dl;
+  }
+  dF[3] = ((((P_R / (1.4 - 1.0)) + Rho_R * Vmag_R) + P_R) * Vdotn_R -
+           (((P_L / (1.4 - 1.0)) + Rho_L * Vmag_L) + P_L) * Vdotn_L) * dl;
+}
+
+/* Conserved jump from the two primitive states, src/MOVERS.cpp:208-211 / src/RICCA.cpp:96-100. */
+static void prim_jump(const double *L, const double *R, double *dU) {
+  double Rho_L = L[0], P_L = L[4], u_L = L[1], v_L = L[2];
+  double Rho_R = R[0], P_R = R[4], u_R = R[1], v_R = R[2];
+  dU[0] = Rho_R - Rho_L;
+  dU[1] = Rho_R * u_R - Rho_L * u_L;
+  dU[2] = Rho_R * v_R - Rho_L * v_L;
+  dU[3] = ((P_R / (1.4 - 1.0)) + 0.5 * Rho_R * (u_R * u_R + v_R * v_R)) -
+          ((P_L / (1.4 - 1.0)) + 0.5 * Rho_L * (u_L * u_L + v_L * v_L));
+}
+
+/* Condition_For_MOVERS, src/MOVERS.cpp:19-43. */
+static void movers_condition(double d_U, double d_F, double L_Max, double L_Min, double *Alpha) {
+  double epsilon = 1e-10;
+  if (fabs(d_F) < epsilon && fabs(d_U) > epsilon) {
+    *Alpha = 0.0;
+  } else if (fabs(d_F) < epsilon && fabs(d_U) < epsilon) {
+    *Alpha = L_Min;
+  } else if (fabs(d_F) > epsilon && fabs(d_U) > epsilon) {
+    *Alpha = fabs(d_F / d_U);
+    if (*Alpha >= L_Max) *Alpha = sgn(*Alpha) * L_Max;
+    else if (*Alpha <= L_Min) *Alpha = sgn(*Alpha) * L_Min;
+  } else {
+    *Alpha = L_Min;
+  }
+}
+
+/* Entropy_Fix, src/MOVERS.cpp:7-17. */
+static void movers_entropy_fix(double *Alpha, double L_Max) {
+  double k = 1.0, delta = k * L_Max;
+  if (fabs(*Alpha) < delta) *Alpha = (*Alpha * *Alpha + delta * delta) / (2.0 * delta);
+  else *Alpha = L_Max;
+}
+
+/* MOVERS, src/MOVERS.cpp:45-167, and MOVERS_2O, :169-276 (primitive jump, sound speeds left at
+ * the zero its globals were reset to, entropy fix on the energy component only). */
+static void movers(orc_state *s, const double *Ur, int c, int N, int f, double *D) {
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  int second = s->c.is_second_order;
+  double C_L = second ? 0.0 : L[5], C_R = second ? 0.0 : R[5];
+  double d_U[4], d_F[4], A[4];
+  if (!second)
+    for (int k = 0; k < 4; k++) d_U[k] = Ur[4 * (size_t)N + k] - Ur[4 * (size_t)c + k];
+  else
+    prim_jump(L, R, d_U);
+  flux_jump(L, R, nx, ny, dl, 1, d_F);
+  double Vdotn_L = (L[1] * nx + L[2] * ny), Vdotn_R = (R[1] * nx + R[2] * ny);
+  double S[6] = {fabs(Vdotn_L - C_L) * dl, fabs(Vdotn_L + C_L) * dl, fabs(Vdotn_L) * dl,
+                 fabs(Vdotn_R - C_R) * dl, fabs(Vdotn_R + C_R) * dl, fabs(Vdotn_R) * dl};
+  double Max1 = max3(S[0], S[1], S[2]), Max2 = max3(S[3], S[4], S[5]);
+  double Lambda_Max = (Max1 >= Max2) ? Max1 : Max2;
+  double Min1 = min3(S[0], S[1], S[2]), Min2 = min3(S[3], S[4], S[5]);
+  double Lambda_Min = (Min1 >= Min2) ? Min1 : Min2;
+  movers_condition(d_U[3], d_F[3], Lambda_Max, Lambda_Min, &A[3]);
+  A[0] = A[1] = A[2] = A[3];
+  if (!s->c.movers_single)
+    for (int k = 0; k < 3; k++) movers_condition(d_U[k], d_F[k], Lambda_Max, Lambda_Min, &A[k]);
+  if (s->c.movers_efix) {
+    if (!second)
+      for (int k = 0; k < 3; k++) movers_entropy_fix(&A[k], Lambda_Max);
+    movers_entropy_fix(&A[3], Lambda_Max);
+  }
+  for (int k = 0; k < 4; k++) D[k] = 0.5 * A[k] * d_U[k];
+}
+
+/* RICCA, src/RICCA.cpp:61-116, and RICCA_2O, :129-199, with Condition_For_RICCA (:31-48); the
+ * reference zeroes its dP in place, so a small dP stays zero for the later components. */
+static void ricca(orc_state *s, const double *Ur, int c, int N, int f, double *D) {
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  double Vdotn_L = L[1] * nx + L[2] * ny, Vdotn_R = R[1] * nx + R[2] * ny;
+  double d_U[4], d_F[4];
+  prim_jump(L, R, d_U);
+  flux_jump(L, R, nx, ny, dl, 1, d_F);
+  double dP = fabs(L[4] - R[4]);
+  double P_I = 0.5 * (L[4] + R[4]);
+  double Rho_I = 0.5 * (L[0] + R[0]);
+  if (s->c.is_second_order) limited_jump(s, Ur, c, f, d_U);
+  for (int i = 0; i < 4; i++) {
+    double epsilon = 1e-8, ita = 1.0, Alpha;
+    if (dP < epsilon) dP = 0.0;
+    double a = fabs(Vdotn_L), b = fabs(Vdotn_R);
+    double Max = (a < b) ? b : a; /* std::max */
+    if (fabs(d_F[i]) < epsilon && fabs(d_U[i]) < epsilon) Alpha = 0.5 * (fabs(Vdotn_L) + fabs(Vdotn_R));
+    else Alpha = Max + ita * sgn(dP) * sqrt(1.4 * P_I / Rho_I);
+    D[i] = 0.5 * Alpha * dl * d_U[i];
+  }
+}
+
+/* MOVERS_NWSC, src/MOVERS_NWSC.cpp:23-107, and MOVERS_NWSC_2O, :109-202, with
+ * Condition_For_MOVERS_NWSC (:6-21). */
+static void movers_nwsc(orc_state *s, const double *Ur, int c, int N, int f, double *D) {
+  const double *L = s->P + 11 * (size_t)c, *R = s->P + 11 * (size_t)N;
+  double nx = s->nrm[8 * c + 2 * f], ny = s->nrm[8 * c + 2 * f + 1], dl = s->len[4 * c + f];
+  int second = s->c.is_second_order;
+  double Vdotn_L = (L[1] * nx + L[2] * ny), Vdotn_R = (R[1] * nx + R[2] * ny);
+  double d_U[4], d_F[4], A[4];
+  if (!second)
+    for (int i = 0; i < 4; i++) d_U[i] = Ur[4 * (size_t)N + i] - Ur[4 * (size_t)c + i];
+  flux_jump(L, R, nx, ny, dl, !second, d_F);
+  if (second) limited_jump(s, Ur, c, f, d_U);
+  for (int i = 0; i < 4; i++) {
+    double epsilon = 1e-8;
+    if (fabs(d_F[i]) <= epsilon && fabs(d_U[i]) >= epsilon) A[i] = 0.0;
+    else A[i] = sgn(d_U[i]) * fabs(d_F[i]);
+  }
+  double d_P = R[4] - L[4];
+  double P_I = 0.5 * (R[4] + L[4]);
+  double Alpha_P = 0.5 * (fabs(Vdotn_R * dl) + fabs(Vdotn_L * dl));
+  double Sensor = 0.21 * fabs(d_P / (2.0 * P_I));
+  for (int i = 0; i < 4; i++) D[i] = 0.5 * (Sensor * A[i] + Alpha_P * d_U[i]);
+}
+
 /* Green-Gauss gradients of (rho, u, v, p) with ghost values on boundary faces (gradient MUSCL
  * form; no reference counterpart). */
 static void muscl_gradients(orc_state *s) {
@@ -746,6 +886,9 @@ void orc_net_flux(orc_state *s) {
                s->len[4 * c + f], A);
       if (s->c.dissipation_type == 3 && !s->c.is_second_order) roe_1o(s, c, N, f, D);
       else if (s->c.dissipation_type == 3) roe_2o(s, Ur, c, N, f, D);
+      else if (s->c.dissipation_type == 2) movers(s, Ur, c, N, f, D);
+      else if (s->c.dissipation_type == 4) ricca(s, Ur, c, N, f, D);
+      else if (s->c.dissipation_type == 5) movers_nwsc(s, Ur, c, N, f, D);
       else llf_1o(s, Ur, c, N, f, D);
       for (int v = 0; v < 4; v++) net[v] += A[v] - D[v];
     }

@@ -23,6 +23,8 @@ typedef struct {
   int weno, weno_char;
   double ef_linear; /* entropy fix of the linear waves in the gradient-MUSCL Roe flux (0: off) */
   double shock_fix; /* Rusanov dissipation on faces with |grad p| |d| > shock_fix * p (0: off) */
+  int movers_single; /* Is_MOVERS_1 */
+  int movers_efix;   /* Enable_Entropy_Fix */
 } orc_config;
 
 typedef struct orc_state orc_state;

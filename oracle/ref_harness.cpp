@@ -200,6 +200,8 @@ int refh_set_param(const char *name, double v) {
   else if (n == "Time_Accurate") Time_Accurate = v != 0.0;
   else if (n == "Local_Time_Stepping") Local_Time_Stepping = v != 0.0;
   else if (n == "Dissipation_Type") Dissipation_Type = (int)v;
+  else if (n == "Is_MOVERS_1") Is_MOVERS_1 = v != 0.0;
+  else if (n == "Enable_Entropy_Fix") Enable_Entropy_Fix = v != 0.0;
   else if (n == "CFL") CFL = v;
   else if (n == "Limiter_Zeta") Limiter_Zeta = v;
   else if (n == "Limiter_Zeta1") Limiter_Zeta1 = v;

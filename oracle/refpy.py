@@ -298,7 +298,8 @@ class _OrcConfig(ctypes.Structure):
                [(n, ctypes.c_double) for n in ["cfl", "zeta", "zeta1", "inlet_rho", "inlet_p", "inlet_p0", "inlet_t0",
                                                "exit_p", "r_gas", "inlet_u", "inlet_v"]] + \
                [(n, ctypes.c_int) for n in ["weno", "weno_char"]] + [("ef_linear", ctypes.c_double),
-                                                                            ("shock_fix", ctypes.c_double)]
+                                                                            ("shock_fix", ctypes.c_double)] + \
+               [(n, ctypes.c_int) for n in ["movers_single", "movers_efix"]]
 
 
 _orc = None
@@ -365,6 +366,8 @@ class OracleRun:
         c.weno_char = params.get("weno_characteristic", 0)
         c.ef_linear = params.get("entropy_fix_linear", 0.0)
         c.shock_fix = params.get("shock_fix", 0.0)
+        c.movers_single = params.get("movers_single_alpha", 0)
+        c.movers_efix = params.get("movers_entropy_fix", 0)
         self.m = mesh
         self._keep = [np.ascontiguousarray(a) for a in (
             mesh.n_faces.astype(np.int32), mesh.neighbours.astype(np.int32), mesh.face_normals, mesh.face_lengths,

@@ -48,6 +48,28 @@ CASES = {
     "bump_weno_explicit_fallback": dict(mesh=("bump", 40, 16, 3.0, 1.0, 0.1, 3, 0.3, 11, 1), ic="freestream",
                                         mach=1.6, dissipation_type=3, is_second_order=1, time_accurate=0, cfl=0.4,
                                         inlet_rho=1.0, inlet_p=1.0 / GAMMA, steps=20, weno=1),
+    # The reference's other dissipation types (src/Net_Flux.cpp:74-91,109-126): MOVERS and
+    # MOVERS_2O with and without Is_MOVERS_1 / Enable_Entropy_Fix, RICCA and RICCA_2O,
+    # MOVERS_NWSC and MOVERS_NWSC_2O, on Sod, the O-grid, the ramp and the mixed bump.
+    "sod_movers1_rk3": dict(mesh=("box", 100, 4, 0.0, 1.0, 0.0, 0.01), ic="sod", dissipation_type=2,
+                            is_second_order=0, time_accurate=1, cfl=0.5, inlet_rho=1.0, inlet_p=1.0, steps=60),
+    "sod_movers1_single_efix_explicit": dict(mesh=("box", 100, 4, 0.0, 1.0, 0.0, 0.01), ic="sod", dissipation_type=2,
+                                             is_second_order=0, time_accurate=0, cfl=0.4, inlet_rho=1.0, inlet_p=1.0,
+                                             steps=60, movers_single_alpha=1, movers_entropy_fix=1),
+    "cyl_movers2_efix_lts": dict(mesh=("half_cylinder", 48, 24, 1.0, 4.0, 1.005), ic="freestream", mach=3.0,
+                                 dissipation_type=2, is_second_order=1, time_accurate=1, local_time_stepping=1,
+                                 cfl=0.8, inlet_rho=1.0, inlet_p=1.0 / GAMMA, steps=30, movers_entropy_fix=1),
+    "ramp_ricca1_explicit": dict(mesh=("ramp", 52, 18, 3.0, 1.0, 1.0, 15.0), ic="freestream", mach=2.0,
+                                 dissipation_type=4, is_second_order=0, time_accurate=0, cfl=0.5, inlet_rho=1.0,
+                                 inlet_p=1.0 / GAMMA, steps=30),
+    "cyl_ricca2_lts": dict(mesh=("half_cylinder", 48, 24, 1.0, 4.0, 1.005), ic="freestream", mach=3.0,
+                           dissipation_type=4, is_second_order=1, time_accurate=1, local_time_stepping=1, cfl=0.8,
+                           inlet_rho=1.0, inlet_p=1.0 / GAMMA, steps=30),
+    "sod_nwsc1_rk3": dict(mesh=("box", 100, 4, 0.0, 1.0, 0.0, 0.01), ic="sod", dissipation_type=5,
+                          is_second_order=0, time_accurate=1, cfl=0.5, inlet_rho=1.0, inlet_p=1.0, steps=60),
+    "bump_nwsc2_rk3": dict(mesh=("bump", 40, 16, 3.0, 1.0, 0.1, 3, 0.3, 11, 1), ic="freestream", mach=1.6,
+                           dissipation_type=5, is_second_order=1, time_accurate=1, cfl=0.5, inlet_rho=1.0,
+                           inlet_p=1.0 / GAMMA, steps=30),
     # Reference subsonic inlet (energy form of src/Inlet_Boundary_Conditions.cpp:32) and the
     # empty subsonic exit, LLF.
     "bump_llf1_subsonic": dict(mesh=("bump", 30, 12, 3.0, 1.0, 0.05, 2, 0.2, 5, 0), ic="freestream", mach=0.5,
@@ -103,7 +125,9 @@ def solver_config(case, **over):
               cfl=case["cfl"], limiter_zeta=case.get("limiter_zeta", 0.5), limiter_zeta1=case.get("limiter_zeta1", 0.5),
               inlet_rho=case["inlet_rho"], inlet_p=case["inlet_p"], inlet_bc=case.get("inlet_bc", 0),
               exit_bc=case.get("exit_bc", 0), weno=case.get("weno", 0),
-              weno_characteristic=case.get("weno_characteristic", 0))
+              weno_characteristic=case.get("weno_characteristic", 0),
+              movers_single_alpha=case.get("movers_single_alpha", 0),
+              movers_entropy_fix=case.get("movers_entropy_fix", 0))
     kw.update(over)
     return cb.default_config(**kw)
 
@@ -114,7 +138,9 @@ def oracle_params(case, **over):
               cfl=case["cfl"], limiter_zeta=case.get("limiter_zeta", 0.5), limiter_zeta1=case.get("limiter_zeta1", 0.5),
               inlet_rho=case["inlet_rho"], inlet_p=case["inlet_p"], inlet_bc=case.get("inlet_bc", 0),
               exit_bc=case.get("exit_bc", 0), weno=case.get("weno", 0),
-              weno_characteristic=case.get("weno_characteristic", 0))
+              weno_characteristic=case.get("weno_characteristic", 0),
+              movers_single_alpha=case.get("movers_single_alpha", 0),
+              movers_entropy_fix=case.get("movers_entropy_fix", 0))
     kw.update(over)
     return kw
 
@@ -127,5 +153,6 @@ def ref_params(case):
          "Inlet_Rho": case["inlet_rho"], "Inlet_P": case["inlet_p"],
          "Is_Inlet_SubSonic": 1 if case.get("inlet_bc", 0) == 1 else 0,
          "Is_Exit_SubSonic": 1 if case.get("exit_bc", 0) == 1 else 0,
-         "Is_WENO": case.get("weno", 0), "Is_Char": case.get("weno_characteristic", 0)}
+         "Is_WENO": case.get("weno", 0), "Is_Char": case.get("weno_characteristic", 0),
+         "Is_MOVERS_1": case.get("movers_single_alpha", 0), "Enable_Entropy_Fix": case.get("movers_entropy_fix", 0)}
     return p

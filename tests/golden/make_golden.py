@@ -1,7 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference's own CPU code.
 
 Run in a container where the reference sources are present:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every case
+    python tests/golden/make_golden.py a b ...    # only the named cases (the others stay as they are)
 It builds oracle/_ref/libcfdref.so from the reference's src/*.cpp (oracle/Makefile), builds the
 meshes with the mesh layer, runs the reference loop (src/Solver.cpp:94-125) through the harness,
 and stores inputs and outputs as compressed .npz.  The fixtures travel with the repository, so
@@ -23,10 +24,16 @@ from oracle import refpy  # noqa: E402
 from cases import CASES, make_mesh, initial_state, ref_params  # noqa: E402
 
 
-def main():
+def main(only=None):
     refpy.build_ref()
+    mpath = os.path.join(HERE, "manifest.json")
     manifest = {}
+    if only and os.path.exists(mpath):
+        with open(mpath) as f:
+            manifest = json.load(f)
     for name, case in CASES.items():
+        if only and name not in only:
+            continue
         mesh = make_mesh(case)
         U0 = initial_state(case, mesh)
         r = refpy.RefRun(mesh, ref_params(case))
@@ -61,6 +68,10 @@ def main():
         print(name, manifest[name])
     # Ausm_Flux (src/Ausm_Flux.cpp:5-205) on a non-uniform state of the mixed bump mesh: the final
     # state of the bump_roe2_rk3 case.
+    if only and "ausm_reference" not in only:
+        with open(mpath, "w") as f:
+            json.dump(manifest, f, indent=1, sort_keys=True)
+        return
     case = CASES["bump_roe2_rk3"]
     mesh = make_mesh(case)
     U = np.load(os.path.join(HERE, "bump_roe2_rk3.npz"))["U"]
@@ -69,9 +80,9 @@ def main():
     r.L.refh_ausm_net_flux()
     np.savez_compressed(os.path.join(HERE, "ausm_reference.npz"), U=U, net_flux=r.state()["net_flux"])
     manifest["ausm_reference"] = {"np": mesh.n_physical}
-    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+    with open(mpath, "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)

@@ -51,6 +51,20 @@ def test_config_json_reference_schema(tmp_path):
     assert c.limiter == cb.LIM_VANLEER and c.integrator == cb.INT_SSPRK3 and c.reconstruct_primitive == 1
     assert c.limiter_zeta == 0.5 and c.limiter_zeta1 == 0.25
     assert c.inlet_bc == cb.INLET_SUPERSONIC and abs(c.inlet_p - 0.714285714) < 1e-15
+    assert c.movers_single_alpha == 0 and c.movers_entropy_fix == 0
+
+
+def test_config_json_movers_keys(tmp_path):
+    """Is_MOVERS_1 and Enable_Entropy_Fix are read from the Solver block as the reference reads them
+    (src/Configuration_Read.cpp:72-73); Flux_Scheme names the three MOVERS-family schemes."""
+    p = tmp_path / "Solver_Config.json"
+    p.write_text('{"Solver": {"Dissipation_Type": 2, "Is_Second_Order": false, "Is_MOVERS_1": true, '
+                 '"Enable_Entropy_Fix": true}}')
+    c = cb.read_config_json(str(p))
+    assert c.dissipation_type == cb.DISS_MOVERS and c.movers_single_alpha == 1 and c.movers_entropy_fix == 1
+    for name, diss in (("ricca", cb.DISS_RICCA), ("movers_nwsc", cb.DISS_MOVERS_NWSC), ("movers", cb.DISS_MOVERS)):
+        p.write_text('{"Solver": {"Flux_Scheme": "%s"}}' % name)
+        assert cb.read_config_json(str(p)).dissipation_type == diss, name
 
 
 def test_config_json_errors(tmp_path):
@@ -76,7 +90,9 @@ def test_create_without_device_is_a_status_not_a_crash():
 
 def test_bad_configs_rejected_before_device_use():
     m = cb.Mesh.box(8, 2)
-    for kw in (dict(dissipation_type=1, is_second_order=1), dict(limiter=9), dict(dissipation_type=2)):
+    for kw in (dict(dissipation_type=1, is_second_order=1), dict(limiter=9), dict(dissipation_type=9),
+               dict(dissipation_type=0), dict(dissipation_type=4, is_second_order=1, muscl=1),
+               dict(dissipation_type=5, is_second_order=1, reconstruct_primitive=1)):
         with pytest.raises(cb.CfdError) as e:
             cb.Solver(m, cb.default_config(**kw))
         assert e.value.status == 1, kw

@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("name", ["sod_roe1_rk3", "sod_roe2_rk3", "sod_llf1_rk3", "sod_roe2_explicit", "cyl_roe2_lts",
                                   "bump_roe2_rk3", "ramp_roe1_explicit", "pulse_weno_rk3", "sod_weno_char_rk3",
-                                  "bump_weno_explicit_fallback"])
+                                  "bump_weno_explicit_fallback", "sod_movers1_single_efix_explicit",
+                                  "cyl_movers2_efix_lts", "cyl_ricca2_lts", "bump_nwsc2_rk3"])
 def test_reference_driver_on_the_gpu_path(name):
     from oracle import refpy
     import os
