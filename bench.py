@@ -844,19 +844,31 @@ def main():
     forms = {}
     nform = min(args.steps, 200)
     # (The reference forms keep the reference's own supersonic inlet, so that they are its scheme.)
+    # The reference's other dissipation types (MOVERS, RICCA, MOVERS_NWSC, second order) are timed
+    # the same way over 50 steps from freestream.
+    ref_form = dict(muscl=0, limiter=0, integrator=0, inlet_bc=0)
     for name, over in [("fp32_flux", dict(precision=1)),
-                       ("reference_roe2_minmod_rk3", dict(muscl=0, limiter=0, integrator=0, inlet_bc=0)),
-                       ("reference_roe1_rk3", dict(muscl=0, is_second_order=0, integrator=0, inlet_bc=0))]:
+                       ("reference_roe2_minmod_rk3", ref_form),
+                       ("reference_roe1_rk3", dict(muscl=0, is_second_order=0, integrator=0, inlet_bc=0)),
+                       ("reference_movers2_rk3", dict(ref_form, dissipation_type=2)),
+                       ("reference_ricca2_minmod_rk3", dict(ref_form, dissipation_type=4)),
+                       ("reference_movers_nwsc2_minmod_rk3", dict(ref_form, dissipation_type=5))]:
         k = dict(kw)
         k.update(over)
         f = cb.Solver(m, cb.default_config(device=local, stream=stream.cuda_stream, **k))
         f.set_option("keep_delu", 0)
         f.upload_state(U0)
-        tune_form = f.autotune(steps=10)
-        f.step_async(3)
-        f.sync()
-        n_timed = min(nform, 50) if name.startswith("reference_roe2") else nform
-        fms, _ = timed_steps(f, stream, n_timed, torch)
+        try:
+            tune_form = f.autotune(steps=10)
+            f.upload_state(U0)
+            f.step_async(3)
+            f.sync()
+            n_timed = nform if name in ("fp32_flux", "reference_roe1_rk3") else min(nform, 50)
+            fms, _ = timed_steps(f, stream, n_timed, torch)
+        except cb.CfdError as e:
+            forms[name] = {"value": None, "error": str(e)}
+            f.close()
+            continue
         forms[name] = {"value": NP * n_timed / (fms * 1e-3), "ms_per_step": fms / n_timed, "steps": n_timed}
         if tune_form:
             forms[name]["launch_options"] = [l.split(":")[0] for l in tune_form.splitlines() if "(chosen)" in l]
