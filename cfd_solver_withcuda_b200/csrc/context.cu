@@ -1909,9 +1909,10 @@ cfd_status cfd_autotune(cfd_ctx *ctx, int steps, char *report, size_t report_len
         for (int p = 0; p < 2; p++)
           cands.push_back({ctx->fp.faces_shape, 1, ctx->fp.lanes, p, 0, ctx->fp.flux_minb, t, 0.0});
   } else {
-    const bool roe2 = ctx->fp.dissipation == 3 && ctx->fp.second_order && !ctx->fp.weno;
+    const int dz = ctx->fp.dissipation;
+    const bool limited = (dz == 3 || dz == 4 || dz == 5) && ctx->fp.second_order && !ctx->fp.weno;
     for (int mb : {1, 6, 8}) {
-      if (mb != 1 && !roe2) continue;
+      if (mb != 1 && !limited) continue;
       cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 1, ctx->dm.pdl, 0, mb, 0, 0.0});
     }
     cands.push_back({ctx->fp.faces_shape, ctx->fuse_gather, 4, ctx->dm.pdl, 0, 1, 0, 0.0});

@@ -614,8 +614,9 @@ __device__ __forceinline__ void min_dt_epilogue(DevState &st, double dt, double 
 // Evaluate_Cell_Net_Flux_1O/2O (src/Net_Flux.cpp:46-129) + Evaluate_Time_Step (src/Time_Step.cpp:293-359)
 // fused, one thread per cell: faces in order, Net += avg - diss; then del_t; block min + Min_dt.
 // MINB: minimum resident blocks per SM the register allocation is made for (1: unconstrained;
-// the second-order Roe form is also built for 6 and 8, which cap its 110 registers at 80 and 64 for
-// more resident warps; the autotuner picks, the results are the same bits).
+// the second-order forms with the directional limiter are also built for 6 and 8, which cap
+// their 114 - 124 registers at 80 and 64 for more resident warps; the autotuner picks, the
+// results are the same bits).
 template <int DISS, int ORDER, int MINB = 1>
 __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
   __shared__ double sh[32];
@@ -2694,6 +2695,18 @@ int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const i
 template <typename T>
 void launch_faces_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 
+// The second-order per-cell forms with the directional limiter (ROE_2O, RICCA_2O, MOVERS_NWSC_2O):
+// one build per register budget (minimum resident blocks of 128 threads per SM: 1 unconstrained,
+// 6 or 8), chosen by fp.flux_minb; every build gives the same bits.
+template <int DISS>
+void launch_flux_limited(int g, cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
+  switch (fp.flux_minb) {
+    case 6: k_flux<DISS, 2, 6><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+    case 8: k_flux<DISS, 2, 8><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+    default: k_flux<DISS, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+  }
+}
+
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
   int n = 0;
   if (fp.second_order && fp.muscl) n += launch_muscl_gradients(s, m, st, fp, 0);
@@ -2713,14 +2726,12 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
     else if (fp.dissipation == 2 && !fp.second_order) k_flux<2, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 2) k_flux<2, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 4 && !fp.second_order) k_flux<4, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 4) k_flux<4, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 5 && !fp.second_order) k_flux<5, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 5) k_flux<5, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 6) k_flux<6, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
     else if (fp.dissipation == 7) k_flux<7, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 3 && fp.flux_minb == 6) k_flux<3, 2, 6><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 3 && fp.flux_minb == 8) k_flux<3, 2, 8><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 3) k_flux<3, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 3) launch_flux_limited<3>(g, s, m, st, fp, src_is_S);
+    else if (fp.dissipation == 4) launch_flux_limited<4>(g, s, m, st, fp, src_is_S);
+    else if (fp.dissipation == 5) launch_flux_limited<5>(g, s, m, st, fp, src_is_S);
     else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
   } else {
     const int g = nblk(4 * m.NP, kFlux4Block);

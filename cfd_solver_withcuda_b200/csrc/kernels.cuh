@@ -134,7 +134,7 @@ struct FluxParams {
   int recon_prim;
   int muscl;            // 0 reference stencil, 1 Green-Gauss-gradient MUSCL
   int lanes;            // threads per cell in the flux kernel: 1 or 4
-  int flux_minb = 1;    // one-lane second-order Roe kernel built for 1, 6 or 8 resident blocks per SM
+  int flux_minb = 1;    // one-lane limited second-order kernels built for 1, 6 or 8 resident blocks per SM
   int persist_minb = 0;  // persistent stage kernel built for 4, 6 or 8 resident blocks per SM (0: 6 in
                          // FP64, 8 in the FP32-flux form)
   int faces_shape;      // face kernel launch: 0 256 threads, 1 256 threads at <= 80 registers, 2 128 threads

@@ -53,8 +53,12 @@ extern "C" cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, co
   if (NP > kMaxCells || cfdb::flux_block_count(NP) > kMaxBlocks)
     return noalloc_fail(CFD_ERR_BAD_ARG, "cfd_evaluate_net_flux_noalloc handles at most " + std::to_string(kMaxCells) +
                                              " physical cells; got " + std::to_string(NP));
-  if (cfg->dissipation_type != CFD_DISS_ROE && cfg->dissipation_type != CFD_DISS_LLF)
-    return noalloc_fail(CFD_ERR_BAD_ARG, "dissipation type must be ROE or LLF");
+  const int diss = cfg->dissipation_type;
+  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && diss != CFD_DISS_MOVERS && diss != CFD_DISS_RICCA &&
+      diss != CFD_DISS_MOVERS_NWSC)
+    return noalloc_fail(CFD_ERR_BAD_ARG, "dissipation type must be LLF, MOVERS, ROE, RICCA or MOVERS_NWSC");
+  if (diss != CFD_DISS_ROE && diss != CFD_DISS_LLF && cfg->is_second_order && cfg->reconstruct_primitive)
+    return noalloc_fail(CFD_ERR_BAD_ARG, "RICCA_2O and MOVERS_NWSC_2O limit the conserved variables");
   if (cfg->dissipation_type == CFD_DISS_LLF && cfg->is_second_order)
     return noalloc_fail(CFD_ERR_BAD_ARG, "LLF is first order only");
   if (cfg->muscl != CFD_MUSCL_REFERENCE || cfg->precision != CFD_PREC_FP64 || cfg->limiter < 0 || cfg->limiter > 4)
@@ -105,6 +109,8 @@ extern "C" cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, co
   st.partial = scratch + kCtlDoubles + kCounterDoubles;
   cfdb::FluxParams fp{};
   fp.dissipation = cfg->dissipation_type;
+  fp.movers_single = cfg->movers_single_alpha ? 1 : 0;
+  fp.movers_efix = cfg->movers_entropy_fix ? 1 : 0;
   fp.second_order = cfg->is_second_order;
   fp.limiter = cfg->limiter;
   fp.recon_prim = cfg->reconstruct_primitive;

@@ -224,8 +224,8 @@ cfd_status cfd_sync(cfd_ctx *ctx, cfd_step_info *info);
  * "fuse_gather" (face-based forms with per-cell dt: one kernel for the face-flux gather and
  * the stage update, default 1), "faces_shape" (face-flux kernel launch shape 0-4, default 3),
  * "flux_lanes" (threads per cell of the per-cell flux kernel, 1 or 4, default 1),
- * "flux_minb" (the one-lane second-order Roe kernel register-capped for 1, 6 or 8 resident blocks per
- * SM, default 1),
+ * "flux_minb" (the one-lane second-order kernels with the directional limiter -- ROE_2O, RICCA_2O,
+ * MOVERS_NWSC_2O -- register-capped for 1 (uncapped), 6 or 8 resident blocks per SM, default 1),
  * "pdl" (launch the kernels of a pseudo-step with programmatic dependent launch, default 0),
  * "patch_stage" (with reorder 3, the face-based forms with a per-cell dt frozen per step run each
  * stage as one kernel: a thread block per 128-cell patch computes the records, face fluxes, gather
@@ -365,7 +365,8 @@ typedef struct {
  * CUDA_MODULE_LOADING=EAGER), and before any stream capture.  The array's device address is
  * looked up in the current context on every call.  Calls share the array and every call clears
  * what must start at zero: calls that overlap on the GPU (different streams, other threads) race.
- * Reference MUSCL stencil, FP64, ROE or first-order LLF only.
+ * Reference MUSCL stencil, FP64; ROE, MOVERS, RICCA, MOVERS_NWSC (first and second order) or
+ * first-order LLF.
  * stream: cudaStream_t (NULL = default stream). */
 cfd_status cfd_evaluate_net_flux_noalloc(const cfd_flux_arrays *a, const cfd_config *cfg, void *stream);
 

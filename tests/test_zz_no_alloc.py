@@ -43,12 +43,15 @@ def limiter_stencil(m):
     return n2, d1, d2
 
 
-def test_noalloc_matches_context_on_two_calls():
+@pytest.mark.parametrize("over", [{}, dict(dissipation_type=2, movers_entropy_fix=1), dict(dissipation_type=4),
+                                  dict(dissipation_type=5), dict(dissipation_type=2, is_second_order=0,
+                                                                 movers_single_alpha=1)])
+def test_noalloc_matches_context_on_two_calls(over):
     import torch
     case = CASES["cyl_roe2_lts"]
     m = make_mesh(case)
     NP, NT = m.n_physical, m.n_total
-    cfg = solver_config(case, reorder=0)
+    cfg = solver_config(case, reorder=0, **over)
     s = cb.Solver(m, cfg)
     s.upload_state(initial_state(case, m))
 
