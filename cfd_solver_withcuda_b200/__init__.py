@@ -143,6 +143,7 @@ SIGNATURES = {
     "cfd_autotune": (_I, [_P, _I, ctypes.c_char_p, ctypes.c_size_t]),
     "cfd_apply_boundary_conditions": (_I, [_P]),
     "cfd_evaluate_net_flux": (_I, [_P]),
+    "cfd_lax_friedrichs": (_I, [_P]),
     "cfd_explicit_method": (_I, [_P]),
     "cfd_runge_kutta_method": (_I, [_P]),
     "cfd_estimate_error": (_I, [_P, _DP]),
@@ -378,6 +379,9 @@ class Solver:
 
     def Explicit_Method(self):
         _check(lib().cfd_explicit_method(self._h))
+
+    def Lax_Fedrichs(self):
+        _check(lib().cfd_lax_friedrichs(self._h))
 
     def Runge_Kutta_Method(self):
         _check(lib().cfd_runge_kutta_method(self._h))

@@ -373,6 +373,8 @@ struct cfd_ctx {
   int n_stage_graphs = 0;
   double *h_ctl = nullptr;  // pinned mirror of the control block
   int *d_perm = nullptr;    // device copy of perm
+  int *d_lf_cells = nullptr;       // Lax_Fedrichs: device cells grouped by wavefront level
+  std::vector<int> lf_level_start;  // first entry of each level in d_lf_cells, plus the end
   // Tile form (reorder 4 on a structured block, option "tile_stage"): the block tables and the two
   // further (rho, u, v, p) row buffers the stages of a step rotate through (st.q4 -> qbuf[0] ->
   // qbuf[1] -> st.q4).
@@ -1611,6 +1613,47 @@ cfd_status cfd_apply_boundary_conditions(cfd_ctx *ctx) {
 cfd_status cfd_evaluate_net_flux(cfd_ctx *ctx) {
   if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
   ctx->launches += launch_flux(ctx->stream, ctx->dm, ctx->ds, ctx->fp, 0);
+  CUDA_TRY(cudaGetLastError());
+  return sync_status(ctx, nullptr);
+}
+
+// Lax_Fedrichs, src/Numerical_Method.cpp:459-481.  The wavefront schedule (reference order: a
+// cell's level is one more than the highest level of its physical neighbours with a lower
+// reference index) is built at the first call from the device's face table.
+cfd_status cfd_lax_friedrichs(cfd_ctx *ctx) {
+  if (!ctx) return fail(CFD_ERR_BAD_ARG, "null context");
+  const int NP = ctx->NP;
+  if (!ctx->d_lf_cells) {
+    std::vector<int> nf(NP), nbr(4 * (size_t)NP);
+    CUDA_TRY(cudaMemcpy(nf.data(), ctx->dm.nf, NP * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(nbr.data(), ctx->dm.nbr, 4 * (size_t)NP * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < NP; i++)
+      if (nf[i] != 4) return fail(CFD_ERR_MESH, "Lax_Fedrichs reads four neighbours per cell: quad meshes only");
+    std::vector<int> level(NP, 0);
+    int nlev = 0;
+    for (int r = 0; r < NP; r++) {
+      const int i = ctx->inv[r];
+      int l = 0;
+      for (int f = 0; f < 4; f++) {
+        const int n = nbr[(size_t)f * NP + i];
+        if (n < NP && ctx->perm[n] < r) l = std::max(l, level[ctx->perm[n]] + 1);
+      }
+      level[r] = l;
+      nlev = std::max(nlev, l + 1);
+    }
+    std::vector<int> start(nlev + 1, 0), cells(NP);
+    for (int r = 0; r < NP; r++) start[level[r] + 1]++;
+    for (int l = 0; l < nlev; l++) start[l + 1] += start[l];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int r = 0; r < NP; r++) cells[fill[level[r]]++] = ctx->inv[r];
+    int *d = nullptr;
+    cfd_status s = ctx_alloc(ctx, (void **)&d, NP * sizeof(int));
+    if (s != CFD_OK) return s;
+    CUDA_TRY(cudaMemcpy(d, cells.data(), NP * sizeof(int), cudaMemcpyHostToDevice));
+    ctx->d_lf_cells = d;
+    ctx->lf_level_start = start;
+  }
+  ctx->launches += launch_lax_friedrichs(ctx->stream, ctx->dm, ctx->ds, ctx->d_lf_cells, ctx->lf_level_start);
   CUDA_TRY(cudaGetLastError());
   return sync_status(ctx, nullptr);
 }

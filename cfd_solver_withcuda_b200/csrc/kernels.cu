@@ -2695,6 +2695,39 @@ int launch_instance_residual(cudaStream_t s, const DevState &st, int NP, const i
 template <typename T>
 void launch_faces_t(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp);
 
+// Lax_Fedrichs (src/Numerical_Method.cpp:459-481): U_c = 0.25 (U_N0 + U_N1 + U_N2 + U_N3) -
+// Min_dt A^-1 R_c, in place.  The reference sweeps the cells in its own order, so a cell reads the
+// neighbours that come before it with their new values and the others with their old ones.  One
+// launch per wavefront level: a cell's level is one more than the highest level of its earlier
+// neighbours, so no two cells of a level are neighbours, a level's earlier neighbours are all
+// done and its later ones not yet started; every cell then sees what the sequential sweep shows
+// it, and the sums are the same bits.
+__global__ void __launch_bounds__(kBlock) k_lax_friedrichs(DevMesh m, DevState st, const int *cells, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = cells[i];
+  const int NP = m.NP, NT = m.NT;
+  const int n0 = m.nbr[c], n1 = m.nbr[NP + c], n2 = m.nbr[2 * NP + c], n3 = m.nbr[3 * NP + c];
+  const double Dt = st.ctl[CTL_DTMIN];
+  const double ia = m.inv_area[c];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double *U = st.U + (size_t)k * NT;
+    st.U[(size_t)k * NT + c] = 0.25 * (U[n0] + U[n1] + U[n2] + U[n3]) - Dt * ia * st.R[(size_t)k * NP + c];
+  }
+}
+
+int launch_lax_friedrichs(cudaStream_t s, const DevMesh &m, DevState &st, const int *cells,
+                          const std::vector<int> &level_start) {
+  int n = 0;
+  for (size_t l = 0; l + 1 < level_start.size(); l++) {
+    const int b = level_start[l], e = level_start[l + 1];
+    k_lax_friedrichs<<<nblk(e - b, kBlock), kBlock, 0, s>>>(m, st, cells + b, e - b);
+    n++;
+  }
+  return n;
+}
+
 // The second-order per-cell forms with the directional limiter (ROE_2O, RICCA_2O, MOVERS_NWSC_2O):
 // one build per register budget (minimum resident blocks of 128 threads per SM: 1 unconstrained,
 // 6 or 8), chosen by fp.flux_minb; every build gives the same bits.

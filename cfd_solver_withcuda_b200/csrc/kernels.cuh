@@ -12,6 +12,7 @@
 //   dtc[NP] (Cell::del_t), dU[4][NP] (Cells_DelU); face-based forms: the primitives again as
 //   q4[NT] (rho, u, v, p), gradients rec[NP][8] and face fluxes F[NF]
 #pragma once
+#include <vector>
 #include <cuda.h>  // CUtensorMap (the tensor maps of the TMA tile form; no driver library is linked)
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -193,6 +194,9 @@ struct TileMaps {
 int launch_prim_all(cudaStream_t s, const DevMesh &m, DevState &st);
 int launch_bc(cudaStream_t s, const DevMesh &m, DevState &st, const BcParams &bp, int stage_src_is_S, int cur_is_S);
 int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int stage_src_is_S);
+// Lax_Fedrichs over cells grouped by wavefront level (cells[level_start[l] .. level_start[l+1])).
+int launch_lax_friedrichs(cudaStream_t s, const DevMesh &m, DevState &st, const int *cells,
+                          const std::vector<int> &level_start);
 // kind: 1,2,3 = reference RK3 stages; 0 = Explicit; 11..14 = RK4 stages; fuse_final = apply
 // Estimate_Error + Update in the last stage's kernel.
 int launch_stage(cudaStream_t s, const DevMesh &m, DevState &st, int kind, int lts, int fuse_final, int keep_delu);

@@ -211,6 +211,12 @@ void Runge_Kutta_Method() {
   changed(false);
 }
 void Implicit_Method() { fprintf(stderr, "Implicit_Method is not part of the B200 path.\n"); }
+// src/Numerical_Method.cpp:459.
+void Lax_Fedrichs() {
+  ensure();
+  b200_check(cfd_lax_friedrichs(g_ctx));
+  changed(false);
+}
 
 // src/Error_Estimate_Update.cpp:10 / :31.
 void Estimate_Error() {

@@ -274,6 +274,12 @@ cfd_status cfd_update(cfd_ctx *ctx);                    /* Update(), src/Error_E
  * next cfd_update adds to U (the reference, SSP-RK3 and RK4 integrators). */
 cfd_status cfd_set_delu(cfd_ctx *ctx, const double *dU);
 cfd_status cfd_get_min_dt(cfd_ctx *ctx, double *min_dt); /* get_Min_dt, src/Numerical_Method.cpp:322 */
+/* Lax_Fedrichs, src/Numerical_Method.cpp:459-481 (declared in the reference's Solver.h, called by
+ * none of its drivers): U_c = 0.25 (sum of the four neighbours' U) - Min_dt / A_c * R_c, in place
+ * with the reference's sweep semantics (neighbours earlier in reference cell order are read with
+ * their new values), from the last net-flux evaluation; primitives are left as they are.  Quad
+ * meshes only (CFD_ERR_MESH otherwise). */
+cfd_status cfd_lax_friedrichs(cfd_ctx *ctx);
 
 /* Downloads (reference cell order).  Any pointer may be NULL.
  *   U      [(NP+NG)*4] U_Cells

@@ -908,6 +908,23 @@ void orc_net_flux(orc_state *s) {
   s->min_dt = m;
 }
 
+/* Lax_Fedrichs, src/Numerical_Method.cpp:459-481: the sequential in-place sweep over the cells
+ * (get_Min_dt is the minimum of the last net-flux evaluation).  Returns -1 on a non-quad cell. */
+int orc_lax_friedrichs(orc_state *s) {
+  for (int c = 0; c < s->NP; c++)
+    if (s->nf[c] != 4) return -1;
+  double Dt = s->min_dt;
+  for (int c = 0; c < s->NP; c++) {
+    int N1 = s->nbr[4 * c], N2 = s->nbr[4 * c + 1], N3 = s->nbr[4 * c + 2], N4 = s->nbr[4 * c + 3];
+    double inv_Area = s->inva[c];
+    for (int k = 0; k < 4; k++)
+      s->U[4 * (size_t)c + k] = 0.25 * (s->U[4 * (size_t)N1 + k] + s->U[4 * (size_t)N2 + k] + s->U[4 * (size_t)N3 + k] +
+                                        s->U[4 * (size_t)N4 + k]) -
+                                Dt * inv_Area * s->R[4 * (size_t)c + k];
+  }
+  return 0;
+}
+
 /* Explicit_Method, src/Numerical_Method.cpp:26-103.  Returns -1 when Min_dt <= 0. */
 int orc_explicit(orc_state *s) {
   s->stage = 0;

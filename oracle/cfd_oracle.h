@@ -37,6 +37,7 @@ void orc_set_state(orc_state *s, const double *U, int n);
 void orc_apply_bc(orc_state *s);
 void orc_net_flux(orc_state *s);
 int orc_explicit(orc_state *s);
+int orc_lax_friedrichs(orc_state *s);
 void orc_rk(orc_state *s);
 void orc_estimate_error(orc_state *s);
 void orc_update(orc_state *s);

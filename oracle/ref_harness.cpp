@@ -298,6 +298,7 @@ void refh_net_flux_by_faces(double *out) {
   quiet_end();
 }
 void refh_explicit() { quiet_begin(); Explicit_Method(); quiet_end(); }
+void refh_lax_friedrichs() { Lax_Fedrichs(); }
 void refh_rk3() { quiet_begin(); Runge_Kutta_Method(); quiet_end(); }
 void refh_estimate_error() { Estimate_Error(); }
 void refh_update() { Update(); }

@@ -149,7 +149,8 @@ def reflib(path=REF_LIB):
     if path not in _ref:
         L = ctypes.CDLL(path)
         for n in ["refh_reset", "refh_clear_boundary_lists", "refh_apply_bc", "refh_net_flux", "refh_explicit",
-                  "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux", "refh_exit_fixed_p"]:
+                  "refh_rk3", "refh_estimate_error", "refh_update", "refh_ausm_net_flux", "refh_exit_fixed_p",
+                  "refh_lax_friedrichs"]:
             getattr(L, n).restype = None
         L.refh_load_vtk.argtypes = [ctypes.c_char_p]
         L.refh_load_vtk.restype = ctypes.c_int
@@ -412,6 +413,9 @@ class OracleRun:
 
     def explicit(self):
         return self.L.orc_explicit(self.h)
+
+    def lax_friedrichs(self):
+        return self.L.orc_lax_friedrichs(self.h)
 
     def rk(self):
         self.L.orc_rk(self.h)

@@ -23,6 +23,8 @@ from oracle import refpy  # noqa: E402
 
 from cases import CASES, make_mesh, initial_state, ref_params  # noqa: E402
 
+LAX_CASES = ("cyl_roe2_lts", "sod_roe1_rk3", "ramp_roe1_explicit")
+
 
 def main(only=None):
     refpy.build_ref()
@@ -66,6 +68,23 @@ def main(only=None):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         manifest[name] = {"iterations": int(n), "np": mesh.n_physical, "ng": mesh.n_ghost}
         print(name, manifest[name])
+    # Lax_Fedrichs (src/Numerical_Method.cpp:459-481) after Apply_Boundary_Conditions and the net
+    # flux, on the final states of three quad-mesh cases (its sweep reads earlier cells' new values).
+    if not only or "lax_friedrichs_reference" in only:
+        out = {}
+        for name in LAX_CASES:
+            case = CASES[name]
+            mesh = make_mesh(case)
+            U = np.load(os.path.join(HERE, name + ".npz"))["U"]
+            r = refpy.RefRun(mesh, ref_params(case))
+            r.set_state(U)
+            r.L.refh_apply_bc()
+            r.L.refh_net_flux()
+            r.L.refh_lax_friedrichs()
+            out[name + "_U0"] = U
+            out[name + "_U"] = r.state()["U"]
+        np.savez_compressed(os.path.join(HERE, "lax_friedrichs_reference.npz"), **out)
+        manifest["lax_friedrichs_reference"] = {"cases": list(LAX_CASES)}
     # Ausm_Flux (src/Ausm_Flux.cpp:5-205) on a non-uniform state of the mixed bump mesh: the final
     # state of the bump_roe2_rk3 case.
     if only and "ausm_reference" not in only:

@@ -88,6 +88,24 @@ def test_calculate_flux_for_all_faces_with_the_reference_dissipation():
     assert_bits_equal(want[1], want[0], "net flux by Calculate_Flux_For_All_Faces (drop-in vs reference)")
 
 
+def test_lax_friedrichs_through_the_shim():
+    """The shim's Lax_Fedrichs (src/Numerical_Method.cpp:459) in a reference process: the same U as
+    the unmodified reference library."""
+    import os
+    from oracle import refpy
+    if not os.path.exists(refpy.DROPIN_LIB):
+        pytest.skip("oracle/_ref/libcfdref_dropin.so not built (reference sources absent at build time)")
+    case = CASES["cyl_roe2_lts"]
+    g = load_golden("lax_friedrichs_reference")
+    m = make_mesh(case)
+    r = refpy.RefRun(m, ref_params(case), lib_path=refpy.DROPIN_LIB)
+    r.set_state(g["cyl_roe2_lts_U0"])
+    r.L.refh_apply_bc()
+    r.L.refh_net_flux()
+    r.L.refh_lax_friedrichs()
+    assert_bits_equal(r.state()["U"], g["cyl_roe2_lts_U"], "U after Lax_Fedrichs through the shim")
+
+
 def test_reference_driver_throughput_on_the_half_cylinder(capsys):
     """The reference's own loop through the drop-in on the full 1024 x 512 half-cylinder O-grid
     (its ROE_2O + MinMod scheme with Runge_Kutta_Method and local dt, M = 3): cell-updates/s with

@@ -53,6 +53,21 @@ def test_oracle_ausm_matches_reference(oracle_lib):
     assert_bits_equal(o.state()["net_flux"], g["net_flux"], "AUSM net flux")
 
 
+@pytest.mark.parametrize("name", ["cyl_roe2_lts", "sod_roe1_rk3", "ramp_roe1_explicit"])
+def test_oracle_lax_friedrichs_matches_reference(name, oracle_lib):
+    """Lax_Fedrichs (src/Numerical_Method.cpp:459-481) after Apply_Boundary_Conditions and the net
+    flux: the restatement's sequential in-place sweep vs the reference's, bit for bit."""
+    g = load_golden("lax_friedrichs_reference")
+    case = CASES[name]
+    m = make_mesh(case)
+    o = oracle_lib.OracleRun(m, **oracle_params(case))
+    o.set_state(g[name + "_U0"])
+    o.apply_bc()
+    o.net_flux()
+    assert o.lax_friedrichs() == 0
+    assert_bits_equal(o.state()["U"], g[name + "_U"], "U after Lax_Fedrichs")
+
+
 def test_sod_physics(oracle_lib):
     """Exact Riemann star state of Sod's problem: p* = 0.30313, u* = 0.92745 (first order smears
     the plateau; the mid-plateau values are within 1 %)."""
