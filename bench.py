@@ -1002,6 +1002,39 @@ def main():
     e2e_seq = world * NP * args.e2e_steps / max_over_ranks(e2e_seq_s, dist if world > 1 else None, device="cuda")
     h2d = host_U.nbytes
     d2h = out_pin[0].nbytes + 8 * 16
+    # The host link bound of the e2e figure: one job's upload and download as plain copies between
+    # the same pinned buffers and device memory, concurrently on two streams (after warm-up), timed
+    # by CUDA events; a job cannot finish faster than the slower of the two.
+    link_dev_in = torch.empty((m.n_total, 4), dtype=torch.float64, device="cuda")
+    link_dev_out = torch.empty((m.n_total, 4), dtype=torch.float64, device="cuda")
+    pin_out = torch.empty((m.n_total, 4), dtype=torch.float64, pin_memory=True)
+    ls_in, ls_out = torch.cuda.Stream(), torch.cuda.Stream()
+    link_ms = {}
+    for direction in ("h2d", "d2h"):
+        for _ in range(5):
+            with torch.cuda.stream(ls_in if direction == "h2d" else ls_out):
+                if direction == "h2d":
+                    link_dev_in.copy_(pin, non_blocking=True)
+                else:
+                    pin_out.copy_(link_dev_out, non_blocking=True)
+    torch.cuda.synchronize()
+    ev = {d: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for d in ("h2d", "d2h")}
+    n_link = 30
+    ev["h2d"][0].record(ls_in)
+    ev["d2h"][0].record(ls_out)
+    for _ in range(n_link):
+        with torch.cuda.stream(ls_in):
+            link_dev_in.copy_(pin, non_blocking=True)
+        with torch.cuda.stream(ls_out):
+            pin_out.copy_(link_dev_out, non_blocking=True)
+    ev["h2d"][1].record(ls_in)
+    ev["d2h"][1].record(ls_out)
+    torch.cuda.synchronize()
+    for d in ("h2d", "d2h"):
+        link_ms[d] = ev[d][0].elapsed_time(ev[d][1]) / n_link
+    link_job_ms = max(link_ms.values())
+    link_bound = world * NP / (link_job_ms * 1e-3)
+    del link_dev_in, link_dev_out
 
     if rank == 0:
         out = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -1022,7 +1055,12 @@ def main():
                        "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                        "mode": "independent one-step solves, %d contexts on %d streams (a solve's copies "
                                "overlap the others' kernels)" % (NCTX, NCTX),
-                       "sequential_value": e2e_seq},
+                       "sequential_value": e2e_seq,
+                       "link": {"h2d_ms": link_ms["h2d"], "d2h_ms": link_ms["d2h"],
+                                "h2d_gbs": h2d / (link_ms["h2d"] * 1e6), "d2h_gbs": d2h / (link_ms["d2h"] * 1e6),
+                                "bound_value": link_bound, "frac": e2e_value / link_bound,
+                                "basis": "one job's upload and download as plain concurrent copies between the "
+                                         "same pinned buffers and device memory (CUDA events)"}},
                "gpu_launches": int(launches),
                "roofline": rl_main,
                "roofline_step": step_roofline,
