@@ -1,7 +1,8 @@
 // Test infrastructure only: C-linkage entries to the reference's own GPU kernels, compiled from
 // the reference's CUDA_KERNELS/*.cu sources by oracle/Makefile (target refcuda) into
 // oracle/_ref/librefcuda.so.  GPU tests use them as the checkers of the HLLC face flux, the phi
-// limiters, the AUSM face flux, the far-field boundary state and the TVD-RK3 / RK4 stage updates.
+// limiters, the AUSM face flux, the far-field boundary state and the TVD-RK3 / RK4 stage updates,
+// and time the reference's Roe and HLLC flux kernels beside this library's on the same GPU.
 #include <vector>
 
 #include "Advanced_Flux_Schemes_Cuda.h"
@@ -11,6 +12,17 @@ extern "C" int refcu_hllc_flux(const double *U, const double *P, const int *nbr,
   cudaError_t e = launch_hllc_flux(U, P, nbr, normals, areas, flux, num_cells, 1.4, 256);
   if (e != cudaSuccess) return (int)e;
   return (int)cudaDeviceSynchronize();
+}
+
+// Launch only (no synchronisation), on the legacy default stream as the reference's wrappers
+// launch: the same-box timing comparison brackets these with CUDA events.
+extern "C" int refcu_hllc_flux_launch(const double *U, const double *P, const int *nbr, const double *normals,
+                                      const double *areas, double *flux, int num_cells) {
+  return (int)launch_hllc_flux(U, P, nbr, normals, areas, flux, num_cells, 1.4, 256);
+}
+extern "C" int refcu_roe_flux_launch(const double *U, const double *P, const int *nbr, const double *normals,
+                                     const double *areas, double *flux, int num_cells) {
+  return (int)launch_roe_flux(U, P, nbr, normals, areas, flux, num_cells, 1.4, 256);
 }
 
 // ---- Further checkers: host arrays in and out; the shim copies them to and from the device and

@@ -72,6 +72,17 @@ def refcuda_hllc(U, P6, nbr, normals, areas, flux, num_cells):
     return L.refcu_hllc_flux(U, P6, nbr, normals, areas, flux, num_cells)
 
 
+def refcuda_flux_launcher(scheme):
+    """The launch-only entry of the reference's roe_flux_kernel ("roe") or hllc_flux_kernel
+    ("hllc") on device arrays given as integer data pointers (legacy default stream, no
+    synchronisation); returns a callable (U, P6, nbr, normals, areas, flux, num_cells) -> status."""
+    L = ctypes.CDLL(REFCUDA_LIB)
+    fn = getattr(L, "refcu_%s_flux_launch" % scheme)
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int]
+    return fn
+
+
 _refcu = []
 
 

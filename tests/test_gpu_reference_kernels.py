@@ -243,3 +243,65 @@ def test_eval_face_flux_matches_solver_schemes():
         G = cb.eval_face_flux(scheme, UR, UL, -nrm, ln)
         assert np.all(np.isfinite(F))
         np.testing.assert_allclose(F, -G, rtol=1e-12, atol=1e-12, err_msg="scheme %d" % scheme)
+
+
+@pytest.mark.parametrize("scheme", ["roe", "hllc"])
+def test_flux_kernel_beside_the_reference_gpu_kernel_on_the_o_grid(scheme, capsys):
+    """Same-GPU comparison with the reference's own flux kernels (CUDA_KERNELS/Roe_Flux_Cuda_Kernels.cu
+    roe_flux_kernel, CUDA_KERNELS/HLLC_LLF_Flux_Cuda_Kernels.cu hllc_flux_kernel, built from source
+    into oracle/_ref) on the 1024 x 512 half-cylinder O-grid from freestream.  The reference kernels
+    write one flux per (cell, face) and skip faces to ghost cells; this library's per-cell forms of
+    the same schemes (k_flux: first-order Roe of the CPU path, the reference GPU HLLC form) also sum
+    the faces in order, take every cell's del_t and the grid's Min_dt.  Both are timed with CUDA
+    events (this library's per launch inside its pseudo-steps, the reference's over 50 launches
+    after 5 untimed ones); the printed times are the record, the test checks only that both ran."""
+    import torch
+    import bench
+    from oracle import refpy
+    if not refpy.refcuda_available():
+        pytest.skip("oracle/_ref/librefcuda.so not built (reference sources absent at build time)")
+    m, U0, kw = bench.workload_state(cb)
+    NP = m.n_physical
+    over = dict(muscl=0, is_second_order=0, integrator=0, inlet_bc=0, reorder=0,
+                dissipation_type=cb.DISS_ROE if scheme == "roe" else cb.DISS_HLLC)
+    k = dict(kw)
+    k.update(over)
+    s = cb.Solver(m, cb.default_config(**k))
+    s.upload_state(U0)
+    s.step(3)
+    s.Apply_Boundary_Conditions()
+    st = s.download()
+    s.set_option("profile", 1)
+    s.step(2)
+    before = s.kernel_time("flux")
+    s.step(17)  # 51 flux launches (three RK stages per pseudo-step), each timed by events
+    after = s.kernel_time("flux")
+    assert after[1] - before[1] == 51
+    mine_ms = (after[0] - before[0]) / (after[1] - before[1])
+    s.close()
+
+    dev = torch.device("cuda", 0)
+    P6 = np.zeros((NP, 6))
+    P6[:, [0, 1, 2, 3, 5]] = st["prim"][:NP][:, [0, 1, 2, 4, 5]]
+    t = {n: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for n, v in dict(
+        U=st["U"][:NP], P=P6, nbr=m.neighbours.astype(np.int32), nrm=m.face_normals, area=m.face_lengths).items()}
+    flux = torch.zeros((NP, 4, 4), dtype=torch.float64, device=dev)
+    launch = refpy.refcuda_flux_launcher(scheme)
+    args = (t["U"].data_ptr(), t["P"].data_ptr(), t["nbr"].data_ptr(), t["nrm"].data_ptr(), t["area"].data_ptr(),
+            flux.data_ptr(), NP)
+    torch.cuda.synchronize()
+    for _ in range(5):
+        assert launch(*args) == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(torch.cuda.default_stream(dev))
+    for _ in range(50):
+        assert launch(*args) == 0
+    e1.record(torch.cuda.default_stream(dev))
+    torch.cuda.synchronize()
+    ref_ms = e0.elapsed_time(e1) / 50
+    assert np.isfinite(flux.cpu().numpy()).all()
+    with capsys.disabled():
+        print("\n%s flux kernel on the 1024x512 O-grid: reference GPU kernel %.1f us, this library's k_flux %.1f us "
+              "(%.2f x)" % (scheme, ref_ms * 1e3, mine_ms * 1e3, ref_ms / mine_ms))
+    assert mine_ms > 0.0 and ref_ms > 0.0
