@@ -616,8 +616,9 @@ __device__ __forceinline__ void min_dt_epilogue(DevState &st, double dt, double 
 // MINB: minimum resident blocks per SM the register allocation is made for (1: unconstrained;
 // the second-order forms with the directional limiter are also built for 6 and 8, which cap
 // their 114 - 124 registers at 80 and 64 for more resident warps; the autotuner picks, the
-// results are the same bits).
-template <int DISS, int ORDER, int MINB = 1>
+// results are the same bits).  SRC_S false: the conserved states come from U only (the caller
+// knows no stage state is read), which saves the per-load choice between U and the stage state.
+template <int DISS, int ORDER, int MINB = 1, bool SRC_S = true>
 __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(DevMesh m, DevState st, FluxParams fp, int src_is_S) {
   __shared__ double sh[32];
   const int NP = m.NP, NT = m.NT;
@@ -625,7 +626,7 @@ __global__ void __launch_bounds__(kFluxBlock, MINB) k_flux(DevMesh m, DevState s
   const bool done = step_done(st.ctl);
   double dt = 1e308 * 10.0;
   if (c < NP && !done) {
-    const USrc us{st.U, st.S, NT, NP, fp.consistent && src_is_S};
+    const USrc us{st.U, st.S, NT, NP, SRC_S && fp.consistent && src_is_S};
     CellState q;
     load_cell<DISS, ORDER>(m, st, us, c, q);
     const int nf = m.nf[c];
@@ -2728,11 +2729,29 @@ int launch_lax_friedrichs(cudaStream_t s, const DevMesh &m, DevState &st, const 
   return n;
 }
 
+// A per-cell form that reads conserved states (limiter, LLF, MOVERS, MOVERS_NWSC, AUSM, HLLC): the
+// build that reads them from U alone when no stage state can be asked for (the reference's
+// integrators, and the first stage of every form), else the one that picks U or the stage state
+// per cell.  Same bits either way.
+template <int DISS, int ORDER>
+void launch_flux_src(int g, cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
+  if (fp.consistent && src_is_S) k_flux<DISS, ORDER, 1, true><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+  else k_flux<DISS, ORDER, 1, false><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+}
+
 // The second-order per-cell forms with the directional limiter (ROE_2O, RICCA_2O, MOVERS_NWSC_2O):
 // one build per register budget (minimum resident blocks of 128 threads per SM: 1 unconstrained,
 // 6 or 8), chosen by fp.flux_minb; every build gives the same bits.
 template <int DISS>
 void launch_flux_limited(int g, cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams &fp, int src_is_S) {
+  if (!(fp.consistent && src_is_S)) {
+    switch (fp.flux_minb) {
+      case 6: k_flux<DISS, 2, 6, false><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+      case 8: k_flux<DISS, 2, 8, false><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+      default: k_flux<DISS, 2, 1, false><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
+    }
+    return;
+  }
   switch (fp.flux_minb) {
     case 6: k_flux<DISS, 2, 6><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
     case 8: k_flux<DISS, 2, 8><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S); break;
@@ -2756,16 +2775,16 @@ int launch_flux(cudaStream_t s, const DevMesh &m, DevState &st, const FluxParams
   if (fp.lanes == 1) {
     const int g = nblk(m.NP, kFluxBlock);
     if (fp.dissipation == 3 && !fp.second_order) k_flux<3, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 2 && !fp.second_order) k_flux<2, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 2) k_flux<2, 2><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 2 && !fp.second_order) launch_flux_src<2, 1>(g, s, m, st, fp, src_is_S);
+    else if (fp.dissipation == 2) launch_flux_src<2, 2>(g, s, m, st, fp, src_is_S);
     else if (fp.dissipation == 4 && !fp.second_order) k_flux<4, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 5 && !fp.second_order) k_flux<5, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 6) k_flux<6, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
-    else if (fp.dissipation == 7) k_flux<7, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else if (fp.dissipation == 5 && !fp.second_order) launch_flux_src<5, 1>(g, s, m, st, fp, src_is_S);
+    else if (fp.dissipation == 6) launch_flux_src<6, 1>(g, s, m, st, fp, src_is_S);
+    else if (fp.dissipation == 7) launch_flux_src<7, 1>(g, s, m, st, fp, src_is_S);
     else if (fp.dissipation == 3) launch_flux_limited<3>(g, s, m, st, fp, src_is_S);
     else if (fp.dissipation == 4) launch_flux_limited<4>(g, s, m, st, fp, src_is_S);
     else if (fp.dissipation == 5) launch_flux_limited<5>(g, s, m, st, fp, src_is_S);
-    else k_flux<1, 1><<<g, kFluxBlock, 0, s>>>(m, st, fp, src_is_S);
+    else launch_flux_src<1, 1>(g, s, m, st, fp, src_is_S);
   } else {
     const int g = nblk(4 * m.NP, kFlux4Block);
     if (fp.dissipation == 3 && !fp.second_order) k_flux4<3, 1><<<g, kFlux4Block, 0, s>>>(m, st, fp, src_is_S);
